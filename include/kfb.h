@@ -1,0 +1,221 @@
+/*
+ * kfb.h -- C ABI of the B200-native FCHL19 local-kernel / RFP-Cholesky library
+ * (libkfb.so).
+ *
+ * Every entry point replaces one routine of the reference's pybind11 modules
+ * kernelforge.local_kernels, kernelforge.kernelmath,
+ * kernelforge.cuda_local_kernels and kernelforge.cuda_global_kernels; the
+ * replaced interface is cited (reference file:line) above each declaration.
+ *
+ * Memory and argument conventions (shared by all calls):
+ *   - X / dX / outputs / RFP arrays / right-hand sides are DEVICE pointers.
+ *     X is (nm, ma, rep), dX is (nm, ma, rep, 3*ma), both C-contiguous; the
+ *     element type is given by a kfb_dtype argument.
+ *   - Q (nm, ma) and N (nm,) are HOST int32 pointers: the atom bucketing by
+ *     label (nuclear charge) is planned on the host, exactly as the reference
+ *     reads its labels on the host (src/local_kernels.cpp:31-149).
+ *   - N is clamped to [0, ma]; padded atoms are ignored.
+ *   - naq = 3 * sum(clamp(N)) (derivative axis length).
+ *   - Work is enqueued on `stream` (a cudaStream_t, NULL = legacy default
+ *     stream); the call returns once the work is enqueued, except where a host
+ *     result is returned (info codes, iteration counts), which synchronises
+ *     the stream.
+ *   - Scratch memory is taken from the device's stream-ordered pool
+ *     (cudaMallocAsync) and released on the same stream.
+ *   - Errors are returned, never abort()ed; kfb_last_error() gives the message
+ *     of the calling thread's last failure.
+ */
+#ifndef KFB_H
+#define KFB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#define KFB_ABI_VERSION 1
+
+typedef enum kfb_status {
+    KFB_OK = 0,
+    KFB_ERR_INVALID_ARG = 1,    /* reference: std::invalid_argument -> ValueError */
+    KFB_ERR_NOT_PD = 2,         /* Cholesky info > 0 (leading minor not positive) */
+    KFB_ERR_ALLOC = 3,          /* device allocation failed */
+    KFB_ERR_CUDA = 4,           /* CUDA / cuBLAS / cuSOLVER error */
+    KFB_ERR_TIMEOUT = 5,        /* a bounded device-side wait gave up */
+    KFB_ERR_NO_CONVERGENCE = 6, /* iterative refinement missed its tolerance */
+    KFB_ERR_UNSUPPORTED = 7     /* device or configuration not supported */
+} kfb_status;
+
+typedef enum kfb_dtype { KFB_F32 = 0, KFB_F64 = 1 } kfb_dtype;
+
+/* Arithmetic of the distance contraction ||x_i - x_j||^2. */
+typedef enum kfb_precision {
+    KFB_PREC_FP64 = 0,      /* FP64 CUDA cores (the plain FP64 GPU path)           */
+    KFB_PREC_FP32 = 1,      /* FP32 CUDA cores                                      */
+    KFB_PREC_SPLIT_F16 = 2  /* tcgen05 tensor cores: x = hi + lo (fp16 pair),
+                               hi*hi + hi*lo + lo*hi with FP32 accumulation in TMEM */
+} kfb_precision;
+
+/* Output storage of a symmetric matrix. */
+typedef enum kfb_layout {
+    KFB_DENSE = 0,  /* full (n, n) row-major                                        */
+    KFB_RFP_U = 1,  /* RFP, TRANSR='N', Fortran UPLO='U' (the CPU modules' packing) */
+    KFB_RFP_L = 2   /* RFP, TRANSR='N', Fortran UPLO='L' (the GPU modules' packing) */
+} kfb_layout;
+
+const char *kfb_last_error(void);
+int kfb_abi_version(void);
+
+/* ---------------------------------------------------------------------- */
+/* Scalar kernels: K[a,b] = sum_{i in a, j in b, q_i = q_j}                */
+/*                          exp(-||x_i - x_j||^2 / (2 sigma^2))            */
+/* ---------------------------------------------------------------------- */
+
+/* K (nm1, nm2) row-major, element type `out_dt`.
+ * Replaces local_kernels.kernel_gaussian (src/local_kernels_bindings.cpp:28-104,
+ * src/local_kernels.cpp:155-298) and cuda_local_kernels.kernel_gaussian_rect
+ * (src/cuda_local_kernels_bindings.cpp:845-851). */
+kfb_status kfb_kernel_gaussian(const void *x1, const void *x2, const int32_t *q1,
+                               const int32_t *q2, const int32_t *n1, const int32_t *n2,
+                               int nm1, int nm2, int ma1, int ma2, int rep, double sigma,
+                               kfb_dtype x_dt, kfb_precision prec, kfb_dtype out_dt, void *out,
+                               void *stream);
+
+/* Symmetric kernel; layout KFB_DENSE fills both triangles of (nm, nm),
+ * KFB_RFP_U / KFB_RFP_L write nm*(nm+1)/2 packed entries.
+ * Replaces local_kernels.kernel_gaussian_symm / _symm_rfp
+ * (src/local_kernels.cpp:584-758, :403-577) and
+ * cuda_local_kernels.kernel_gaussian_symm / _symm_rfp
+ * (src/cuda_local_kernels.cu:2989-3131, :3224-3359). */
+kfb_status kfb_kernel_gaussian_symm(const void *x, const int32_t *q, const int32_t *n, int nm,
+                                    int ma, int rep, double sigma, kfb_dtype x_dt,
+                                    kfb_precision prec, kfb_layout layout, kfb_dtype out_dt,
+                                    void *out, void *stream);
+
+/* ---------------------------------------------------------------------- */
+/* Derivative kernels (element type of x, dx and out: `dt`)                */
+/* ---------------------------------------------------------------------- */
+
+/* K (nm1, naq2): +dK/dR2.  Replaces local_kernels.kernel_gaussian_jacobian
+ * (src/local_kernels_bindings.cpp:158-270, src/local_kernels.cpp:791-974). */
+kfb_status kfb_kernel_gaussian_jacobian(const void *x1, const void *x2, const void *dx2,
+                                        const int32_t *q1, const int32_t *q2, const int32_t *n1,
+                                        const int32_t *n2, int nm1, int nm2, int ma1, int ma2,
+                                        int rep, int naq2, double sigma, kfb_dtype dt,
+                                        kfb_precision prec, void *out, void *stream);
+
+/* K (naq1, nm2): +dK/dR1.  Replaces local_kernels.kernel_gaussian_jacobian_t
+ * (src/local_kernels_bindings.cpp:272-386, src/local_kernels.cpp:991-1166). */
+kfb_status kfb_kernel_gaussian_jacobian_t(const void *x1, const void *dx1, const void *x2,
+                                          const int32_t *q1, const int32_t *q2,
+                                          const int32_t *n1, const int32_t *n2, int nm1, int nm2,
+                                          int ma1, int ma2, int rep, int naq1, double sigma,
+                                          kfb_dtype dt, kfb_precision prec, void *out,
+                                          void *stream);
+
+/* H (naq1, naq2).  Replaces local_kernels.kernel_gaussian_hessian
+ * (src/local_kernels_bindings.cpp:388-525, src/local_kernels.cpp:1171-1419). */
+kfb_status kfb_kernel_gaussian_hessian(const void *x1, const void *dx1, const void *x2,
+                                       const void *dx2, const int32_t *q1, const int32_t *q2,
+                                       const int32_t *n1, const int32_t *n2, int nm1, int nm2,
+                                       int ma1, int ma2, int rep, int naq1, int naq2,
+                                       double sigma, kfb_dtype dt, kfb_precision prec,
+                                       void *out, void *stream);
+
+/* Symmetric Hessian.  KFB_DENSE: (naq, naq) with only the lower triangle
+ * filled (upper triangle zero), as kernel_gaussian_hessian_symm
+ * (src/local_kernels.cpp:1421-1655); KFB_RFP_U / KFB_RFP_L: packed, as
+ * kernel_gaussian_hessian_symm_rfp (src/local_kernels.cpp:1664-1900). */
+kfb_status kfb_kernel_gaussian_hessian_symm(const void *x, const void *dx, const int32_t *q,
+                                            const int32_t *n, int nm, int ma, int rep, int naq,
+                                            double sigma, kfb_dtype dt, kfb_precision prec,
+                                            kfb_layout layout, void *out, void *stream);
+
+/* Full energy+force kernel ((nm1+naq1), (nm2+naq2)); blocks [scalar, +jacobian;
+ * -jacobian_t, hessian].  Replaces local_kernels.kernel_gaussian_full
+ * (src/local_kernels.cpp:1918-2188). */
+kfb_status kfb_kernel_gaussian_full(const void *x1, const void *dx1, const void *x2,
+                                    const void *dx2, const int32_t *q1, const int32_t *q2,
+                                    const int32_t *n1, const int32_t *n2, int nm1, int nm2,
+                                    int ma1, int ma2, int rep, int naq1, int naq2, double sigma,
+                                    kfb_dtype dt, kfb_precision prec, void *out, void *stream);
+
+/* Symmetric full kernel of order BIG = nm + naq; KFB_DENSE is fully filled.
+ * Replaces local_kernels.kernel_gaussian_full_symm / _full_symm_rfp
+ * (src/local_kernels.cpp:2201-2498, :2511-2815) and
+ * cuda_local_kernels.kernel_gaussian_full_symm / _full_symm_rfp
+ * (src/cuda_local_kernels.cu:1871-2342, :3657-4097). */
+kfb_status kfb_kernel_gaussian_full_symm(const void *x, const void *dx, const int32_t *q,
+                                         const int32_t *n, int nm, int ma, int rep, int naq,
+                                         double sigma, kfb_dtype dt, kfb_precision prec,
+                                         kfb_layout layout, void *out, void *stream);
+
+/* ---------------------------------------------------------------------- */
+/* RFP storage and the Cholesky solve                                      */
+/* ---------------------------------------------------------------------- */
+
+/* Symmetric dense (n, n) <-> RFP.  Replaces kernelmath.full_to_rfp /
+ * rfp_to_full (src/math_bindings.cpp:85-180, src/math.cpp:173-211). */
+kfb_status kfb_full_to_rfp(const void *a, int n, kfb_layout uplo, kfb_dtype dt, void *arf,
+                           void *stream);
+kfb_status kfb_rfp_to_full(const void *arf, int n, kfb_layout uplo, kfb_dtype dt, void *a,
+                           void *stream);
+
+/* arf[diag(i)] += l2.  Replaces add_l2_diag_rfp_kernel / _upper_kernel
+ * (src/cuda_global_kernels.cu:436-475). */
+kfb_status kfb_rfp_add_diag(void *arf, int n, double l2, kfb_layout uplo, kfb_dtype dt,
+                            void *stream);
+
+/* In-place Cholesky of an RFP matrix after adding l2 to its diagonal; *info is
+ * 0 or the order of the first non-positive leading minor (synchronises).
+ * Replaces cuda_global_kernels.rfp_potrf (src/cuda_global_kernels.cu:847-868,
+ * src/curfp_spftrf.cpp:182-292) for F32 and LAPACK dpftrf for F64. */
+kfb_status kfb_rfp_potrf(void *arf, int n, double l2, kfb_layout uplo, kfb_dtype dt, int *info,
+                         void *stream);
+
+/* Solve with the factor from kfb_rfp_potrf; B is (n, nrhs) column-major
+ * (ldb = n), overwritten with X.  Replaces cuda_global_kernels.rfp_potrs
+ * (src/cuda_global_kernels.cu:880-893, src/curfp_spftrs.cpp:215-302). */
+kfb_status kfb_rfp_potrs(const void *arf, void *b, int n, int nrhs, kfb_layout uplo,
+                         kfb_dtype dt, void *stream);
+
+/* FP64 (K + l2 I) alpha = y, K in FP64 RFP (overwritten with the factor);
+ * *info as LAPACK.  Replaces kernelmath.cho_solve_rfp
+ * (src/math_bindings.cpp:49-76, src/math.cpp:134-171). */
+kfb_status kfb_cho_solve_rfp(void *arf, const double *y, int n, double l2, kfb_layout uplo,
+                             double *alpha, int *info, void *stream);
+
+/* Mixed-precision KRR solve: (K + l2 I) alpha = y with K given as an FP32 RFP
+ * array (not modified).  The factor is FP32 (tensor-free RFP Cholesky of
+ * K + (l2 + shift) I); residuals, corrections and norms are FP64: classic
+ * iterative refinement, switching to FP32-preconditioned conjugate gradients
+ * when refinement stalls.  Stops at ||r|| <= tol * ||y||.
+ * No reference counterpart: it replaces the reference's FP32 rfp_potrf +
+ * rfp_potrs pair and its CPU FP64 fallback (models/cuda_local_krr.py:640-675). */
+typedef struct kfb_solve_info {
+    int iterations;       /* refinement / CG iterations taken            */
+    int factor_info;      /* potrf info of the last factorisation tried  */
+    double shift;         /* diagonal shift added to the FP32 factor      */
+    double rel_residual;  /* final ||y - (K + l2 I) alpha|| / ||y||     */
+    int used_cg;          /* 1 if CG was needed                           */
+} kfb_solve_info;
+
+kfb_status kfb_krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2,
+                               kfb_layout uplo, double tol, int maxit, double *alpha,
+                               kfb_solve_info *info, void *stream);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KFB_H */

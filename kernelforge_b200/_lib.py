@@ -1,0 +1,96 @@
+"""ctypes binding of libkfb.so (include/kfb.h).
+
+The library is built in-tree (kernelforge_b200/libkfb.so, see build.py).  There
+is no CPU fallback: importing works without a GPU (so the CPU test suite can
+check the exports), but every compute call raises if no CUDA device is present.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libkfb.so")
+
+KFB_OK, KFB_ERR_INVALID_ARG, KFB_ERR_NOT_PD, KFB_ERR_ALLOC = 0, 1, 2, 3
+KFB_ERR_CUDA, KFB_ERR_TIMEOUT, KFB_ERR_NO_CONVERGENCE, KFB_ERR_UNSUPPORTED = 4, 5, 6, 7
+KFB_F32, KFB_F64 = 0, 1
+PREC = {"fp64": 0, "fp32": 1, "split_f16": 2}
+KFB_DENSE, KFB_RFP_U, KFB_RFP_L = 0, 1, 2
+
+# every function declared in include/kfb.h
+EXPORTS = (
+    "kfb_last_error", "kfb_abi_version", "kfb_kernel_gaussian", "kfb_kernel_gaussian_symm",
+    "kfb_kernel_gaussian_jacobian", "kfb_kernel_gaussian_jacobian_t",
+    "kfb_kernel_gaussian_hessian", "kfb_kernel_gaussian_hessian_symm",
+    "kfb_kernel_gaussian_full", "kfb_kernel_gaussian_full_symm", "kfb_full_to_rfp",
+    "kfb_rfp_to_full", "kfb_rfp_add_diag", "kfb_rfp_potrf", "kfb_rfp_potrs",
+    "kfb_cho_solve_rfp", "kfb_krr_solve_mixed",
+)
+
+
+class KfbError(RuntimeError):
+    """A libkfb call failed (CUDA error, timeout, allocation, no convergence)."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = status
+
+
+class SolveInfo(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("factor_info", ctypes.c_int),
+                ("shift", ctypes.c_double), ("rel_residual", ctypes.c_double),
+                ("used_cg", ctypes.c_int)]
+
+
+_lib = None
+P = ctypes.c_void_p
+I = ctypes.c_int
+D = ctypes.c_double
+
+_SIGS = {
+    "kfb_last_error": (ctypes.c_char_p, []),
+    "kfb_abi_version": (I, []),
+    "kfb_kernel_gaussian": (I, [P, P, P, P, P, P, I, I, I, I, I, D, I, I, I, P, P]),
+    "kfb_kernel_gaussian_symm": (I, [P, P, P, I, I, I, D, I, I, I, I, P, P]),
+    "kfb_kernel_gaussian_jacobian": (I, [P, P, P, P, P, P, P, I, I, I, I, I, I, D, I, I, P, P]),
+    "kfb_kernel_gaussian_jacobian_t": (I, [P, P, P, P, P, P, P, I, I, I, I, I, I, D, I, I, P, P]),
+    "kfb_kernel_gaussian_hessian": (I, [P, P, P, P, P, P, P, P, I, I, I, I, I, I, I, D, I, I, P,
+                                        P]),
+    "kfb_kernel_gaussian_hessian_symm": (I, [P, P, P, P, I, I, I, I, D, I, I, I, P, P]),
+    "kfb_kernel_gaussian_full": (I, [P, P, P, P, P, P, P, P, I, I, I, I, I, I, I, D, I, I, P, P]),
+    "kfb_kernel_gaussian_full_symm": (I, [P, P, P, P, I, I, I, I, D, I, I, I, P, P]),
+    "kfb_full_to_rfp": (I, [P, I, I, I, P, P]),
+    "kfb_rfp_to_full": (I, [P, I, I, I, P, P]),
+    "kfb_rfp_add_diag": (I, [P, I, D, I, I, P]),
+    "kfb_rfp_potrf": (I, [P, I, D, I, I, ctypes.POINTER(I), P]),
+    "kfb_rfp_potrs": (I, [P, P, I, I, I, I, P]),
+    "kfb_cho_solve_rfp": (I, [P, P, I, D, I, P, ctypes.POINTER(I), P]),
+    "kfb_krr_solve_mixed": (I, [P, P, I, D, I, D, I, P, ctypes.POINTER(SolveInfo), P]),
+}
+
+
+def lib():
+    """The loaded libkfb (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} not found: build it with `python -m kernelforge_b200.build`")
+        handle = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(handle, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = handle
+    return _lib
+
+
+def check(status: int) -> None:
+    """Raise the reference's exception type for a failed call."""
+    if status == KFB_OK:
+        return
+    msg = lib().kfb_last_error().decode(errors="replace")
+    if status == KFB_ERR_INVALID_ARG:
+        raise ValueError(msg)
+    raise KfbError(status, msg)

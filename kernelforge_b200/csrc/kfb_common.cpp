@@ -1,0 +1,118 @@
+// Host-side helpers of libkfb: error reporting, scratch buffers, label
+// bucketing and derivative offsets.
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <set>
+
+#include "kfb_internal.h"
+
+namespace kfb {
+
+static thread_local std::string g_last_error;
+
+kfb_status set_error(kfb_status st, const char *fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return st;
+}
+
+const char *last_error() { return g_last_error.c_str(); }
+
+kfb_status DevBuf::alloc(size_t nbytes, cudaStream_t s) {
+    release();
+    stream = s;
+    bytes = nbytes ? nbytes : 16;
+    cudaError_t e = cudaMallocAsync(&ptr, bytes, s);
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        (void)cudaGetLastError();
+        return set_error(KFB_ERR_ALLOC, "cudaMallocAsync(%zu bytes) failed: %s", bytes,
+                         cudaGetErrorString(e));
+    }
+    return KFB_OK;
+}
+
+void DevBuf::release() {
+    if (ptr) cudaFreeAsync(ptr, stream);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+std::vector<int> collect_labels(const SetView &a, const SetView *b) {
+    std::set<int> seen;
+    for (int m = 0; m < a.nm; ++m)
+        for (int i = 0; i < a.natoms(m); ++i) seen.insert(a.q[(size_t)m * a.ma + i]);
+    if (b)
+        for (int m = 0; m < b->nm; ++m)
+            for (int i = 0; i < b->natoms(m); ++i) seen.insert(b->q[(size_t)m * b->ma + i]);
+    return std::vector<int>(seen.begin(), seen.end());
+}
+
+Buckets make_buckets(const SetView &s, const std::vector<int> &labels) {
+    Buckets bk;
+    bk.labels = labels;
+    const int L = (int)labels.size();
+    std::vector<int> count(L + 1, 0);
+    auto lidx = [&](int lbl) {
+        return (int)(std::lower_bound(labels.begin(), labels.end(), lbl) - labels.begin());
+    };
+    for (int m = 0; m < s.nm; ++m)
+        for (int i = 0; i < s.natoms(m); ++i) {
+            const int l = lidx(s.q[(size_t)m * s.ma + i]);
+            if (l < L && labels[l] == s.q[(size_t)m * s.ma + i]) count[l + 1]++;
+        }
+    bk.lab_start.assign(L + 1, 0);
+    for (int l = 0; l < L; ++l) bk.lab_start[l + 1] = bk.lab_start[l] + count[l + 1];
+    const int R = bk.lab_start[L];
+    bk.src.resize(R);
+    bk.mol.resize(R);
+    std::vector<int> fill(bk.lab_start.begin(), bk.lab_start.end() - 1);
+    for (int m = 0; m < s.nm; ++m)
+        for (int i = 0; i < s.natoms(m); ++i) {
+            const int q = s.q[(size_t)m * s.ma + i];
+            const int l = lidx(q);
+            if (l >= L || labels[l] != q) continue;
+            const int r = fill[l]++;
+            bk.src[r] = m * s.ma + i;
+            bk.mol[r] = m;
+        }
+    return bk;
+}
+
+long long deriv_offsets(const SetView &s, std::vector<int> &offs) {
+    offs.resize(s.nm + 1);
+    long long acc = 0;
+    for (int m = 0; m < s.nm; ++m) {
+        offs[m] = (int)acc;
+        acc += 3LL * s.natoms(m);
+    }
+    offs[s.nm] = (int)acc;
+    return acc;
+}
+
+kfb_status zero(void *ptr, size_t bytes, cudaStream_t s) {
+    if (bytes) KFB_CUDA_TRY(cudaMemsetAsync(ptr, 0, bytes, s));
+    return KFB_OK;
+}
+
+int device_sm_count() {
+    int dev = 0, n = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 1;
+}
+
+bool device_is_sm100() {
+    int dev = 0, major = 0, minor = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev);
+    return major == 10 && minor == 0;
+}
+
+}  // namespace kfb

@@ -1,0 +1,565 @@
+// Scalar FCHL19 local kernel on the sm_100a tensor cores (tcgen05 + TMEM + TMA).
+//
+// Same-label atoms are packed per label bucket (molecules in order), centred
+// on the bucket mean and split into an fp16 pair x = hi + lo.  One persistent
+// CTA per SM walks a list of 128 x 128 same-label tiles:
+//
+//   warp 0      TMA producer: 64-wide K slices of A_hi, A_lo, B_hi, B_lo
+//               (128B-swizzled) into a 3-stage shared-memory ring;
+//   warp 1      MMA issuer: per K16 step, tcgen05.mma kind::f16
+//               hi*hi + hi*lo + lo*hi into an FP32 accumulator in TMEM
+//               (two accumulators, so the epilogue of tile t overlaps the
+//               MMAs of tile t+1);
+//   warp 2      TMEM allocator;
+//   warps 4..7  epilogue: tcgen05.ld of 32 x 32 accumulator blocks,
+//               e_ij = exp2(c n_i + c n_j - 2c g_ij) with c = -log2(e)/(2 sigma^2),
+//               reduction over (molecule a) x (molecule b) rectangles in
+//               shared memory, one atomic add per rectangle into the output.
+//
+// Nothing of size N_atoms^2 leaves the SM.  Every mbarrier wait is bounded
+// (about two seconds of %globaltimer); a wait that gives up raises an error
+// flag that the host turns into KFB_ERR_TIMEOUT.
+//
+// Mathematics: kernel_gaussian / _symm / _symm_rfp, src/local_kernels.cpp:155-758.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cmath>
+#include <mutex>
+
+#include "kernels_common.cuh"
+#include "scalar_plan.h"
+
+namespace kfb {
+
+namespace {
+
+constexpr int BM = 128;          // rows of A per tile (TMEM lanes)
+constexpr int BN = 128;          // rows of B per tile (TMEM columns per accumulator)
+constexpr int BK = 64;           // fp16 elements per K slice (128 bytes: one swizzle row)
+constexpr int NSTAGE = 3;
+constexpr int TILE_A_BYTES = BM * BK * 2;
+constexpr int TILE_B_BYTES = BN * BK * 2;
+constexpr int STAGE_BYTES = 2 * TILE_A_BYTES + 2 * TILE_B_BYTES;
+constexpr int NUM_THREADS = 256;
+constexpr int EPI_WARP0 = 4;
+constexpr int TMEM_COLS = 2 * BN;
+constexpr int SCR_LD = 33;
+constexpr int SCR_FLOATS = 32 * SCR_LD;       // per epilogue warp
+constexpr int RUN_INTS = 4 * 33;              // rstart, cstart, rmol, cmol per warp
+
+constexpr int OFF_STAGES = 0;
+constexpr int OFF_SCR = OFF_STAGES + NSTAGE * STAGE_BYTES;
+constexpr int OFF_RUNS = OFF_SCR + 4 * SCR_FLOATS * 4;
+constexpr int OFF_BARS = (OFF_RUNS + 4 * RUN_INTS * 4 + 7) / 8 * 8;
+constexpr int NBARS = 2 * NSTAGE + 4 + 1;     // full, empty, tmem_full x2, tmem_empty x2, mma_done
+constexpr int OFF_TMEM = OFF_BARS + NBARS * 8;
+constexpr int SMEM_BYTES = OFF_TMEM + 16;
+constexpr int SMEM_ALLOC = SMEM_BYTES + 1024;  // slack for 1024-byte alignment
+static_assert(SMEM_ALLOC <= 227 * 1024, "shared memory budget");
+
+constexpr unsigned long long WAIT_NS = 2000000000ull;
+
+// ---------------------------------------------------------------- PTX helpers
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ unsigned long long globaltimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: false (and the error flag raised) after WAIT_NS, or as soon as
+// another role has raised the flag.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int *err) {
+    for (int i = 0; i < 64; ++i)
+        if (mbar_try(bar, parity)) return true;
+    const unsigned long long t0 = globaltimer();
+    while (true) {
+        if (mbar_try(bar, parity)) return true;
+        if (*(volatile int *)err != 0) return false;
+        if (globaltimer() - t0 > WAIT_NS) {
+            atomicExch(err, 1);
+            return false;
+        }
+    }
+}
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y,
+                                            uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+__device__ __forceinline__ float fast_exp2(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
+// 1024 bytes apart (SBO), version 1 (sm_100).
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
+    return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)1 << 16) |
+           ((uint64_t)(1024 >> 4) << 32) | ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+// Instruction descriptor, kind::f16: fp16 A and B (K-major), FP32 accumulator.
+constexpr uint32_t IDESC = (1u << 4) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+
+__device__ __forceinline__ void umma_f16(uint32_t dtmem, uint64_t a, uint64_t b, uint32_t acc) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(dtmem),
+        "l"(a), "l"(b), "r"(IDESC), "r"(acc)
+        : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+    asm volatile(
+        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+        : "memory");
+}
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+        "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
+        "%28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+          "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+          "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+          "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// ------------------------------------------------------------------ kernel
+__global__ void __launch_bounds__(NUM_THREADS, 1)
+    scalar_tc_kernel(const __grid_constant__ CUtensorMap tm_a_hi,
+                     const __grid_constant__ CUtensorMap tm_a_lo,
+                     const __grid_constant__ CUtensorMap tm_b_hi,
+                     const __grid_constant__ CUtensorMap tm_b_lo, int rep,
+                     const float *__restrict__ nA, const float *__restrict__ nB,
+                     const int *__restrict__ molA, const int *__restrict__ molB,
+                     const PairTile *__restrict__ tiles, int ntiles, float m2c, PairSink sink,
+                     int *err) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t s_base = smem_u32(smem);
+    const uint32_t bar0 = s_base + OFF_BARS;
+    auto full_bar = [&](int s) { return bar0 + 8u * s; };
+    auto empty_bar = [&](int s) { return bar0 + 8u * (NSTAGE + s); };
+    auto tfull_bar = [&](int a) { return bar0 + 8u * (2 * NSTAGE + a); };
+    auto tempty_bar = [&](int a) { return bar0 + 8u * (2 * NSTAGE + 2 + a); };
+    const uint32_t done_bar = bar0 + 8u * (2 * NSTAGE + 4);
+    uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(smem + OFF_TMEM);
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < NSTAGE; ++s) {
+            mbar_init(full_bar(s), 1);
+            mbar_init(empty_bar(s), 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(tfull_bar(a), 1);
+            mbar_init(tempty_bar(a), 4);
+        }
+        mbar_init(done_bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 2) {
+        asm volatile(
+            "tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                smem_u32(tmem_holder)),
+            "r"(TMEM_COLS)
+            : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_holder;
+    const int nkb = (rep + BK - 1) / BK;
+
+    if (warp == 0) {
+        // ------------------------------------------------ TMA producer
+        if (lane == 0) {
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tm_a_hi)));
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tm_a_lo)));
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tm_b_hi)));
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tm_b_lo)));
+            int stage = 0;
+            uint32_t ph = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+                const PairTile tl = tiles[t];
+                for (int kb = 0; kb < nkb; ++kb) {
+                    if (!mbar_wait(empty_bar(stage), ph ^ 1u, err)) {
+                        ok = false;
+                        break;
+                    }
+                    const uint32_t sa = s_base + OFF_STAGES + stage * STAGE_BYTES;
+                    mbar_expect_tx(full_bar(stage), STAGE_BYTES);
+                    tma_load_2d(sa, &tm_a_hi, kb * BK, tl.a0, full_bar(stage));
+                    tma_load_2d(sa + TILE_A_BYTES, &tm_a_lo, kb * BK, tl.a0, full_bar(stage));
+                    tma_load_2d(sa + 2 * TILE_A_BYTES, &tm_b_hi, kb * BK, tl.b0,
+                                full_bar(stage));
+                    tma_load_2d(sa + 2 * TILE_A_BYTES + TILE_B_BYTES, &tm_b_lo, kb * BK, tl.b0,
+                                full_bar(stage));
+                    if (++stage == NSTAGE) {
+                        stage = 0;
+                        ph ^= 1u;
+                    }
+                }
+            }
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------ MMA issuer
+        if (lane == 0) {
+            int stage = 0, acc = 0;
+            uint32_t ph = 0, aph = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+                if (!mbar_wait(tempty_bar(acc), aph ^ 1u, err)) break;
+                tc_fence_after();
+                const uint32_t dtm = tmem_base + (uint32_t)(acc * BN);
+                for (int kb = 0; kb < nkb; ++kb) {
+                    if (!mbar_wait(full_bar(stage), ph, err)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t sa = s_base + OFF_STAGES + stage * STAGE_BYTES;
+                    const int nks = min(BK / 16, (rep - kb * BK + 15) / 16);
+                    for (int ks = 0; ks < nks; ++ks) {
+                        const uint64_t ahi = sdesc(sa + ks * 32);
+                        const uint64_t alo = sdesc(sa + TILE_A_BYTES + ks * 32);
+                        const uint64_t bhi = sdesc(sa + 2 * TILE_A_BYTES + ks * 32);
+                        const uint64_t blo = sdesc(sa + 2 * TILE_A_BYTES + TILE_B_BYTES + ks * 32);
+                        umma_f16(dtm, ahi, bhi, (kb | ks) != 0 ? 1u : 0u);
+                        umma_f16(dtm, ahi, blo, 1u);
+                        umma_f16(dtm, alo, bhi, 1u);
+                    }
+                    umma_commit(empty_bar(stage));
+                    if (++stage == NSTAGE) {
+                        stage = 0;
+                        ph ^= 1u;
+                    }
+                }
+                if (!ok) break;
+                umma_commit(tfull_bar(acc));
+                if (++acc == 2) {
+                    acc = 0;
+                    aph ^= 1u;
+                }
+            }
+            // make sure every MMA issued has retired before TMEM is released
+            umma_commit(done_bar);
+            mbar_wait(done_bar, 0, err);
+        }
+    } else if (warp >= EPI_WARP0) {
+        // ------------------------------------------------ epilogue
+        const int q = warp - EPI_WARP0;  // TMEM lane quadrant (warp % 4)
+        float *scr = reinterpret_cast<float *>(smem + OFF_SCR) + q * SCR_FLOATS;
+        int *runs = reinterpret_cast<int *>(smem + OFF_RUNS) + q * RUN_INTS;
+        int *rstart = runs, *cstart = runs + 33, *rmol = runs + 66, *cmol = runs + 99;
+        const unsigned lt_mask = (1u << lane) - 1u;
+        int acc = 0;
+        uint32_t aph = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+            const PairTile tl = tiles[t];
+            const int nra = min(BM, tl.a_end - tl.a0);
+            const int nrb = min(BN, tl.b_end - tl.b0);
+            const int row = q * 32 + lane;
+            const bool rvalid = row < nra;
+            const int rm = rvalid ? molA[tl.a0 + row] : -1;
+            const float rn = rvalid ? nA[tl.a0 + row] : 0.f;
+            const int rm_prev = __shfl_up_sync(0xffffffffu, rm, 1);
+            const bool rst = rvalid && (lane == 0 || rm != rm_prev);
+            const unsigned rmask = __ballot_sync(0xffffffffu, rst);
+            const int nvr = __popc(__ballot_sync(0xffffffffu, rvalid));
+            const int nr = __popc(rmask);
+            if (rst) rstart[__popc(rmask & lt_mask)] = lane;
+            rmol[lane] = rm;
+            if (lane == 0) rstart[nr] = nvr;
+
+            const bool got = mbar_wait(tfull_bar(acc), aph, err);
+            if (!__all_sync(0xffffffffu, got)) break;
+            tc_fence_after();
+            const uint32_t tbase = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN);
+#pragma unroll 1
+            for (int c = 0; c < BN / 32; ++c) {
+                const int col = c * 32 + lane;
+                const bool cvalid = col < nrb;
+                const int cm = cvalid ? molB[tl.b0 + col] : -1;
+                const float cn = cvalid ? nB[tl.b0 + col] : 0.f;
+                const int cm_prev = __shfl_up_sync(0xffffffffu, cm, 1);
+                const bool cst = cvalid && (lane == 0 || cm != cm_prev);
+                const unsigned cmask = __ballot_sync(0xffffffffu, cst);
+                const int nvc = __popc(__ballot_sync(0xffffffffu, cvalid));
+                const int nc = __popc(cmask);
+                float v[32];
+                tmem_ld32(tbase + (uint32_t)(c * 32), v);
+                __syncwarp();
+                if (cst) cstart[__popc(cmask & lt_mask)] = lane;
+                cmol[lane] = cm;
+                if (lane == 0) cstart[nc] = nvc;
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const float cnj = __shfl_sync(0xffffffffu, cn, j);
+                    const float e = fast_exp2(fmaf(m2c, v[j], rn + cnj));
+                    scr[j * SCR_LD + lane] = (rvalid && j < nvc) ? e : 0.f;
+                }
+                __syncwarp();
+                for (int p = lane; p < nr * nc; p += 32) {
+                    const int ri = p / nc, ci = p - ri * nc;
+                    const int r0 = rstart[ri], r1 = rstart[ri + 1];
+                    const int c0 = cstart[ci], c1 = cstart[ci + 1];
+                    float s = 0.f;
+                    for (int j = c0; j < c1; ++j)
+                        for (int r = r0; r < r1; ++r) s += scr[j * SCR_LD + r];
+                    emit_pair(sink, rmol[r0], cmol[c0], (double)s, tl.diag);
+                }
+                __syncwarp();
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(tempty_bar(acc));
+            if (++acc == 2) {
+                acc = 0;
+                aph ^= 1u;
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 2) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
+                     "r"(TMEM_COLS)
+                     : "memory");
+    }
+}
+
+// Per-label mean of the set's active rows (FP64 partial sums, atomically
+// combined): the centre each bucket is shifted to before the fp16 split.
+template <class Tin>
+__global__ void label_mean_kernel(const Tin *__restrict__ x, const int *__restrict__ src,
+                                  const int *__restrict__ lab_start, int rep, int nsplit,
+                                  double *__restrict__ mean) {
+    const int l = blockIdx.z;
+    const int s = lab_start[l], e = lab_start[l + 1];
+    const int R = e - s;
+    if (R <= 0) return;
+    const int chunk = (R + nsplit - 1) / nsplit;
+    const int r0 = s + blockIdx.y * chunk, r1 = min(e, r0 + chunk);
+    const int k = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int w = threadIdx.x >> 5;
+    __shared__ double part[8][32];
+    double acc = 0.0;
+    if (k < rep)
+        for (int r = r0 + w; r < r1; r += 8) acc += (double)x[(size_t)src[r] * rep + k];
+    part[w][threadIdx.x & 31] = acc;
+    __syncthreads();
+    if (w == 0 && k < rep) {
+        double t = 0.0;
+        for (int i = 0; i < 8; ++i) t += part[i][threadIdx.x];
+        atomicAdd(&mean[(size_t)l * rep + k], t / (double)R);
+    }
+}
+
+// Packed split rows: v = x - mean(label); hi = fp16(v); lo = fp16(v - hi);
+// norm = c * ||v||^2 (FP64 sum, stored as float).
+template <class Tin>
+__global__ void pack_split_kernel(const Tin *__restrict__ x, const int *__restrict__ src,
+                                  const int *__restrict__ lab_start, int L, int R, int rep, int Dp,
+                                  const double *__restrict__ mean, double c,
+                                  __half *__restrict__ hi, __half *__restrict__ lo,
+                                  float *__restrict__ norm) {
+    const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (r >= R) return;
+    int l = 0;
+    while (l + 1 < L && r >= lab_start[l + 1]) ++l;
+    const Tin *xr = x + (size_t)src[r] * rep;
+    const double *mu = mean + (size_t)l * rep;
+    double s = 0.0;
+    for (int k = lane; k < Dp; k += 32) {
+        __half h = __float2half_rn(0.f), o = __float2half_rn(0.f);
+        if (k < rep) {
+            const double v = (double)xr[k] - mu[k];
+            h = __float2half_rn((float)v);
+            o = __float2half_rn((float)(v - (double)__half2float(h)));
+            s += v * v;
+        }
+        hi[(size_t)r * Dp + k] = h;
+        lo[(size_t)r * Dp + k] = o;
+    }
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) norm[r] = (float)(c * s);
+}
+
+// ---------------------------------------------------------------- host side
+PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+kfb_status make_map(CUtensorMap *m, const __half *ptr, int rows, int Dp, int box_rows) {
+    auto enc = get_encode();
+    if (!enc) return set_error(KFB_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    cuuint64_t gdim[2] = {(cuuint64_t)Dp, (cuuint64_t)std::max(rows, 1)};
+    cuuint64_t gstride[1] = {(cuuint64_t)Dp * sizeof(__half)};
+    cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, const_cast<__half *>(ptr), gdim,
+                     gstride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_error(KFB_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return KFB_OK;
+}
+
+struct SplitSet {
+    DevBuf hi, lo, norm, mol, src, lab;
+};
+
+template <class Tin>
+kfb_status pack_split(const Tin *x, const Buckets &bk, int rep, int Dp, const double *mean,
+                      double c, SplitSet &o, cudaStream_t s) {
+    const int R = bk.rows();
+    const int L = (int)bk.labels.size();
+    KFB_TRY(upload(o.src, bk.src, s));
+    KFB_TRY(upload(o.mol, bk.mol, s));
+    KFB_TRY(upload(o.lab, bk.lab_start, s));
+    KFB_TRY(o.hi.alloc((size_t)std::max(R, 1) * Dp * sizeof(__half), s));
+    KFB_TRY(o.lo.alloc((size_t)std::max(R, 1) * Dp * sizeof(__half), s));
+    KFB_TRY(o.norm.alloc((size_t)std::max(R, 1) * sizeof(float), s));
+    if (R > 0) {
+        pack_split_kernel<Tin><<<(R + 7) / 8, 256, 0, s>>>(
+            x, o.src.as<int>(), o.lab.as<int>(), L, R, rep, Dp, mean, c, o.hi.as<__half>(),
+            o.lo.as<__half>(), o.norm.as<float>());
+        KFB_CUDA_TRY(cudaGetLastError());
+    }
+    return KFB_OK;
+}
+
+template <class Tin>
+kfb_status run_tc(const ScalarProblem &p, const PairSink &sink, cudaStream_t s) {
+    std::vector<int> labels = collect_labels(p.s1, p.symmetric ? nullptr : &p.s2);
+    if (labels.empty()) return KFB_OK;
+    Buckets b1 = make_buckets(p.s1, labels);
+    Buckets b2 = p.symmetric ? Buckets() : make_buckets(p.s2, labels);
+    const Buckets &bb = p.symmetric ? b1 : b2;
+    std::vector<PairTile> tiles = make_pair_tiles(b1, bb, p.symmetric, BM, BN);
+    if (tiles.empty()) return KFB_OK;
+    const int L = (int)labels.size();
+    const int Dp = (p.rep + 7) / 8 * 8;
+    const double log2e = 1.4426950408889634;
+    const double c = -log2e / (2.0 * p.sigma * p.sigma);
+
+    // per-label centre from set 1
+    DevBuf mean;
+    KFB_TRY(mean.alloc((size_t)L * p.rep * sizeof(double), s));
+    KFB_TRY(zero(mean.ptr, (size_t)L * p.rep * sizeof(double), s));
+    SplitSet A, B;
+    {
+        DevBuf src1, lab1;
+        KFB_TRY(upload(src1, b1.src, s));
+        KFB_TRY(upload(lab1, b1.lab_start, s));
+        const int nsplit = 16;
+        dim3 g((p.rep + 31) / 32, nsplit, L);
+        label_mean_kernel<Tin><<<g, 256, 0, s>>>(static_cast<const Tin *>(p.x1), src1.as<int>(),
+                                                 lab1.as<int>(), p.rep, nsplit,
+                                                 mean.as<double>());
+        KFB_CUDA_TRY(cudaGetLastError());
+    }
+    KFB_TRY(pack_split<Tin>(static_cast<const Tin *>(p.x1), b1, p.rep, Dp, mean.as<double>(), c,
+                            A, s));
+    if (!p.symmetric)
+        KFB_TRY(pack_split<Tin>(static_cast<const Tin *>(p.x2), b2, p.rep, Dp,
+                                mean.as<double>(), c, B, s));
+    const SplitSet &BB = p.symmetric ? A : B;
+
+    CUtensorMap ma_hi, ma_lo, mb_hi, mb_lo;
+    KFB_TRY(make_map(&ma_hi, A.hi.as<__half>(), b1.rows(), Dp, BM));
+    KFB_TRY(make_map(&ma_lo, A.lo.as<__half>(), b1.rows(), Dp, BM));
+    KFB_TRY(make_map(&mb_hi, BB.hi.as<__half>(), bb.rows(), Dp, BN));
+    KFB_TRY(make_map(&mb_lo, BB.lo.as<__half>(), bb.rows(), Dp, BN));
+
+    DevBuf dtiles, derr;
+    KFB_TRY(upload(dtiles, tiles, s));
+    KFB_TRY(derr.alloc(sizeof(int), s));
+    KFB_TRY(zero(derr.ptr, sizeof(int), s));
+
+    static bool attr_set = false;
+    if (!attr_set) {
+        KFB_CUDA_TRY(cudaFuncSetAttribute(scalar_tc_kernel,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_ALLOC));
+        attr_set = true;
+    }
+    const int ntiles = (int)tiles.size();
+    const int grid = std::min(ntiles, device_sm_count());
+    scalar_tc_kernel<<<grid, NUM_THREADS, SMEM_ALLOC, s>>>(
+        ma_hi, ma_lo, mb_hi, mb_lo, p.rep, A.norm.as<float>(), BB.norm.as<float>(),
+        A.mol.as<int>(), BB.mol.as<int>(), dtiles.as<PairTile>(), ntiles, (float)(-2.0 * c),
+        sink, derr.as<int>());
+    KFB_CUDA_TRY(cudaGetLastError());
+    int herr = 0;
+    KFB_CUDA_TRY(cudaMemcpyAsync(&herr, derr.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
+    KFB_CUDA_TRY(cudaStreamSynchronize(s));
+    if (herr) return set_error(KFB_ERR_TIMEOUT, "tensor-core scalar kernel: a pipeline wait timed out");
+    return KFB_OK;
+}
+
+}  // namespace
+
+kfb_status scalar_tc(const ScalarProblem &p, const PairSink &sink, cudaStream_t s) {
+    if (!device_is_sm100())
+        return set_error(KFB_ERR_UNSUPPORTED,
+                         "the split-fp16 tensor-core path needs an sm_100 (B200) device");
+    if (p.x_dt == KFB_F64) return run_tc<double>(p, sink, s);
+    return run_tc<float>(p, sink, s);
+}
+
+}  // namespace kfb

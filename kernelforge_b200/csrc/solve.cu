@@ -1,0 +1,522 @@
+// RFP storage kernels, the in-place RFP Cholesky factorisation / solve, and
+// the mixed-precision (FP32 factor, FP64 residual) KRR solve.
+//
+// The RFP Cholesky follows the LAPACK dpftrf / dpftrs block structure for
+// TRANSR='N' (an RFP array is a column-major (n+1) x n/2 or n x (n+1)/2 matrix
+// holding two triangles and one rectangle): potrf on the first triangle, trsm
+// on the rectangle, syrk into the second triangle, potrf on it.  The four
+// block operations are issued on the caller's stream with one host
+// synchronisation at the end (the reference's curfpSpftrf synchronises twice,
+// src/curfp_spftrf.cpp:259,281).
+#include <cublas_v2.h>
+#include <cusolverDn.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "kernels_common.cuh"
+
+namespace kfb {
+
+namespace {
+
+struct Handles {
+    cublasHandle_t blas = nullptr;
+    cusolverDnHandle_t solver = nullptr;
+    int device = -1;
+};
+
+kfb_status get_handles(cudaStream_t s, Handles *&out) {
+    static thread_local Handles h[16];
+    int dev = 0;
+    KFB_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 16) return set_error(KFB_ERR_UNSUPPORTED, "device index %d", dev);
+    Handles &hd = h[dev];
+    if (!hd.blas) {
+        if (cublasCreate(&hd.blas) != CUBLAS_STATUS_SUCCESS)
+            return set_error(KFB_ERR_CUDA, "cublasCreate failed");
+        if (cusolverDnCreate(&hd.solver) != CUSOLVER_STATUS_SUCCESS)
+            return set_error(KFB_ERR_CUDA, "cusolverDnCreate failed");
+        cublasSetMathMode(hd.blas, CUBLAS_PEDANTIC_MATH);  // no reduced-precision shortcuts
+    }
+    cublasSetStream(hd.blas, s);
+    cusolverDnSetStream(hd.solver, s);
+    out = &hd;
+    return KFB_OK;
+}
+
+#define KFB_BLAS_TRY(expr)                                                                  \
+    do {                                                                                    \
+        cublasStatus_t _b = (expr);                                                         \
+        if (_b != CUBLAS_STATUS_SUCCESS)                                                    \
+            return set_error(KFB_ERR_CUDA, "%s failed: cublas status %d", #expr, (int)_b);  \
+    } while (0)
+#define KFB_SOLVER_TRY(expr)                                                                \
+    do {                                                                                    \
+        cusolverStatus_t _b = (expr);                                                       \
+        if (_b != CUSOLVER_STATUS_SUCCESS)                                                  \
+            return set_error(KFB_ERR_CUDA, "%s failed: cusolver status %d", #expr, (int)_b); \
+    } while (0)
+
+// -------------------------------------------------- typed BLAS / LAPACK shims
+template <class T> struct Blas;
+template <> struct Blas<float> {
+    static cublasStatus_t trsm(cublasHandle_t h, cublasSideMode_t sd, cublasFillMode_t u,
+                               cublasOperation_t t, int m, int n, const float *al, const float *A,
+                               int lda, float *B, int ldb) {
+        return cublasStrsm(h, sd, u, t, CUBLAS_DIAG_NON_UNIT, m, n, al, A, lda, B, ldb);
+    }
+    static cublasStatus_t syrk(cublasHandle_t h, cublasFillMode_t u, cublasOperation_t t, int n,
+                               int k, const float *al, const float *A, int lda, const float *be,
+                               float *C, int ldc) {
+        return cublasSsyrk(h, u, t, n, k, al, A, lda, be, C, ldc);
+    }
+    static cublasStatus_t gemm(cublasHandle_t h, cublasOperation_t ta, cublasOperation_t tb, int m,
+                               int n, int k, const float *al, const float *A, int lda,
+                               const float *B, int ldb, const float *be, float *C, int ldc) {
+        return cublasSgemm(h, ta, tb, m, n, k, al, A, lda, B, ldb, be, C, ldc);
+    }
+    static cusolverStatus_t potrf_ws(cusolverDnHandle_t h, cublasFillMode_t u, int n, float *A,
+                                     int lda, int *lw) {
+        return cusolverDnSpotrf_bufferSize(h, u, n, A, lda, lw);
+    }
+    static cusolverStatus_t potrf(cusolverDnHandle_t h, cublasFillMode_t u, int n, float *A,
+                                  int lda, float *ws, int lw, int *info) {
+        return cusolverDnSpotrf(h, u, n, A, lda, ws, lw, info);
+    }
+};
+template <> struct Blas<double> {
+    static cublasStatus_t trsm(cublasHandle_t h, cublasSideMode_t sd, cublasFillMode_t u,
+                               cublasOperation_t t, int m, int n, const double *al,
+                               const double *A, int lda, double *B, int ldb) {
+        return cublasDtrsm(h, sd, u, t, CUBLAS_DIAG_NON_UNIT, m, n, al, A, lda, B, ldb);
+    }
+    static cublasStatus_t syrk(cublasHandle_t h, cublasFillMode_t u, cublasOperation_t t, int n,
+                               int k, const double *al, const double *A, int lda,
+                               const double *be, double *C, int ldc) {
+        return cublasDsyrk(h, u, t, n, k, al, A, lda, be, C, ldc);
+    }
+    static cublasStatus_t gemm(cublasHandle_t h, cublasOperation_t ta, cublasOperation_t tb, int m,
+                               int n, int k, const double *al, const double *A, int lda,
+                               const double *B, int ldb, const double *be, double *C, int ldc) {
+        return cublasDgemm(h, ta, tb, m, n, k, al, A, lda, B, ldb, be, C, ldc);
+    }
+    static cusolverStatus_t potrf_ws(cusolverDnHandle_t h, cublasFillMode_t u, int n, double *A,
+                                     int lda, int *lw) {
+        return cusolverDnDpotrf_bufferSize(h, u, n, A, lda, lw);
+    }
+    static cusolverStatus_t potrf(cusolverDnHandle_t h, cublasFillMode_t u, int n, double *A,
+                                  int lda, double *ws, int lw, int *info) {
+        return cusolverDnDpotrf(h, u, n, A, lda, ws, lw, info);
+    }
+};
+
+// The three blocks of an RFP array (TRANSR='N'), as column-major sub-matrices.
+struct RfpBlocks {
+    long long t1, s, t2;  // offsets of T1 (lower-stored), S (rectangle), T2 (upper-stored)
+    int n1, n2, ld;       // T1 is n1 x n1, T2 is n2 x n2; S is n2 x n1 (lower) / n1 x n2 (upper)
+};
+
+RfpBlocks rfp_blocks(int n, bool lower) {
+    RfpBlocks b{};
+    if (n & 1) {
+        b.ld = n;
+        if (lower) {
+            b.n1 = n - n / 2;
+            b.n2 = n / 2;
+            b.t1 = 0;
+            b.s = b.n1;
+            b.t2 = n;
+        } else {
+            b.n1 = n / 2;
+            b.n2 = n - n / 2;
+            b.t1 = b.n2;
+            b.s = 0;
+            b.t2 = b.n1;
+        }
+    } else {
+        const int k = n / 2;
+        b.ld = n + 1;
+        b.n1 = b.n2 = k;
+        if (lower) {
+            b.t1 = 1;
+            b.s = k + 1;
+            b.t2 = 0;
+        } else {
+            b.t1 = k + 1;
+            b.s = 0;
+            b.t2 = k;
+        }
+    }
+    return b;
+}
+
+template <class T>
+kfb_status rfp_potrf_t(T *a, int n, bool lower, int *info, cudaStream_t s) {
+    *info = 0;
+    if (n == 0) return KFB_OK;
+    Handles *h = nullptr;
+    KFB_TRY(get_handles(s, h));
+    const RfpBlocks b = rfp_blocks(n, lower);
+    const T one = T(1), mone = T(-1);
+    int lw1 = 0, lw2 = 0;
+    KFB_SOLVER_TRY(Blas<T>::potrf_ws(h->solver, CUBLAS_FILL_MODE_LOWER, b.n1, a + b.t1, b.ld, &lw1));
+    if (b.n2 > 0)
+        KFB_SOLVER_TRY(
+            Blas<T>::potrf_ws(h->solver, CUBLAS_FILL_MODE_UPPER, b.n2, a + b.t2, b.ld, &lw2));
+    DevBuf ws, dinfo;
+    KFB_TRY(ws.alloc((size_t)std::max(std::max(lw1, lw2), 1) * sizeof(T), s));
+    KFB_TRY(dinfo.alloc(2 * sizeof(int), s));
+    KFB_TRY(zero(dinfo.ptr, 2 * sizeof(int), s));
+    int *di = dinfo.as<int>();
+    KFB_SOLVER_TRY(Blas<T>::potrf(h->solver, CUBLAS_FILL_MODE_LOWER, b.n1, a + b.t1, b.ld,
+                                  ws.as<T>(), lw1, di));
+    if (b.n2 > 0) {
+        if (lower) {
+            KFB_BLAS_TRY(Blas<T>::trsm(h->blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER,
+                                       CUBLAS_OP_T, b.n2, b.n1, &one, a + b.t1, b.ld, a + b.s,
+                                       b.ld));
+            KFB_BLAS_TRY(Blas<T>::syrk(h->blas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, b.n2, b.n1,
+                                       &mone, a + b.s, b.ld, &one, a + b.t2, b.ld));
+        } else {
+            KFB_BLAS_TRY(Blas<T>::trsm(h->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER,
+                                       CUBLAS_OP_N, b.n1, b.n2, &one, a + b.t1, b.ld, a + b.s,
+                                       b.ld));
+            KFB_BLAS_TRY(Blas<T>::syrk(h->blas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, b.n2, b.n1,
+                                       &mone, a + b.s, b.ld, &one, a + b.t2, b.ld));
+        }
+        KFB_SOLVER_TRY(Blas<T>::potrf(h->solver, CUBLAS_FILL_MODE_UPPER, b.n2, a + b.t2, b.ld,
+                                      ws.as<T>(), lw2, di + 1));
+    }
+    int hi[2] = {0, 0};
+    KFB_CUDA_TRY(cudaMemcpyAsync(hi, di, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    KFB_CUDA_TRY(cudaStreamSynchronize(s));
+    if (hi[0] > 0)
+        *info = hi[0];
+    else if (hi[1] > 0)
+        *info = hi[1] + b.n1;
+    else if (hi[0] < 0 || hi[1] < 0)
+        return set_error(KFB_ERR_CUDA, "potrf reported an invalid argument");
+    return KFB_OK;
+}
+
+template <class T>
+kfb_status rfp_potrs_t(const T *a, T *B, int n, int nrhs, bool lower, cudaStream_t s) {
+    if (n == 0 || nrhs == 0) return KFB_OK;
+    Handles *h = nullptr;
+    KFB_TRY(get_handles(s, h));
+    const RfpBlocks b = rfp_blocks(n, lower);
+    const T one = T(1), mone = T(-1);
+    T *B1 = B, *B2 = B + b.n1;
+    const int ldb = n;
+    const cublasSideMode_t L = CUBLAS_SIDE_LEFT;
+    const cublasFillMode_t LO = CUBLAS_FILL_MODE_LOWER, UP = CUBLAS_FILL_MODE_UPPER;
+    // forward: (L or U^T) y = b ; T1 lower-stored, T2 upper-stored in both cases
+    KFB_BLAS_TRY(Blas<T>::trsm(h->blas, L, LO, CUBLAS_OP_N, b.n1, nrhs, &one, a + b.t1, b.ld, B1, ldb));
+    if (b.n2 > 0) {
+        if (lower)
+            KFB_BLAS_TRY(Blas<T>::gemm(h->blas, CUBLAS_OP_N, CUBLAS_OP_N, b.n2, nrhs, b.n1, &mone,
+                                       a + b.s, b.ld, B1, ldb, &one, B2, ldb));
+        else
+            KFB_BLAS_TRY(Blas<T>::gemm(h->blas, CUBLAS_OP_T, CUBLAS_OP_N, b.n2, nrhs, b.n1, &mone,
+                                       a + b.s, b.ld, B1, ldb, &one, B2, ldb));
+        KFB_BLAS_TRY(Blas<T>::trsm(h->blas, L, UP, CUBLAS_OP_T, b.n2, nrhs, &one, a + b.t2, b.ld, B2, ldb));
+        // backward
+        KFB_BLAS_TRY(Blas<T>::trsm(h->blas, L, UP, CUBLAS_OP_N, b.n2, nrhs, &one, a + b.t2, b.ld, B2, ldb));
+        if (lower)
+            KFB_BLAS_TRY(Blas<T>::gemm(h->blas, CUBLAS_OP_T, CUBLAS_OP_N, b.n1, nrhs, b.n2, &mone,
+                                       a + b.s, b.ld, B2, ldb, &one, B1, ldb));
+        else
+            KFB_BLAS_TRY(Blas<T>::gemm(h->blas, CUBLAS_OP_N, CUBLAS_OP_N, b.n1, nrhs, b.n2, &mone,
+                                       a + b.s, b.ld, B2, ldb, &one, B1, ldb));
+    }
+    KFB_BLAS_TRY(Blas<T>::trsm(h->blas, L, LO, CUBLAS_OP_T, b.n1, nrhs, &one, a + b.t1, b.ld, B1, ldb));
+    return KFB_OK;
+}
+
+// ------------------------------------------------------------ small kernels
+template <class T>
+__global__ void add_diag_kernel(T *arf, int n, T l2, int layout) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) arf[sym_index((kfb_layout)layout, n, i, i)] += l2;
+}
+
+template <class T>
+__global__ void full_to_rfp_kernel(const T *A, int n, int layout, T *arf) {
+    const long long i = blockIdx.y * (long long)blockDim.y + threadIdx.y;
+    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n && j < n && i <= j) arf[sym_index((kfb_layout)layout, n, i, j)] = A[i * n + j];
+}
+
+template <class Tin, class Tout>
+__global__ void rfp_to_full_kernel(const Tin *arf, int n, int layout, Tout *A) {
+    const long long i = blockIdx.y * (long long)blockDim.y + threadIdx.y;
+    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n && j < n) A[i * n + j] = (Tout)arf[sym_index((kfb_layout)layout, n, i, j)];
+}
+
+// r = y - (K + l2 I) x with K dense FP32 (row-major, symmetric), FP64 vectors.
+__global__ void residual_kernel(const float *__restrict__ K, const double *__restrict__ x,
+                                const double *__restrict__ y, int n, double l2,
+                                double *__restrict__ r) {
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const float *kr = K + (size_t)row * n;
+    double acc = 0.0;
+    for (int j = lane; j < n; j += 32) acc = fma((double)kr[j], x[j], acc);
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) r[row] = (y ? y[row] : 0.0) - acc - l2 * x[row];
+}
+
+// out = sum_i a_i b_i  (FP64), one partial per block then atomically combined
+__global__ void dot_kernel(const double *a, const double *b, int n, double *out) {
+    double acc = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        acc = fma(a[i], b[i], acc);
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    __shared__ double part[32];
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = threadIdx.x < (blockDim.x >> 5) ? part[threadIdx.x] : 0.0;
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) atomicAdd(out, v);
+    }
+}
+
+__global__ void scale_to_float_kernel(const double *a, double s, int n, float *out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (float)(a[i] * s);
+}
+// x += s * (double)d
+__global__ void axpy_float_kernel(const float *d, double s, int n, double *x) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] += s * (double)d[i];
+}
+// y += s * x
+__global__ void axpy_kernel(const double *x, double s, int n, double *y) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] += s * x[i];
+}
+// p = z + beta * p
+__global__ void xpby_kernel(const double *z, double beta, int n, double *p) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = z[i] + beta * p[i];
+}
+__global__ void float_to_double_kernel(const float *a, double s, int n, double *out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = s * (double)a[i];
+}
+__global__ void max_diag_kernel(const float *K, int n, float *out) {
+    float m = 0.f;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        m = fmaxf(m, fabsf(K[(size_t)i * n + i]));
+    for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<int *>(out), __float_as_int(m));
+}
+
+inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+struct Dot {
+    DevBuf buf;
+    kfb_status init(cudaStream_t s) { return buf.alloc(sizeof(double), s); }
+    kfb_status operator()(const double *a, const double *b, int n, cudaStream_t s, double &out) {
+        KFB_TRY(zero(buf.ptr, sizeof(double), s));
+        dot_kernel<<<std::min(nblk(n, 256), 1184u), 256, 0, s>>>(a, b, n, buf.as<double>());
+        KFB_CUDA_TRY(cudaGetLastError());
+        KFB_CUDA_TRY(cudaMemcpyAsync(&out, buf.ptr, sizeof(double), cudaMemcpyDeviceToHost, s));
+        KFB_CUDA_TRY(cudaStreamSynchronize(s));
+        return KFB_OK;
+    }
+};
+
+}  // namespace
+
+// ----------------------------------------------------------------- exported
+kfb_status rfp_add_diag(void *arf, int n, double l2, kfb_layout uplo, kfb_dtype dt,
+                        cudaStream_t s) {
+    if (n <= 0 || l2 == 0.0) return KFB_OK;
+    if (dt == KFB_F64)
+        add_diag_kernel<double><<<nblk(n, 256), 256, 0, s>>>(static_cast<double *>(arf), n, l2, uplo);
+    else
+        add_diag_kernel<float><<<nblk(n, 256), 256, 0, s>>>(static_cast<float *>(arf), n, (float)l2, uplo);
+    KFB_CUDA_TRY(cudaGetLastError());
+    return KFB_OK;
+}
+
+kfb_status full_to_rfp(const void *A, int n, kfb_layout uplo, kfb_dtype dt, void *arf,
+                       cudaStream_t s) {
+    if (n <= 0) return KFB_OK;
+    dim3 blk(32, 8), grd(nblk(n, 32), nblk(n, 8));
+    if (dt == KFB_F64)
+        full_to_rfp_kernel<double><<<grd, blk, 0, s>>>(static_cast<const double *>(A), n, uplo,
+                                                       static_cast<double *>(arf));
+    else
+        full_to_rfp_kernel<float><<<grd, blk, 0, s>>>(static_cast<const float *>(A), n, uplo,
+                                                      static_cast<float *>(arf));
+    KFB_CUDA_TRY(cudaGetLastError());
+    return KFB_OK;
+}
+
+kfb_status rfp_to_full(const void *arf, int n, kfb_layout uplo, kfb_dtype dt, void *A,
+                       cudaStream_t s) {
+    if (n <= 0) return KFB_OK;
+    dim3 blk(32, 8), grd(nblk(n, 32), nblk(n, 8));
+    if (dt == KFB_F64)
+        rfp_to_full_kernel<double, double><<<grd, blk, 0, s>>>(static_cast<const double *>(arf), n,
+                                                               uplo, static_cast<double *>(A));
+    else
+        rfp_to_full_kernel<float, float><<<grd, blk, 0, s>>>(static_cast<const float *>(arf), n,
+                                                             uplo, static_cast<float *>(A));
+    KFB_CUDA_TRY(cudaGetLastError());
+    return KFB_OK;
+}
+
+kfb_status rfp_potrf(void *arf, int n, double l2, kfb_layout uplo, kfb_dtype dt, int *info,
+                     cudaStream_t s) {
+    KFB_TRY(rfp_add_diag(arf, n, l2, uplo, dt, s));
+    if (dt == KFB_F64) return rfp_potrf_t<double>(static_cast<double *>(arf), n, uplo == KFB_RFP_L, info, s);
+    return rfp_potrf_t<float>(static_cast<float *>(arf), n, uplo == KFB_RFP_L, info, s);
+}
+
+kfb_status rfp_potrs(const void *arf, void *B, int n, int nrhs, kfb_layout uplo, kfb_dtype dt,
+                     cudaStream_t s) {
+    if (dt == KFB_F64)
+        return rfp_potrs_t<double>(static_cast<const double *>(arf), static_cast<double *>(B), n,
+                                   nrhs, uplo == KFB_RFP_L, s);
+    return rfp_potrs_t<float>(static_cast<const float *>(arf), static_cast<float *>(B), n, nrhs,
+                              uplo == KFB_RFP_L, s);
+}
+
+kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2,
+                           kfb_layout uplo, double tol, int maxit, double *alpha,
+                           kfb_solve_info *info, cudaStream_t s) {
+    kfb_solve_info inf{};
+    const size_t nt = (size_t)n * (n + 1) / 2;
+    DevBuf Kd, F, r, z, p, q, f32v, dmax;
+    KFB_TRY(Kd.alloc((size_t)n * n * sizeof(float), s));
+    KFB_TRY(rfp_to_full(k_rfp, n, uplo, KFB_F32, Kd.ptr, s));
+    KFB_TRY(F.alloc(nt * sizeof(float), s));
+    KFB_TRY(r.alloc((size_t)n * sizeof(double), s));
+    KFB_TRY(z.alloc((size_t)n * sizeof(double), s));
+    KFB_TRY(p.alloc((size_t)n * sizeof(double), s));
+    KFB_TRY(q.alloc((size_t)n * sizeof(double), s));
+    KFB_TRY(f32v.alloc((size_t)n * sizeof(float), s));
+    KFB_TRY(dmax.alloc(sizeof(float), s));
+    Dot dot;
+    KFB_TRY(dot.init(s));
+
+    // FP32 factor of K + (l2 + shift) I; the shift grows until potrf succeeds
+    KFB_TRY(zero(dmax.ptr, sizeof(float), s));
+    max_diag_kernel<<<std::min(nblk(n, 256), 148u), 256, 0, s>>>(Kd.as<float>(), n, dmax.as<float>());
+    float hmax = 0.f;
+    KFB_CUDA_TRY(cudaMemcpyAsync(&hmax, dmax.ptr, sizeof(float), cudaMemcpyDeviceToHost, s));
+    KFB_CUDA_TRY(cudaStreamSynchronize(s));
+    double shift = 0.0;
+    int finfo = 0;
+    for (int attempt = 0; attempt < 12; ++attempt) {
+        KFB_CUDA_TRY(cudaMemcpyAsync(F.ptr, k_rfp, nt * sizeof(float), cudaMemcpyDeviceToDevice, s));
+        KFB_TRY(rfp_potrf(F.ptr, n, l2 + shift, uplo, KFB_F32, &finfo, s));
+        if (finfo == 0) break;
+        shift = (shift == 0.0) ? std::max(1e-7 * (double)hmax, 10.0 * l2) : shift * 10.0;
+    }
+    inf.factor_info = finfo;
+    inf.shift = shift;
+    if (finfo != 0) {
+        if (info) *info = inf;
+        return set_error(KFB_ERR_NOT_PD, "FP32 RFP Cholesky failed even with shift %g (info=%d)",
+                         shift, finfo);
+    }
+
+    double ynorm2 = 0.0;
+    KFB_TRY(dot(y, y, n, s, ynorm2));
+    const double ynorm = std::sqrt(ynorm2);
+    KFB_TRY(zero(alpha, (size_t)n * sizeof(double), s));
+    if (ynorm == 0.0) {
+        if (info) *info = inf;
+        return KFB_OK;
+    }
+    const unsigned gb = nblk(n, 256), gw = nblk((long long)n * 32, 256);
+    // M^{-1} v via the FP32 factor, with v scaled to unit norm first
+    auto precond = [&](const double *v, double vnorm, double *out) -> kfb_status {
+        const double sc = vnorm > 0.0 ? 1.0 / vnorm : 1.0;
+        scale_to_float_kernel<<<gb, 256, 0, s>>>(v, sc, n, f32v.as<float>());
+        KFB_TRY(rfp_potrs(F.ptr, f32v.ptr, n, 1, uplo, KFB_F32, s));
+        float_to_double_kernel<<<gb, 256, 0, s>>>(f32v.as<float>(), vnorm > 0.0 ? vnorm : 1.0, n,
+                                                  out);
+        KFB_CUDA_TRY(cudaGetLastError());
+        return KFB_OK;
+    };
+
+    // classic iterative refinement
+    double rn = ynorm, prev = ynorm;
+    int it = 0, stall = 0;
+    residual_kernel<<<gw, 256, 0, s>>>(Kd.as<float>(), alpha, y, n, l2, r.as<double>());
+    for (; it < maxit; ++it) {
+        double rr = 0.0;
+        KFB_TRY(dot(r.as<double>(), r.as<double>(), n, s, rr));
+        rn = std::sqrt(rr);
+        if (rn <= tol * ynorm) break;
+        if (it > 0 && rn > 0.5 * prev) {
+            if (++stall >= 2) break;
+        } else {
+            stall = 0;
+        }
+        prev = rn;
+        KFB_TRY(precond(r.as<double>(), rn, z.as<double>()));
+        axpy_kernel<<<gb, 256, 0, s>>>(z.as<double>(), 1.0, n, alpha);
+        residual_kernel<<<gw, 256, 0, s>>>(Kd.as<float>(), alpha, y, n, l2, r.as<double>());
+        KFB_CUDA_TRY(cudaGetLastError());
+    }
+    inf.iterations = it;
+    if (rn > tol * ynorm && it < maxit) {
+        // preconditioned conjugate gradients (FP64), FP32 factor as preconditioner
+        inf.used_cg = 1;
+        KFB_TRY(precond(r.as<double>(), rn, z.as<double>()));
+        KFB_CUDA_TRY(cudaMemcpyAsync(p.ptr, z.ptr, (size_t)n * sizeof(double),
+                                     cudaMemcpyDeviceToDevice, s));
+        double rz = 0.0;
+        KFB_TRY(dot(r.as<double>(), z.as<double>(), n, s, rz));
+        for (; it < maxit; ++it) {
+            residual_kernel<<<gw, 256, 0, s>>>(Kd.as<float>(), p.as<double>(), nullptr, n, l2,
+                                               q.as<double>());  // q = -(K + l2 I) p
+            double pq = 0.0;
+            KFB_TRY(dot(p.as<double>(), q.as<double>(), n, s, pq));
+            pq = -pq;
+            if (!(pq > 0.0)) break;
+            const double a = rz / pq;
+            axpy_kernel<<<gb, 256, 0, s>>>(p.as<double>(), a, n, alpha);
+            axpy_kernel<<<gb, 256, 0, s>>>(q.as<double>(), a, n, r.as<double>());  // r -= a A p
+            double rr = 0.0;
+            KFB_TRY(dot(r.as<double>(), r.as<double>(), n, s, rr));
+            rn = std::sqrt(rr);
+            if (rn <= tol * ynorm) {
+                ++it;
+                break;
+            }
+            KFB_TRY(precond(r.as<double>(), rn, z.as<double>()));
+            double rz_new = 0.0;
+            KFB_TRY(dot(r.as<double>(), z.as<double>(), n, s, rz_new));
+            xpby_kernel<<<gb, 256, 0, s>>>(z.as<double>(), rz_new / rz, n, p.as<double>());
+            rz = rz_new;
+        }
+        // true residual
+        residual_kernel<<<gw, 256, 0, s>>>(Kd.as<float>(), alpha, y, n, l2, r.as<double>());
+        double rr = 0.0;
+        KFB_TRY(dot(r.as<double>(), r.as<double>(), n, s, rr));
+        rn = std::sqrt(rr);
+        inf.iterations = it;
+    }
+    inf.rel_residual = rn / ynorm;
+    if (info) *info = inf;
+    if (inf.rel_residual > tol)
+        return set_error(KFB_ERR_NO_CONVERGENCE,
+                         "refinement stopped at relative residual %.3e (tol %.1e) after %d "
+                         "iterations",
+                         inf.rel_residual, tol, inf.iterations);
+    return KFB_OK;
+}
+
+}  // namespace kfb

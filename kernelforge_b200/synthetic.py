@@ -166,17 +166,20 @@ def _fchl19_one(R: torch.Tensor, zidx: torch.Tensor, nelem: int = 5, nRs2: int =
     return out
 
 
-def _zidx(z: np.ndarray) -> torch.Tensor:
-    lut = {e: i for i, e in enumerate(ELEMENTS)}
+def _zidx(z: np.ndarray, elements=ELEMENTS) -> torch.Tensor:
+    lut = {e: i for i, e in enumerate(elements)}
     return torch.tensor([lut[int(v)] for v in z], dtype=torch.long)
 
 
 def fchl19(mols: Molecules, gradients: bool = False, max_atoms: int | None = None,
-           dtype=np.float64):
-    """Padded FCHL19 arrays: X (nm, ma, 720) [, dX (nm, ma, 720, 3*ma)], Q, N."""
+           dtype=np.float64, elements=ELEMENTS, nRs2: int = 24, nRs3: int = 20):
+    """Padded FCHL19 arrays: X (nm, ma, rep) [, dX (nm, ma, rep, 3*ma)], Q, N
+    (rep = 720 for the default elements and basis sizes)."""
     nm = mols.nm
     ma = max_atoms or max(len(z) for z in mols.Z)
-    rep = rep_size()
+    nel = len(elements)
+    rep = rep_size(nel, nRs2, nRs3)
+    kw = dict(nelem=nel, nRs2=nRs2, nRs3=nRs3)
     X = np.zeros((nm, ma, rep), dtype=dtype)
     dX = np.zeros((nm, ma, rep, 3 * ma), dtype=dtype) if gradients else None
     Q = np.zeros((nm, ma), dtype=np.int32)
@@ -186,13 +189,13 @@ def fchl19(mols: Molecules, gradients: bool = False, max_atoms: int | None = Non
             z = mols.Z[m]
             n = len(z)
             R = torch.tensor(mols.R[m], dtype=torch.float64)
-            zi = _zidx(z)
+            zi = _zidx(z, elements)
             if gradients:
-                J = torch.func.jacfwd(lambda rr: _fchl19_one(rr, zi))(R)   # (n, rep, n, 3)
-                rep_m = _fchl19_one(R, zi).detach().numpy()
+                J = torch.func.jacfwd(lambda rr: _fchl19_one(rr, zi, **kw))(R)   # (n, rep, n, 3)
+                rep_m = _fchl19_one(R, zi, **kw).detach().numpy()
                 dX[m, :n, :, : 3 * n] = J.reshape(n, rep, 3 * n).numpy()
             else:
-                rep_m = _fchl19_one(R, zi).numpy()
+                rep_m = _fchl19_one(R, zi, **kw).numpy()
             X[m, :n] = rep_m
             Q[m, :n] = z
             N[m] = n

@@ -1,0 +1,87 @@
+"""Jacobian / Hessian / full kernels on the GPU against the oracle and the
+reference's golden outputs.  FP64: rtol 1e-10 (the reference's own tolerance
+for these kernels); FP32: rtol 1e-4 relative to max|K|."""
+import numpy as np
+import pytest
+
+from conftest import load_golden, make_set
+from oracle import oracle as o
+
+pytestmark = pytest.mark.gpu
+
+
+def close(got, ref, precision):
+    if precision == "fp64":
+        np.testing.assert_allclose(got, ref, rtol=1e-10, atol=1e-10 * max(1.0, np.abs(ref).max()))
+    else:
+        np.testing.assert_allclose(got, ref, rtol=1e-3, atol=1e-4 * max(1.0, np.abs(ref).max()))
+
+
+GOLDEN_CASES = [
+    ("kernel_gaussian_jacobian", ("X1", "X2", "dX2", "Q1", "Q2", "N1", "N2")),
+    ("kernel_gaussian_jacobian_t", ("X1", "dX1", "X2", "Q1", "Q2", "N1", "N2")),
+    ("kernel_gaussian_hessian", ("X1", "dX1", "X2", "dX2", "Q1", "Q2", "N1", "N2")),
+    ("kernel_gaussian_hessian_symm", ("X1", "dX1", "Q1", "N1")),
+    ("kernel_gaussian_hessian_symm_rfp", ("X1", "dX1", "Q1", "N1")),
+    ("kernel_gaussian_full", ("X1", "dX1", "X2", "dX2", "Q1", "Q2", "N1", "N2")),
+    ("kernel_gaussian_full_symm", ("X1", "dX1", "Q1", "N1")),
+    ("kernel_gaussian_full_symm_rfp", ("X1", "dX1", "Q1", "N1")),
+]
+
+
+@pytest.mark.parametrize("name,args", GOLDEN_CASES)
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_golden_random(name, args, precision):
+    from kernelforge_b200 import local_kernels as lk
+    g = load_golden("golden_random.npz")
+    got = getattr(lk, name)(*[g[a] for a in args], float(g["sigma"]), precision=precision)
+    assert got.shape == g[name].shape
+    close(got, g[name], precision)
+
+
+def test_golden_fchl19():
+    from kernelforge_b200 import local_kernels as lk
+    g = load_golden("golden_fchl19.npz")
+    X, dX, Q, N, s = g["X"], g["dX"], g["Q"], g["N"], float(g["sigma"])
+    close(lk.kernel_gaussian_jacobian(X[:4], X[2:], dX[2:], Q[:4], Q[2:], N[:4], N[2:], s),
+          g["kernel_gaussian_jacobian"], "fp64")
+    close(lk.kernel_gaussian_hessian_symm_rfp(X, dX, Q, N, s), g["kernel_gaussian_hessian_symm_rfp"],
+          "fp64")
+    close(lk.kernel_gaussian_full_symm_rfp(X, dX, Q, N, s), g["kernel_gaussian_full_symm_rfp"],
+          "fp64")
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_larger_ragged_sets(seed):
+    from kernelforge_b200 import local_kernels as lk
+    X1, dX1, Q1, N1 = make_set(9, 7, 33, 3, seed)
+    X2, dX2, Q2, N2 = make_set(6, 5, 33, 3, seed + 10)
+    X1 *= 0.4
+    X2 *= 0.4
+    s = 2.0
+    close(lk.kernel_gaussian_jacobian(X1, X2, dX2, Q1, Q2, N1, N2, s),
+          o.kernel_gaussian_jacobian(X1, X2, dX2, Q1, Q2, N1, N2, s), "fp64")
+    close(lk.kernel_gaussian_jacobian_t(X1, dX1, X2, Q1, Q2, N1, N2, s),
+          o.kernel_gaussian_jacobian_t(X1, dX1, X2, Q1, Q2, N1, N2, s), "fp64")
+    close(lk.kernel_gaussian_hessian(X1, dX1, X2, dX2, Q1, Q2, N1, N2, s),
+          o.kernel_gaussian_hessian(X1, dX1, X2, dX2, Q1, Q2, N1, N2, s), "fp64")
+    close(lk.kernel_gaussian_full(X1, dX1, X2, dX2, Q1, Q2, N1, N2, s),
+          o.kernel_gaussian_full(X1, dX1, X2, dX2, Q1, Q2, N1, N2, s), "fp64")
+
+
+def test_jacobian_t_is_minus_jacobian_transposed():
+    from kernelforge_b200 import local_kernels as lk
+    X1, dX1, Q1, N1 = make_set(5, 6, 10, 2, 3)
+    X2, dX2, Q2, N2 = make_set(4, 6, 10, 2, 4)
+    jt = lk.kernel_gaussian_jacobian_t(X1, dX1, X2, Q1, Q2, N1, N2, 2.0)
+    j = lk.kernel_gaussian_jacobian(X2, X1, dX1, Q2, Q1, N2, N1, 2.0)
+    np.testing.assert_allclose(jt, -j.T, rtol=1e-12, atol=1e-12)
+
+
+def test_full_symm_is_symmetric_and_matches_asym():
+    from kernelforge_b200 import local_kernels as lk
+    X, dX, Q, N = make_set(5, 5, 12, 2, 8)
+    F = lk.kernel_gaussian_full_symm(X, dX, Q, N, 2.0)
+    np.testing.assert_allclose(F, F.T, rtol=1e-12, atol=1e-12)
+    Fa = lk.kernel_gaussian_full(X, dX, X, dX, Q, Q, N, N, 2.0)
+    np.testing.assert_allclose(F, Fa, rtol=1e-10, atol=1e-10)
