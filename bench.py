@@ -1,0 +1,399 @@
+"""Benchmark: FCHL19 local-kernel KRR fit on one B200 (and N replicas).
+
+Workload (one step): 10,000 seeded synthetic molecules (9-21 atoms, H/C/N/O,
+~150k atoms, 720-dim FCHL19 descriptors) -> the symmetric local Gaussian
+kernel (sigma = 2) written straight to RFP on the tcgen05 tensor cores
+(split-fp16, FP32 accumulation; 50,005,000 packed entries) -> the KRR solve
+(K + 1e-8 I) alpha = y with an FP32 RFP Cholesky factor and FP64 refinement to a
+relative residual of 1e-10.  Labels are Morse energies (mean removed).
+
+Metric: kernel entries per second of the whole fit step (value = packed kernel
+entries / step time, summed over ranks).  Descriptors are generated once,
+before timing (the reference times descriptors separately).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference's own CPU FP64 implementation (the
+kernel_gaussian_symm_rfp + cho_solve_rfp pybind modules built from its sources
+into oracle/_ref/) on a bounded sample of the same workload on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SIGMA = 2.0
+L2 = 1e-8
+TOL = 1e-10
+SEED = 20261204
+NMOL = 10000
+REP = 720
+CPU_SAMPLE_NMOL = 3000
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nmol", type=int, default=NMOL)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_setup(n_gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def workload(nmol, seed, device="cuda"):
+    from kernelforge_b200 import synthetic
+    mols = synthetic.make_molecules(nmol, 9, 21, seed=seed)
+    X, Q, N = synthetic.fchl19_batched(mols, dtype=np.float32, device=device, chunk=128)
+    y = mols.E - mols.E.mean()
+    return X, Q, N, y
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.th = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.th:
+            self.th.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def p_sym(Q, N):
+    """Unique same-label atom pairs sum_e R_e (R_e + 1) / 2."""
+    ma = Q.shape[1]
+    act = np.arange(ma)[None, :] < np.clip(N, 0, ma)[:, None]
+    labs, counts = np.unique(Q[act], return_counts=True)
+    return int(sum(int(c) * (int(c) + 1) // 2 for c in counts)), dict(zip(labs.tolist(),
+                                                                          counts.tolist()))
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, \
+            "fallback"
+
+
+def traffic_per_launch():
+    """DRAM bytes of the tensor-core tile kernel from the committed ncu summary
+    (scaled to the bench workload there), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "scalar_tc_traffic.json")) as f:
+            return json.load(f).get("bytes_per_launch_bench_workload")
+    except (OSError, ValueError):
+        return None
+
+
+def count_our_launches(step):
+    """Kernels of libkfb launched by one step (CUPTI via torch.profiler)."""
+    try:
+        from torch.profiler import ProfilerActivity, profile
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            step()
+        n = 0
+        for ev in prof.events():
+            if ev.device_type is not None and "cuda" in str(ev.device_type).lower() \
+                    and "kfb" in ev.name:
+                n += 1
+        return n
+    except Exception:
+        return None
+
+
+def cpu_reference_step(X, Q, N, y, nmol):
+    """The reference's CPU FP64 path on the first `nmol` molecules; returns
+    (seconds, packed entries)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))
+    import kernelmath as km  # noqa: E402  (reference build)
+    import local_kernels as lk  # noqa: E402
+    Xs = np.ascontiguousarray(X[:nmol], dtype=np.float64)
+    t0 = time.perf_counter()
+    arf = lk.kernel_gaussian_symm_rfp(Xs, Q[:nmol], N[:nmol], SIGMA)
+    km.cho_solve_rfp(arf, y[:nmol], L2)
+    return time.perf_counter() - t0, nmol * (nmol + 1) // 2
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    ref_dir = os.path.join(ROOT, "oracle", "_ref")
+    built = os.path.isdir(ref_dir) and any(f.startswith("local_kernels")
+                                           for f in os.listdir(ref_dir))
+    if not built:
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "reference CPU modules not built (oracle/build_ref.sh)"}))
+        return
+    cores = os.cpu_count()
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    X, Q, N, y = workload(CPU_SAMPLE_NMOL, SEED, device="cuda" if _has_cuda() else "cpu")
+    for _ in range(args.warmup):
+        cpu_reference_step(X, Q, N, y, CPU_SAMPLE_NMOL)
+    times = []
+    for _ in range(args.steps):
+        dt, entries = cpu_reference_step(X, Q, N, y, CPU_SAMPLE_NMOL)
+        times.append(dt)
+    t = sum(times) / len(times)
+    val = entries / t
+    unit = "entries/s"
+    line = {"metric": "FCHL19 local-kernel KRR fit: kernel entries/s", "value": val, "unit": unit,
+            "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"symmetric FCHL19 local kernel (RFP) + Cholesky KRR solve, "
+                                   f"sample of {CPU_SAMPLE_NMOL} of the {NMOL} molecules",
+                       "sigma": SIGMA, "l2": L2, "rep": REP},
+            "cpu_baseline": {"value": val, "unit": unit, "cores": cores, "kind": "reference",
+                             "sample": f"{CPU_SAMPLE_NMOL} molecules (kernel_gaussian_symm_rfp + "
+                                       f"cho_solve_rfp), OMP threads {cores}"},
+            "e2e": {"value": val, "unit": unit, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def _has_cuda():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+def run_ours(args, rank, world, local):
+    import torch
+
+    from kernelforge_b200 import _lib
+    from kernelforge_b200 import cuda_global_kernels as cgk
+    from kernelforge_b200 import cuda_local_kernels as clk
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    X, Q, N, y = workload(args.nmol, SEED + rank)
+    nm = X.shape[0]
+    entries = nm * (nm + 1) // 2
+    Xd = torch.tensor(X, device=dev)
+    yd = torch.tensor(y, dtype=torch.float64, device=dev)
+    Qh, Nh = Q, N
+    solve_info = {}
+
+    def step():
+        K = clk.kernel_gaussian_symm_rfp(Xd, Qh, Nh, SIGMA)
+        alpha, info = cgk.krr_solve_mixed(K, yd, l2=L2, uplo="L", tol=TOL)
+        solve_info.update(info)
+        return alpha
+
+    # e2e: host buffers in, alpha back to the host
+    Xh = torch.from_numpy(X).pin_memory()
+    yh = torch.from_numpy(np.ascontiguousarray(y)).pin_memory()
+    alpha_h = torch.empty((nm,), dtype=torch.float64).pin_memory()
+
+    def step_e2e():
+        Xg = Xh.to(dev, non_blocking=True)
+        yg = yh.to(dev, non_blocking=True)
+        K = clk.kernel_gaussian_symm_rfp(Xg, Qh, Nh, SIGMA)
+        alpha, _ = cgk.krr_solve_mixed(K, yg, l2=L2, uplo="L", tol=TOL)
+        alpha_h.copy_(alpha, non_blocking=True)
+        return alpha_h
+
+    h2d = X.nbytes + y.nbytes + Q.nbytes + N.nbytes
+    d2h = alpha_h.numel() * 8
+
+    _lib.lib().kfb_set_timing(1)
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    clocks = ClockSampler(local)
+    clocks.start()
+    kernel_ms = []
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(args.steps):
+        step()
+        kernel_ms.append(_lib.lib().kfb_last_kernel_ms())
+    t1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk_info = clocks.stop()
+    ms = t0.elapsed_time(t1) / args.steps
+    ms = max_over_ranks(ms, world)
+    _lib.lib().kfb_set_timing(0)
+
+    # e2e (host buffers, copies inside the timed region)
+    for _ in range(2):
+        step_e2e()
+    torch.cuda.synchronize()
+    barrier(world)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step_e2e()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
+    barrier(world)
+
+    launches_per_step = count_our_launches(step) if rank == 0 else None
+
+    if rank != 0:
+        return
+    peaks, peak_kind = load_peaks()
+    psym, per_label = p_sym(Q, N)
+    # the three compensated fp16 products over the unique same-label pairs
+    flops = 3 * 2.0 * REP * psym
+    kms = statistics.median(kernel_ms)
+    achieved = flops / (kms * 1e-3) / 1e12
+    peak = peaks.get("bf16_tflops")
+    cpu = None
+    if not args.no_cpu_baseline:
+        try:
+            dt, ent = cpu_reference_step(X, Q, N, y, CPU_SAMPLE_NMOL)
+            cpu = {"value": ent / dt, "unit": "entries/s", "cores": os.cpu_count(),
+                   "kind": "reference",
+                   "sample": f"{CPU_SAMPLE_NMOL} of the {nm} molecules: reference "
+                             "kernel_gaussian_symm_rfp + cho_solve_rfp (FP64, OpenMP + OpenBLAS)"}
+        except Exception as exc:  # the reference build is optional on a user's machine
+            cpu = {"value": None, "unit": "entries/s", "cores": os.cpu_count(),
+                   "kind": "reference", "sample": f"unavailable: {exc}"}
+    line = {
+        "metric": "FCHL19 local-kernel KRR fit: kernel entries/s",
+        "value": entries * world / (ms * 1e-3),
+        "unit": "entries/s",
+        "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3),
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f16x3 (split fp16, fp32 accumulate) + f32/f64 solve",
+        "data": "synthetic (seeded molecules, FCHL19 descriptors, Morse labels)",
+        "config": {"workload": f"{nm}-molecule symmetric FCHL19 local kernel -> RFP (tcgen05 "
+                               "split-fp16) + FP32 RFP Cholesky / FP64 refinement solve",
+                   "molecules_per_gpu": nm, "atoms_per_gpu": int(np.clip(N, 0, None).sum()),
+                   "rep": REP, "sigma": SIGMA, "l2": L2, "tol": TOL,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2_flush": "inputs larger than L2 (X is %.0f MB)" % (X.nbytes / 1e6)},
+        "fit_s": ms * 1e-3,
+        "kernel_ms": kms,
+        "solve": {k: solve_info.get(k) for k in ("iterations", "shift", "rel_residual",
+                                                  "used_cg")},
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak if peak else None, "traffic": traffic_per_launch(),
+                     "peak_kind": f"{peak_kind} bf16 dense (f16 MMAs run at the same rate)",
+                     "flops_per_launch": flops, "unique_pairs": psym},
+        "cpu_baseline": cpu,
+        "clocks": clk_info,
+        "e2e": {"value": entries * world / (e2e_ms * 1e-3), "unit": "entries/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": (launches_per_step * args.steps) if launches_per_step else None,
+    }
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_setup(args.gpus)
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -72,6 +72,15 @@ typedef enum kfb_layout {
 const char *kfb_last_error(void);
 int kfb_abi_version(void);
 
+/* Tracing.  When enabled, each call brackets its main tile kernel (the tensor-
+ * core or CUDA-core tile kernel of the scalar kernels) with CUDA events on the
+ * caller's stream and keeps the elapsed time, read back by
+ * kfb_last_kernel_ms() (milliseconds; the call synchronises the stream).
+ * No reference counterpart: the reference prints always-on stage timers to
+ * stderr (src/cuda_local_kernels.cu:1902-1909). */
+kfb_status kfb_set_timing(int enable);
+double kfb_last_kernel_ms(void);
+
 /* ---------------------------------------------------------------------- */
 /* Scalar kernels: K[a,b] = sum_{i in a, j in b, q_i = q_j}                */
 /*                          exp(-||x_i - x_j||^2 / (2 sigma^2))            */

@@ -17,6 +17,8 @@ kfb_status rfp_potrf(void *arf, int n, double l2, kfb_layout uplo, kfb_dtype dt,
 kfb_status rfp_potrs(const void *arf, void *B, int n, int nrhs, kfb_layout uplo, kfb_dtype dt, cudaStream_t s);
 kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2, kfb_layout uplo,
                            double tol, int maxit, double *alpha, kfb_solve_info *info, cudaStream_t s);
+double last_kernel_ms();
+void set_timing(bool on);
 }  // namespace kfb
 
 using namespace kfb;
@@ -116,6 +118,12 @@ extern "C" {
 
 const char *kfb_last_error(void) { return last_error(); }
 int kfb_abi_version(void) { return KFB_ABI_VERSION; }
+
+kfb_status kfb_set_timing(int enable) {
+    set_timing(enable != 0);
+    return KFB_OK;
+}
+double kfb_last_kernel_ms(void) { return last_kernel_ms(); }
 
 kfb_status kfb_kernel_gaussian(const void *x1, const void *x2, const int32_t *q1,
                                const int32_t *q2, const int32_t *n1, const int32_t *n2, int nm1,

@@ -107,6 +107,35 @@ int device_sm_count() {
     return n > 0 ? n : 1;
 }
 
+static bool g_timing = false;
+static thread_local double g_last_ms = 0.0;
+
+bool timing_enabled() { return g_timing; }
+
+KernelTimer::KernelTimer(cudaStream_t s) : stream(s) {
+    if (!g_timing) return;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+}
+KernelTimer::~KernelTimer() {
+    if (t0) cudaEventDestroy(t0);
+    if (t1) cudaEventDestroy(t1);
+}
+void KernelTimer::start() {
+    if (t0) cudaEventRecord(t0, stream);
+}
+void KernelTimer::stop() {
+    if (!t1) return;
+    cudaEventRecord(t1, stream);
+    cudaEventSynchronize(t1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, t0, t1);
+    g_last_ms = ms;
+}
+
+double last_kernel_ms() { return g_last_ms; }
+void set_timing(bool on) { g_timing = on; }
+
 bool device_is_sm100() {
     int dev = 0, major = 0, minor = 0;
     cudaGetDevice(&dev);

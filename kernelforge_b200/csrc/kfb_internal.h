@@ -160,4 +160,15 @@ kfb_status zero(void *ptr, size_t bytes, cudaStream_t s);
 int device_sm_count();
 bool device_is_sm100();
 
+// Optional event timing of the main tile kernel of a call (kfb_set_timing).
+bool timing_enabled();
+struct KernelTimer {
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    cudaStream_t stream = nullptr;
+    explicit KernelTimer(cudaStream_t s);
+    ~KernelTimer();
+    void start();
+    void stop();
+};
+
 }  // namespace kfb

@@ -174,6 +174,8 @@ kfb_status run_simt(const ScalarProblem &p, const PairSink &sink, cudaStream_t s
                  &MB = p.symmetric ? ma : mb;
     // grid-stride over tiles in launches of at most 2^31-1 blocks
     const size_t ntiles = tiles.size();
+    KernelTimer timer(s);
+    timer.start();
     for (size_t off = 0; off < ntiles; off += (size_t)1 << 30) {
         const unsigned nb_ = (unsigned)std::min<size_t>(ntiles - off, (size_t)1 << 30);
         scalar_tile_kernel<T><<<nb_, 256, 0, s>>>(pa.as<T>(), PB.as<T>(), Dp, na.as<T>(),
@@ -181,6 +183,7 @@ kfb_status run_simt(const ScalarProblem &p, const PairSink &sink, cudaStream_t s
                                                    dt.as<PairTile>() + off, coef, sink);
         KFB_CUDA_TRY(cudaGetLastError());
     }
+    timer.stop();
     return KFB_OK;
 }
 

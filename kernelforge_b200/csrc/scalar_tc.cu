@@ -335,10 +335,13 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                 if (cst) cstart[__popc(cmask & lt_mask)] = lane;
                 cmol[lane] = cm;
                 if (lane == 0) cstart[nc] = nvc;
+                // the self pair (same packed row) of a diagonal tile is exactly 1
+                const int self_j = (tl.diag && (row >> 5) == c) ? lane : -1;
 #pragma unroll
                 for (int j = 0; j < 32; ++j) {
                     const float cnj = __shfl_sync(0xffffffffu, cn, j);
-                    const float e = fast_exp2(fmaf(m2c, v[j], rn + cnj));
+                    float e = fast_exp2(fmaf(m2c, v[j], rn + cnj));
+                    if (j == self_j) e = 1.f;
                     scr[j * SCR_LD + lane] = (rvalid && j < nvc) ? e : 0.f;
                 }
                 __syncwarp();
@@ -540,11 +543,14 @@ kfb_status run_tc(const ScalarProblem &p, const PairSink &sink, cudaStream_t s) 
     }
     const int ntiles = (int)tiles.size();
     const int grid = std::min(ntiles, device_sm_count());
+    KernelTimer timer(s);
+    timer.start();
     scalar_tc_kernel<<<grid, NUM_THREADS, SMEM_ALLOC, s>>>(
         ma_hi, ma_lo, mb_hi, mb_lo, p.rep, A.norm.as<float>(), BB.norm.as<float>(),
         A.mol.as<int>(), BB.mol.as<int>(), dtiles.as<PairTile>(), ntiles, (float)(-2.0 * c),
         sink, derr.as<int>());
     KFB_CUDA_TRY(cudaGetLastError());
+    timer.stop();
     int herr = 0;
     KFB_CUDA_TRY(cudaMemcpyAsync(&herr, derr.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
     KFB_CUDA_TRY(cudaStreamSynchronize(s));

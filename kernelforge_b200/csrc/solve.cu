@@ -420,7 +420,7 @@ kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2
         KFB_CUDA_TRY(cudaMemcpyAsync(F.ptr, k_rfp, nt * sizeof(float), cudaMemcpyDeviceToDevice, s));
         KFB_TRY(rfp_potrf(F.ptr, n, l2 + shift, uplo, KFB_F32, &finfo, s));
         if (finfo == 0) break;
-        shift = (shift == 0.0) ? std::max(1e-7 * (double)hmax, 10.0 * l2) : shift * 10.0;
+        shift = (shift == 0.0) ? std::max(1e-6 * (double)hmax, 10.0 * l2) : shift * 10.0;
     }
     inf.factor_info = finfo;
     inf.shift = shift;
@@ -450,19 +450,25 @@ kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2
         return KFB_OK;
     };
 
-    // classic iterative refinement
+    // classic iterative refinement (only when the FP32 factor needed no shift);
+    // a correction that increases the residual is undone and CG takes over
     double rn = ynorm, prev = ynorm;
-    int it = 0, stall = 0;
+    int it = 0;
     residual_kernel<<<gw, 256, 0, s>>>(Kd.as<float>(), alpha, y, n, l2, r.as<double>());
-    for (; it < maxit; ++it) {
+    bool need_cg = shift > 0.0;
+    for (; !need_cg && it < maxit; ++it) {
         double rr = 0.0;
         KFB_TRY(dot(r.as<double>(), r.as<double>(), n, s, rr));
         rn = std::sqrt(rr);
         if (rn <= tol * ynorm) break;
         if (it > 0 && rn > 0.5 * prev) {
-            if (++stall >= 2) break;
-        } else {
-            stall = 0;
+            if (rn > prev) {  // diverging: undo the last correction
+                axpy_kernel<<<gb, 256, 0, s>>>(z.as<double>(), -1.0, n, alpha);
+                residual_kernel<<<gw, 256, 0, s>>>(Kd.as<float>(), alpha, y, n, l2, r.as<double>());
+                rn = prev;
+            }
+            need_cg = true;
+            break;
         }
         prev = rn;
         KFB_TRY(precond(r.as<double>(), rn, z.as<double>()));
@@ -470,9 +476,14 @@ kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2
         residual_kernel<<<gw, 256, 0, s>>>(Kd.as<float>(), alpha, y, n, l2, r.as<double>());
         KFB_CUDA_TRY(cudaGetLastError());
     }
+    if (need_cg && shift > 0.0) {
+        double rr = 0.0;
+        KFB_TRY(dot(r.as<double>(), r.as<double>(), n, s, rr));
+        rn = std::sqrt(rr);
+    }
     inf.iterations = it;
     if (rn > tol * ynorm && it < maxit) {
-        // preconditioned conjugate gradients (FP64), FP32 factor as preconditioner
+            // preconditioned conjugate gradients (FP64), FP32 factor as preconditioner
         inf.used_cg = 1;
         KFB_TRY(precond(r.as<double>(), rn, z.as<double>()));
         KFB_CUDA_TRY(cudaMemcpyAsync(p.ptr, z.ptr, (size_t)n * sizeof(double),

@@ -104,10 +104,11 @@ def _fchl19_one(R: torch.Tensor, zidx: torch.Tensor, nelem: int = 5, nRs2: int =
     dt = R.dtype
     eps = 1e-12
     rep = rep_size(nelem, nRs2, nRs3)
-    Rs2 = torch.arange(1, nRs2 + 1, dtype=dt) * (rcut / nRs2)
-    Rs3 = torch.arange(1, nRs3 + 1, dtype=dt) * (acut / nRs3)
+    dev = R.device
+    Rs2 = torch.arange(1, nRs2 + 1, dtype=dt, device=dev) * (rcut / nRs2)
+    Rs3 = torch.arange(1, nRs3 + 1, dtype=dt, device=dev) * (acut / nRs3)
     diff = R[None, :, :] - R[:, None, :]                 # diff[i, j] = R_j - R_i
-    eye = torch.eye(n, dtype=torch.bool)
+    eye = torch.eye(n, dtype=torch.bool, device=dev)
     r2 = (diff * diff).sum(-1)
     r = torch.sqrt(torch.where(eye, torch.ones_like(r2), r2))
     r = torch.where(eye, torch.zeros_like(r), r)
@@ -149,7 +150,7 @@ def _fchl19_one(R: torch.Tensor, zidx: torch.Tensor, nelem: int = 5, nRs2: int =
     rbar = 0.5 * (rij + rik)
     radial = torch.exp(-eta3 * (rbar[..., None] - Rs3) ** 2) * \
         (decay3[:, :, None] * decay3[:, None, :])[..., None]          # (n, n, n, nRs3)
-    idx = torch.arange(n)
+    idx = torch.arange(n, device=dev)
     valid = (idx[None, :, None] < idx[None, None, :]) & (idx[:, None, None] != idx[None, :, None]) \
         & (idx[:, None, None] != idx[None, None, :])
     valid = valid & (r[:, :, None] <= acut) & (r[:, None, :] <= acut)

@@ -89,16 +89,34 @@ def test_rfp_potrf_reports_info():
 
 
 def test_mixed_solve_reaches_tolerance():
+    """A real FCHL19 kernel matrix (FP32 RFP) at lambda = 1e-8: the FP64 residual
+    of the returned alpha against the FP32-stored matrix is below 1e-10."""
     import torch
 
     from kernelforge_b200 import cuda_global_kernels as cgk
-    n = 300
-    A = spd(n, 5, cond=1e9)
-    y = np.random.default_rng(2).standard_normal(n)
-    K = torch.tensor(o.full_to_rfp(A, uplo_lower=True), dtype=torch.float32, device="cuda")
-    A32 = o.rfp_to_full(K.cpu().numpy().astype(np.float64), n, uplo_lower=True)
+    from kernelforge_b200 import cuda_local_kernels as clk
+    from kernelforge_b200 import synthetic
+    mols = synthetic.make_molecules(300, 9, 21, seed=3)
+    X, Q, N = synthetic.fchl19_batched(mols, dtype=np.float32)
+    K = clk.kernel_gaussian_symm_rfp(torch.tensor(X, device="cuda"), Q, N, 2.0)
+    y = mols.E - mols.E.mean()
+    n = len(y)
     alpha, info = cgk.krr_solve_mixed(K, torch.tensor(y), l2=1e-8, uplo="L", tol=1e-10)
     assert info["converged"], info
-    a = alpha.cpu().numpy()
-    r = y - (A32 + 1e-8 * np.eye(n)) @ a
-    assert np.linalg.norm(r) <= 1.5e-10 * np.linalg.norm(y)
+    A32 = o.rfp_to_full(K.cpu().numpy().astype(np.float64), n, uplo_lower=True)
+    r = y - (A32 + 1e-8 * np.eye(n)) @ alpha.cpu().numpy()
+    assert np.linalg.norm(r) <= 2e-10 * np.linalg.norm(y)
+
+
+def test_mixed_solve_matches_fp64_solution_when_well_conditioned():
+    import torch
+
+    from kernelforge_b200 import cuda_global_kernels as cgk
+    n = 200
+    A = spd(n, 9, cond=1e4)
+    y = np.random.default_rng(4).standard_normal(n)
+    K = torch.tensor(o.full_to_rfp(A, uplo_lower=True), dtype=torch.float32, device="cuda")
+    A32 = o.rfp_to_full(K.cpu().numpy().astype(np.float64), n, uplo_lower=True)
+    alpha, info = cgk.krr_solve_mixed(K, torch.tensor(y), l2=0.0, uplo="L", tol=1e-12)
+    assert info["converged"] and not info["used_cg"], info
+    np.testing.assert_allclose(alpha.cpu().numpy(), np.linalg.solve(A32, y), rtol=1e-9, atol=1e-11)
