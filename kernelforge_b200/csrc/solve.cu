@@ -309,12 +309,16 @@ __global__ void float_to_double_kernel(const float *a, double s, int n, double *
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] = s * (double)a[i];
 }
-__global__ void max_diag_kernel(const float *K, int n, float *out) {
-    float m = 0.f;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        m = fmaxf(m, fabsf(K[(size_t)i * n + i]));
-    for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<int *>(out), __float_as_int(m));
+// max_i sum_j |K_ij| (a Gershgorin bound on ||K||_2), one warp per row
+__global__ void max_rowsum_kernel(const float *K, int n, float *out) {
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const float *kr = K + (size_t)row * n;
+    float acc = 0.f;
+    for (int j = lane; j < n; j += 32) acc += fabsf(kr[j]);
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) atomicMax(reinterpret_cast<int *>(out), __float_as_int(acc));
 }
 
 inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
@@ -408,19 +412,23 @@ kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2
     Dot dot;
     KFB_TRY(dot.init(s));
 
-    // FP32 factor of K + (l2 + shift) I; the shift grows until potrf succeeds
+    // FP32 factor of K + (l2 + shift) I.  FP32 Cholesky is stable once the
+    // diagonal shift is of the order of the unit roundoff times ||K||_2, so the
+    // first attempt takes shift = max(0, 2 u32 g - l2) with g the Gershgorin
+    // bound max_i sum_j |K_ij|; the shift grows 4x per failed attempt.
     KFB_TRY(zero(dmax.ptr, sizeof(float), s));
-    max_diag_kernel<<<std::min(nblk(n, 256), 148u), 256, 0, s>>>(Kd.as<float>(), n, dmax.as<float>());
-    float hmax = 0.f;
-    KFB_CUDA_TRY(cudaMemcpyAsync(&hmax, dmax.ptr, sizeof(float), cudaMemcpyDeviceToHost, s));
+    max_rowsum_kernel<<<nblk((long long)n * 32, 256), 256, 0, s>>>(Kd.as<float>(), n, dmax.as<float>());
+    float gersh = 0.f;
+    KFB_CUDA_TRY(cudaMemcpyAsync(&gersh, dmax.ptr, sizeof(float), cudaMemcpyDeviceToHost, s));
     KFB_CUDA_TRY(cudaStreamSynchronize(s));
-    double shift = 0.0;
+    const double u32 = 5.960464477539063e-08;
+    double shift = std::max(0.0, 2.0 * u32 * (double)gersh - l2);
     int finfo = 0;
     for (int attempt = 0; attempt < 12; ++attempt) {
         KFB_CUDA_TRY(cudaMemcpyAsync(F.ptr, k_rfp, nt * sizeof(float), cudaMemcpyDeviceToDevice, s));
         KFB_TRY(rfp_potrf(F.ptr, n, l2 + shift, uplo, KFB_F32, &finfo, s));
         if (finfo == 0) break;
-        shift = (shift == 0.0) ? std::max(1e-6 * (double)hmax, 10.0 * l2) : shift * 10.0;
+        shift = (shift == 0.0) ? std::max(u32 * (double)gersh, 10.0 * l2) : shift * 4.0;
     }
     inf.factor_info = finfo;
     inf.shift = shift;
@@ -496,7 +504,15 @@ kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2
             double pq = 0.0;
             KFB_TRY(dot(p.as<double>(), q.as<double>(), n, s, pq));
             pq = -pq;
-            if (!(pq > 0.0)) break;
+            if (!(pq > 0.0)) {  // K + l2 I is not positive definite at this precision
+                inf.iterations = it;
+                inf.rel_residual = rn / ynorm;
+                if (info) *info = inf;
+                return set_error(KFB_ERR_NOT_PD,
+                                 "K + l2 I is indefinite at FP32 storage precision (p^T A p = "
+                                 "%.3e after %d CG iterations); use a larger l2",
+                                 -pq, it);
+            }
             const double a = rz / pq;
             axpy_kernel<<<gb, 256, 0, s>>>(p.as<double>(), a, n, alpha);
             axpy_kernel<<<gb, 256, 0, s>>>(q.as<double>(), a, n, r.as<double>());  // r -= a A p

@@ -79,6 +79,8 @@ def krr_solve_mixed(K_rfp, y, l2=0.0, uplo="L", tol=1e-10, maxit=500):
                                         ctypes.byref(info), stream_handle())
     res = {"iterations": info.iterations, "factor_info": info.factor_info, "shift": info.shift,
            "rel_residual": info.rel_residual, "used_cg": bool(info.used_cg)}
+    if st == _lib.KFB_ERR_NOT_PD:
+        raise RuntimeError(_lib.lib().kfb_last_error().decode())
     if st != _lib.KFB_OK and st != _lib.KFB_ERR_NO_CONVERGENCE:
         _lib.check(st)
     res["converged"] = st == _lib.KFB_OK
