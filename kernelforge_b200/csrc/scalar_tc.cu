@@ -42,17 +42,19 @@ constexpr int NSTAGE = 3;
 constexpr int TILE_A_BYTES = BM * BK * 2;
 constexpr int TILE_B_BYTES = BN * BK * 2;
 constexpr int STAGE_BYTES = 2 * TILE_A_BYTES + 2 * TILE_B_BYTES;
-constexpr int NUM_THREADS = 256;
 constexpr int EPI_WARP0 = 4;
+constexpr int NUM_EPI_WARPS = 8;              // two per TMEM lane quadrant
+constexpr int NUM_THREADS = 32 * (EPI_WARP0 + NUM_EPI_WARPS);
+constexpr int CHUNKS_PER_WARP = BN / 32 / (NUM_EPI_WARPS / 4);
 constexpr int TMEM_COLS = 2 * BN;
 constexpr int SCR_LD = 33;
-constexpr int SCR_FLOATS = 32 * SCR_LD;       // per epilogue warp
+constexpr int SCR_FLOATS = 16 * SCR_LD;       // per epilogue warp: 16 column runs x 32 rows
 constexpr int RUN_INTS = 4 * 33;              // rstart, cstart, rmol, cmol per warp
 
 constexpr int OFF_STAGES = 0;
 constexpr int OFF_SCR = OFF_STAGES + NSTAGE * STAGE_BYTES;
-constexpr int OFF_RUNS = OFF_SCR + 4 * SCR_FLOATS * 4;
-constexpr int OFF_BARS = (OFF_RUNS + 4 * RUN_INTS * 4 + 7) / 8 * 8;
+constexpr int OFF_RUNS = OFF_SCR + NUM_EPI_WARPS * SCR_FLOATS * 4;
+constexpr int OFF_BARS = (OFF_RUNS + NUM_EPI_WARPS * RUN_INTS * 4 + 7) / 8 * 8;
 constexpr int NBARS = 2 * NSTAGE + 4 + 1;     // full, empty, tmem_full x2, tmem_empty x2, mma_done
 constexpr int OFF_TMEM = OFF_BARS + NBARS * 8;
 constexpr int SMEM_BYTES = OFF_TMEM + 16;
@@ -193,7 +195,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
         }
         for (int a = 0; a < 2; ++a) {
             mbar_init(tfull_bar(a), 1);
-            mbar_init(tempty_bar(a), 4);
+            mbar_init(tempty_bar(a), NUM_EPI_WARPS);
         }
         mbar_init(done_bar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -290,10 +292,14 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
         }
     } else if (warp >= EPI_WARP0) {
         // ------------------------------------------------ epilogue
-        const int q = warp - EPI_WARP0;  // TMEM lane quadrant (warp % 4)
-        float *scr = reinterpret_cast<float *>(smem + OFF_SCR) + q * SCR_FLOATS;
-        int *runs = reinterpret_cast<int *>(smem + OFF_RUNS) + q * RUN_INTS;
-        int *rstart = runs, *cstart = runs + 33, *rmol = runs + 66, *cmol = runs + 99;
+        // warp e handles TMEM lane quadrant q = warp % 4 (rows 32q..32q+31) and
+        // column chunks [h * CHUNKS_PER_WARP, (h + 1) * CHUNKS_PER_WARP)
+        const int e_id = warp - EPI_WARP0;
+        const int q = warp & 3;
+        const int h = e_id >> 2;
+        float *scr = reinterpret_cast<float *>(smem + OFF_SCR) + e_id * SCR_FLOATS;
+        int *runs = reinterpret_cast<int *>(smem + OFF_RUNS) + e_id * RUN_INTS;
+        int *rstart = runs, *cstart = runs + 33, *rmolr = runs + 66, *cmolr = runs + 99;
         const unsigned lt_mask = (1u << lane) - 1u;
         int acc = 0;
         uint32_t aph = 0;
@@ -301,6 +307,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             const PairTile tl = tiles[t];
             const int nra = min(BM, tl.a_end - tl.a0);
             const int nrb = min(BN, tl.b_end - tl.b0);
+            // molecule runs of this warp's 32 rows
             const int row = q * 32 + lane;
             const bool rvalid = row < nra;
             const int rm = rvalid ? molA[tl.a0 + row] : -1;
@@ -310,8 +317,10 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             const unsigned rmask = __ballot_sync(0xffffffffu, rst);
             const int nvr = __popc(__ballot_sync(0xffffffffu, rvalid));
             const int nr = __popc(rmask);
-            if (rst) rstart[__popc(rmask & lt_mask)] = lane;
-            rmol[lane] = rm;
+            if (rst) {
+                rstart[__popc(rmask & lt_mask)] = lane;
+                rmolr[__popc(rmask & lt_mask)] = rm;
+            }
             if (lane == 0) rstart[nr] = nvr;
 
             const bool got = mbar_wait(tfull_bar(acc), aph, err);
@@ -319,40 +328,60 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             tc_fence_after();
             const uint32_t tbase = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN);
 #pragma unroll 1
-            for (int c = 0; c < BN / 32; ++c) {
+            for (int cc = 0; cc < CHUNKS_PER_WARP; ++cc) {
+                const int c = h * CHUNKS_PER_WARP + cc;
                 const int col = c * 32 + lane;
                 const bool cvalid = col < nrb;
                 const int cm = cvalid ? molB[tl.b0 + col] : -1;
                 const float cn = cvalid ? nB[tl.b0 + col] : 0.f;
                 const int cm_prev = __shfl_up_sync(0xffffffffu, cm, 1);
-                const bool cst = cvalid && (lane == 0 || cm != cm_prev);
+                const int cm_next = __shfl_down_sync(0xffffffffu, cm, 1);
+                // column runs never cross the middle of the chunk, so each half
+                // of 16 columns has at most 16 runs
+                const bool cst = cvalid && (lane == 0 || lane == 16 || cm != cm_prev);
+                const bool cend = cvalid && (lane == 15 || lane == 31 || cm != cm_next);
                 const unsigned cmask = __ballot_sync(0xffffffffu, cst);
-                const int nvc = __popc(__ballot_sync(0xffffffffu, cvalid));
-                const int nc = __popc(cmask);
+                const unsigned emask = __ballot_sync(0xffffffffu, cend);
                 float v[32];
                 tmem_ld32(tbase + (uint32_t)(c * 32), v);
-                __syncwarp();
-                if (cst) cstart[__popc(cmask & lt_mask)] = lane;
-                cmol[lane] = cm;
-                if (lane == 0) cstart[nc] = nvc;
                 // the self pair (same packed row) of a diagonal tile is exactly 1
                 const int self_j = (tl.diag && (row >> 5) == c) ? lane : -1;
 #pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    const float cnj = __shfl_sync(0xffffffffu, cn, j);
-                    float e = fast_exp2(fmaf(m2c, v[j], rn + cnj));
-                    if (j == self_j) e = 1.f;
-                    scr[j * SCR_LD + lane] = (rvalid && j < nvc) ? e : 0.f;
-                }
-                __syncwarp();
-                for (int p = lane; p < nr * nc; p += 32) {
-                    const int ri = p / nc, ci = p - ri * nc;
-                    const int r0 = rstart[ri], r1 = rstart[ri + 1];
-                    const int c0 = cstart[ci], c1 = cstart[ci + 1];
-                    float s = 0.f;
-                    for (int j = c0; j < c1; ++j)
-                        for (int r = r0; r < r1; ++r) s += scr[j * SCR_LD + r];
-                    emit_pair(sink, rmol[r0], cmol[c0], (double)s, tl.diag);
+                for (int hh = 0; hh < 2; ++hh) {
+                    const unsigned hmask = hh ? 0xFFFF0000u : 0x0000FFFFu;
+                    const unsigned cm_h = cmask & hmask;
+                    const int nc = __popc(cm_h);
+                    __syncwarp();
+                    if (cst && (hmask & (1u << lane))) cmolr[__popc(cm_h & lt_mask)] = cm;
+                    // per row: sums over each column run, kept in registers until
+                    // the run ends (run boundaries are the same for every lane)
+                    float run_sum = 0.f;
+                    int k = 0;
+#pragma unroll
+                    for (int jj = 0; jj < 16; ++jj) {
+                        const int j = hh * 16 + jj;
+                        const float cnj = __shfl_sync(0xffffffffu, cn, j);
+                        float e = fast_exp2(fmaf(m2c, v[j], rn + cnj));
+                        if (j == self_j) e = 1.f;
+                        run_sum += e;
+                        if (emask & (1u << j)) {
+                            scr[k * SCR_LD + lane] = run_sum;
+                            ++k;
+                            run_sum = 0.f;
+                        }
+                    }
+                    __syncwarp();
+                    // cross-row sums: one (row run, column run) rectangle per lane
+                    const float inv_nc = 1.f / (float)max(nc, 1);
+                    for (int p = lane; p < nr * nc; p += 32) {
+                        const int ri = __float2int_rz(((float)p + 0.5f) * inv_nc);
+                        const int ci = p - ri * nc;
+                        const int r0 = rstart[ri], r1 = rstart[ri + 1];
+                        const float *col_sums = scr + ci * SCR_LD;
+                        float sum = 0.f;
+                        for (int r = r0; r < r1; ++r) sum += col_sums[r];
+                        emit_pair(sink, rmolr[ri], cmolr[ci], (double)sum, tl.diag);
+                    }
                 }
                 __syncwarp();
             }
