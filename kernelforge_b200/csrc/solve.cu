@@ -321,6 +321,30 @@ __global__ void max_rowsum_kernel(const float *K, int n, float *out) {
     if (lane == 0) atomicMax(reinterpret_cast<int *>(out), __float_as_int(acc));
 }
 
+__global__ void fill_kernel(double *x, double v, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] = v;
+}
+// a start vector with no special alignment to the constant vector
+__global__ void fill_alt_kernel(double *x, double v, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] = (i % 3 == 0 ? -2.0 : 1.0) * v * (1.0 + 1e-3 * (i % 7));
+}
+__global__ void scale_copy_kernel(const double *a, double s, int n, double *out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = s * a[i];
+}
+// F = K - mu v v^T over the stored RFP triangle (FP64 arithmetic, FP32 result)
+__global__ void rfp_deflate_kernel(const float *K, int n, int layout, const double *v, double mu,
+                                   float *F) {
+    const long long i = blockIdx.y * (long long)blockDim.y + threadIdx.y;
+    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n && j < n && i <= j) {
+        const long long idx = sym_index((kfb_layout)layout, n, i, j);
+        F[idx] = (float)((double)K[idx] - mu * v[i] * v[j]);
+    }
+}
+
 inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 
 struct Dot {
@@ -412,32 +436,6 @@ kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2
     Dot dot;
     KFB_TRY(dot.init(s));
 
-    // FP32 factor of K + (l2 + shift) I.  FP32 Cholesky is stable once the
-    // diagonal shift is of the order of the unit roundoff times ||K||_2, so the
-    // first attempt takes shift = max(0, 2 u32 g - l2) with g the Gershgorin
-    // bound max_i sum_j |K_ij|; the shift grows 4x per failed attempt.
-    KFB_TRY(zero(dmax.ptr, sizeof(float), s));
-    max_rowsum_kernel<<<nblk((long long)n * 32, 256), 256, 0, s>>>(Kd.as<float>(), n, dmax.as<float>());
-    float gersh = 0.f;
-    KFB_CUDA_TRY(cudaMemcpyAsync(&gersh, dmax.ptr, sizeof(float), cudaMemcpyDeviceToHost, s));
-    KFB_CUDA_TRY(cudaStreamSynchronize(s));
-    const double u32 = 5.960464477539063e-08;
-    double shift = std::max(0.0, 2.0 * u32 * (double)gersh - l2);
-    int finfo = 0;
-    for (int attempt = 0; attempt < 12; ++attempt) {
-        KFB_CUDA_TRY(cudaMemcpyAsync(F.ptr, k_rfp, nt * sizeof(float), cudaMemcpyDeviceToDevice, s));
-        KFB_TRY(rfp_potrf(F.ptr, n, l2 + shift, uplo, KFB_F32, &finfo, s));
-        if (finfo == 0) break;
-        shift = (shift == 0.0) ? std::max(u32 * (double)gersh, 10.0 * l2) : shift * 4.0;
-    }
-    inf.factor_info = finfo;
-    inf.shift = shift;
-    if (finfo != 0) {
-        if (info) *info = inf;
-        return set_error(KFB_ERR_NOT_PD, "FP32 RFP Cholesky failed even with shift %g (info=%d)",
-                         shift, finfo);
-    }
-
     double ynorm2 = 0.0;
     KFB_TRY(dot(y, y, n, s, ynorm2));
     const double ynorm = std::sqrt(ynorm2);
@@ -447,13 +445,98 @@ kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2
         return KFB_OK;
     }
     const unsigned gb = nblk(n, 256), gw = nblk((long long)n * 32, 256);
-    // M^{-1} v via the FP32 factor, with v scaled to unit norm first
-    auto precond = [&](const double *v, double vnorm, double *out) -> kfb_status {
+
+    // Deflation of the dominant eigenpair.  A Gaussian kernel matrix has
+    // non-negative entries and one eigenvalue far above the others (the mode
+    // shared by all molecules, about n * mean(K)); that eigenvalue alone sets
+    // the diagonal shift FP32 Cholesky needs (unit roundoff times ||K||_2).
+    // Power iteration gives (mu, v); the FP32 factor is of
+    //   F = K - mu v v^T + (l2 + shift) I
+    // and the preconditioner is M^{-1} = (F + mu v v^T)^{-1}, applied with the
+    // Sherman-Morrison formula.  FP64 residuals always use K itself.
+    DevBuf dv, dw, dtmp;
+    KFB_TRY(dv.alloc((size_t)n * sizeof(double), s));
+    KFB_TRY(dw.alloc((size_t)n * sizeof(double), s));
+    KFB_TRY(dtmp.alloc((size_t)n * sizeof(double), s));
+    double mu = 0.0;
+    {
+        fill_kernel<<<gb, 256, 0, s>>>(dv.as<double>(), 1.0 / std::sqrt((double)n), n);
+        for (int k = 0; k < 30; ++k) {
+            residual_kernel<<<gw, 256, 0, s>>>(Kd.as<float>(), dv.as<double>(), nullptr, n, 0.0,
+                                               dtmp.as<double>());  // -K v
+            double vkv = 0.0, ww = 0.0;
+            KFB_TRY(dot(dv.as<double>(), dtmp.as<double>(), n, s, vkv));
+            KFB_TRY(dot(dtmp.as<double>(), dtmp.as<double>(), n, s, ww));
+            const double mu_new = -vkv;
+            scale_copy_kernel<<<gb, 256, 0, s>>>(dtmp.as<double>(), -1.0 / std::sqrt(ww), n,
+                                                 dv.as<double>());
+            const bool done = k > 2 && std::fabs(mu_new - mu) <= 1e-9 * std::fabs(mu_new);
+            mu = mu_new;
+            if (done) break;
+        }
+    }
+    // a few power steps on the deflated operator estimate ||K - mu v v^T||_2
+    double lam2 = 0.0;
+    {
+        fill_alt_kernel<<<gb, 256, 0, s>>>(dw.as<double>(), 1.0 / std::sqrt((double)n), n);
+        for (int k = 0; k < 8; ++k) {
+            double vw = 0.0;
+            KFB_TRY(dot(dv.as<double>(), dw.as<double>(), n, s, vw));
+            axpy_kernel<<<gb, 256, 0, s>>>(dv.as<double>(), -vw, n, dw.as<double>());
+            residual_kernel<<<gw, 256, 0, s>>>(Kd.as<float>(), dw.as<double>(), nullptr, n, 0.0,
+                                               dtmp.as<double>());  // -K w
+            double wkw = 0.0, tt = 0.0, ww = 0.0;
+            KFB_TRY(dot(dw.as<double>(), dtmp.as<double>(), n, s, wkw));
+            KFB_TRY(dot(dw.as<double>(), dw.as<double>(), n, s, ww));
+            KFB_TRY(dot(dtmp.as<double>(), dtmp.as<double>(), n, s, tt));
+            lam2 = std::max(lam2, -wkw / std::max(ww, 1e-300));
+            scale_copy_kernel<<<gb, 256, 0, s>>>(dtmp.as<double>(), -1.0 / std::sqrt(tt), n,
+                                                 dw.as<double>());
+        }
+        lam2 *= 1.5;  // Rayleigh quotients approach ||.||_2 from below
+    }
+
+    // FP32 factor of F; the shift starts at max(0, 2 u32 lam2 - l2) and grows 4x
+    // per failed attempt
+    const double u32 = 5.960464477539063e-08;
+    double shift = std::max(0.0, 2.0 * u32 * lam2 - l2);
+    int finfo = 0;
+    const dim3 blk2(32, 8), grd2(nblk(n, 32), nblk(n, 8));
+    for (int attempt = 0; attempt < 12; ++attempt) {
+        rfp_deflate_kernel<<<grd2, blk2, 0, s>>>(k_rfp, n, uplo, dv.as<double>(), mu,
+                                                 F.as<float>());
+        KFB_CUDA_TRY(cudaGetLastError());
+        KFB_TRY(rfp_potrf(F.ptr, n, l2 + shift, uplo, KFB_F32, &finfo, s));
+        if (finfo == 0) break;
+        shift = (shift == 0.0) ? std::max(u32 * lam2, 10.0 * l2) : shift * 4.0;
+    }
+    inf.factor_info = finfo;
+    inf.shift = shift;
+    if (finfo != 0) {
+        if (info) *info = inf;
+        return set_error(KFB_ERR_NOT_PD, "FP32 RFP Cholesky failed even with shift %g (info=%d)",
+                         shift, finfo);
+    }
+    // F^{-1} v via the FP32 factor, with v scaled to unit norm first
+    auto solve_f = [&](const double *v, double vnorm, double *out) -> kfb_status {
         const double sc = vnorm > 0.0 ? 1.0 / vnorm : 1.0;
         scale_to_float_kernel<<<gb, 256, 0, s>>>(v, sc, n, f32v.as<float>());
         KFB_TRY(rfp_potrs(F.ptr, f32v.ptr, n, 1, uplo, KFB_F32, s));
         float_to_double_kernel<<<gb, 256, 0, s>>>(f32v.as<float>(), vnorm > 0.0 ? vnorm : 1.0, n,
                                                   out);
+        KFB_CUDA_TRY(cudaGetLastError());
+        return KFB_OK;
+    };
+    KFB_TRY(solve_f(dv.as<double>(), 1.0, dw.as<double>()));  // w = F^{-1} v
+    double vfv = 0.0;
+    KFB_TRY(dot(dv.as<double>(), dw.as<double>(), n, s, vfv));
+    const double sm_coef = mu / (1.0 + mu * vfv);
+    // M^{-1} r = F^{-1} r - sm_coef (w . r) w
+    auto precond = [&](const double *v, double vnorm, double *out) -> kfb_status {
+        KFB_TRY(solve_f(v, vnorm, out));
+        double wr = 0.0;
+        KFB_TRY(dot(dw.as<double>(), v, n, s, wr));
+        axpy_kernel<<<gb, 256, 0, s>>>(dw.as<double>(), -sm_coef * wr, n, out);
         KFB_CUDA_TRY(cudaGetLastError());
         return KFB_OK;
     };
