@@ -272,9 +272,11 @@ def run_ours(args, rank, world, local):
     solve_info = {}
 
     def step():
+        torch.cuda.nvtx.range_push("kfb_fit_step")
         K = clk.kernel_gaussian_symm_rfp(Xd, Qh, Nh, SIGMA)
         alpha, info = cgk.krr_solve_mixed(K, yd, l2=L2, uplo="L", tol=TOL)
         solve_info.update(info)
+        torch.cuda.nvtx.range_pop()
         return alpha
 
     # e2e: host buffers in, alpha back to the host

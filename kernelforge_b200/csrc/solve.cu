@@ -450,10 +450,14 @@ kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2
     // non-negative entries and one eigenvalue far above the others (the mode
     // shared by all molecules, about n * mean(K)); that eigenvalue alone sets
     // the diagonal shift FP32 Cholesky needs (unit roundoff times ||K||_2).
-    // Power iteration gives (mu, v); the FP32 factor is of
-    //   F = K - mu v v^T + (l2 + shift) I
-    // and the preconditioner is M^{-1} = (F + mu v v^T)^{-1}, applied with the
-    // Sherman-Morrison formula.  FP64 residuals always use K itself.
+    // Power iteration gives (mu, v) and an estimate sigma of the next
+    // eigenvalue; the FP32 factor is of
+    //   F = K - (mu - sigma) v v^T + (l2 + shift) I,
+    // whose eigenvalue along v is sigma (not ~0, which would make F^{-1} v huge
+    // and the correction below cancel), and the preconditioner
+    //   M^{-1} = (F + (mu - sigma) v v^T)^{-1}
+    // is applied with the Sherman-Morrison formula.  FP64 residuals always use
+    // K itself.
     DevBuf dv, dw, dtmp;
     KFB_TRY(dv.alloc((size_t)n * sizeof(double), s));
     KFB_TRY(dw.alloc((size_t)n * sizeof(double), s));
@@ -499,11 +503,12 @@ kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2
     // FP32 factor of F; the shift starts at max(0, 2 u32 lam2 - l2) and grows 4x
     // per failed attempt
     const double u32 = 5.960464477539063e-08;
+    const double defl = std::max(0.0, mu - lam2);
     double shift = std::max(0.0, 2.0 * u32 * lam2 - l2);
     int finfo = 0;
     const dim3 blk2(32, 8), grd2(nblk(n, 32), nblk(n, 8));
     for (int attempt = 0; attempt < 12; ++attempt) {
-        rfp_deflate_kernel<<<grd2, blk2, 0, s>>>(k_rfp, n, uplo, dv.as<double>(), mu,
+        rfp_deflate_kernel<<<grd2, blk2, 0, s>>>(k_rfp, n, uplo, dv.as<double>(), defl,
                                                  F.as<float>());
         KFB_CUDA_TRY(cudaGetLastError());
         KFB_TRY(rfp_potrf(F.ptr, n, l2 + shift, uplo, KFB_F32, &finfo, s));
@@ -530,7 +535,7 @@ kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2
     KFB_TRY(solve_f(dv.as<double>(), 1.0, dw.as<double>()));  // w = F^{-1} v
     double vfv = 0.0;
     KFB_TRY(dot(dv.as<double>(), dw.as<double>(), n, s, vfv));
-    const double sm_coef = mu / (1.0 + mu * vfv);
+    const double sm_coef = defl / (1.0 + defl * vfv);
     // M^{-1} r = F^{-1} r - sm_coef (w . r) w
     auto precond = [&](const double *v, double vnorm, double *out) -> kfb_status {
         KFB_TRY(solve_f(v, vnorm, out));
