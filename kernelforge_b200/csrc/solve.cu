@@ -235,74 +235,6 @@ kfb_status rfp_potrs_t(const T *a, T *B, int n, int nrhs, bool lower, cudaStream
     return KFB_OK;
 }
 
-// Replace the two triangles of an FP32 RFP Cholesky factor by their inverses
-// (in place), so that applying the factor's inverse becomes matrix-vector
-// products (bandwidth-bound) instead of triangular solves (latency-bound).
-kfb_status rfp_invert_triangles_f32(float *a, int n, bool lower, cudaStream_t s) {
-    if (n == 0) return KFB_OK;
-    Handles *h = nullptr;
-    KFB_TRY(get_handles(s, h));
-    const RfpBlocks b = rfp_blocks(n, lower);
-    size_t d1 = 0, h1 = 0, d2 = 0, h2 = 0;
-    KFB_SOLVER_TRY(cusolverDnXtrtri_bufferSize(h->solver, CUBLAS_FILL_MODE_LOWER,
-                                               CUBLAS_DIAG_NON_UNIT, b.n1, CUDA_R_32F, a + b.t1,
-                                               b.ld, &d1, &h1));
-    if (b.n2 > 0)
-        KFB_SOLVER_TRY(cusolverDnXtrtri_bufferSize(h->solver, CUBLAS_FILL_MODE_UPPER,
-                                                   CUBLAS_DIAG_NON_UNIT, b.n2, CUDA_R_32F,
-                                                   a + b.t2, b.ld, &d2, &h2));
-    DevBuf dws, dinfo;
-    KFB_TRY(dws.alloc(std::max<size_t>(std::max(d1, d2), 16), s));
-    std::vector<char> hws(std::max<size_t>(std::max(h1, h2), 16));
-    KFB_TRY(dinfo.alloc(2 * sizeof(int), s));
-    KFB_TRY(zero(dinfo.ptr, 2 * sizeof(int), s));
-    KFB_SOLVER_TRY(cusolverDnXtrtri(h->solver, CUBLAS_FILL_MODE_LOWER, CUBLAS_DIAG_NON_UNIT, b.n1,
-                                    CUDA_R_32F, a + b.t1, b.ld, dws.ptr, dws.bytes, hws.data(),
-                                    hws.size(), dinfo.as<int>()));
-    if (b.n2 > 0)
-        KFB_SOLVER_TRY(cusolverDnXtrtri(h->solver, CUBLAS_FILL_MODE_UPPER, CUBLAS_DIAG_NON_UNIT,
-                                        b.n2, CUDA_R_32F, a + b.t2, b.ld, dws.ptr, dws.bytes,
-                                        hws.data(), hws.size(), dinfo.as<int>() + 1));
-    int hi[2] = {0, 0};
-    KFB_CUDA_TRY(cudaMemcpyAsync(hi, dinfo.ptr, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
-    KFB_CUDA_TRY(cudaStreamSynchronize(s));
-    if (hi[0] != 0 || hi[1] != 0)
-        return set_error(KFB_ERR_NOT_PD, "trtri of the FP32 factor failed (%d, %d)", hi[0], hi[1]);
-    return KFB_OK;
-}
-
-// x <- (factor)^{-1} x for an FP32 RFP factor whose triangles were inverted by
-// rfp_invert_triangles_f32 (one right-hand side, in place).
-kfb_status rfp_apply_inverse_f32(const float *a, float *x, int n, bool lower, cudaStream_t s) {
-    if (n == 0) return KFB_OK;
-    Handles *h = nullptr;
-    KFB_TRY(get_handles(s, h));
-    const RfpBlocks b = rfp_blocks(n, lower);
-    const float one = 1.f, mone = -1.f;
-    float *x1 = x, *x2 = x + b.n1;
-    const cublasFillMode_t LO = CUBLAS_FILL_MODE_LOWER, UP = CUBLAS_FILL_MODE_UPPER;
-    const cublasDiagType_t ND = CUBLAS_DIAG_NON_UNIT;
-    KFB_BLAS_TRY(cublasStrmv(h->blas, LO, CUBLAS_OP_N, ND, b.n1, a + b.t1, b.ld, x1, 1));
-    if (b.n2 > 0) {
-        if (lower)
-            KFB_BLAS_TRY(cublasSgemv(h->blas, CUBLAS_OP_N, b.n2, b.n1, &mone, a + b.s, b.ld, x1, 1,
-                                     &one, x2, 1));
-        else
-            KFB_BLAS_TRY(cublasSgemv(h->blas, CUBLAS_OP_T, b.n1, b.n2, &mone, a + b.s, b.ld, x1, 1,
-                                     &one, x2, 1));
-        KFB_BLAS_TRY(cublasStrmv(h->blas, UP, CUBLAS_OP_T, ND, b.n2, a + b.t2, b.ld, x2, 1));
-        KFB_BLAS_TRY(cublasStrmv(h->blas, UP, CUBLAS_OP_N, ND, b.n2, a + b.t2, b.ld, x2, 1));
-        if (lower)
-            KFB_BLAS_TRY(cublasSgemv(h->blas, CUBLAS_OP_T, b.n2, b.n1, &mone, a + b.s, b.ld, x2, 1,
-                                     &one, x1, 1));
-        else
-            KFB_BLAS_TRY(cublasSgemv(h->blas, CUBLAS_OP_N, b.n1, b.n2, &mone, a + b.s, b.ld, x2, 1,
-                                     &one, x1, 1));
-    }
-    KFB_BLAS_TRY(cublasStrmv(h->blas, LO, CUBLAS_OP_T, ND, b.n1, a + b.t1, b.ld, x1, 1));
-    return KFB_OK;
-}
-
 // ------------------------------------------------------------ small kernels
 template <class T>
 __global__ void add_diag_kernel(T *arf, int n, T l2, int layout) {
@@ -590,12 +522,11 @@ kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2
         return set_error(KFB_ERR_NOT_PD, "FP32 RFP Cholesky failed even with shift %g (info=%d)",
                          shift, finfo);
     }
-    KFB_TRY(rfp_invert_triangles_f32(F.as<float>(), n, uplo == KFB_RFP_L, s));
     // F^{-1} v via the FP32 factor, with v scaled to unit norm first
     auto solve_f = [&](const double *v, double vnorm, double *out) -> kfb_status {
         const double sc = vnorm > 0.0 ? 1.0 / vnorm : 1.0;
         scale_to_float_kernel<<<gb, 256, 0, s>>>(v, sc, n, f32v.as<float>());
-        KFB_TRY(rfp_apply_inverse_f32(F.as<float>(), f32v.as<float>(), n, uplo == KFB_RFP_L, s));
+        KFB_TRY(rfp_potrs(F.ptr, f32v.ptr, n, 1, uplo, KFB_F32, s));
         float_to_double_kernel<<<gb, 256, 0, s>>>(f32v.as<float>(), vnorm > 0.0 ? vnorm : 1.0, n,
                                                   out);
         KFB_CUDA_TRY(cudaGetLastError());
