@@ -219,6 +219,32 @@ kfb_status kfb_krr_solve_mixed(const float *k_rfp, const double *y, int n, doubl
                                kfb_layout uplo, double tol, int maxit, double *alpha,
                                kfb_solve_info *info, void *stream);
 
+/* ---------------------------------------------------------------------- */
+/* Allocation-free entry point                                             */
+/* ---------------------------------------------------------------------- */
+
+/* Size of the fixed device scratch array behind kfb_kernel_gaussian_symm_noalloc
+ * (held by every GPU that loads the library, until the process exits). */
+#define KFB_NOALLOC_SCRATCH_BYTES (64u << 20)
+
+/* The symmetric scalar kernel of kfb_kernel_gaussian_symm with FP64 CUDA-core
+ * arithmetic and a double output (layout KFB_DENSE / KFB_RFP_U / KFB_RFP_L),
+ * allocating no device memory: for callers that cannot allocate during a call
+ * (a host framework that has reserved the device-memory budget up front, or a
+ * loop that must not let cudaMalloc / cudaFree synchronise the device).  Its
+ * scratch (packed same-label atoms, norms, molecule indices, tile list) lives in
+ * one file-scope __device__ array of KFB_NOALLOC_SCRATCH_BYTES; a problem whose
+ * scratch exceeds it is rejected with KFB_ERR_INVALID_ARG before any device
+ * work (about 11,000 active atoms at rep = 720).  The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress) -- make it before
+ * any stream capture.  Calls share the array: calls that overlap on the GPU
+ * (two streams or two host threads) race.
+ * No counterpart in the reference: it is an addition of this library. */
+kfb_status kfb_kernel_gaussian_symm_noalloc(const void *x, const int32_t *q, const int32_t *n,
+                                            int nm, int ma, int rep, double sigma,
+                                            kfb_dtype x_dt, kfb_layout layout, void *out,
+                                            void *stream);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

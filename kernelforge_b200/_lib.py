@@ -25,7 +25,7 @@ EXPORTS = (
     "kfb_kernel_gaussian_hessian", "kfb_kernel_gaussian_hessian_symm",
     "kfb_kernel_gaussian_full", "kfb_kernel_gaussian_full_symm", "kfb_full_to_rfp",
     "kfb_rfp_to_full", "kfb_rfp_add_diag", "kfb_rfp_potrf", "kfb_rfp_potrs",
-    "kfb_cho_solve_rfp", "kfb_krr_solve_mixed",
+    "kfb_cho_solve_rfp", "kfb_krr_solve_mixed", "kfb_kernel_gaussian_symm_noalloc",
 )
 
 
@@ -69,6 +69,7 @@ _SIGS = {
     "kfb_rfp_potrs": (I, [P, P, I, I, I, I, P]),
     "kfb_cho_solve_rfp": (I, [P, P, I, D, I, P, ctypes.POINTER(I), P]),
     "kfb_krr_solve_mixed": (I, [P, P, I, D, I, D, I, P, ctypes.POINTER(SolveInfo), P]),
+    "kfb_kernel_gaussian_symm_noalloc": (I, [P, P, P, I, I, I, D, I, I, P, P]),
 }
 
 
