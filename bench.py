@@ -54,6 +54,12 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the FP64-GPU fit and the accuracy check (profiling runs)")
+    ap.add_argument("--workload", default="fit10k",
+                    choices=["fit10k", "config1", "config3", "config4"],
+                    help="fit10k (default): the 10,000-molecule kernel + solve; config1: FP64 "
+                         "1,000-molecule fit+predict; config3: Jacobian kernel 1,000 x 1,000 "
+                         "molecules; config4: energy+force kernel of 300 x 21-atom molecules "
+                         "+ solve")
     return ap.parse_args()
 
 
@@ -452,8 +458,183 @@ def fp64_and_accuracy(X, Q, N, y, dev, nsub=2000, ntrain=1600):
     return out
 
 
+def _events_ms(fn, steps, warmup):
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def _ref_modules():
+    sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))
+    import kernelmath as km  # noqa: E402  (reference build)
+    import local_kernels as lk  # noqa: E402
+    return lk, km
+
+
+def _line(metric, value, unit, ms, args, workload, dtype, extra):
+    base = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+            "data": "synthetic (seeded molecules, FCHL19 descriptors, Morse labels)",
+            "config": {"workload": workload}}
+    base.update(extra)
+    print(json.dumps(base))
+
+
+def run_config3(args):
+    """Jacobian kernel: 1,000 training x 1,000 test molecules (9-30 atoms), FP32."""
+    import torch
+
+    from kernelforge_b200 import _lib, synthetic
+    tr = synthetic.make_molecules(1000, 9, 30, seed=SEED + 3)
+    te = synthetic.make_molecules(1000, 9, 30, seed=SEED + 30)
+    X1, Q1, N1 = synthetic.fchl19_batched(tr, dtype=np.float32, device="cuda", chunk=64)
+    X2, dX2, Q2, N2 = synthetic.fchl19_batched_grad(te, dtype=np.float32, device="cuda",
+                                                   chunk=16)
+    nm1, ma1, rep = X1.shape
+    nm2, ma2 = X2.shape[:2]
+    naq2 = int(3 * N2.sum())
+    x1, x2, dx2 = (torch.tensor(a, device="cuda") for a in (X1, X2, dX2))
+    out = torch.empty((nm1, naq2), dtype=torch.float32, device="cuda")
+    lib = _lib.lib()
+
+    def step():
+        _lib.check(lib.kfb_kernel_gaussian_jacobian(
+            x1.data_ptr(), x2.data_ptr(), dx2.data_ptr(), Q1.ctypes.data, Q2.ctypes.data,
+            N1.ctypes.data, N2.ctypes.data, nm1, nm2, ma1, ma2, rep, naq2, SIGMA, _lib.KFB_F32,
+            _lib.PREC["fp32"], out.data_ptr(), torch.cuda.current_stream().cuda_stream))
+
+    ms = _events_ms(step, args.steps, max(args.warmup, 3))
+    entries = nm1 * naq2
+    cpu = None
+    if not args.no_cpu_baseline:
+        lk, _ = _ref_modules()
+        n1, n2 = 100, 100
+        t0 = time.perf_counter()
+        ref = lk.kernel_gaussian_jacobian(X1[:n1].astype(np.float64), X2[:n2].astype(np.float64),
+                                          dX2[:n2].astype(np.float64), Q1[:n1], Q2[:n2], N1[:n1],
+                                          N2[:n2], SIGMA)
+        dt = time.perf_counter() - t0
+        cpu = {"value": ref.size / dt, "unit": "entries/s", "cores": os.cpu_count(),
+               "kind": "reference", "sample": f"{n1} x {n2} molecules, FP64 OpenMP"}
+        # accuracy of the FP32 GPU kernel on that sample against the reference
+        sub = torch.empty((n1, ref.shape[1]), dtype=torch.float32, device="cuda")
+        Q2s, N2s = np.ascontiguousarray(Q2[:n2]), np.ascontiguousarray(N2[:n2])
+        _lib.check(lib.kfb_kernel_gaussian_jacobian(
+            x1.data_ptr(), x2.data_ptr(), dx2.data_ptr(), Q1.ctypes.data, Q2s.ctypes.data,
+            N1.ctypes.data, N2s.ctypes.data, n1, n2, ma1, ma2, rep, ref.shape[1], SIGMA,
+            _lib.KFB_F32, _lib.PREC["fp32"], sub.data_ptr(),
+            torch.cuda.current_stream().cuda_stream))
+        err = sub.double().cpu().numpy() - ref
+        cpu["gpu_fp32_rel_frobenius_err"] = float(np.linalg.norm(err) / np.linalg.norm(ref))
+    _line("FCHL19 local Jacobian kernel: entries/s", entries / (ms * 1e-3), "entries/s", ms, args,
+          f"kernel_gaussian_jacobian {nm1} x {nm2} molecules (9-30 atoms), naq2={naq2}, FP32 "
+          "CUDA cores", "f32", {"cpu_baseline": cpu, "shape": [nm1, naq2]})
+
+
+def run_config4(args):
+    """Energy+force kernel (BIG = nm + naq) of 300 molecules x 21 atoms in RFP,
+    FP32 (split-fp16 scalar block) + mixed-precision solve at lambda 1e-6."""
+    import torch
+
+    from kernelforge_b200 import cuda_global_kernels as cgk
+    from kernelforge_b200 import cuda_local_kernels as clk
+    from kernelforge_b200 import synthetic
+    mols = synthetic.make_molecules(300, 21, 21, seed=SEED + 4)
+    X, dX, Q, N = synthetic.fchl19_batched_grad(mols, dtype=np.float32, device="cuda", chunk=16)
+    nm = X.shape[0]
+    naq = int(3 * N.sum())
+    big = nm + naq
+    x, dx = torch.tensor(X, device="cuda"), torch.tensor(dX, device="cuda")
+    F = np.concatenate([mols.F[m] for m in range(nm)]).ravel()
+    yv = np.concatenate([mols.E - mols.E.mean(), -F])
+    y = torch.tensor(yv, dtype=torch.float64, device="cuda")
+    info = {}
+
+    def kernel():
+        return clk.kernel_gaussian_full_symm_rfp(x, dx, Q, N, SIGMA)
+
+    def step():
+        K = kernel()
+        alpha, inf = cgk.krr_solve_mixed(K, y, l2=1e-6, uplo="L", tol=TOL)
+        info.update(inf)
+
+    kms = _events_ms(kernel, max(1, args.steps // 2), 2)
+    ms = _events_ms(step, args.steps, max(args.warmup, 3))
+    entries = big * (big + 1) // 2
+    cpu = None
+    if not args.no_cpu_baseline:
+        lk, km = _ref_modules()
+        ns = 40
+        Xs, dXs = X[:ns].astype(np.float64), dX[:ns].astype(np.float64)
+        t0 = time.perf_counter()
+        arf = lk.kernel_gaussian_full_symm_rfp(Xs, dXs, Q[:ns], N[:ns], SIGMA)
+        ys = np.concatenate([yv[:ns], yv[nm:nm + 3 * int(N[:ns].sum())]])
+        km.cho_solve_rfp(arf.copy(), ys, 1e-6)
+        dt = time.perf_counter() - t0
+        cpu = {"value": arf.size / dt, "unit": "entries/s", "cores": os.cpu_count(),
+               "kind": "reference", "sample": f"{ns} molecules (full_symm_rfp + cho_solve_rfp)"}
+    _line("FCHL19 energy+force KRR fit: kernel entries/s", entries / (ms * 1e-3), "entries/s",
+          ms, args, f"kernel_gaussian_full_symm_rfp {nm} x 21 atoms (BIG={big}) + mixed solve "
+          "lambda 1e-6", "f32 + f64 refinement",
+          {"kernel_ms": kms, "solve": {k: info.get(k) for k in ("iterations", "shift",
+                                                                 "rel_residual", "used_cg")},
+           "cpu_baseline": cpu})
+
+
+def run_config1(args):
+    """Plain FP64 energy-only KRR, 1,000 molecules, 800/200 split, lambda 1e-8:
+    FP64 GPU kernel + FP64 RFP Cholesky + FP64 prediction kernel."""
+    from kernelforge_b200 import kernelmath as km_ours
+    from kernelforge_b200 import local_kernels as lk_ours
+    from kernelforge_b200 import synthetic
+    mols = synthetic.make_molecules(1000, 9, 21, seed=SEED + 1)
+    X, Q, N = synthetic.fchl19_batched(mols, dtype=np.float64, device="cuda", chunk=128)
+    y = mols.E
+    ntr = 800
+
+    def fit_predict(lk, km):
+        K = lk.kernel_gaussian_symm_rfp(X[:ntr], Q[:ntr], N[:ntr], SIGMA)
+        ym = y[:ntr].mean()
+        alpha = km.cho_solve_rfp(K, y[:ntr] - ym, 1e-8)
+        Kt = lk.kernel_gaussian(X[ntr:], X[:ntr], Q[ntr:], Q[:ntr], N[ntr:], N[:ntr], SIGMA)
+        return float(np.abs(Kt @ alpha + ym - y[ntr:]).mean())
+
+    for _ in range(max(args.warmup, 3)):
+        mae = fit_predict(lk_ours, km_ours)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        mae = fit_predict(lk_ours, km_ours)
+    dt = (time.perf_counter() - t0) / args.steps
+    cpu = None
+    if not args.no_cpu_baseline:
+        lk, km = _ref_modules()
+        fit_predict(lk, km)
+        t0 = time.perf_counter()
+        mae_ref = fit_predict(lk, km)
+        dtc = time.perf_counter() - t0
+        cpu = {"value": dtc, "unit": "s", "cores": os.cpu_count(), "kind": "reference",
+               "sample": "the full workload (1,000 molecules)", "mae": mae_ref}
+    _line("FCHL19 energy KRR fit+predict time (FP64)", dt, "s", dt * 1e3, args,
+          "1,000 molecules, 800/200, symm_rfp + cho_solve_rfp + rect kernel, FP64 GPU "
+          "(host NumPy in/out through the drop-in modules)", "f64",
+          {"higher_is_better": False, "test_mae": mae, "cpu_baseline": cpu})
+
+
 def main():
     args = parse()
+    if args.workload != "fit10k":
+        {"config1": run_config1, "config3": run_config3, "config4": run_config4}[args.workload](args)
+        return
     rank, world, local = dist_setup(args.gpus)
     try:
         if args.impl == "reference":

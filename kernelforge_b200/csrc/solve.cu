@@ -551,7 +551,9 @@ kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2
     double rn = ynorm, prev = ynorm;
     int it = 0;
     residual_kernel<<<gw, 256, 0, s>>>(Kd.as<float>(), alpha, y, n, l2, r.as<double>());
-    bool need_cg = shift > 0.0;
+    // conjugate gradients converge at least as fast as classic refinement with
+    // the same preconditioner; classic refinement is kept for maxit <= 1 callers
+    bool need_cg = shift > 0.0 || maxit > 1;
     for (; !need_cg && it < maxit; ++it) {
         double rr = 0.0;
         KFB_TRY(dot(r.as<double>(), r.as<double>(), n, s, rr));

@@ -126,7 +126,7 @@ def _fchl19_one(R: torch.Tensor, zidx: torch.Tensor, nelem: int = 5, nRs2: int =
     val = pref[:, :, None] * g                           # (n, n, nRs2): centre i, neighbour j
     mask2 = (~eye) & (r <= rcut)
     val = val * mask2[:, :, None].to(dt)
-    onehot = torch.nn.functional.one_hot(zidx.long(), nelem).to(dt)   # (n, nelem)
+    onehot = (zidx.long()[:, None] == torch.arange(nelem, device=dev)).to(dt)  # (n, nelem)
     two = torch.einsum("ijk,je->iek", val, onehot).reshape(n, nelem * nRs2)
 
     # ---- three-body: ATM-weighted angular/radial terms for neighbour pairs (j<k)
@@ -160,7 +160,7 @@ def _fchl19_one(R: torch.Tensor, zidx: torch.Tensor, nelem: int = 5, nRs2: int =
     p = torch.minimum(zidx[:, None], zidx[None, :]).long()
     q = torch.maximum(zidx[:, None], zidx[None, :]).long()
     pair = -p * (p + 1) // 2 + q + nelem * p            # (n, n) over (j, k)
-    pair_oh = torch.nn.functional.one_hot(pair, npair).to(dt)        # (n, n, npair)
+    pair_oh = (pair[..., None] == torch.arange(npair, device=dev)).to(dt)  # (n, n, npair)
     three = torch.einsum("ijkla,jkp->ipla", coef, pair_oh).reshape(n, npair * nRs3 * 2)
     out = torch.cat([two, three], dim=1)
     assert out.shape[1] == rep
@@ -228,3 +228,37 @@ def fchl19_batched(mols: Molecules, max_atoms: int | None = None, dtype=np.float
                 Q[m, :n] = mols.Z[m]
             N[sel] = n
     return X, Q, N
+
+
+def fchl19_batched_grad(mols: Molecules, max_atoms: int | None = None, dtype=np.float32,
+                        device: str = "cuda", chunk: int = 8):
+    """Descriptors and Jacobians (X, dX, Q, N), vectorised over molecules of
+    equal size with torch.func (vmap of jacfwd); used for the derivative-kernel
+    workloads.  dX is (nm, ma, 720, 3*ma)."""
+    nm = mols.nm
+    ma = max_atoms or max(len(z) for z in mols.Z)
+    rep = rep_size()
+    X = np.zeros((nm, ma, rep), dtype=dtype)
+    dX = np.zeros((nm, ma, rep, 3 * ma), dtype=dtype)
+    Q = np.zeros((nm, ma), dtype=np.int32)
+    N = np.zeros((nm,), dtype=np.int32)
+    sizes = np.array([len(z) for z in mols.Z])
+    f = torch.vmap(_fchl19_one)
+    jf = torch.vmap(torch.func.jacfwd(_fchl19_one, argnums=0))
+    for n in np.unique(sizes):
+        ids = np.nonzero(sizes == n)[0]
+        for s in range(0, len(ids), chunk):
+            sel = ids[s:s + chunk]
+            R = torch.tensor(np.stack([mols.R[m] for m in sel]), dtype=torch.float64,
+                             device=device)
+            zi = torch.stack([_zidx(mols.Z[m]) for m in sel]).to(device)
+            with torch.no_grad():
+                out = f(R, zi)
+            J = jf(R, zi)                                   # (b, n, rep, n, 3)
+            X[sel, :n] = out.cpu().numpy().astype(dtype)
+            dX[sel, :n, :, : 3 * n] = J.reshape(len(sel), n, rep, 3 * n).detach().cpu().numpy() \
+                .astype(dtype)
+            for m in sel:
+                Q[m, :n] = mols.Z[m]
+            N[sel] = n
+    return X, dX, Q, N
