@@ -541,23 +541,49 @@ def run_config3(args):
           "CUDA cores", "f32", {"cpu_baseline": cpu, "shape": [nm1, naq2]})
 
 
-def run_config4(args):
-    """Energy+force kernel (BIG = nm + naq) of 300 molecules x 21 atoms in RFP,
-    FP32 (split-fp16 scalar block) + mixed-precision solve at lambda 1e-6."""
+def _full_asym(X1, dX1, Q1, N1, X2, dX2, Q2, N2, precision, dt):
+    """Device energy+force kernel ((nm1+naq1), (nm2+naq2)) through the C ABI."""
     import torch
 
+    from kernelforge_b200 import _lib
+    nm1, ma1, rep = X1.shape
+    nm2, ma2 = X2.shape[:2]
+    naq1, naq2 = int(3 * N1.sum()), int(3 * N2.sum())
+    out = torch.empty((nm1 + naq1, nm2 + naq2), dtype=dt, device="cuda")
+    _lib.check(_lib.lib().kfb_kernel_gaussian_full(
+        X1.data_ptr(), dX1.data_ptr(), X2.data_ptr(), dX2.data_ptr(), Q1.ctypes.data,
+        Q2.ctypes.data, N1.ctypes.data, N2.ctypes.data, nm1, nm2, ma1, ma2, rep, naq1, naq2,
+        SIGMA, _lib.KFB_F64 if dt == torch.float64 else _lib.KFB_F32, _lib.PREC[precision],
+        out.data_ptr(), torch.cuda.current_stream().cuda_stream))
+    return out
+
+
+def run_config4(args):
+    """Energy+force KRR of 300 x 21-atom molecules (BIG = nm + naq = 19,200):
+    symmetric full kernel in RFP (split-fp16 scalar block, FP32 derivative
+    blocks) + FP32-factor / FP64-refinement solve at lambda 1e-6; energy and
+    force MAE on 100 test molecules against the FP64 KRR on the same data."""
+    import ctypes
+
+    import torch
+
+    from kernelforge_b200 import _lib
     from kernelforge_b200 import cuda_global_kernels as cgk
     from kernelforge_b200 import cuda_local_kernels as clk
     from kernelforge_b200 import synthetic
-    mols = synthetic.make_molecules(300, 21, 21, seed=SEED + 4)
-    X, dX, Q, N = synthetic.fchl19_batched_grad(mols, dtype=np.float32, device="cuda", chunk=16)
-    nm = X.shape[0]
-    naq = int(3 * N.sum())
+    lam = 1e-6
+    tr = synthetic.make_molecules(300, 21, 21, seed=SEED + 4)
+    te = synthetic.make_molecules(100, 21, 21, seed=SEED + 40)
+    X, dX, Q, N = synthetic.fchl19_batched_grad(tr, dtype=np.float32, device="cuda", chunk=16)
+    Xt, dXt, Qt, Nt = synthetic.fchl19_batched_grad(te, dtype=np.float32, device="cuda", chunk=16)
+    nm, naq = X.shape[0], int(3 * N.sum())
     big = nm + naq
     x, dx = torch.tensor(X, device="cuda"), torch.tensor(dX, device="cuda")
-    F = np.concatenate([mols.F[m] for m in range(nm)]).ravel()
-    yv = np.concatenate([mols.E - mols.E.mean(), -F])
+    xt, dxt = torch.tensor(Xt, device="cuda"), torch.tensor(dXt, device="cuda")
+    em = tr.E.mean()
+    yv = np.concatenate([tr.E - em, -np.concatenate(tr.F).ravel()])
     y = torch.tensor(yv, dtype=torch.float64, device="cuda")
+    Ft = np.concatenate(te.F).ravel()
     info = {}
 
     def kernel():
@@ -565,12 +591,45 @@ def run_config4(args):
 
     def step():
         K = kernel()
-        alpha, inf = cgk.krr_solve_mixed(K, y, l2=1e-6, uplo="L", tol=TOL)
+        alpha, inf = cgk.krr_solve_mixed(K, y, l2=lam, uplo="L", tol=TOL, lambda_floor=True)
         info.update(inf)
+        return alpha
 
-    kms = _events_ms(kernel, max(1, args.steps // 2), 2)
+    kms = _events_ms(kernel, 2, 1)
     ms = _events_ms(step, args.steps, max(args.warmup, 3))
-    entries = big * (big + 1) // 2
+    alpha = step()
+
+    def mae(Kt, a):
+        pred = (Kt.double() @ a).cpu().numpy()
+        return (float(np.abs(pred[:100] + em - te.E).mean()),
+                float(np.abs(-pred[100:] - Ft).mean()))
+
+    Kt32 = _full_asym(xt, dxt, Qt, Nt, x, dx, Q, N, "split_f16", torch.float32)
+    mae_e, mae_f = mae(Kt32, alpha)
+    del Kt32
+    # FP64 KRR on the same data (FP64 GPU kernels, which match the CPU oracle to 1e-10)
+    x64, dx64 = x.double(), dx.double()
+    t0 = time.perf_counter()
+    K64 = torch.empty((big * (big + 1) // 2,), dtype=torch.float64, device="cuda")
+    _lib.check(_lib.lib().kfb_kernel_gaussian_full_symm(
+        x64.data_ptr(), dx64.data_ptr(), Q.ctypes.data, N.ctypes.data, nm, X.shape[1], REP, naq,
+        SIGMA, _lib.KFB_F64, _lib.PREC["fp64"], _lib.KFB_RFP_L, K64.data_ptr(),
+        torch.cuda.current_stream().cuda_stream))
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    a64 = torch.empty((big,), dtype=torch.float64, device="cuda")
+    inf64 = ctypes.c_int(0)
+    st = _lib.lib().kfb_cho_solve_rfp(K64.data_ptr(), y.data_ptr(), big, lam, _lib.KFB_RFP_L,
+                                      a64.data_ptr(), ctypes.byref(inf64),
+                                      torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    fp64 = {"kernel_s": t1 - t0, "solve_s": t2 - t1, "cholesky_info": inf64.value}
+    if st == _lib.KFB_OK:
+        del K64
+        Kt64 = _full_asym(xt.double(), dxt.double(), Qt, Nt, x64, dx64, Q, N, "fp64",
+                          torch.float64)
+        fp64["test_mae_energy"], fp64["test_mae_force"] = mae(Kt64, a64)
     cpu = None
     if not args.no_cpu_baseline:
         lk, km = _ref_modules()
@@ -579,15 +638,16 @@ def run_config4(args):
         t0 = time.perf_counter()
         arf = lk.kernel_gaussian_full_symm_rfp(Xs, dXs, Q[:ns], N[:ns], SIGMA)
         ys = np.concatenate([yv[:ns], yv[nm:nm + 3 * int(N[:ns].sum())]])
-        km.cho_solve_rfp(arf.copy(), ys, 1e-6)
+        km.cho_solve_rfp(arf.copy(), ys, lam)
         dt = time.perf_counter() - t0
         cpu = {"value": arf.size / dt, "unit": "entries/s", "cores": os.cpu_count(),
                "kind": "reference", "sample": f"{ns} molecules (full_symm_rfp + cho_solve_rfp)"}
-    _line("FCHL19 energy+force KRR fit: kernel entries/s", entries / (ms * 1e-3), "entries/s",
-          ms, args, f"kernel_gaussian_full_symm_rfp {nm} x 21 atoms (BIG={big}) + mixed solve "
-          "lambda 1e-6", "f32 + f64 refinement",
+    _line("FCHL19 energy+force KRR fit: kernel entries/s", big * (big + 1) / 2 / (ms * 1e-3),
+          "entries/s", ms, args, f"kernel_gaussian_full_symm_rfp {nm} x 21 atoms (BIG={big}) + "
+          f"mixed solve, lambda {lam}", "f32 kernel (split-fp16 scalar block) + f64 refinement",
           {"kernel_ms": kms, "solve": {k: info.get(k) for k in ("iterations", "shift",
-                                                                 "rel_residual", "used_cg")},
+                                                                 "rel_residual", "lambda_eff")},
+           "test_mae_energy": mae_e, "test_mae_force": mae_f, "fp64_krr": fp64,
            "cpu_baseline": cpu})
 
 

@@ -201,23 +201,30 @@ kfb_status kfb_cho_solve_rfp(void *arf, const double *y, int n, double l2, kfb_l
                              double *alpha, int *info, void *stream);
 
 /* Mixed-precision KRR solve: (K + l2 I) alpha = y with K given as an FP32 RFP
- * array (not modified).  The factor is FP32 (tensor-free RFP Cholesky of
- * K + (l2 + shift) I); residuals, corrections and norms are FP64: classic
- * iterative refinement, switching to FP32-preconditioned conjugate gradients
- * when refinement stalls.  Stops at ||r|| <= tol * ||y||.
+ * array (not modified).  The factor is FP32 (RFP Cholesky of K with its
+ * dominant eigenpair deflated, plus (l2 + shift) I); residuals, corrections and
+ * norms are FP64 (conjugate-gradient refinement preconditioned by the FP32
+ * factor).  Stops at ||r|| <= tol * ||y||; KFB_ERR_NOT_PD if K + l2 I is
+ * indefinite at FP32 storage precision (unless KFB_SOLVE_LAMBDA_FLOOR).
  * No reference counterpart: it replaces the reference's FP32 rfp_potrf +
  * rfp_potrs pair and its CPU FP64 fallback (models/cuda_local_krr.py:640-675). */
 typedef struct kfb_solve_info {
-    int iterations;       /* refinement / CG iterations taken            */
-    int factor_info;      /* potrf info of the last factorisation tried  */
-    double shift;         /* diagonal shift added to the FP32 factor      */
-    double rel_residual;  /* final ||y - (K + l2 I) alpha|| / ||y||     */
-    int used_cg;          /* 1 if CG was needed                           */
+    int iterations;       /* refinement (CG) iterations taken              */
+    int factor_info;      /* potrf info of the last factorisation tried    */
+    double shift;         /* diagonal shift added to the FP32 factor only  */
+    double rel_residual;  /* final ||y - (K + l2_eff I) alpha|| / ||y||  */
+    int used_cg;          /* 1 if CG refinement ran                        */
+    double lambda_eff;    /* regularisation of the system solved           */
 } kfb_solve_info;
 
+/* flags of kfb_krr_solve_mixed */
+#define KFB_SOLVE_LAMBDA_FLOOR 1  /* if K + l2 I is indefinite at FP32 storage
+                                     precision, raise l2 (x10 steps) until it is
+                                     not, and report it in lambda_eff */
+
 kfb_status kfb_krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2,
-                               kfb_layout uplo, double tol, int maxit, double *alpha,
-                               kfb_solve_info *info, void *stream);
+                               kfb_layout uplo, double tol, int maxit, int flags,
+                               double *alpha, kfb_solve_info *info, void *stream);
 
 /* ---------------------------------------------------------------------- */
 /* Allocation-free entry point                                             */

@@ -17,6 +17,7 @@ KFB_ERR_CUDA, KFB_ERR_TIMEOUT, KFB_ERR_NO_CONVERGENCE, KFB_ERR_UNSUPPORTED = 4, 
 KFB_F32, KFB_F64 = 0, 1
 PREC = {"fp64": 0, "fp32": 1, "split_f16": 2}
 KFB_DENSE, KFB_RFP_U, KFB_RFP_L = 0, 1, 2
+KFB_SOLVE_LAMBDA_FLOOR = 1
 
 # every function declared in include/kfb.h
 EXPORTS = (
@@ -40,7 +41,7 @@ class KfbError(RuntimeError):
 class SolveInfo(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int), ("factor_info", ctypes.c_int),
                 ("shift", ctypes.c_double), ("rel_residual", ctypes.c_double),
-                ("used_cg", ctypes.c_int)]
+                ("used_cg", ctypes.c_int), ("lambda_eff", ctypes.c_double)]
 
 
 _lib = None
@@ -68,7 +69,7 @@ _SIGS = {
     "kfb_rfp_potrf": (I, [P, I, D, I, I, ctypes.POINTER(I), P]),
     "kfb_rfp_potrs": (I, [P, P, I, I, I, I, P]),
     "kfb_cho_solve_rfp": (I, [P, P, I, D, I, P, ctypes.POINTER(I), P]),
-    "kfb_krr_solve_mixed": (I, [P, P, I, D, I, D, I, P, ctypes.POINTER(SolveInfo), P]),
+    "kfb_krr_solve_mixed": (I, [P, P, I, D, I, D, I, I, P, ctypes.POINTER(SolveInfo), P]),
     "kfb_kernel_gaussian_symm_noalloc": (I, [P, P, P, I, I, I, D, I, I, P, P]),
 }
 

@@ -16,7 +16,8 @@ kfb_status rfp_to_full(const void *arf, int n, kfb_layout uplo, kfb_dtype dt, vo
 kfb_status rfp_potrf(void *arf, int n, double l2, kfb_layout uplo, kfb_dtype dt, int *info, cudaStream_t s);
 kfb_status rfp_potrs(const void *arf, void *B, int n, int nrhs, kfb_layout uplo, kfb_dtype dt, cudaStream_t s);
 kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2, kfb_layout uplo,
-                           double tol, int maxit, double *alpha, kfb_solve_info *info, cudaStream_t s);
+                           double tol, int maxit, int flags, double *alpha, kfb_solve_info *info,
+                           cudaStream_t s);
 double last_kernel_ms();
 void set_timing(bool on);
 }  // namespace kfb
@@ -459,14 +460,15 @@ kfb_status kfb_cho_solve_rfp(void *arf, const double *y, int n, double l2, kfb_l
 }
 
 kfb_status kfb_krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2,
-                               kfb_layout uplo, double tol, int maxit, double *alpha,
+                               kfb_layout uplo, double tol, int maxit, int flags, double *alpha,
                                kfb_solve_info *info, void *stream) {
     if (n <= 0) return set_error(KFB_ERR_INVALID_ARG, "n must be > 0");
     if (!k_rfp || !y || !alpha) return set_error(KFB_ERR_INVALID_ARG, "null pointer");
     if (uplo != KFB_RFP_U && uplo != KFB_RFP_L)
         return set_error(KFB_ERR_INVALID_ARG, "uplo must be RFP");
     if (!(tol > 0.0) || maxit < 0) return set_error(KFB_ERR_INVALID_ARG, "bad tol / maxit");
-    return krr_solve_mixed(k_rfp, y, n, l2, uplo, tol, maxit, alpha, info, as_stream(stream));
+    return krr_solve_mixed(k_rfp, y, n, l2, uplo, tol, maxit, flags, alpha, info,
+                           as_stream(stream));
 }
 
 }  // extern "C"

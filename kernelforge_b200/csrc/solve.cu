@@ -419,11 +419,12 @@ kfb_status rfp_potrs(const void *arf, void *B, int n, int nrhs, kfb_layout uplo,
 }
 
 kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2,
-                           kfb_layout uplo, double tol, int maxit, double *alpha,
+                           kfb_layout uplo, double tol, int maxit, int flags, double *alpha,
                            kfb_solve_info *info, cudaStream_t s) {
     kfb_solve_info inf{};
+    inf.lambda_eff = l2;
     const size_t nt = (size_t)n * (n + 1) / 2;
-    DevBuf Kd, F, r, z, p, q, f32v, dmax;
+    DevBuf Kd, F, r, z, p, q, f32v;
     KFB_TRY(Kd.alloc((size_t)n * n * sizeof(float), s));
     KFB_TRY(rfp_to_full(k_rfp, n, uplo, KFB_F32, Kd.ptr, s));
     KFB_TRY(F.alloc(nt * sizeof(float), s));
@@ -432,7 +433,6 @@ kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2
     KFB_TRY(p.alloc((size_t)n * sizeof(double), s));
     KFB_TRY(q.alloc((size_t)n * sizeof(double), s));
     KFB_TRY(f32v.alloc((size_t)n * sizeof(float), s));
-    KFB_TRY(dmax.alloc(sizeof(float), s));
     Dot dot;
     KFB_TRY(dot.init(s));
 
@@ -452,7 +452,7 @@ kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2
     // the diagonal shift FP32 Cholesky needs (unit roundoff times ||K||_2).
     // Power iteration gives (mu, v) and an estimate sigma of the next
     // eigenvalue; the FP32 factor is of
-    //   F = K - (mu - sigma) v v^T + (l2 + shift) I,
+    //   F = K - (mu - sigma) v v^T + (lambda + shift) I,
     // whose eigenvalue along v is sigma (not ~0, which would make F^{-1} v huge
     // and the correction below cancel), and the preconditioner
     //   M^{-1} = (F + (mu - sigma) v v^T)^{-1}
@@ -499,29 +499,10 @@ kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2
         }
         lam2 *= 1.5;  // Rayleigh quotients approach ||.||_2 from below
     }
-
-    // FP32 factor of F; the shift starts at max(0, 2 u32 lam2 - l2) and grows 4x
-    // per failed attempt
     const double u32 = 5.960464477539063e-08;
     const double defl = std::max(0.0, mu - lam2);
-    double shift = std::max(0.0, 2.0 * u32 * lam2 - l2);
-    int finfo = 0;
     const dim3 blk2(32, 8), grd2(nblk(n, 32), nblk(n, 8));
-    for (int attempt = 0; attempt < 12; ++attempt) {
-        rfp_deflate_kernel<<<grd2, blk2, 0, s>>>(k_rfp, n, uplo, dv.as<double>(), defl,
-                                                 F.as<float>());
-        KFB_CUDA_TRY(cudaGetLastError());
-        KFB_TRY(rfp_potrf(F.ptr, n, l2 + shift, uplo, KFB_F32, &finfo, s));
-        if (finfo == 0) break;
-        shift = (shift == 0.0) ? std::max(u32 * lam2, 10.0 * l2) : shift * 4.0;
-    }
-    inf.factor_info = finfo;
-    inf.shift = shift;
-    if (finfo != 0) {
-        if (info) *info = inf;
-        return set_error(KFB_ERR_NOT_PD, "FP32 RFP Cholesky failed even with shift %g (info=%d)",
-                         shift, finfo);
-    }
+
     // F^{-1} v via the FP32 factor, with v scaled to unit norm first
     auto solve_f = [&](const double *v, double vnorm, double *out) -> kfb_status {
         const double sc = vnorm > 0.0 ? 1.0 / vnorm : 1.0;
@@ -532,76 +513,64 @@ kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2
         KFB_CUDA_TRY(cudaGetLastError());
         return KFB_OK;
     };
-    KFB_TRY(solve_f(dv.as<double>(), 1.0, dw.as<double>()));  // w = F^{-1} v
-    double vfv = 0.0;
-    KFB_TRY(dot(dv.as<double>(), dw.as<double>(), n, s, vfv));
-    const double sm_coef = defl / (1.0 + defl * vfv);
-    // M^{-1} r = F^{-1} r - sm_coef (w . r) w
-    auto precond = [&](const double *v, double vnorm, double *out) -> kfb_status {
-        KFB_TRY(solve_f(v, vnorm, out));
-        double wr = 0.0;
-        KFB_TRY(dot(dw.as<double>(), v, n, s, wr));
-        axpy_kernel<<<gb, 256, 0, s>>>(dw.as<double>(), -sm_coef * wr, n, out);
-        KFB_CUDA_TRY(cudaGetLastError());
-        return KFB_OK;
-    };
 
-    // classic iterative refinement (only when the FP32 factor needed no shift);
-    // a correction that increases the residual is undone and CG takes over
-    double rn = ynorm, prev = ynorm;
-    int it = 0;
-    residual_kernel<<<gw, 256, 0, s>>>(Kd.as<float>(), alpha, y, n, l2, r.as<double>());
-    // conjugate gradients converge at least as fast as classic refinement with
-    // the same preconditioner; classic refinement is kept for maxit <= 1 callers
-    bool need_cg = shift > 0.0 || maxit > 1;
-    for (; !need_cg && it < maxit; ++it) {
-        double rr = 0.0;
-        KFB_TRY(dot(r.as<double>(), r.as<double>(), n, s, rr));
-        rn = std::sqrt(rr);
-        if (rn <= tol * ynorm) break;
-        if (it > 0 && rn > 0.5 * prev) {
-            if (rn > prev) {  // diverging: undo the last correction
-                axpy_kernel<<<gb, 256, 0, s>>>(z.as<double>(), -1.0, n, alpha);
-                residual_kernel<<<gw, 256, 0, s>>>(Kd.as<float>(), alpha, y, n, l2, r.as<double>());
-                rn = prev;
-            }
-            need_cg = true;
-            break;
+    // One attempt at (K + lam I) alpha = y: FP32 factor (the shift starts at
+    // max(0, 2 u32 lam2 - lam) and grows 4x per failed factorisation), then
+    // preconditioned CG in FP64.  KFB_ERR_NOT_PD if CG meets a non-positive
+    // curvature p^T (K + lam I) p, i.e. K + lam I is indefinite at FP32 storage
+    // precision.
+    auto attempt = [&](double lam) -> kfb_status {
+        double shift = std::max(0.0, 2.0 * u32 * lam2 - lam);
+        int finfo = 0;
+        for (int a = 0; a < 12; ++a) {
+            rfp_deflate_kernel<<<grd2, blk2, 0, s>>>(k_rfp, n, uplo, dv.as<double>(), defl,
+                                                     F.as<float>());
+            KFB_CUDA_TRY(cudaGetLastError());
+            KFB_TRY(rfp_potrf(F.ptr, n, lam + shift, uplo, KFB_F32, &finfo, s));
+            if (finfo == 0) break;
+            shift = (shift == 0.0) ? std::max(u32 * lam2, 10.0 * lam) : shift * 4.0;
         }
-        prev = rn;
-        KFB_TRY(precond(r.as<double>(), rn, z.as<double>()));
-        axpy_kernel<<<gb, 256, 0, s>>>(z.as<double>(), 1.0, n, alpha);
-        residual_kernel<<<gw, 256, 0, s>>>(Kd.as<float>(), alpha, y, n, l2, r.as<double>());
-        KFB_CUDA_TRY(cudaGetLastError());
-    }
-    if (need_cg && shift > 0.0) {
-        double rr = 0.0;
-        KFB_TRY(dot(r.as<double>(), r.as<double>(), n, s, rr));
-        rn = std::sqrt(rr);
-    }
-    inf.iterations = it;
-    if (rn > tol * ynorm && it < maxit) {
-            // preconditioned conjugate gradients (FP64), FP32 factor as preconditioner
-        inf.used_cg = 1;
+        inf.factor_info = finfo;
+        inf.shift = shift;
+        if (finfo != 0)
+            return set_error(KFB_ERR_NOT_PD,
+                             "FP32 RFP Cholesky failed even with shift %g (info=%d)", shift, finfo);
+        KFB_TRY(solve_f(dv.as<double>(), 1.0, dw.as<double>()));  // w = F^{-1} v
+        double vfv = 0.0;
+        KFB_TRY(dot(dv.as<double>(), dw.as<double>(), n, s, vfv));
+        const double sm_coef = defl / (1.0 + defl * vfv);
+        // M^{-1} r = F^{-1} r - sm_coef (w . r) w
+        auto precond = [&](const double *vec, double vnorm, double *out) -> kfb_status {
+            KFB_TRY(solve_f(vec, vnorm, out));
+            double wr = 0.0;
+            KFB_TRY(dot(dw.as<double>(), vec, n, s, wr));
+            axpy_kernel<<<gb, 256, 0, s>>>(dw.as<double>(), -sm_coef * wr, n, out);
+            KFB_CUDA_TRY(cudaGetLastError());
+            return KFB_OK;
+        };
+        // preconditioned conjugate gradients in FP64 from alpha = 0
+        KFB_TRY(zero(alpha, (size_t)n * sizeof(double), s));
+        KFB_CUDA_TRY(cudaMemcpyAsync(r.ptr, y, (size_t)n * sizeof(double),
+                                     cudaMemcpyDeviceToDevice, s));
+        double rn = ynorm;
         KFB_TRY(precond(r.as<double>(), rn, z.as<double>()));
         KFB_CUDA_TRY(cudaMemcpyAsync(p.ptr, z.ptr, (size_t)n * sizeof(double),
                                      cudaMemcpyDeviceToDevice, s));
         double rz = 0.0;
         KFB_TRY(dot(r.as<double>(), z.as<double>(), n, s, rz));
+        int it = 0;
         for (; it < maxit; ++it) {
-            residual_kernel<<<gw, 256, 0, s>>>(Kd.as<float>(), p.as<double>(), nullptr, n, l2,
-                                               q.as<double>());  // q = -(K + l2 I) p
+            residual_kernel<<<gw, 256, 0, s>>>(Kd.as<float>(), p.as<double>(), nullptr, n, lam,
+                                               q.as<double>());  // q = -(K + lam I) p
             double pq = 0.0;
             KFB_TRY(dot(p.as<double>(), q.as<double>(), n, s, pq));
             pq = -pq;
-            if (!(pq > 0.0)) {  // K + l2 I is not positive definite at this precision
+            if (!(pq > 0.0)) {
                 inf.iterations = it;
-                inf.rel_residual = rn / ynorm;
-                if (info) *info = inf;
                 return set_error(KFB_ERR_NOT_PD,
                                  "K + l2 I is indefinite at FP32 storage precision (p^T A p = "
-                                 "%.3e after %d CG iterations); use a larger l2",
-                                 -pq, it);
+                                 "%.3e after %d CG iterations, l2 = %g); use a larger l2",
+                                 -pq, it, lam);
             }
             const double a = rz / pq;
             axpy_kernel<<<gb, 256, 0, s>>>(p.as<double>(), a, n, alpha);
@@ -619,21 +588,32 @@ kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2
             xpby_kernel<<<gb, 256, 0, s>>>(z.as<double>(), rz_new / rz, n, p.as<double>());
             rz = rz_new;
         }
-        // true residual
-        residual_kernel<<<gw, 256, 0, s>>>(Kd.as<float>(), alpha, y, n, l2, r.as<double>());
+        // true residual of the returned alpha
+        residual_kernel<<<gw, 256, 0, s>>>(Kd.as<float>(), alpha, y, n, lam, r.as<double>());
         double rr = 0.0;
         KFB_TRY(dot(r.as<double>(), r.as<double>(), n, s, rr));
-        rn = std::sqrt(rr);
         inf.iterations = it;
+        inf.used_cg = 1;
+        inf.rel_residual = std::sqrt(rr) / ynorm;
+        if (inf.rel_residual > tol)
+            return set_error(KFB_ERR_NO_CONVERGENCE,
+                             "refinement stopped at relative residual %.3e (tol %.1e) after %d "
+                             "iterations",
+                             inf.rel_residual, tol, it);
+        return KFB_OK;
+    };
+
+    double lam = l2;
+    kfb_status st = KFB_OK;
+    for (int tries = 0; tries < 10; ++tries) {
+        st = attempt(lam);
+        inf.lambda_eff = lam;
+        if (st != KFB_ERR_NOT_PD || !(flags & KFB_SOLVE_LAMBDA_FLOOR)) break;
+        // raise the regularisation until K + lam I is definite at FP32 precision
+        lam = (tries == 0) ? std::max(10.0 * l2, u32 * lam2) : lam * 10.0;
     }
-    inf.rel_residual = rn / ynorm;
     if (info) *info = inf;
-    if (inf.rel_residual > tol)
-        return set_error(KFB_ERR_NO_CONVERGENCE,
-                         "refinement stopped at relative residual %.3e (tol %.1e) after %d "
-                         "iterations",
-                         inf.rel_residual, tol, inf.iterations);
-    return KFB_OK;
+    return st;
 }
 
 }  // namespace kfb

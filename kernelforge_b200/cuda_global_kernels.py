@@ -60,10 +60,14 @@ def rfp_potrs(L_rfp, B, uplo="L"):
                                         _dt(L_rfp), stream_handle()))
 
 
-def krr_solve_mixed(K_rfp, y, l2=0.0, uplo="L", tol=1e-10, maxit=500):
+def krr_solve_mixed(K_rfp, y, l2=0.0, uplo="L", tol=1e-10, maxit=500, *, lambda_floor=False):
     """(K + l2 I) alpha = y with an FP32 RFP kernel matrix (not modified): FP32
-    Cholesky factor, FP64 residuals / corrections / norms.  Returns (alpha
-    float64, info dict)."""
+    Cholesky factor (dominant eigenpair deflated), FP64 conjugate-gradient
+    refinement of residuals against K.  Returns (alpha float64, info dict).
+
+    Raises RuntimeError if K + l2 I is indefinite at FP32 storage precision;
+    with ``lambda_floor=True`` l2 is raised in x10 steps until it is not, and
+    info["lambda_eff"] reports the value used."""
     require_cuda()
     import torch
     if K_rfp.dtype != torch.float32 or not K_rfp.is_cuda or not K_rfp.is_contiguous():
@@ -74,11 +78,13 @@ def krr_solve_mixed(K_rfp, y, l2=0.0, uplo="L", tol=1e-10, maxit=500):
         raise RuntimeError("K_rfp must have n*(n+1)/2 elements")
     alpha = torch.empty((n,), dtype=torch.float64, device=K_rfp.device)
     info = _lib.SolveInfo()
+    flags = _lib.KFB_SOLVE_LAMBDA_FLOOR if lambda_floor else 0
     st = _lib.lib().kfb_krr_solve_mixed(K_rfp.data_ptr(), yd.data_ptr(), n, float(l2),
-                                        _uplo(uplo), float(tol), int(maxit), alpha.data_ptr(),
-                                        ctypes.byref(info), stream_handle())
+                                        _uplo(uplo), float(tol), int(maxit), flags,
+                                        alpha.data_ptr(), ctypes.byref(info), stream_handle())
     res = {"iterations": info.iterations, "factor_info": info.factor_info, "shift": info.shift,
-           "rel_residual": info.rel_residual, "used_cg": bool(info.used_cg)}
+           "rel_residual": info.rel_residual, "used_cg": bool(info.used_cg),
+           "lambda_eff": info.lambda_eff}
     if st == _lib.KFB_ERR_NOT_PD:
         raise RuntimeError(_lib.lib().kfb_last_error().decode())
     if st != _lib.KFB_OK and st != _lib.KFB_ERR_NO_CONVERGENCE:
