@@ -85,24 +85,29 @@ kfb_status naq_check(const SetView &v, long long naq, const char *message) {
     return KFB_OK;
 }
 
-template <class T>
-kfb_status jac(const DerivSet &outer, const DerivSet &inner, int rep, double sigma, double alpha,
-               const ElemSink &sink, cudaStream_t s) {
-    return jacobian_core<T>(outer, inner, rep, sigma, alpha, sink, s);
+// The split-fp16 precision runs the derivative kernels' contraction GEMMs on the
+// tensor cores when rep is a multiple of 16 (TMA rows of whole 16-byte units);
+// otherwise, and for the FP64 / FP32 precisions, they run on CUDA cores.
+bool use_tc(kfb_precision prec, int rep) {
+    return prec == KFB_PREC_SPLIT_F16 && rep % 16 == 0 && device_is_sm100();
 }
 
-kfb_status jac_any(kfb_dtype dt, const DerivSet &outer, const DerivSet &inner, int rep,
-                   double sigma, double alpha, const ElemSink &sink, cudaStream_t s) {
+kfb_status jac_any(kfb_dtype dt, kfb_precision prec, const DerivSet &outer,
+                   const DerivSet &inner, int rep, double sigma, double alpha,
+                   const ElemSink &sink, cudaStream_t s) {
     if (rep <= 0) return KFB_OK;
-    if (dt == KFB_F64) return jac<double>(outer, inner, rep, sigma, alpha, sink, s);
-    return jac<float>(outer, inner, rep, sigma, alpha, sink, s);
+    const bool tc = use_tc(prec, rep);
+    if (dt == KFB_F64) return jacobian_core<double>(outer, inner, rep, sigma, alpha, tc, sink, s);
+    return jacobian_core<float>(outer, inner, rep, sigma, alpha, tc, sink, s);
 }
 
-kfb_status hess_any(kfb_dtype dt, const DerivSet &s1, const DerivSet &s2, int rep, double sigma,
-                    bool symmetric, const ElemSink &sink, cudaStream_t s) {
+kfb_status hess_any(kfb_dtype dt, kfb_precision prec, const DerivSet &s1, const DerivSet &s2,
+                    int rep, double sigma, bool symmetric, const ElemSink &sink,
+                    cudaStream_t s) {
     if (rep <= 0) return KFB_OK;
-    if (dt == KFB_F64) return hessian_core<double>(s1, s2, rep, sigma, symmetric, sink, s);
-    return hessian_core<float>(s1, s2, rep, sigma, symmetric, sink, s);
+    const bool tc = use_tc(prec, rep);
+    if (dt == KFB_F64) return hessian_core<double>(s1, s2, rep, sigma, symmetric, tc, sink, s);
+    return hessian_core<float>(s1, s2, rep, sigma, symmetric, tc, sink, s);
 }
 
 DerivSet dset(const void *x, const void *dx, const int32_t *q, const int32_t *n, int nm, int ma) {
@@ -208,7 +213,7 @@ kfb_status kfb_kernel_gaussian_jacobian(const void *x1, const void *x2, const vo
     sink.f64 = dt == KFB_F64;
     sink.mode = EM_RECT;
     sink.ld = naq2;
-    return jac_any(dt, dset(x1, nullptr, q1, n1, nm1, ma1), dset(x2, dx2, q2, n2, nm2, ma2), rep,
+    return jac_any(dt, prec, dset(x1, nullptr, q1, n1, nm1, ma1), dset(x2, dx2, q2, n2, nm2, ma2), rep,
                    sigma, 1.0, sink, s);
 }
 
@@ -238,7 +243,7 @@ kfb_status kfb_kernel_gaussian_jacobian_t(const void *x1, const void *dx1, const
     sink.f64 = dt == KFB_F64;
     sink.mode = EM_RECT_T;
     sink.ld = nm2;
-    return jac_any(dt, dset(x2, nullptr, q2, n2, nm2, ma2), dset(x1, dx1, q1, n1, nm1, ma1), rep,
+    return jac_any(dt, prec, dset(x2, nullptr, q2, n2, nm2, ma2), dset(x1, dx1, q1, n1, nm1, ma1), rep,
                    sigma, -1.0, sink, s);
 }
 
@@ -267,7 +272,7 @@ kfb_status kfb_kernel_gaussian_hessian(const void *x1, const void *dx1, const vo
     sink.f64 = dt == KFB_F64;
     sink.mode = EM_RECT;
     sink.ld = naq2;
-    return hess_any(dt, dset(x1, dx1, q1, n1, nm1, ma1), dset(x2, dx2, q2, n2, nm2, ma2), rep,
+    return hess_any(dt, prec, dset(x1, dx1, q1, n1, nm1, ma1), dset(x2, dx2, q2, n2, nm2, ma2), rep,
                     sigma, false, sink, s);
 }
 
@@ -295,7 +300,7 @@ kfb_status kfb_kernel_gaussian_hessian_symm(const void *x, const void *dx, const
     sink.layout = layout == KFB_DENSE ? LAYOUT_DENSE_LOWER : layout;
     sink.ld = naq;
     DerivSet d = dset(x, dx, q, n, nm, ma);
-    return hess_any(dt, d, d, rep, sigma, true, sink, s);
+    return hess_any(dt, prec, d, d, rep, sigma, true, sink, s);
 }
 
 kfb_status kfb_kernel_gaussian_full(const void *x1, const void *dx1, const void *x2,
@@ -339,7 +344,7 @@ kfb_status kfb_kernel_gaussian_full(const void *x1, const void *dx1, const void 
     sj.mode = EM_RECT;
     sj.ld = C;
     sj.col_base = nm2;
-    KFB_TRY(jac_any(dt, d1, d2, rep, sigma, 1.0, sj, s));
+    KFB_TRY(jac_any(dt, prec, d1, d2, rep, sigma, 1.0, sj, s));
     // [nm1:, 0:nm2] = -jacobian_t(X1, dX1, X2) = G^T with G from (outer 2, inner 1)
     ElemSink st;
     st.out = out;
@@ -347,7 +352,7 @@ kfb_status kfb_kernel_gaussian_full(const void *x1, const void *dx1, const void 
     st.mode = EM_RECT_T;
     st.ld = C;
     st.col_base = nm1;
-    KFB_TRY(jac_any(dt, d2, d1, rep, sigma, 1.0, st, s));
+    KFB_TRY(jac_any(dt, prec, d2, d1, rep, sigma, 1.0, st, s));
     // [nm1:, nm2:] = hessian
     ElemSink sh;
     sh.out = out;
@@ -356,7 +361,7 @@ kfb_status kfb_kernel_gaussian_full(const void *x1, const void *dx1, const void 
     sh.ld = C;
     sh.row_base = nm1;
     sh.col_base = nm2;
-    return hess_any(dt, d1, d2, rep, sigma, false, sh, s);
+    return hess_any(dt, prec, d1, d2, rep, sigma, false, sh, s);
 }
 
 kfb_status kfb_kernel_gaussian_full_symm(const void *x, const void *dx, const int32_t *q,
@@ -399,7 +404,7 @@ kfb_status kfb_kernel_gaussian_full_symm(const void *x, const void *dx, const in
     sj.layout = layout;
     sj.ld = big;
     sj.col_base = nm;
-    KFB_TRY(jac_any(dt, d, d, rep, sigma, 1.0, sj, s));
+    KFB_TRY(jac_any(dt, prec, d, d, rep, sigma, 1.0, sj, s));
     ElemSink sh;
     sh.out = out;
     sh.f64 = dt == KFB_F64;
@@ -408,7 +413,7 @@ kfb_status kfb_kernel_gaussian_full_symm(const void *x, const void *dx, const in
     sh.ld = big;
     sh.row_base = nm;
     sh.col_base = nm;
-    return hess_any(dt, d, d, rep, sigma, true, sh, s);
+    return hess_any(dt, prec, d, d, rep, sigma, true, sh, s);
 }
 
 kfb_status kfb_full_to_rfp(const void *a, int n, kfb_layout uplo, kfb_dtype dt, void *arf,

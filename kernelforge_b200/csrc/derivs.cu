@@ -20,6 +20,7 @@
 
 #include "derivs.h"
 #include "kernels_common.cuh"
+#include "tc_gemm.h"
 
 namespace kfb {
 
@@ -270,7 +271,7 @@ size_t budget_bytes() {
 // ---------------------------------------------------------------------------
 template <class T>
 kfb_status jacobian_core(const DerivSet &outer, const DerivSet &inner, int rep, double sigma,
-                         double alpha, ElemSink sink, cudaStream_t s) {
+                         double alpha, bool tc, ElemSink sink, cudaStream_t s) {
     std::vector<int> in_offs;
     deriv_offsets(inner.v, in_offs);
     // active inner atoms in molecule order
@@ -292,11 +293,22 @@ kfb_status jacobian_core(const DerivSet &outer, const DerivSet &inner, int rep, 
     std::vector<int> no(outer.v.n, outer.v.n + outer.v.nm);
     KFB_TRY(upload(d_qo, qo, s));
     KFB_TRY(upload(d_no, no, s));
-    const size_t row_bytes = (size_t)NU * rep * sizeof(T);
+    const size_t row_bytes = (size_t)NU * rep * (sizeof(T) + (tc ? 2 * sizeof(__half) : 0));
     int chunk = (int)std::max<size_t>(1, budget_bytes() / std::max<size_t>(row_bytes, 1));
     chunk = std::min(chunk, outer.v.nm);
-    DevBuf V;
-    KFB_TRY(V.alloc((size_t)chunk * row_bytes, s));
+    DevBuf V, vh, vl, jth, jtl;
+    KFB_TRY(V.alloc((size_t)chunk * NU * rep * sizeof(T), s));
+    const int ma_in = inner.v.ma;
+    if (tc) {
+        // inner Jacobians as K-major split rows: Jt[(m, c)][(j, k)]
+        const size_t jt_elems = (size_t)inner.v.nm * 3 * ma_in * ma_in * rep;
+        KFB_TRY(jth.alloc(jt_elems * sizeof(__half), s));
+        KFB_TRY(jtl.alloc(jt_elems * sizeof(__half), s));
+        KFB_TRY(transpose_split_dx<T>(static_cast<const T *>(inner.dx), inner.v.nm, ma_in, rep,
+                                      jth.as<__half>(), jtl.as<__half>(), s));
+        KFB_TRY(vh.alloc((size_t)chunk * NU * rep * sizeof(__half), s));
+        KFB_TRY(vl.alloc((size_t)chunk * NU * rep * sizeof(__half), s));
+    }
     const T c2 = T(-1.0 / (2.0 * sigma * sigma)), is2 = T(1.0 / (sigma * sigma));
     const int ld_in = 3 * inner.v.ma;
     for (int o0 = 0; o0 < outer.v.nm; o0 += chunk) {
@@ -309,6 +321,39 @@ kfb_status jacobian_core(const DerivSet &outer, const DerivSet &inner, int rep, 
             nout, static_cast<const T *>(inner.x), d_usrc.as<int>(), d_ulab.as<int>(), NU, rep,
             c2, is2, V.as<T>());
         KFB_CUDA_TRY(cudaGetLastError());
+        if (tc) {
+            KFB_TRY(split_rows<T>(V.as<T>(), (long long)nout * NU * rep, vh.as<__half>(),
+                                  vl.as<__half>(), s));
+            std::vector<TcProb> tprobs;
+            for (int m = 0; m < inner.v.nm; ++m) {
+                const int nb = inner.v.natoms(m);
+                if (nb == 0) continue;
+                TcProb p{};
+                p.a_row0 = 0;
+                p.a_k0 = u_first[m] * rep;
+                p.b_row0 = m * 3 * ma_in;
+                p.b_k0 = 0;
+                p.M = nout;
+                p.N = 3 * nb;
+                p.K = nb * rep;
+                p.row_off = o0;
+                p.col_off = in_offs[m];
+                p.diag = 0;
+                p.alpha = alpha;
+                tprobs.push_back(p);
+            }
+            TcOperand A, B;
+            A.hi = vh.ptr;
+            A.lo = vl.ptr;
+            A.rows = nout;
+            A.cols = (long long)NU * rep;
+            B.hi = jth.ptr;
+            B.lo = jtl.ptr;
+            B.rows = (long long)inner.v.nm * 3 * ma_in;
+            B.cols = (long long)ma_in * rep;
+            KFB_TRY(tc_gemm_grouped(A, B, 3, false, tprobs, sink, s));
+            continue;
+        }
         std::vector<GemmProb> probs;
         for (int m = 0; m < inner.v.nm; ++m) {
             const int nb = inner.v.natoms(m);
@@ -339,7 +384,7 @@ kfb_status jacobian_core(const DerivSet &outer, const DerivSet &inner, int rep, 
 // ---------------------------------------------------------------------------
 template <class T>
 kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double sigma,
-                        bool symmetric, ElemSink sink, cudaStream_t s) {
+                        bool symmetric, bool tc, ElemSink sink, cudaStream_t s) {
     std::vector<int> off1, off2;
     deriv_offsets(s1.v, off1);
     deriv_offsets(s2.v, off2);
@@ -360,7 +405,8 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
     KFB_TRY(upload(d_q1, q1, s));
     KFB_TRY(upload(d_q2, q2, s));
     const int ma1 = s1.v.ma, ma2 = s2.v.ma, ld1 = 3 * ma1, ld2 = 3 * ma2;
-    const size_t per_pair = ((size_t)ma1 * ma2 * (2 + ld2) + (size_t)ma1 * rep * ld2) * sizeof(T);
+    const size_t per_pair = ((size_t)ma1 * ma2 * (2 + ld2) + (size_t)ma1 * rep * ld2) * sizeof(T) +
+                            (tc ? (size_t)ma1 * rep * ld2 * 2 * sizeof(__half) : 0);
     int batch = (int)std::max<size_t>(1, budget_bytes() / per_pair);
     batch = std::min<int>(batch, (int)pairs.size());
     batch = std::min(batch, 65535);
@@ -370,6 +416,17 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
     KFB_TRY(Tt.alloc((size_t)batch * ma1 * ma2 * ld2 * sizeof(T), s));
     KFB_TRY(Y.alloc((size_t)batch * ma1 * rep * ld2 * sizeof(T), s));
     KFB_TRY(dpairs.alloc((size_t)batch * sizeof(HessPair), s));
+    DevBuf jth, jtl, yth, ytl;
+    if (tc) {
+        // set-1 Jacobians as K-major split rows Jt[(a, c)][(i, k)]
+        const size_t jt_elems = (size_t)s1.v.nm * ld1 * ma1 * rep;
+        KFB_TRY(jth.alloc(jt_elems * sizeof(__half), s));
+        KFB_TRY(jtl.alloc(jt_elems * sizeof(__half), s));
+        KFB_TRY(transpose_split_dx<T>(static_cast<const T *>(s1.dx), s1.v.nm, ma1, rep,
+                                      jth.as<__half>(), jtl.as<__half>(), s));
+        KFB_TRY(yth.alloc((size_t)batch * ld2 * ma1 * rep * sizeof(__half), s));
+        KFB_TRY(ytl.alloc((size_t)batch * ld2 * ma1 * rep * sizeof(__half), s));
+    }
     const T c2 = T(-1.0 / (2.0 * sigma * sigma)), is2 = T(1.0 / (sigma * sigma));
     const T is4 = is2 * is2;
     for (size_t p0 = 0; p0 < pairs.size(); p0 += batch) {
@@ -386,6 +443,39 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
             static_cast<const T *>(s2.dx), ma1, ma2, rep, W.as<T>(), W2.as<T>(), Tt.as<T>(),
             Y.as<T>());
         KFB_CUDA_TRY(cudaGetLastError());
+        if (tc) {
+            KFB_TRY(transpose_split_y<T>(Y.as<T>(), np, ma1, rep, ld2, yth.as<__half>(),
+                                         ytl.as<__half>(), s));
+            std::vector<TcProb> tprobs;
+            tprobs.reserve(np);
+            for (int k = 0; k < np; ++k) {
+                const HessPair &pr = pairs[p0 + k];
+                TcProb p{};
+                p.a_row0 = pr.a * ld1;
+                p.a_k0 = 0;
+                p.b_row0 = k * ld2;
+                p.b_k0 = 0;
+                p.M = 3 * pr.na;
+                p.N = 3 * pr.nb;
+                p.K = pr.na * rep;
+                p.row_off = off1[pr.a];
+                p.col_off = off2[pr.b];
+                p.diag = (symmetric && pr.a == pr.b) ? 1 : 0;
+                p.alpha = 1.0;
+                tprobs.push_back(p);
+            }
+            TcOperand A, B;
+            A.hi = jth.ptr;
+            A.lo = jtl.ptr;
+            A.rows = (long long)s1.v.nm * ld1;
+            A.cols = (long long)ma1 * rep;
+            B.hi = yth.ptr;
+            B.lo = ytl.ptr;
+            B.rows = (long long)np * ld2;
+            B.cols = (long long)ma1 * rep;
+            KFB_TRY(tc_gemm_grouped(A, B, 3, false, tprobs, sink, s));
+            continue;
+        }
         std::vector<GemmProb> probs;
         probs.reserve(np);
         for (int k = 0; k < np; ++k) {
@@ -411,12 +501,12 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
 }
 
 template kfb_status jacobian_core<double>(const DerivSet &, const DerivSet &, int, double,
-                                          double, ElemSink, cudaStream_t);
+                                          double, bool, ElemSink, cudaStream_t);
 template kfb_status jacobian_core<float>(const DerivSet &, const DerivSet &, int, double, double,
-                                         ElemSink, cudaStream_t);
+                                         bool, ElemSink, cudaStream_t);
 template kfb_status hessian_core<double>(const DerivSet &, const DerivSet &, int, double, bool,
-                                         ElemSink, cudaStream_t);
+                                         bool, ElemSink, cudaStream_t);
 template kfb_status hessian_core<float>(const DerivSet &, const DerivSet &, int, double, bool,
-                                        ElemSink, cudaStream_t);
+                                        bool, ElemSink, cudaStream_t);
 
 }  // namespace kfb

@@ -73,12 +73,14 @@ __device__ __forceinline__ void sink_store(const ElemSink &s, long long R, long 
     }
 }
 
+// tc: run the contraction GEMMs on the tensor cores (split fp16, three
+// products); needs rep % 16 == 0 and an sm_100 device.
 template <class T>
 kfb_status jacobian_core(const DerivSet &outer, const DerivSet &inner, int rep, double sigma,
-                         double alpha, ElemSink sink, cudaStream_t s);
+                         double alpha, bool tc, ElemSink sink, cudaStream_t s);
 
 template <class T>
 kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double sigma,
-                        bool symmetric, ElemSink sink, cudaStream_t s);
+                        bool symmetric, bool tc, ElemSink sink, cudaStream_t s);
 
 }  // namespace kfb

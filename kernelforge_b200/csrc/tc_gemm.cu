@@ -1,0 +1,439 @@
+// Grouped tcgen05 GEMM: C = A . B^T for a list of problems whose operands are
+// row blocks / column windows of two K-major 2-D arrays, written through an
+// ElemSink (dense, transposed or symmetric / RFP output).
+//
+// Operands are fp16 (or bf16) arrays; with NPROD = 3 each operand is a split
+// pair x = hi + lo and the MMA issuer accumulates hi*hi + hi*lo + lo*hi (about
+// 22 significant bits per operand, FP32 accumulation in TMEM).  Roles as in the
+// scalar kernel: warp 0 TMA producer, warp 1 MMA issuer, warp 2 TMEM
+// allocator, warps 4..11 epilogue (two per TMEM lane quadrant).  One persistent
+// CTA per SM walks the tile list (problem, m0, n0).  All waits are bounded.
+//
+// Used for the Jacobian contraction (V . J^T per inner molecule) and the
+// Hessian contraction (J_a^T . Y per molecule pair), which are the FLOP-heavy
+// parts of src/local_kernels.cpp:791-974 and :1171-1900.
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <mutex>
+
+#include "derivs.h"
+#include "tc_common.cuh"
+#include "tc_gemm.h"
+
+namespace kfb {
+
+namespace {
+
+using namespace tc;
+
+constexpr int BM = 128, BN = 128, BK = 64;
+constexpr int TILE_A = BM * BK * 2, TILE_B = BN * BK * 2;
+constexpr int EPI_WARP0 = 4, NUM_EPI_WARPS = 8;
+constexpr int NUM_THREADS = 32 * (EPI_WARP0 + NUM_EPI_WARPS);
+constexpr int TMEM_COLS = 2 * BN;
+constexpr int STAGE_BUDGET = 196608;
+
+template <int NPROD>
+struct Cfg {
+    static constexpr int NOP = NPROD == 3 ? 2 : 1;  // arrays per operand
+    static constexpr int STAGE = NOP * (TILE_A + TILE_B);
+    static constexpr int NSTAGE = STAGE_BUDGET / STAGE > 6 ? 6 : STAGE_BUDGET / STAGE;
+    static constexpr int OFF_BARS = NSTAGE * STAGE;
+    static constexpr int NBARS = 2 * NSTAGE + 5;
+    static constexpr int OFF_TMEM = OFF_BARS + NBARS * 8;
+    static constexpr int SMEM = OFF_TMEM + 16 + 1024;
+};
+
+constexpr unsigned long long WAIT_LIMIT_NS = 2000000000ull;
+
+__device__ __forceinline__ bool wait_bar(uint32_t bar, uint32_t parity, int *err) {
+    for (int i = 0; i < 64; ++i)
+        if (mbar_try(bar, parity)) return true;
+    const unsigned long long t0 = globaltimer();
+    while (true) {
+        if (mbar_try(bar, parity)) return true;
+        if (*(volatile int *)err != 0) return false;
+        if (globaltimer() - t0 > WAIT_LIMIT_NS) {
+            atomicExch(err, 1);
+            return false;
+        }
+    }
+}
+
+template <int NPROD>
+__global__ void __launch_bounds__(NUM_THREADS, 1)
+    tc_gemm_kernel(const __grid_constant__ CUtensorMap ta_hi, const __grid_constant__ CUtensorMap ta_lo,
+                   const __grid_constant__ CUtensorMap tb_hi, const __grid_constant__ CUtensorMap tb_lo,
+                   const TcProb *__restrict__ probs, const TcTile *__restrict__ tiles, int ntiles,
+                   uint32_t idesc, ElemSink sink, int *err) {
+    using C = Cfg<NPROD>;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t s_base = smem_u32(smem);
+    const uint32_t bar0 = s_base + C::OFF_BARS;
+    auto full_bar = [&](int s) { return bar0 + 8u * s; };
+    auto empty_bar = [&](int s) { return bar0 + 8u * (C::NSTAGE + s); };
+    auto tfull_bar = [&](int a) { return bar0 + 8u * (2 * C::NSTAGE + a); };
+    auto tempty_bar = [&](int a) { return bar0 + 8u * (2 * C::NSTAGE + 2 + a); };
+    const uint32_t done_bar = bar0 + 8u * (2 * C::NSTAGE + 4);
+    uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(smem + C::OFF_TMEM);
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < C::NSTAGE; ++s) {
+            mbar_init(full_bar(s), 1);
+            mbar_init(empty_bar(s), 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(tfull_bar(a), 1);
+            mbar_init(tempty_bar(a), NUM_EPI_WARPS);
+        }
+        mbar_init(done_bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 2) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_holder)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_holder;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t ph = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+                const TcTile tl = tiles[t];
+                const TcProb pb = probs[tl.prob];
+                const int nkb = (pb.K + BK - 1) / BK;
+                for (int kb = 0; kb < nkb; ++kb) {
+                    if (!wait_bar(empty_bar(stage), ph ^ 1u, err)) {
+                        ok = false;
+                        break;
+                    }
+                    const uint32_t sa = s_base + stage * C::STAGE;
+                    mbar_expect_tx(full_bar(stage), C::STAGE);
+                    const int xa = pb.a_k0 + kb * BK, xb = pb.b_k0 + kb * BK;
+                    tma_load_2d(sa, &ta_hi, xa, pb.a_row0 + tl.m0, full_bar(stage));
+                    tma_load_2d(sa + C::NOP * TILE_A, &tb_hi, xb, pb.b_row0 + tl.n0,
+                                full_bar(stage));
+                    if (NPROD == 3) {
+                        tma_load_2d(sa + TILE_A, &ta_lo, xa, pb.a_row0 + tl.m0, full_bar(stage));
+                        tma_load_2d(sa + 2 * TILE_A + TILE_B, &tb_lo, xb, pb.b_row0 + tl.n0,
+                                    full_bar(stage));
+                    }
+                    if (++stage == C::NSTAGE) {
+                        stage = 0;
+                        ph ^= 1u;
+                    }
+                }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            int stage = 0, acc = 0;
+            uint32_t ph = 0, aph = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+                const TcProb pb = probs[tiles[t].prob];
+                const int nkb = (pb.K + BK - 1) / BK;
+                if (!wait_bar(tempty_bar(acc), aph ^ 1u, err)) break;
+                tc_fence_after();
+                const uint32_t dtm = tmem_base + (uint32_t)(acc * BN);
+                for (int kb = 0; kb < nkb; ++kb) {
+                    if (!wait_bar(full_bar(stage), ph, err)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t sa = s_base + stage * C::STAGE;
+                    const int nks = min(BK / 16, (pb.K - kb * BK) / 16);
+                    for (int ks = 0; ks < nks; ++ks) {
+                        const uint64_t ahi = sdesc(sa + ks * 32);
+                        const uint64_t bhi = sdesc(sa + C::NOP * TILE_A + ks * 32);
+                        umma_f16_idesc(dtm, ahi, bhi, idesc, (kb | ks) != 0 ? 1u : 0u);
+                        if (NPROD == 3) {
+                            const uint64_t alo = sdesc(sa + TILE_A + ks * 32);
+                            const uint64_t blo = sdesc(sa + 2 * TILE_A + TILE_B + ks * 32);
+                            umma_f16_idesc(dtm, ahi, blo, idesc, 1u);
+                            umma_f16_idesc(dtm, alo, bhi, idesc, 1u);
+                        }
+                    }
+                    umma_commit(empty_bar(stage));
+                    if (++stage == C::NSTAGE) {
+                        stage = 0;
+                        ph ^= 1u;
+                    }
+                }
+                if (!ok) break;
+                umma_commit(tfull_bar(acc));
+                if (++acc == 2) {
+                    acc = 0;
+                    aph ^= 1u;
+                }
+            }
+            umma_commit(done_bar);
+            wait_bar(done_bar, 0, err);
+        }
+    } else if (warp >= EPI_WARP0) {
+        const int q = warp & 3;
+        const int h = (warp - EPI_WARP0) >> 2;  // column half
+        int acc = 0;
+        uint32_t aph = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+            const TcTile tl = tiles[t];
+            const TcProb pb = probs[tl.prob];
+            const bool got = wait_bar(tfull_bar(acc), aph, err);
+            if (!__all_sync(0xffffffffu, got)) break;
+            tc_fence_after();
+            const int m = tl.m0 + q * 32 + lane;
+            const uint32_t tbase = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN);
+#pragma unroll 1
+            for (int cc = 0; cc < BN / 64; ++cc) {
+                const int c = h * (BN / 64) + cc;
+                float v[32];
+                tmem_ld32(tbase + (uint32_t)(c * 32), v);
+                if (m < pb.M) {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const int n = tl.n0 + c * 32 + j;
+                        if (n < pb.N)
+                            sink_store(sink, pb.row_off + m, pb.col_off + n,
+                                       (double)v[j] * pb.alpha, pb.diag);
+                    }
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(tempty_bar(acc));
+            if (++acc == 2) {
+                acc = 0;
+                aph ^= 1u;
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 2) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
+                     "r"(TMEM_COLS)
+                     : "memory");
+    }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+kfb_status map2d(CUtensorMap *m, const void *ptr, long long rows, long long cols, int box_rows,
+                 bool bf16) {
+    auto enc = encoder();
+    if (!enc) return set_error(KFB_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    if (cols % 8 != 0) return set_error(KFB_ERR_INVALID_ARG, "TMA operand rows must be 16-byte multiples");
+    cuuint64_t gdim[2] = {(cuuint64_t)cols, (cuuint64_t)std::max<long long>(rows, 1)};
+    cuuint64_t gstride[1] = {(cuuint64_t)cols * 2};
+    cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(m, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16,
+                     2, const_cast<void *>(ptr), gdim, gstride, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_error(KFB_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return KFB_OK;
+}
+
+template <int NPROD>
+kfb_status launch(const TcOperand &A, const TcOperand &B, bool bf16,
+                  const std::vector<TcProb> &probs, const ElemSink &sink, cudaStream_t s) {
+    using C = Cfg<NPROD>;
+    std::vector<TcTile> tiles;
+    for (int p = 0; p < (int)probs.size(); ++p) {
+        const TcProb &pb = probs[p];
+        if (pb.K % 16 != 0 || pb.a_k0 % 8 != 0 || pb.b_k0 % 8 != 0)
+            return set_error(KFB_ERR_INVALID_ARG, "tc_gemm: K and column offsets must be multiples of 16 / 8");
+        for (int m0 = 0; m0 < pb.M; m0 += BM)
+            for (int n0 = 0; n0 < pb.N; n0 += BN) tiles.push_back(TcTile{p, m0, n0, 0});
+    }
+    if (tiles.empty()) return KFB_OK;
+    CUtensorMap ma_hi, ma_lo, mb_hi, mb_lo;
+    KFB_TRY(map2d(&ma_hi, A.hi, A.rows, A.cols, BM, bf16));
+    KFB_TRY(map2d(&mb_hi, B.hi, B.rows, B.cols, BN, bf16));
+    if (NPROD == 3) {
+        KFB_TRY(map2d(&ma_lo, A.lo, A.rows, A.cols, BM, bf16));
+        KFB_TRY(map2d(&mb_lo, B.lo, B.rows, B.cols, BN, bf16));
+    } else {
+        ma_lo = ma_hi;
+        mb_lo = mb_hi;
+    }
+    DevBuf dp, dt, derr;
+    KFB_TRY(upload(dp, probs, s));
+    KFB_TRY(upload(dt, tiles, s));
+    KFB_TRY(derr.alloc(sizeof(int), s));
+    KFB_TRY(zero(derr.ptr, sizeof(int), s));
+    static bool attr = false;
+    if (!attr) {
+        KFB_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_kernel<NPROD>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
+        attr = true;
+    }
+    const int grid = std::min((int)tiles.size(), device_sm_count());
+    const uint32_t idesc = make_idesc(BM, BN, bf16 ? 1 : 0);
+    tc_gemm_kernel<NPROD><<<grid, NUM_THREADS, C::SMEM, s>>>(
+        ma_hi, ma_lo, mb_hi, mb_lo, dp.as<TcProb>(), dt.as<TcTile>(), (int)tiles.size(), idesc,
+        sink, derr.as<int>());
+    KFB_CUDA_TRY(cudaGetLastError());
+    int herr = 0;
+    KFB_CUDA_TRY(cudaMemcpyAsync(&herr, derr.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
+    KFB_CUDA_TRY(cudaStreamSynchronize(s));
+    if (herr) return set_error(KFB_ERR_TIMEOUT, "tensor-core GEMM: a pipeline wait timed out");
+    return KFB_OK;
+}
+
+// ---------------------------------------------------------------- packing
+template <class T>
+__global__ void split_rows_kernel(const T *__restrict__ src, long long n, __half *__restrict__ hi,
+                                  __half *__restrict__ lo) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const float v = (float)src[i];
+        const __half h = __float2half_rn(v);
+        hi[i] = h;
+        lo[i] = __float2half_rn(v - __half2float(h));
+    }
+}
+
+// Jt[(m, c)][(j, k)] = dX[m][j][k][c] for c < 3 ma (zero rows and columns
+// beyond the molecule's atoms are copied as they are: the padding is zero).
+// Tiles of 32 (j,k) x 32 c through shared memory.
+template <class T>
+__global__ void transpose_split_dx_kernel(const T *__restrict__ dx, int ma, int rep,
+                                          __half *__restrict__ hi, __half *__restrict__ lo) {
+    __shared__ float tile[32][33];
+    const int m = blockIdx.z;
+    const int ld = 3 * ma;
+    const long long kk_total = (long long)ma * rep;
+    const long long kk0 = (long long)blockIdx.x * 32;
+    const int c0 = blockIdx.y * 32;
+    const T *base = dx + (size_t)m * kk_total * ld;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const long long kk = kk0 + r;
+        const int c = c0 + threadIdx.x;
+        tile[r][threadIdx.x] = (kk < kk_total && c < ld) ? (float)base[kk * ld + c] : 0.f;
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int c = c0 + r;
+        const long long kk = kk0 + threadIdx.x;
+        if (c < ld && kk < kk_total) {
+            const float v = tile[threadIdx.x][r];
+            const __half h = __float2half_rn(v);
+            const size_t o = ((size_t)m * ld + c) * kk_total + kk;
+            hi[o] = h;
+            lo[o] = __float2half_rn(v - __half2float(h));
+        }
+    }
+}
+
+// Yt[(p, c)][(i, k)] = Y[p][i][k][c], Y with row stride ld (the Hessian's
+// per-pair Y blocks, ma1 x rep x ld each).
+template <class T>
+__global__ void transpose_split_y_kernel(const T *__restrict__ Y, int ma1, int rep, int ld,
+                                         __half *__restrict__ hi, __half *__restrict__ lo) {
+    __shared__ float tile[32][33];
+    const int p = blockIdx.z;
+    const long long kk_total = (long long)ma1 * rep;
+    const long long kk0 = (long long)blockIdx.x * 32;
+    const int c0 = blockIdx.y * 32;
+    const T *base = Y + (size_t)p * kk_total * ld;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const long long kk = kk0 + r;
+        const int c = c0 + threadIdx.x;
+        tile[r][threadIdx.x] = (kk < kk_total && c < ld) ? (float)base[kk * ld + c] : 0.f;
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int c = c0 + r;
+        const long long kk = kk0 + threadIdx.x;
+        if (c < ld && kk < kk_total) {
+            const float v = tile[threadIdx.x][r];
+            const __half h = __float2half_rn(v);
+            const size_t o = ((size_t)p * ld + c) * kk_total + kk;
+            hi[o] = h;
+            lo[o] = __float2half_rn(v - __half2float(h));
+        }
+    }
+}
+
+}  // namespace
+
+kfb_status tc_gemm_grouped(const TcOperand &A, const TcOperand &B, int nprod, bool bf16,
+                           const std::vector<TcProb> &probs, const ElemSink &sink,
+                           cudaStream_t s) {
+    if (!device_is_sm100())
+        return set_error(KFB_ERR_UNSUPPORTED, "tensor-core GEMM needs an sm_100 (B200) device");
+    if (nprod == 3) return launch<3>(A, B, bf16, probs, sink, s);
+    return launch<1>(A, B, bf16, probs, sink, s);
+}
+
+template <class T>
+kfb_status split_rows(const T *src, long long n, __half *hi, __half *lo, cudaStream_t s) {
+    if (n <= 0) return KFB_OK;
+    const unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 148LL * 64);
+    split_rows_kernel<T><<<blocks, 256, 0, s>>>(src, n, hi, lo);
+    KFB_CUDA_TRY(cudaGetLastError());
+    return KFB_OK;
+}
+
+template <class T>
+kfb_status transpose_split_dx(const T *dx, int nm, int ma, int rep, __half *hi, __half *lo,
+                              cudaStream_t s) {
+    if (nm <= 0) return KFB_OK;
+    const long long kk = (long long)ma * rep;
+    dim3 grid((unsigned)((kk + 31) / 32), (unsigned)((3 * ma + 31) / 32), (unsigned)nm);
+    transpose_split_dx_kernel<T><<<grid, dim3(32, 8), 0, s>>>(dx, ma, rep, hi, lo);
+    KFB_CUDA_TRY(cudaGetLastError());
+    return KFB_OK;
+}
+
+template <class T>
+kfb_status transpose_split_y(const T *Y, int np, int ma1, int rep, int ld, __half *hi, __half *lo,
+                             cudaStream_t s) {
+    if (np <= 0) return KFB_OK;
+    const long long kk = (long long)ma1 * rep;
+    dim3 grid((unsigned)((kk + 31) / 32), (unsigned)((ld + 31) / 32), (unsigned)np);
+    transpose_split_y_kernel<T><<<grid, dim3(32, 8), 0, s>>>(Y, ma1, rep, ld, hi, lo);
+    KFB_CUDA_TRY(cudaGetLastError());
+    return KFB_OK;
+}
+
+template kfb_status split_rows<float>(const float *, long long, __half *, __half *, cudaStream_t);
+template kfb_status split_rows<double>(const double *, long long, __half *, __half *, cudaStream_t);
+template kfb_status transpose_split_dx<float>(const float *, int, int, int, __half *, __half *,
+                                              cudaStream_t);
+template kfb_status transpose_split_dx<double>(const double *, int, int, int, __half *, __half *,
+                                               cudaStream_t);
+template kfb_status transpose_split_y<float>(const float *, int, int, int, int, __half *,
+                                             __half *, cudaStream_t);
+template kfb_status transpose_split_y<double>(const double *, int, int, int, int, __half *,
+                                              __half *, cudaStream_t);
+
+}  // namespace kfb

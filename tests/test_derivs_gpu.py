@@ -85,3 +85,31 @@ def test_full_symm_is_symmetric_and_matches_asym():
     np.testing.assert_allclose(F, F.T, rtol=1e-12, atol=1e-12)
     Fa = lk.kernel_gaussian_full(X, dX, X, dX, Q, Q, N, N, 2.0)
     np.testing.assert_allclose(F, Fa, rtol=1e-10, atol=1e-10)
+
+
+@pytest.mark.parametrize("rep", [48, 720])
+def test_tensor_core_contractions_match_oracle(rep):
+    """precision='split_f16' runs the Jacobian and Hessian contraction GEMMs on
+    the tcgen05 tensor cores (rep a multiple of 16): FP32-level agreement."""
+    from kernelforge_b200 import local_kernels as lk
+    X1, dX1, Q1, N1 = make_set(7, 6, rep, 3, 21)
+    X2, dX2, Q2, N2 = make_set(5, 6, rep, 3, 22)
+    sc = 1.0 / np.sqrt(rep)
+    X1 *= 2 * sc
+    X2 *= 2 * sc
+    dX1 *= sc
+    dX2 *= sc
+    s = 2.0
+    p = "split_f16"
+    close(lk.kernel_gaussian_jacobian(X1, X2, dX2, Q1, Q2, N1, N2, s, precision=p),
+          o.kernel_gaussian_jacobian(X1, X2, dX2, Q1, Q2, N1, N2, s), p)
+    close(lk.kernel_gaussian_jacobian_t(X1, dX1, X2, Q1, Q2, N1, N2, s, precision=p),
+          o.kernel_gaussian_jacobian_t(X1, dX1, X2, Q1, Q2, N1, N2, s), p)
+    close(lk.kernel_gaussian_hessian(X1, dX1, X2, dX2, Q1, Q2, N1, N2, s, precision=p),
+          o.kernel_gaussian_hessian(X1, dX1, X2, dX2, Q1, Q2, N1, N2, s), p)
+    close(lk.kernel_gaussian_hessian_symm_rfp(X1, dX1, Q1, N1, s, precision=p),
+          o.kernel_gaussian_hessian_symm_rfp(X1, dX1, Q1, N1, s), p)
+    close(lk.kernel_gaussian_full_symm_rfp(X1, dX1, Q1, N1, s, precision=p),
+          o.kernel_gaussian_full_symm_rfp(X1, dX1, Q1, N1, s), p)
+    close(lk.kernel_gaussian_full(X1, dX1, X2, dX2, Q1, Q2, N1, N2, s, precision=p),
+          o.kernel_gaussian_full(X1, dX1, X2, dX2, Q1, Q2, N1, N2, s), p)
