@@ -297,6 +297,7 @@ kfb_status jacobian_core(const DerivSet &outer, const DerivSet &inner, int rep, 
     int chunk = (int)std::max<size_t>(1, budget_bytes() / std::max<size_t>(row_bytes, 1));
     chunk = std::min(chunk, outer.v.nm);
     DevBuf V, vh, vl, jth, jtl;
+    float jt_scale = 1.f;
     KFB_TRY(V.alloc((size_t)chunk * NU * rep * sizeof(T), s));
     const int ma_in = inner.v.ma;
     if (tc) {
@@ -305,7 +306,7 @@ kfb_status jacobian_core(const DerivSet &outer, const DerivSet &inner, int rep, 
         KFB_TRY(jth.alloc(jt_elems * sizeof(__half), s));
         KFB_TRY(jtl.alloc(jt_elems * sizeof(__half), s));
         KFB_TRY(transpose_split_dx<T>(static_cast<const T *>(inner.dx), inner.v.nm, ma_in, rep,
-                                      jth.as<__half>(), jtl.as<__half>(), s));
+                                      jth.as<__half>(), jtl.as<__half>(), &jt_scale, s));
         KFB_TRY(vh.alloc((size_t)chunk * NU * rep * sizeof(__half), s));
         KFB_TRY(vl.alloc((size_t)chunk * NU * rep * sizeof(__half), s));
     }
@@ -322,8 +323,9 @@ kfb_status jacobian_core(const DerivSet &outer, const DerivSet &inner, int rep, 
             c2, is2, V.as<T>());
         KFB_CUDA_TRY(cudaGetLastError());
         if (tc) {
+            float v_scale = 1.f;
             KFB_TRY(split_rows<T>(V.as<T>(), (long long)nout * NU * rep, vh.as<__half>(),
-                                  vl.as<__half>(), s));
+                                  vl.as<__half>(), &v_scale, s));
             std::vector<TcProb> tprobs;
             for (int m = 0; m < inner.v.nm; ++m) {
                 const int nb = inner.v.natoms(m);
@@ -339,7 +341,7 @@ kfb_status jacobian_core(const DerivSet &outer, const DerivSet &inner, int rep, 
                 p.row_off = o0;
                 p.col_off = in_offs[m];
                 p.diag = 0;
-                p.alpha = alpha;
+                p.alpha = alpha / ((double)v_scale * (double)jt_scale);
                 tprobs.push_back(p);
             }
             TcOperand A, B;
@@ -417,13 +419,14 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
     KFB_TRY(Y.alloc((size_t)batch * ma1 * rep * ld2 * sizeof(T), s));
     KFB_TRY(dpairs.alloc((size_t)batch * sizeof(HessPair), s));
     DevBuf jth, jtl, yth, ytl;
+    float jt_scale = 1.f;
     if (tc) {
         // set-1 Jacobians as K-major split rows Jt[(a, c)][(i, k)]
         const size_t jt_elems = (size_t)s1.v.nm * ld1 * ma1 * rep;
         KFB_TRY(jth.alloc(jt_elems * sizeof(__half), s));
         KFB_TRY(jtl.alloc(jt_elems * sizeof(__half), s));
         KFB_TRY(transpose_split_dx<T>(static_cast<const T *>(s1.dx), s1.v.nm, ma1, rep,
-                                      jth.as<__half>(), jtl.as<__half>(), s));
+                                      jth.as<__half>(), jtl.as<__half>(), &jt_scale, s));
         KFB_TRY(yth.alloc((size_t)batch * ld2 * ma1 * rep * sizeof(__half), s));
         KFB_TRY(ytl.alloc((size_t)batch * ld2 * ma1 * rep * sizeof(__half), s));
     }
@@ -444,8 +447,9 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
             Y.as<T>());
         KFB_CUDA_TRY(cudaGetLastError());
         if (tc) {
+            float y_scale = 1.f;
             KFB_TRY(transpose_split_y<T>(Y.as<T>(), np, ma1, rep, ld2, yth.as<__half>(),
-                                         ytl.as<__half>(), s));
+                                         ytl.as<__half>(), &y_scale, s));
             std::vector<TcProb> tprobs;
             tprobs.reserve(np);
             for (int k = 0; k < np; ++k) {
@@ -461,7 +465,7 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
                 p.row_off = off1[pr.a];
                 p.col_off = off2[pr.b];
                 p.diag = (symmetric && pr.a == pr.b) ? 1 : 0;
-                p.alpha = 1.0;
+                p.alpha = 1.0 / ((double)jt_scale * (double)y_scale);
                 tprobs.push_back(p);
             }
             TcOperand A, B;

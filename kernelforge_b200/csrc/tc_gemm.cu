@@ -310,11 +310,22 @@ kfb_status launch(const TcOperand &A, const TcOperand &B, bool bf16,
 
 // ---------------------------------------------------------------- packing
 template <class T>
-__global__ void split_rows_kernel(const T *__restrict__ src, long long n, __half *__restrict__ hi,
-                                  __half *__restrict__ lo) {
+__global__ void absmax_kernel(const T *__restrict__ src, long long n, float *out) {
+    float m = 0.f;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        m = fmaxf(m, fabsf((float)src[i]));
+    for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    // non-negative floats order like their bit patterns
+    if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<int *>(out), __float_as_int(m));
+}
+
+template <class T>
+__global__ void split_rows_kernel(const T *__restrict__ src, long long n, float scale,
+                                  __half *__restrict__ hi, __half *__restrict__ lo) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
-        const float v = (float)src[i];
+        const float v = (float)src[i] * scale;
         const __half h = __float2half_rn(v);
         hi[i] = h;
         lo[i] = __float2half_rn(v - __half2float(h));
@@ -325,7 +336,7 @@ __global__ void split_rows_kernel(const T *__restrict__ src, long long n, __half
 // beyond the molecule's atoms are copied as they are: the padding is zero).
 // Tiles of 32 (j,k) x 32 c through shared memory.
 template <class T>
-__global__ void transpose_split_dx_kernel(const T *__restrict__ dx, int ma, int rep,
+__global__ void transpose_split_dx_kernel(const T *__restrict__ dx, int ma, int rep, float scale,
                                           __half *__restrict__ hi, __half *__restrict__ lo) {
     __shared__ float tile[32][33];
     const int m = blockIdx.z;
@@ -344,7 +355,7 @@ __global__ void transpose_split_dx_kernel(const T *__restrict__ dx, int ma, int 
         const int c = c0 + r;
         const long long kk = kk0 + threadIdx.x;
         if (c < ld && kk < kk_total) {
-            const float v = tile[threadIdx.x][r];
+            const float v = tile[threadIdx.x][r] * scale;
             const __half h = __float2half_rn(v);
             const size_t o = ((size_t)m * ld + c) * kk_total + kk;
             hi[o] = h;
@@ -357,7 +368,8 @@ __global__ void transpose_split_dx_kernel(const T *__restrict__ dx, int ma, int 
 // per-pair Y blocks, ma1 x rep x ld each).
 template <class T>
 __global__ void transpose_split_y_kernel(const T *__restrict__ Y, int ma1, int rep, int ld,
-                                         __half *__restrict__ hi, __half *__restrict__ lo) {
+                                         float scale, __half *__restrict__ hi,
+                                         __half *__restrict__ lo) {
     __shared__ float tile[32][33];
     const int p = blockIdx.z;
     const long long kk_total = (long long)ma1 * rep;
@@ -374,7 +386,7 @@ __global__ void transpose_split_y_kernel(const T *__restrict__ Y, int ma1, int r
         const int c = c0 + r;
         const long long kk = kk0 + threadIdx.x;
         if (c < ld && kk < kk_total) {
-            const float v = tile[threadIdx.x][r];
+            const float v = tile[threadIdx.x][r] * scale;
             const __half h = __float2half_rn(v);
             const size_t o = ((size_t)p * ld + c) * kk_total + kk;
             hi[o] = h;
@@ -394,46 +406,72 @@ kfb_status tc_gemm_grouped(const TcOperand &A, const TcOperand &B, int nprod, bo
     return launch<1>(A, B, bf16, probs, sink, s);
 }
 
+// Power of two that brings the largest |value| to about 2^14: keeps the hi/lo
+// fp16 pair out of fp16's subnormal range for the small entries (the pair
+// then carries ~22 significant bits over ~28 binades below the maximum).
 template <class T>
-kfb_status split_rows(const T *src, long long n, __half *hi, __half *lo, cudaStream_t s) {
+kfb_status pow2_scale(const T *src, long long n, cudaStream_t s, float *scale) {
+    *scale = 1.f;
+    if (n <= 0) return KFB_OK;
+    DevBuf d;
+    KFB_TRY(d.alloc(sizeof(float), s));
+    KFB_TRY(zero(d.ptr, sizeof(float), s));
+    const unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 148LL * 16);
+    absmax_kernel<T><<<blocks, 256, 0, s>>>(src, n, d.as<float>());
+    KFB_CUDA_TRY(cudaGetLastError());
+    float m = 0.f;
+    KFB_CUDA_TRY(cudaMemcpyAsync(&m, d.ptr, sizeof(float), cudaMemcpyDeviceToHost, s));
+    KFB_CUDA_TRY(cudaStreamSynchronize(s));
+    if (m > 0.f && std::isfinite(m)) *scale = std::ldexp(1.f, 14 - (int)std::ceil(std::log2(m)));
+    return KFB_OK;
+}
+
+template <class T>
+kfb_status split_rows(const T *src, long long n, __half *hi, __half *lo, float *scale,
+                      cudaStream_t s) {
+    KFB_TRY(pow2_scale(src, n, s, scale));
     if (n <= 0) return KFB_OK;
     const unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 148LL * 64);
-    split_rows_kernel<T><<<blocks, 256, 0, s>>>(src, n, hi, lo);
+    split_rows_kernel<T><<<blocks, 256, 0, s>>>(src, n, *scale, hi, lo);
     KFB_CUDA_TRY(cudaGetLastError());
     return KFB_OK;
 }
 
 template <class T>
 kfb_status transpose_split_dx(const T *dx, int nm, int ma, int rep, __half *hi, __half *lo,
-                              cudaStream_t s) {
-    if (nm <= 0) return KFB_OK;
+                              float *scale, cudaStream_t s) {
     const long long kk = (long long)ma * rep;
+    KFB_TRY(pow2_scale(dx, (long long)nm * kk * 3 * ma, s, scale));
+    if (nm <= 0) return KFB_OK;
     dim3 grid((unsigned)((kk + 31) / 32), (unsigned)((3 * ma + 31) / 32), (unsigned)nm);
-    transpose_split_dx_kernel<T><<<grid, dim3(32, 8), 0, s>>>(dx, ma, rep, hi, lo);
+    transpose_split_dx_kernel<T><<<grid, dim3(32, 8), 0, s>>>(dx, ma, rep, *scale, hi, lo);
     KFB_CUDA_TRY(cudaGetLastError());
     return KFB_OK;
 }
 
 template <class T>
 kfb_status transpose_split_y(const T *Y, int np, int ma1, int rep, int ld, __half *hi, __half *lo,
-                             cudaStream_t s) {
-    if (np <= 0) return KFB_OK;
+                             float *scale, cudaStream_t s) {
     const long long kk = (long long)ma1 * rep;
+    KFB_TRY(pow2_scale(Y, (long long)np * kk * ld, s, scale));
+    if (np <= 0) return KFB_OK;
     dim3 grid((unsigned)((kk + 31) / 32), (unsigned)((ld + 31) / 32), (unsigned)np);
-    transpose_split_y_kernel<T><<<grid, dim3(32, 8), 0, s>>>(Y, ma1, rep, ld, hi, lo);
+    transpose_split_y_kernel<T><<<grid, dim3(32, 8), 0, s>>>(Y, ma1, rep, ld, *scale, hi, lo);
     KFB_CUDA_TRY(cudaGetLastError());
     return KFB_OK;
 }
 
-template kfb_status split_rows<float>(const float *, long long, __half *, __half *, cudaStream_t);
-template kfb_status split_rows<double>(const double *, long long, __half *, __half *, cudaStream_t);
+template kfb_status split_rows<float>(const float *, long long, __half *, __half *, float *,
+                                      cudaStream_t);
+template kfb_status split_rows<double>(const double *, long long, __half *, __half *, float *,
+                                       cudaStream_t);
 template kfb_status transpose_split_dx<float>(const float *, int, int, int, __half *, __half *,
-                                              cudaStream_t);
+                                              float *, cudaStream_t);
 template kfb_status transpose_split_dx<double>(const double *, int, int, int, __half *, __half *,
-                                               cudaStream_t);
+                                               float *, cudaStream_t);
 template kfb_status transpose_split_y<float>(const float *, int, int, int, int, __half *,
-                                             __half *, cudaStream_t);
+                                             __half *, float *, cudaStream_t);
 template kfb_status transpose_split_y<double>(const double *, int, int, int, int, __half *,
-                                              __half *, cudaStream_t);
+                                              __half *, float *, cudaStream_t);
 
 }  // namespace kfb

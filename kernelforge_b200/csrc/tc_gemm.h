@@ -36,13 +36,17 @@ kfb_status tc_gemm_grouped(const TcOperand &A, const TcOperand &B, int nprod, bo
                            const std::vector<TcProb> &probs, const ElemSink &sink,
                            cudaStream_t s);
 
+// Split packers: multiply by a power-of-two scale (returned in *scale; the
+// largest magnitude lands near 2^14) and write the fp16 pair hi = fp16(v),
+// lo = fp16(v - hi).  GEMM results are divided by the two operands' scales.
 template <class T>
-kfb_status split_rows(const T *src, long long n, __half *hi, __half *lo, cudaStream_t s);
+kfb_status split_rows(const T *src, long long n, __half *hi, __half *lo, float *scale,
+                      cudaStream_t s);
 template <class T>
 kfb_status transpose_split_dx(const T *dx, int nm, int ma, int rep, __half *hi, __half *lo,
-                              cudaStream_t s);
+                              float *scale, cudaStream_t s);
 template <class T>
 kfb_status transpose_split_y(const T *Y, int np, int ma1, int rep, int ld, __half *hi,
-                             __half *lo, cudaStream_t s);
+                             __half *lo, float *scale, cudaStream_t s);
 
 }  // namespace kfb
