@@ -227,6 +227,81 @@ kfb_status kfb_krr_solve_mixed(const float *k_rfp, const double *y, int n, doubl
                                double *alpha, kfb_solve_info *info, void *stream);
 
 /* ---------------------------------------------------------------------- */
+/* Feature maps summed per molecule and their normal equations             */
+/* ---------------------------------------------------------------------- */
+
+/* Element-stratified random Fourier features, summed per molecule:
+ *   z[m][:] = sum over atoms a of molecule m: sqrt(2/d) cos(x_a . w[e_a] + b[e_a])
+ * q (nm, ma) HOST int32 element INDICES (0 .. nelem-1, -1 = padding, unlike
+ * the nuclear charges of the kernels above); w (nelem, rep, d) and b (nelem, d)
+ * device float32; z (nm, d) device float32, overwritten.  x . w runs on the
+ * tensor cores as split-fp16 products (FP32-class accuracy); rep % 16 == 0.
+ * Replaces rff_features_elemental_cuda (src/cuda_rff_features.hpp:47-53, bound
+ * in src/cuda_rff_features_bindings.cpp:70-80) and the CPU
+ * kf::rff::rff_features_elemental (src/rff_elemental.hpp:20-24). */
+kfb_status kfb_rff_features_elemental(const void *x, const int32_t *q, const int32_t *n, int nm,
+                                      int ma, int rep, const float *w, const float *b, int nelem,
+                                      int d, kfb_dtype x_dt, float *z, void *stream);
+
+/* Normal equations of a linear ridge model on per-molecule features:
+ * ztz = Z^T Z (d x d; KFB_DENSE both triangles, or RFP), zty = Z^T y (float64;
+ * skipped when y is NULL).  z (nm, d) device float32, y (nm,) device float64.
+ * FP32 SYRK without reduced-precision shortcuts.  Replaces the Gramian half of
+ * rff_gramian_elemental_rfp_cuda (src/cuda_rff_features.hpp:85-93; SSFRK +
+ * SGEMV in src/cuda_rff_features.cu:1602-1670). */
+kfb_status kfb_feature_gramian(const float *z, const double *y, int nm, int d, kfb_layout layout,
+                               float *ztz, double *zty, void *stream);
+
+/* Exact local-kernel values of atom pairs, the training targets of the learned
+ * map: out[p] = exp(-|x[pi[p]] - x[pj[p]]|^2 / (2 sigma^2)), x (nrows, rep)
+ * device, pi / pj device int32 row indices (an index outside [0, nrows) gives
+ * KFB_ERR_INVALID_ARG; the kernel checks every index).  The pair term of the scalar
+ * kernel (src/local_kernels.cpp:276-285). */
+kfb_status kfb_pair_gaussian(const void *x, long long nrows, const int32_t *pi,
+                             const int32_t *pj, int npairs, int rep, double sigma, kfb_dtype x_dt,
+                             float *out, void *stream);
+
+/* Learned cos-MLP feature map (no counterpart in the reference; it stands in
+ * for the random Fourier features above).  Per element e:
+ *   phi_e(x) = sqrt(2/d) cos(W2_e cos(W1_e x + b1_e) + b2_e)
+ * W1 (nelem, hidden, rep), b1 (nelem, hidden), W2 (nelem, d, hidden),
+ * b2 (nelem, d): FP32 master copies on the device, BF16 copies feed the tensor
+ * cores (FP32 accumulation).  The handle owns parameters, Adam state and the
+ * workspace of batches of up to max_pairs atom pairs. */
+typedef struct kfb_cosmlp kfb_cosmlp;
+
+kfb_status kfb_cosmlp_create(int nelem, int rep, int hidden, int d, int max_pairs,
+                             kfb_cosmlp **out);
+void kfb_cosmlp_destroy(kfb_cosmlp *h);
+/* Device pointers to the FP32 parameters (write them, then kfb_cosmlp_sync). */
+kfb_status kfb_cosmlp_params(kfb_cosmlp *h, float **w1, float **b1, float **w2, float **b2);
+/* Device pointers to the gradients of the last pair step (one element's
+ * tensors: (hidden, rep), (hidden,), (d, hidden), (d,)). */
+kfb_status kfb_cosmlp_grads(kfb_cosmlp *h, float **w1, float **b1, float **w2, float **b2);
+/* Refresh the BF16 copies from the FP32 parameters; optionally zero the Adam
+ * moments and step counts. */
+kfb_status kfb_cosmlp_sync(kfb_cosmlp *h, int reset_optimizer, void *stream);
+/* Adam state for checkpoints: m[4], v[4] device pointers (same shapes as the
+ * parameters), steps[nelem] host copy of the per-element step counts. */
+kfb_status kfb_cosmlp_optimizer_state(kfb_cosmlp *h, float **m, float **v, int *steps);
+kfb_status kfb_cosmlp_set_steps(kfb_cosmlp *h, const int *steps);
+/* One training step of element elem on npairs pairs: rows pi[p], pj[p] of x
+ * (nrows, rep) device, target (npairs,) device float32; an index outside
+ * [0, nrows) gives KFB_ERR_INVALID_ARG (the gather checks every index).  Loss
+ * mean_p (phi(x_i) . phi(x_j) - target_p)^2 (returned in *loss when not NULL);
+ * gradients are left in the handle; update != 0 applies an Adam step
+ * (beta 0.9 / 0.999, eps 1e-8) with learning rate lr.  Synchronises the stream. */
+kfb_status kfb_cosmlp_pair_step(kfb_cosmlp *h, int elem, const void *x, long long nrows,
+                                kfb_dtype x_dt, const int32_t *pi, const int32_t *pj,
+                                const float *target, int npairs, float lr, int update,
+                                double *loss, void *stream);
+/* Learned features summed per molecule, the analogue of
+ * kfb_rff_features_elemental (same x / q / n conventions): z (nm, d) float32. */
+kfb_status kfb_cosmlp_features_elemental(kfb_cosmlp *h, const void *x, const int32_t *q,
+                                         const int32_t *n, int nm, int ma, int rep,
+                                         kfb_dtype x_dt, float *z, void *stream);
+
+/* ---------------------------------------------------------------------- */
 /* Allocation-free entry point                                             */
 /* ---------------------------------------------------------------------- */
 

@@ -26,7 +26,11 @@ EXPORTS = (
     "kfb_kernel_gaussian_hessian", "kfb_kernel_gaussian_hessian_symm",
     "kfb_kernel_gaussian_full", "kfb_kernel_gaussian_full_symm", "kfb_full_to_rfp",
     "kfb_rfp_to_full", "kfb_rfp_add_diag", "kfb_rfp_potrf", "kfb_rfp_potrs",
-    "kfb_cho_solve_rfp", "kfb_krr_solve_mixed", "kfb_kernel_gaussian_symm_noalloc",
+    "kfb_cho_solve_rfp", "kfb_krr_solve_mixed", "kfb_rff_features_elemental",
+    "kfb_feature_gramian", "kfb_pair_gaussian", "kfb_cosmlp_create", "kfb_cosmlp_destroy",
+    "kfb_cosmlp_params", "kfb_cosmlp_grads", "kfb_cosmlp_sync", "kfb_cosmlp_optimizer_state",
+    "kfb_cosmlp_set_steps", "kfb_cosmlp_pair_step", "kfb_cosmlp_features_elemental",
+    "kfb_kernel_gaussian_symm_noalloc",
 )
 
 
@@ -70,6 +74,21 @@ _SIGS = {
     "kfb_rfp_potrs": (I, [P, P, I, I, I, I, P]),
     "kfb_cho_solve_rfp": (I, [P, P, I, D, I, P, ctypes.POINTER(I), P]),
     "kfb_krr_solve_mixed": (I, [P, P, I, D, I, D, I, I, P, ctypes.POINTER(SolveInfo), P]),
+    "kfb_rff_features_elemental": (I, [P, P, P, I, I, I, P, P, I, I, I, P, P]),
+    "kfb_feature_gramian": (I, [P, P, I, I, I, P, P, P]),
+    "kfb_pair_gaussian": (I, [P, ctypes.c_longlong, P, P, I, I, D, I, P, P]),
+    "kfb_cosmlp_create": (I, [I, I, I, I, I, ctypes.POINTER(P)]),
+    "kfb_cosmlp_destroy": (None, [P]),
+    "kfb_cosmlp_params": (I, [P, ctypes.POINTER(P), ctypes.POINTER(P), ctypes.POINTER(P),
+                              ctypes.POINTER(P)]),
+    "kfb_cosmlp_grads": (I, [P, ctypes.POINTER(P), ctypes.POINTER(P), ctypes.POINTER(P),
+                             ctypes.POINTER(P)]),
+    "kfb_cosmlp_sync": (I, [P, I, P]),
+    "kfb_cosmlp_optimizer_state": (I, [P, P, P, P]),
+    "kfb_cosmlp_set_steps": (I, [P, P]),
+    "kfb_cosmlp_pair_step": (I, [P, I, P, ctypes.c_longlong, I, P, P, P, I, ctypes.c_float, I,
+                                 ctypes.POINTER(D), P]),
+    "kfb_cosmlp_features_elemental": (I, [P, P, P, P, I, I, I, I, P, P]),
     "kfb_kernel_gaussian_symm_noalloc": (I, [P, P, P, I, I, I, D, I, I, P, P]),
 }
 

@@ -15,6 +15,8 @@ kfb_status full_to_rfp(const void *A, int n, kfb_layout uplo, kfb_dtype dt, void
 kfb_status rfp_to_full(const void *arf, int n, kfb_layout uplo, kfb_dtype dt, void *A, cudaStream_t s);
 kfb_status rfp_potrf(void *arf, int n, double l2, kfb_layout uplo, kfb_dtype dt, int *info, cudaStream_t s);
 kfb_status rfp_potrs(const void *arf, void *B, int n, int nrhs, kfb_layout uplo, kfb_dtype dt, cudaStream_t s);
+kfb_status feature_gramian(const float *z, const double *y, int nm, int d, kfb_layout layout,
+                           float *ztz, double *zty, cudaStream_t s);
 kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2, kfb_layout uplo,
                            double tol, int maxit, int flags, double *alpha, kfb_solve_info *info,
                            cudaStream_t s);
@@ -474,6 +476,15 @@ kfb_status kfb_krr_solve_mixed(const float *k_rfp, const double *y, int n, doubl
     if (!(tol > 0.0) || maxit < 0) return set_error(KFB_ERR_INVALID_ARG, "bad tol / maxit");
     return krr_solve_mixed(k_rfp, y, n, l2, uplo, tol, maxit, flags, alpha, info,
                            as_stream(stream));
+}
+
+kfb_status kfb_feature_gramian(const float *z, const double *y, int nm, int d, kfb_layout layout,
+                               float *ztz, double *zty, void *stream) {
+    if (nm <= 0 || d <= 0) return set_error(KFB_ERR_INVALID_ARG, "All dims must be positive.");
+    if (!z || !ztz || (y && !zty)) return set_error(KFB_ERR_INVALID_ARG, "null pointer");
+    if (layout != KFB_DENSE && layout != KFB_RFP_U && layout != KFB_RFP_L)
+        return set_error(KFB_ERR_INVALID_ARG, "layout must be dense or RFP");
+    return feature_gramian(z, y, nm, d, layout, ztz, zty, as_stream(stream));
 }
 
 }  // extern "C"

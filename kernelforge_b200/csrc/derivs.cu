@@ -208,10 +208,11 @@ __global__ void hess_y_kernel(const HessPair *__restrict__ pairs, const T *__res
                               const T *__restrict__ x2, const T *__restrict__ dx2, int ma1,
                               int ma2, int rep, const T *__restrict__ W,
                               const T *__restrict__ W2, const T *__restrict__ Tt,
-                              T *__restrict__ Y) {
+                              T *__restrict__ Y, float *__restrict__ amax) {
     const HessPair pr = pairs[blockIdx.z];
     const int i = blockIdx.y;
     if (i >= pr.na) return;
+    float vmax = 0.f;
     const int ld2 = 3 * ma2;
     const int ncol = 3 * pr.nb;
     const size_t wbase = ((size_t)blockIdx.z * ma1 + i) * ma2;
@@ -232,6 +233,12 @@ __global__ void hess_y_kernel(const HessPair *__restrict__ pairs, const T *__res
             acc = fma(-W2[wbase + j] * dk, Tt[(wbase + j) * ld2 + c], acc);
         }
         Yi[(size_t)k * ld2 + c] = acc;
+        vmax = fmaxf(vmax, fabsf((float)acc));
+    }
+    if (amax) {
+        // largest |entry| written, for the power-of-two scale of the fp16 split
+        for (int o = 16; o; o >>= 1) vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+        if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<int *>(amax), __float_as_int(vmax));
     }
 }
 
@@ -305,8 +312,13 @@ kfb_status jacobian_core(const DerivSet &outer, const DerivSet &inner, int rep, 
         const size_t jt_elems = (size_t)inner.v.nm * 3 * ma_in * ma_in * rep;
         KFB_TRY(jth.alloc(jt_elems * sizeof(__half), s));
         KFB_TRY(jtl.alloc(jt_elems * sizeof(__half), s));
+        std::vector<int> nin(inner.v.nm);
+        for (int m = 0; m < inner.v.nm; ++m) nin[m] = inner.v.natoms(m);
+        DevBuf d_nin;
+        KFB_TRY(upload(d_nin, nin, s));
         KFB_TRY(transpose_split_dx<T>(static_cast<const T *>(inner.dx), inner.v.nm, ma_in, rep,
-                                      jth.as<__half>(), jtl.as<__half>(), &jt_scale, s));
+                                      d_nin.as<int>(), jth.as<__half>(), jtl.as<__half>(),
+                                      &jt_scale, s));
         KFB_TRY(vh.alloc((size_t)chunk * NU * rep * sizeof(__half), s));
         KFB_TRY(vl.alloc((size_t)chunk * NU * rep * sizeof(__half), s));
     }
@@ -418,15 +430,21 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
     KFB_TRY(Tt.alloc((size_t)batch * ma1 * ma2 * ld2 * sizeof(T), s));
     KFB_TRY(Y.alloc((size_t)batch * ma1 * rep * ld2 * sizeof(T), s));
     KFB_TRY(dpairs.alloc((size_t)batch * sizeof(HessPair), s));
-    DevBuf jth, jtl, yth, ytl;
+    DevBuf jth, jtl, yth, ytl, yamax;
     float jt_scale = 1.f;
     if (tc) {
         // set-1 Jacobians as K-major split rows Jt[(a, c)][(i, k)]
         const size_t jt_elems = (size_t)s1.v.nm * ld1 * ma1 * rep;
         KFB_TRY(jth.alloc(jt_elems * sizeof(__half), s));
         KFB_TRY(jtl.alloc(jt_elems * sizeof(__half), s));
+        std::vector<int> n1(s1.v.nm);
+        for (int m = 0; m < s1.v.nm; ++m) n1[m] = s1.v.natoms(m);
+        DevBuf d_n1;
+        KFB_TRY(upload(d_n1, n1, s));
         KFB_TRY(transpose_split_dx<T>(static_cast<const T *>(s1.dx), s1.v.nm, ma1, rep,
-                                      jth.as<__half>(), jtl.as<__half>(), &jt_scale, s));
+                                      d_n1.as<int>(), jth.as<__half>(), jtl.as<__half>(),
+                                      &jt_scale, s));
+        KFB_TRY(yamax.alloc(sizeof(float), s));
         KFB_TRY(yth.alloc((size_t)batch * ld2 * ma1 * rep * sizeof(__half), s));
         KFB_TRY(ytl.alloc((size_t)batch * ld2 * ma1 * rep * sizeof(__half), s));
     }
@@ -441,15 +459,16 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
             static_cast<const T *>(s2.dx), d_q1.as<int>(), d_q2.as<int>(), ma1, ma2, rep, c2,
             is2, is4, W.as<T>(), W2.as<T>(), Tt.as<T>());
         KFB_CUDA_TRY(cudaGetLastError());
+        if (tc) KFB_TRY(zero(yamax.ptr, sizeof(float), s));
         hess_y_kernel<T><<<dim3((rep + 31) / 32, ma1, np), 256, 0, s>>>(
             dpairs.as<HessPair>(), static_cast<const T *>(s1.x), static_cast<const T *>(s2.x),
             static_cast<const T *>(s2.dx), ma1, ma2, rep, W.as<T>(), W2.as<T>(), Tt.as<T>(),
-            Y.as<T>());
+            Y.as<T>(), tc ? yamax.as<float>() : nullptr);
         KFB_CUDA_TRY(cudaGetLastError());
         if (tc) {
             float y_scale = 1.f;
-            KFB_TRY(transpose_split_y<T>(Y.as<T>(), np, ma1, rep, ld2, yth.as<__half>(),
-                                         ytl.as<__half>(), &y_scale, s));
+            KFB_TRY(transpose_split_y<T>(Y.as<T>(), np, ma1, rep, ld2, yamax.as<float>(),
+                                         yth.as<__half>(), ytl.as<__half>(), &y_scale, s));
             std::vector<TcProb> tprobs;
             tprobs.reserve(np);
             for (int k = 0; k < np; ++k) {

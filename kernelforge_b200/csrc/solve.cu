@@ -616,4 +616,59 @@ kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2
     return st;
 }
 
+// ---------------------------------------------------------------- normal equations
+namespace {
+
+// zty[c] = sum_m z[m][c] y[m] (FP64 accumulation), one thread per column,
+// molecules split over blockIdx.y and combined with atomics
+__global__ void zty_kernel(const float *__restrict__ z, const double *__restrict__ y, int nm,
+                           int d, int mchunk, double *__restrict__ zty) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= d) return;
+    const int m0 = blockIdx.y * mchunk, m1 = min(nm, m0 + mchunk);
+    double t = 0.0;
+    for (int m = m0; m < m1; ++m) t += (double)z[(size_t)m * d + c] * y[m];
+    atomicAdd(zty + c, t);
+}
+
+// mirror the upper triangle (row-major) of a symmetric d x d array into its lower
+__global__ void mirror_upper_kernel(float *a, int d) {
+    const long long i = blockIdx.y * (long long)blockDim.y + threadIdx.y;
+    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < d && j < d && i > j) a[i * d + j] = a[j * d + i];
+}
+
+}  // namespace
+
+kfb_status feature_gramian(const float *z, const double *y, int nm, int d, kfb_layout layout,
+                           float *ztz, double *zty, cudaStream_t s) {
+    Handles *hd = nullptr;
+    KFB_TRY(get_handles(s, hd));
+    // Z is (nm, d) row-major = a column-major d x nm matrix Zc; Z^T Z = Zc Zc^T.
+    // SYRK fills the column-major lower triangle = the row-major upper one.
+    DevBuf full;
+    float *dense = ztz;
+    if (layout != KFB_DENSE) {
+        KFB_TRY(full.alloc((size_t)d * d * sizeof(float), s));
+        dense = full.as<float>();
+    }
+    const float one = 1.f, zero_f = 0.f;
+    KFB_BLAS_TRY(cublasSsyrk(hd->blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, d, nm, &one, z, d,
+                             &zero_f, dense, d));
+    dim3 blk(32, 8), grd(nblk(d, 32), nblk(d, 8));
+    if (layout == KFB_DENSE) {
+        mirror_upper_kernel<<<grd, blk, 0, s>>>(dense, d);
+        KFB_CUDA_TRY(cudaGetLastError());
+    } else {
+        KFB_TRY(full_to_rfp(dense, d, layout, KFB_F32, ztz, s));
+    }
+    if (y && zty) {
+        KFB_TRY(zero(zty, (size_t)d * sizeof(double), s));
+        const int mchunk = 256;
+        zty_kernel<<<dim3(nblk(d, 128), nblk(nm, mchunk)), 128, 0, s>>>(z, y, nm, d, mchunk, zty);
+        KFB_CUDA_TRY(cudaGetLastError());
+    }
+    return KFB_OK;
+}
+
 }  // namespace kfb

@@ -47,6 +47,11 @@ struct Cfg {
 
 constexpr unsigned long long WAIT_LIMIT_NS = 2000000000ull;
 
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+    const __nv_bfloat162 t = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<const uint32_t *>(&t);
+}
+
 __device__ __forceinline__ bool wait_bar(uint32_t bar, uint32_t parity, int *err) {
     for (int i = 0; i < 64; ++i)
         if (mbar_try(bar, parity)) return true;
@@ -66,7 +71,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     tc_gemm_kernel(const __grid_constant__ CUtensorMap ta_hi, const __grid_constant__ CUtensorMap ta_lo,
                    const __grid_constant__ CUtensorMap tb_hi, const __grid_constant__ CUtensorMap tb_lo,
                    const TcProb *__restrict__ probs, const TcTile *__restrict__ tiles, int ntiles,
-                   uint32_t idesc, ElemSink sink, int *err) {
+                   uint32_t idesc, ElemSink sink, TcEpi epi, int *err) {
     using C = Cfg<NPROD>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>(
@@ -186,6 +191,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     } else if (warp >= EPI_WARP0) {
         const int q = warp & 3;
         const int h = (warp - EPI_WARP0) >> 2;  // column half
+        __shared__ float molsum_scr[NUM_EPI_WARPS][32][33];
         int acc = 0;
         uint32_t aph = 0;
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
@@ -195,20 +201,130 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             if (!__all_sync(0xffffffffu, got)) break;
             tc_fence_after();
             const int m = tl.m0 + q * 32 + lane;
+            const bool mvalid = m < pb.M;
+            const long long grow = (long long)pb.row_off + m;
             const uint32_t tbase = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN);
 #pragma unroll 1
             for (int cc = 0; cc < BN / 64; ++cc) {
                 const int c = h * (BN / 64) + cc;
                 float v[32];
                 tmem_ld32(tbase + (uint32_t)(c * 32), v);
-                if (m < pb.M) {
+                const int n0 = tl.n0 + c * 32;
+                if (epi.mode == EPI_SINK) {
+                    if (mvalid) {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) {
+                            const int n = n0 + j;
+                            if (n < pb.N)
+                                sink_store(sink, pb.row_off + m, pb.col_off + n,
+                                           (double)v[j] * pb.alpha, pb.diag);
+                        }
+                    }
+                    continue;
+                }
+                const int nvalid = min(32, pb.N - n0);
+                const long long gcol0 = (long long)pb.col_off + n0;
+                const float alpha = (float)pb.alpha;
+                const bool vec = epi.vec && nvalid == 32;
+                if (epi.mode == EPI_DENSE) {
+                    if (nvalid <= 0 || !mvalid) continue;
+                    float z[32];
+#pragma unroll
+                    for (int j = 0; j < 32; ++j)
+                        z[j] = v[j] * alpha + ((epi.bias && j < nvalid) ? epi.bias[gcol0 + j] : 0.f);
+                    if (epi.zf32) {
+                        float *d = epi.zf32 + grow * epi.ld + gcol0;
+                        if (vec) {
+#pragma unroll
+                            for (int j = 0; j < 32; j += 4)
+                                *reinterpret_cast<float4 *>(d + j) =
+                                    make_float4(z[j], z[j + 1], z[j + 2], z[j + 3]);
+                        } else {
+#pragma unroll
+                            for (int j = 0; j < 32; ++j)
+                                if (j < nvalid) d[j] = z[j];
+                        }
+                    }
+                    if (epi.act || epi.act_t) {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) z[j] = cosf(z[j]);
+                        if (epi.act) {
+                            __nv_bfloat16 *d = epi.act + grow * epi.ld + gcol0;
+                            if (vec) {
+#pragma unroll
+                                for (int j = 0; j < 32; j += 8) {
+                                    uint4 u;
+                                    u.x = pack_bf16(z[j], z[j + 1]);
+                                    u.y = pack_bf16(z[j + 2], z[j + 3]);
+                                    u.z = pack_bf16(z[j + 4], z[j + 5]);
+                                    u.w = pack_bf16(z[j + 6], z[j + 7]);
+                                    *reinterpret_cast<uint4 *>(d + j) = u;
+                                }
+                            } else {
+#pragma unroll
+                                for (int j = 0; j < 32; ++j)
+                                    if (j < nvalid) d[j] = __float2bfloat16_rn(z[j]);
+                            }
+                        }
+                        if (epi.act_t) {
+                            // lanes hold consecutive rows: these stores coalesce
+#pragma unroll
+                            for (int j = 0; j < 32; ++j)
+                                if (j < nvalid)
+                                    epi.act_t[(gcol0 + j) * epi.ld_t + grow] =
+                                        __float2bfloat16_rn(z[j]);
+                        }
+                    }
+                } else if (epi.mode == EPI_DSIN_T) {
+                    if (nvalid <= 0 || !mvalid) continue;
+                    const float *a = epi.aux + grow * epi.ld + gcol0;
+                    float g[32];
+                    if (vec) {
+#pragma unroll
+                        for (int j = 0; j < 32; j += 4) {
+                            const float4 t4 = *reinterpret_cast<const float4 *>(a + j);
+                            g[j] = t4.x;
+                            g[j + 1] = t4.y;
+                            g[j + 2] = t4.z;
+                            g[j + 3] = t4.w;
+                        }
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) g[j] = j < nvalid ? a[j] : 0.f;
+                    }
+#pragma unroll
+                    for (int j = 0; j < 32; ++j)
+                        if (j < nvalid)
+                            epi.act_t[(gcol0 + j) * epi.ld_t + grow] =
+                                __float2bfloat16_rn(-v[j] * alpha * sinf(g[j]));
+                } else {  // EPI_COS_MOLSUM
+                    // rows of one molecule are consecutive: sum each run of rows per
+                    // column through shared memory, one atomic add per (run, column)
+                    float(*scr)[33] = molsum_scr[warp - EPI_WARP0];
+                    const int mol = mvalid ? epi.mol[grow] : -1;
 #pragma unroll
                     for (int j = 0; j < 32; ++j) {
-                        const int n = tl.n0 + c * 32 + j;
-                        if (n < pb.N)
-                            sink_store(sink, pb.row_off + m, pb.col_off + n,
-                                       (double)v[j] * pb.alpha, pb.diag);
+                        const bool ok = mvalid && j < nvalid;
+                        const float bias = (ok && epi.bias) ? epi.bias[gcol0 + j] : 0.f;
+                        scr[j][lane] = ok ? epi.scale * cosf(v[j] * alpha + bias) : 0.f;
                     }
+                    __syncwarp();
+                    // lane l owns column n0 + l and walks the 32 rows by molecule runs
+                    const bool cok = lane < nvalid;
+                    float *col = epi.molsum + gcol0 + lane;
+                    float run = 0.f;
+                    int cur = __shfl_sync(0xffffffffu, mol, 0);
+                    for (int r = 0; r < 32; ++r) {
+                        const int mr = __shfl_sync(0xffffffffu, mol, r);
+                        if (mr != cur) {
+                            if (cur >= 0 && cok) atomicAdd(col + (long long)cur * epi.ld, run);
+                            run = 0.f;
+                            cur = mr;
+                        }
+                        run += scr[lane][r];
+                    }
+                    if (cur >= 0 && cok) atomicAdd(col + (long long)cur * epi.ld, run);
+                    __syncwarp();
                 }
             }
             tc_fence_before();
@@ -263,7 +379,8 @@ kfb_status map2d(CUtensorMap *m, const void *ptr, long long rows, long long cols
 
 template <int NPROD>
 kfb_status launch(const TcOperand &A, const TcOperand &B, bool bf16,
-                  const std::vector<TcProb> &probs, const ElemSink &sink, cudaStream_t s) {
+                  const std::vector<TcProb> &probs, const ElemSink &sink, const TcEpi &epi,
+                  int *err_flag, cudaStream_t s) {
     using C = Cfg<NPROD>;
     std::vector<TcTile> tiles;
     for (int p = 0; p < (int)probs.size(); ++p) {
@@ -274,6 +391,13 @@ kfb_status launch(const TcOperand &A, const TcOperand &B, bool bf16,
             for (int n0 = 0; n0 < pb.N; n0 += BN) tiles.push_back(TcTile{p, m0, n0, 0});
     }
     if (tiles.empty()) return KFB_OK;
+    TcEpi e = epi;
+    if (e.mode != EPI_SINK) {
+        auto al = [](const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
+        bool v = e.ld % 8 == 0 && al(e.zf32) && al(e.act) && al(e.aux);
+        for (const TcProb &pb : probs) v = v && pb.col_off % 8 == 0;
+        e.vec = v ? 1 : 0;
+    }
     CUtensorMap ma_hi, ma_lo, mb_hi, mb_lo;
     KFB_TRY(map2d(&ma_hi, A.hi, A.rows, A.cols, BM, bf16));
     KFB_TRY(map2d(&mb_hi, B.hi, B.rows, B.cols, BN, bf16));
@@ -287,8 +411,12 @@ kfb_status launch(const TcOperand &A, const TcOperand &B, bool bf16,
     DevBuf dp, dt, derr;
     KFB_TRY(upload(dp, probs, s));
     KFB_TRY(upload(dt, tiles, s));
-    KFB_TRY(derr.alloc(sizeof(int), s));
-    KFB_TRY(zero(derr.ptr, sizeof(int), s));
+    int *errp = err_flag;
+    if (!errp) {
+        KFB_TRY(derr.alloc(sizeof(int), s));
+        KFB_TRY(zero(derr.ptr, sizeof(int), s));
+        errp = derr.as<int>();
+    }
     static bool attr = false;
     if (!attr) {
         KFB_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_kernel<NPROD>,
@@ -299,8 +427,9 @@ kfb_status launch(const TcOperand &A, const TcOperand &B, bool bf16,
     const uint32_t idesc = make_idesc(BM, BN, bf16 ? 1 : 0);
     tc_gemm_kernel<NPROD><<<grid, NUM_THREADS, C::SMEM, s>>>(
         ma_hi, ma_lo, mb_hi, mb_lo, dp.as<TcProb>(), dt.as<TcTile>(), (int)tiles.size(), idesc,
-        sink, derr.as<int>());
+        sink, e, errp);
     KFB_CUDA_TRY(cudaGetLastError());
+    if (err_flag) return KFB_OK;
     int herr = 0;
     KFB_CUDA_TRY(cudaMemcpyAsync(&herr, derr.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
     KFB_CUDA_TRY(cudaStreamSynchronize(s));
@@ -318,6 +447,28 @@ __global__ void absmax_kernel(const T *__restrict__ src, long long n, float *out
     for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
     // non-negative floats order like their bit patterns
     if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<int *>(out), __float_as_int(m));
+}
+
+// max |dX[m][j][k][c]| over the real atoms of each molecule (j < nat[m],
+// c < 3 nat[m]); padding entries are never read by the GEMMs and may hold
+// anything
+template <class T>
+__global__ void absmax_dx_kernel(const T *__restrict__ dx, int ma, int rep,
+                                 const int *__restrict__ nat, float *out) {
+    const int m = blockIdx.y;
+    const int na = min(max(nat[m], 0), ma);
+    const int ld = 3 * ma, nc = 3 * na;
+    const long long n = (long long)na * rep * nc;
+    const T *base = dx + (size_t)m * ma * rep * ld;
+    float v = 0.f;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long row = i / nc;
+        const int c = (int)(i - row * nc);
+        v = fmaxf(v, fabsf((float)base[row * ld + c]));
+    }
+    for (int o = 16; o; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<int *>(out), __float_as_int(v));
 }
 
 template <class T>
@@ -399,16 +550,25 @@ __global__ void transpose_split_y_kernel(const T *__restrict__ Y, int ma1, int r
 
 kfb_status tc_gemm_grouped(const TcOperand &A, const TcOperand &B, int nprod, bool bf16,
                            const std::vector<TcProb> &probs, const ElemSink &sink,
-                           cudaStream_t s) {
+                           cudaStream_t s, const TcEpi &epi, int *err_flag) {
     if (!device_is_sm100())
         return set_error(KFB_ERR_UNSUPPORTED, "tensor-core GEMM needs an sm_100 (B200) device");
-    if (nprod == 3) return launch<3>(A, B, bf16, probs, sink, s);
-    return launch<1>(A, B, bf16, probs, sink, s);
+    if (nprod == 3) return launch<3>(A, B, bf16, probs, sink, epi, err_flag, s);
+    return launch<1>(A, B, bf16, probs, sink, epi, err_flag, s);
 }
 
 // Power of two that brings the largest |value| to about 2^14: keeps the hi/lo
 // fp16 pair out of fp16's subnormal range for the small entries (the pair
 // then carries ~22 significant bits over ~28 binades below the maximum).
+kfb_status pow2_from_device(const float *dmax, cudaStream_t s, float *scale) {
+    float m = 0.f;
+    KFB_CUDA_TRY(cudaMemcpyAsync(&m, dmax, sizeof(float), cudaMemcpyDeviceToHost, s));
+    KFB_CUDA_TRY(cudaStreamSynchronize(s));
+    *scale = 1.f;
+    if (m > 0.f && std::isfinite(m)) *scale = std::ldexp(1.f, 14 - (int)std::ceil(std::log2(m)));
+    return KFB_OK;
+}
+
 template <class T>
 kfb_status pow2_scale(const T *src, long long n, cudaStream_t s, float *scale) {
     *scale = 1.f;
@@ -419,11 +579,7 @@ kfb_status pow2_scale(const T *src, long long n, cudaStream_t s, float *scale) {
     const unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 148LL * 16);
     absmax_kernel<T><<<blocks, 256, 0, s>>>(src, n, d.as<float>());
     KFB_CUDA_TRY(cudaGetLastError());
-    float m = 0.f;
-    KFB_CUDA_TRY(cudaMemcpyAsync(&m, d.ptr, sizeof(float), cudaMemcpyDeviceToHost, s));
-    KFB_CUDA_TRY(cudaStreamSynchronize(s));
-    if (m > 0.f && std::isfinite(m)) *scale = std::ldexp(1.f, 14 - (int)std::ceil(std::log2(m)));
-    return KFB_OK;
+    return pow2_from_device(d.as<float>(), s, scale);
 }
 
 template <class T>
@@ -438,11 +594,21 @@ kfb_status split_rows(const T *src, long long n, __half *hi, __half *lo, float *
 }
 
 template <class T>
-kfb_status transpose_split_dx(const T *dx, int nm, int ma, int rep, __half *hi, __half *lo,
-                              float *scale, cudaStream_t s) {
+kfb_status transpose_split_dx(const T *dx, int nm, int ma, int rep, const int *nat, __half *hi,
+                              __half *lo, float *scale, cudaStream_t s) {
     const long long kk = (long long)ma * rep;
-    KFB_TRY(pow2_scale(dx, (long long)nm * kk * 3 * ma, s, scale));
+    *scale = 1.f;
     if (nm <= 0) return KFB_OK;
+    {
+        DevBuf d;
+        KFB_TRY(d.alloc(sizeof(float), s));
+        KFB_TRY(zero(d.ptr, sizeof(float), s));
+        const long long per = kk * 3 * ma;
+        const unsigned bx = (unsigned)std::min<long long>((per + 255) / 256, 64);
+        absmax_dx_kernel<T><<<dim3(bx, (unsigned)nm), 256, 0, s>>>(dx, ma, rep, nat, d.as<float>());
+        KFB_CUDA_TRY(cudaGetLastError());
+        KFB_TRY(pow2_from_device(d.as<float>(), s, scale));
+    }
     dim3 grid((unsigned)((kk + 31) / 32), (unsigned)((3 * ma + 31) / 32), (unsigned)nm);
     transpose_split_dx_kernel<T><<<grid, dim3(32, 8), 0, s>>>(dx, ma, rep, *scale, hi, lo);
     KFB_CUDA_TRY(cudaGetLastError());
@@ -450,10 +616,10 @@ kfb_status transpose_split_dx(const T *dx, int nm, int ma, int rep, __half *hi, 
 }
 
 template <class T>
-kfb_status transpose_split_y(const T *Y, int np, int ma1, int rep, int ld, __half *hi, __half *lo,
-                             float *scale, cudaStream_t s) {
+kfb_status transpose_split_y(const T *Y, int np, int ma1, int rep, int ld, const float *amax,
+                             __half *hi, __half *lo, float *scale, cudaStream_t s) {
     const long long kk = (long long)ma1 * rep;
-    KFB_TRY(pow2_scale(Y, (long long)np * kk * ld, s, scale));
+    KFB_TRY(pow2_from_device(amax, s, scale));
     if (np <= 0) return KFB_OK;
     dim3 grid((unsigned)((kk + 31) / 32), (unsigned)((ld + 31) / 32), (unsigned)np);
     transpose_split_y_kernel<T><<<grid, dim3(32, 8), 0, s>>>(Y, ma1, rep, ld, *scale, hi, lo);
@@ -465,13 +631,13 @@ template kfb_status split_rows<float>(const float *, long long, __half *, __half
                                       cudaStream_t);
 template kfb_status split_rows<double>(const double *, long long, __half *, __half *, float *,
                                        cudaStream_t);
-template kfb_status transpose_split_dx<float>(const float *, int, int, int, __half *, __half *,
-                                              float *, cudaStream_t);
-template kfb_status transpose_split_dx<double>(const double *, int, int, int, __half *, __half *,
-                                               float *, cudaStream_t);
-template kfb_status transpose_split_y<float>(const float *, int, int, int, int, __half *,
-                                             __half *, float *, cudaStream_t);
-template kfb_status transpose_split_y<double>(const double *, int, int, int, int, __half *,
+template kfb_status transpose_split_dx<float>(const float *, int, int, int, const int *, __half *,
                                               __half *, float *, cudaStream_t);
+template kfb_status transpose_split_dx<double>(const double *, int, int, int, const int *,
+                                               __half *, __half *, float *, cudaStream_t);
+template kfb_status transpose_split_y<float>(const float *, int, int, int, int, const float *,
+                                             __half *, __half *, float *, cudaStream_t);
+template kfb_status transpose_split_y<double>(const double *, int, int, int, int, const float *,
+                                              __half *, __half *, float *, cudaStream_t);
 
 }  // namespace kfb

@@ -2,6 +2,7 @@
 // row blocks / column windows of two K-major fp16 (or bf16) 2-D arrays.
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
 #include <vector>
@@ -31,22 +32,58 @@ struct TcTile {
     int prob, m0, n0, pad;
 };
 
+// Epilogue of the grouped GEMM.  EPI_SINK writes alpha * acc through the
+// ElemSink.  The other modes serve the feature-map kernels; (row, col) is the
+// global position (row_off + m, col_off + n) and z = alpha * acc + bias[col]
+// (bias optional):
+//   EPI_DENSE      zf32[row * ld + col] = z                (FP32, optional)
+//                  act[row * ld + col] = bf16(cos z)       (optional)
+//                  act_t[col * ld_t + row] = bf16(cos z)   (optional)
+//   EPI_DSIN_T     act_t[col * ld_t + row] = bf16(-alpha * acc * sin(aux[row * ld + col]))
+//                  (back-propagation through a cos activation)
+//   EPI_COS_MOLSUM molsum[mol[row] * ld + col] += scale * cos z, each run of
+//                  rows of one molecule summed before its atomic add
+enum TcEpiMode : int { EPI_SINK = 0, EPI_DENSE = 1, EPI_DSIN_T = 2, EPI_COS_MOLSUM = 3 };
+
+struct TcEpi {
+    int mode = EPI_SINK;
+    int vec = 0;  // set by tc_gemm_grouped: 16-byte row stores allowed
+    float *zf32 = nullptr;
+    __nv_bfloat16 *act = nullptr;
+    __nv_bfloat16 *act_t = nullptr;
+    const float *aux = nullptr;
+    const float *bias = nullptr;
+    const int *mol = nullptr;
+    float *molsum = nullptr;
+    long long ld = 0, ld_t = 0;
+    float scale = 1.f;
+};
+
 // nprod = 3: split operands, hi*hi + hi*lo + lo*hi; nprod = 1: hi only.
+// err_flag: null = wait for the kernel and report a pipeline timeout now;
+// otherwise the kernel raises *err_flag (device int) and the call returns
+// without synchronising (the caller checks the flag later).
 kfb_status tc_gemm_grouped(const TcOperand &A, const TcOperand &B, int nprod, bool bf16,
                            const std::vector<TcProb> &probs, const ElemSink &sink,
-                           cudaStream_t s);
+                           cudaStream_t s, const TcEpi &epi = TcEpi(), int *err_flag = nullptr);
 
 // Split packers: multiply by a power-of-two scale (returned in *scale; the
-// largest magnitude lands near 2^14) and write the fp16 pair hi = fp16(v),
-// lo = fp16(v - hi).  GEMM results are divided by the two operands' scales.
+// largest magnitude of the entries the GEMMs read lands near 2^14) and write
+// the fp16 pair hi = fp16(v), lo = fp16(v - hi).  GEMM results are divided by
+// the two operands' scales.
+//   split_rows:         every entry of src is read;
+//   transpose_split_dx: nat (device int32, per molecule) limits the scale to
+//                       the real atoms, padding may hold anything;
+//   transpose_split_y:  amax (device float) is the largest |entry| the
+//                       producer wrote (the rest of Y is never read).
 template <class T>
 kfb_status split_rows(const T *src, long long n, __half *hi, __half *lo, float *scale,
                       cudaStream_t s);
 template <class T>
-kfb_status transpose_split_dx(const T *dx, int nm, int ma, int rep, __half *hi, __half *lo,
-                              float *scale, cudaStream_t s);
+kfb_status transpose_split_dx(const T *dx, int nm, int ma, int rep, const int *nat, __half *hi,
+                              __half *lo, float *scale, cudaStream_t s);
 template <class T>
-kfb_status transpose_split_y(const T *Y, int np, int ma1, int rep, int ld, __half *hi,
-                             __half *lo, float *scale, cudaStream_t s);
+kfb_status transpose_split_y(const T *Y, int np, int ma1, int rep, int ld, const float *amax,
+                             __half *hi, __half *lo, float *scale, cudaStream_t s);
 
 }  // namespace kfb

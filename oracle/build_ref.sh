@@ -1,6 +1,6 @@
 #!/usr/bin/env bash
 # Build the reference's own CPU FP64 modules (local_kernels, kernelmath,
-# fchl19_repr) from their sources under the reference checkout, into
+# fchl19_repr, kitchen_sinks = the random-Fourier-feature module) from their sources under the reference checkout, into
 # oracle/_ref/ (git-ignored).  TEST INFRASTRUCTURE ONLY: the result is the
 # "reference" CPU arm of bench.py and the generator of tests/golden fixtures.
 #
@@ -79,5 +79,7 @@ build() {
 build local_kernels "$SRC/local_kernels.cpp" "$SRC/local_kernels_bindings.cpp" &
 build kernelmath "$SRC/math.cpp" "$SRC/math_bindings.cpp" &
 build fchl19_repr "$SRC/fchl19_repr.cpp" "$SRC/fchl19_repr_bindings.cpp" &
+build kitchen_sinks "$SRC/rff_features.cpp" "$SRC/rff_features_bindings.cpp" \
+    "$SRC/rff_elemental.cpp" "$SRC/rff_elemental_bindings.cpp" &
 wait
 echo "reference modules in $OUT"
