@@ -252,6 +252,18 @@ kfb_status kfb_rff_features_elemental(const void *x, const int32_t *q, const int
 kfb_status kfb_feature_gramian(const float *z, const double *y, int nm, int d, kfb_layout layout,
                                float *ztz, double *zty, void *stream);
 
+/* Linear ridge weights on per-molecule features: (Z^T Z + l2 I) w = Z^T y,
+ * z (nm, d) device float32, y (nm,) device float64, w (d,) device float64.
+ * FP32 factor of the normal equations formed from Z with its dominant
+ * direction projected out (and restored by a Sherman-Morrison term), FP64
+ * conjugate-gradient refinement against the exact operator Z^T (Z w) applied
+ * from Z; stops at ||r|| <= tol ||Z^T y||.  Flags and info as for
+ * kfb_krr_solve_mixed.  Replaces the FP32 normal-equation solve of
+ * models/cuda_local_rff.py:684-712 (rfp_potrf / rfp_potrs on Z^T Z). */
+kfb_status kfb_ridge_solve_mixed(const float *z, const double *y, int nm, int d, double l2,
+                                 double tol, int maxit, int flags, double *w,
+                                 kfb_solve_info *info, void *stream);
+
 /* Exact local-kernel values of atom pairs, the training targets of the learned
  * map: out[p] = exp(-|x[pi[p]] - x[pj[p]]|^2 / (2 sigma^2)), x (nrows, rep)
  * device, pi / pj device int32 row indices (an index outside [0, nrows) gives

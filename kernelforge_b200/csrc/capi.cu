@@ -17,6 +17,9 @@ kfb_status rfp_potrf(void *arf, int n, double l2, kfb_layout uplo, kfb_dtype dt,
 kfb_status rfp_potrs(const void *arf, void *B, int n, int nrhs, kfb_layout uplo, kfb_dtype dt, cudaStream_t s);
 kfb_status feature_gramian(const float *z, const double *y, int nm, int d, kfb_layout layout,
                            float *ztz, double *zty, cudaStream_t s);
+kfb_status ridge_solve_mixed(const float *zf, const double *y, int nm, int d, double l2,
+                             double tol, int maxit, int flags, double *w, kfb_solve_info *info,
+                             cudaStream_t s);
 kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2, kfb_layout uplo,
                            double tol, int maxit, int flags, double *alpha, kfb_solve_info *info,
                            cudaStream_t s);
@@ -485,6 +488,16 @@ kfb_status kfb_feature_gramian(const float *z, const double *y, int nm, int d, k
     if (layout != KFB_DENSE && layout != KFB_RFP_U && layout != KFB_RFP_L)
         return set_error(KFB_ERR_INVALID_ARG, "layout must be dense or RFP");
     return feature_gramian(z, y, nm, d, layout, ztz, zty, as_stream(stream));
+}
+
+kfb_status kfb_ridge_solve_mixed(const float *z, const double *y, int nm, int d, double l2,
+                                 double tol, int maxit, int flags, double *w,
+                                 kfb_solve_info *info, void *stream) {
+    if (nm <= 0 || d <= 0) return set_error(KFB_ERR_INVALID_ARG, "All dims must be positive.");
+    if (!z || !y || !w) return set_error(KFB_ERR_INVALID_ARG, "null pointer");
+    if (!(tol > 0.0) || maxit < 0 || !(l2 >= 0.0))
+        return set_error(KFB_ERR_INVALID_ARG, "bad l2 / tol / maxit");
+    return ridge_solve_mixed(z, y, nm, d, l2, tol, maxit, flags, w, info, as_stream(stream));
 }
 
 }  // extern "C"

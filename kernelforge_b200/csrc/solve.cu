@@ -13,6 +13,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <functional>
 #include <vector>
 
 #include "kernels_common.cuh"
@@ -418,113 +419,153 @@ kfb_status rfp_potrs(const void *arf, void *B, int n, int nrhs, kfb_layout uplo,
                               uplo == KFB_RFP_L, s);
 }
 
-kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2,
-                           kfb_layout uplo, double tol, int maxit, int flags, double *alpha,
-                           kfb_solve_info *info, cudaStream_t s) {
-    kfb_solve_info inf{};
-    inf.lambda_eff = l2;
+namespace {
+
+// (A + lam I) x of the operator a mixed solve refines against, FP64 vectors
+using ApplyFn = std::function<kfb_status(const double *x, double lam, double *out)>;
+
+// out = (K + l2 I) x with K dense FP32 (row-major, symmetric), one warp per row
+__global__ void dense_apply_kernel(const float *__restrict__ K, const double *__restrict__ x,
+                                   int n, double l2, double *__restrict__ out) {
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const float *kr = K + (size_t)row * n;
+    double acc = 0.0;
+    for (int j = lane; j < n; j += 32) acc = fma((double)kr[j], x[j], acc);
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) out[row] = acc + l2 * x[row];
+}
+
+// t[m] = sum_c z[m][c] x[c] (FP32 features, FP64 accumulation), one warp per row
+__global__ void zx_kernel(const float *__restrict__ z, const double *__restrict__ x, int nm,
+                          int d, double *__restrict__ t) {
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= nm) return;
+    const float *zr = z + (size_t)row * d;
+    double acc = 0.0;
+    for (int c = lane; c < d; c += 32) acc = fma((double)zr[c], x[c], acc);
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) t[row] = acc;
+}
+
+// zty[c] += sum_m z[m][c] y[m] (FP64 accumulation), one thread per column,
+// molecules split over blockIdx.y and combined with atomics
+__global__ void zty_kernel(const float *__restrict__ z, const double *__restrict__ y, int nm,
+                           int d, int mchunk, double *__restrict__ zty) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= d) return;
+    const int m0 = blockIdx.y * mchunk, m1 = min(nm, m0 + mchunk);
+    double t = 0.0;
+    for (int m = m0; m < m1; ++m) t += (double)z[(size_t)m * d + c] * y[m];
+    atomicAdd(zty + c, t);
+}
+
+// z1[m][c] = z[m][c] - t[m] v[c] with t = z v: the features with the dominant
+// direction v of Z^T Z projected out (FP64 arithmetic, FP32 result)
+__global__ void project_out_kernel(const float *__restrict__ z, const double *__restrict__ t,
+                                   const double *__restrict__ v, long long nm, int d,
+                                   float *__restrict__ z1) {
+    const long long n = nm * d;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long m = i / d;
+        const int c = (int)(i - m * d);
+        z1[i] = (float)((double)z[i] - t[m] * v[c]);
+    }
+}
+
+// The dominant eigenpair (mu, v) of a symmetric positive semi-definite
+// operator by power iteration, and lam2, an upper estimate of the norm of the
+// operator with that pair removed (a few power steps orthogonal to v; Rayleigh
+// quotients approach the norm from below, hence the factor 1.5).
+kfb_status power_dominant(const ApplyFn &A, int n, double *v, double *w, double *tmp, Dot &dot,
+                          cudaStream_t s, double &mu, double &lam2) {
+    const unsigned gb = nblk(n, 256);
+    mu = 0.0;
+    fill_kernel<<<gb, 256, 0, s>>>(v, 1.0 / std::sqrt((double)n), n);
+    for (int k = 0; k < 30; ++k) {
+        KFB_TRY(A(v, 0.0, tmp));
+        double vav = 0.0, tt = 0.0;
+        KFB_TRY(dot(v, tmp, n, s, vav));
+        KFB_TRY(dot(tmp, tmp, n, s, tt));
+        if (!(tt > 0.0)) break;
+        scale_copy_kernel<<<gb, 256, 0, s>>>(tmp, 1.0 / std::sqrt(tt), n, v);
+        const bool done = k > 2 && std::fabs(vav - mu) <= 1e-13 * std::fabs(vav);
+        mu = vav;
+        if (done) break;
+    }
+    lam2 = 0.0;
+    fill_alt_kernel<<<gb, 256, 0, s>>>(w, 1.0 / std::sqrt((double)n), n);
+    for (int k = 0; k < 8; ++k) {
+        double vw = 0.0;
+        KFB_TRY(dot(v, w, n, s, vw));
+        axpy_kernel<<<gb, 256, 0, s>>>(v, -vw, n, w);
+        KFB_TRY(A(w, 0.0, tmp));
+        double waw = 0.0, tt = 0.0, ww = 0.0;
+        KFB_TRY(dot(w, tmp, n, s, waw));
+        KFB_TRY(dot(w, w, n, s, ww));
+        KFB_TRY(dot(tmp, tmp, n, s, tt));
+        lam2 = std::max(lam2, waw / std::max(ww, 1e-300));
+        if (!(tt > 0.0)) break;
+        scale_copy_kernel<<<gb, 256, 0, s>>>(tmp, 1.0 / std::sqrt(tt), n, w);
+    }
+    lam2 *= 1.5;
+    KFB_CUDA_TRY(cudaGetLastError());
+    return KFB_OK;
+}
+
+// Mixed-precision solve of (A + l2 I) x = y.  The FP32 factor is of
+//   F = B - fcoef v v^T + (lam + shift) I       (B an FP32 RFP matrix)
+// chosen so that F + defl v v^T approximates A + lam I; the preconditioner
+//   M^{-1} = (F + defl v v^T)^{-1}
+// is applied with the Sherman-Morrison formula, and conjugate gradients in
+// FP64 refine against the operator A itself.  With the dominant eigenvalue mu
+// of A removed from the factor (defl = mu - lam2) its eigenvalue along v is
+// about lam2 rather than ~0, so F^{-1} v stays bounded and the Sherman-Morrison
+// correction does not cancel.  The shift starts at max(0, 2 u32 lam2 - lam)
+// and grows 4x per failed factorisation; CG meeting a non-positive curvature
+// p^T (A + lam I) p means A + lam I is indefinite at the precision A is held
+// in (KFB_ERR_NOT_PD; with KFB_SOLVE_LAMBDA_FLOOR lam is raised x10 instead).
+kfb_status mixed_core(const ApplyFn &A, const float *B, int n, kfb_layout uplo, const double *v,
+                      double fcoef, double defl, double lam2, const double *y, double l2,
+                      double tol, int maxit, int flags, double *alpha, kfb_solve_info &inf,
+                      Dot &dot, cudaStream_t s) {
     const size_t nt = (size_t)n * (n + 1) / 2;
-    DevBuf Kd, F, r, z, p, q, f32v;
-    KFB_TRY(Kd.alloc((size_t)n * n * sizeof(float), s));
-    KFB_TRY(rfp_to_full(k_rfp, n, uplo, KFB_F32, Kd.ptr, s));
+    DevBuf F, r, z, p, q, f32v, dw;
     KFB_TRY(F.alloc(nt * sizeof(float), s));
     KFB_TRY(r.alloc((size_t)n * sizeof(double), s));
     KFB_TRY(z.alloc((size_t)n * sizeof(double), s));
     KFB_TRY(p.alloc((size_t)n * sizeof(double), s));
     KFB_TRY(q.alloc((size_t)n * sizeof(double), s));
+    KFB_TRY(dw.alloc((size_t)n * sizeof(double), s));
     KFB_TRY(f32v.alloc((size_t)n * sizeof(float), s));
-    Dot dot;
-    KFB_TRY(dot.init(s));
-
+    const unsigned gb = nblk(n, 256);
+    const dim3 blk2(32, 8), grd2(nblk(n, 32), nblk(n, 8));
+    const double u32 = 5.960464477539063e-08;
     double ynorm2 = 0.0;
     KFB_TRY(dot(y, y, n, s, ynorm2));
     const double ynorm = std::sqrt(ynorm2);
     KFB_TRY(zero(alpha, (size_t)n * sizeof(double), s));
-    if (ynorm == 0.0) {
-        if (info) *info = inf;
-        return KFB_OK;
-    }
-    const unsigned gb = nblk(n, 256), gw = nblk((long long)n * 32, 256);
+    if (ynorm == 0.0) return KFB_OK;
 
-    // Deflation of the dominant eigenpair.  A Gaussian kernel matrix has
-    // non-negative entries and one eigenvalue far above the others (the mode
-    // shared by all molecules, about n * mean(K)); that eigenvalue alone sets
-    // the diagonal shift FP32 Cholesky needs (unit roundoff times ||K||_2).
-    // Power iteration gives (mu, v) and an estimate sigma of the next
-    // eigenvalue; the FP32 factor is of
-    //   F = K - (mu - sigma) v v^T + (lambda + shift) I,
-    // whose eigenvalue along v is sigma (not ~0, which would make F^{-1} v huge
-    // and the correction below cancel), and the preconditioner
-    //   M^{-1} = (F + (mu - sigma) v v^T)^{-1}
-    // is applied with the Sherman-Morrison formula.  FP64 residuals always use
-    // K itself.
-    DevBuf dv, dw, dtmp;
-    KFB_TRY(dv.alloc((size_t)n * sizeof(double), s));
-    KFB_TRY(dw.alloc((size_t)n * sizeof(double), s));
-    KFB_TRY(dtmp.alloc((size_t)n * sizeof(double), s));
-    double mu = 0.0;
-    {
-        fill_kernel<<<gb, 256, 0, s>>>(dv.as<double>(), 1.0 / std::sqrt((double)n), n);
-        for (int k = 0; k < 30; ++k) {
-            residual_kernel<<<gw, 256, 0, s>>>(Kd.as<float>(), dv.as<double>(), nullptr, n, 0.0,
-                                               dtmp.as<double>());  // -K v
-            double vkv = 0.0, ww = 0.0;
-            KFB_TRY(dot(dv.as<double>(), dtmp.as<double>(), n, s, vkv));
-            KFB_TRY(dot(dtmp.as<double>(), dtmp.as<double>(), n, s, ww));
-            const double mu_new = -vkv;
-            scale_copy_kernel<<<gb, 256, 0, s>>>(dtmp.as<double>(), -1.0 / std::sqrt(ww), n,
-                                                 dv.as<double>());
-            const bool done = k > 2 && std::fabs(mu_new - mu) <= 1e-9 * std::fabs(mu_new);
-            mu = mu_new;
-            if (done) break;
-        }
-    }
-    // a few power steps on the deflated operator estimate ||K - mu v v^T||_2
-    double lam2 = 0.0;
-    {
-        fill_alt_kernel<<<gb, 256, 0, s>>>(dw.as<double>(), 1.0 / std::sqrt((double)n), n);
-        for (int k = 0; k < 8; ++k) {
-            double vw = 0.0;
-            KFB_TRY(dot(dv.as<double>(), dw.as<double>(), n, s, vw));
-            axpy_kernel<<<gb, 256, 0, s>>>(dv.as<double>(), -vw, n, dw.as<double>());
-            residual_kernel<<<gw, 256, 0, s>>>(Kd.as<float>(), dw.as<double>(), nullptr, n, 0.0,
-                                               dtmp.as<double>());  // -K w
-            double wkw = 0.0, tt = 0.0, ww = 0.0;
-            KFB_TRY(dot(dw.as<double>(), dtmp.as<double>(), n, s, wkw));
-            KFB_TRY(dot(dw.as<double>(), dw.as<double>(), n, s, ww));
-            KFB_TRY(dot(dtmp.as<double>(), dtmp.as<double>(), n, s, tt));
-            lam2 = std::max(lam2, -wkw / std::max(ww, 1e-300));
-            scale_copy_kernel<<<gb, 256, 0, s>>>(dtmp.as<double>(), -1.0 / std::sqrt(tt), n,
-                                                 dw.as<double>());
-        }
-        lam2 *= 1.5;  // Rayleigh quotients approach ||.||_2 from below
-    }
-    const double u32 = 5.960464477539063e-08;
-    const double defl = std::max(0.0, mu - lam2);
-    const dim3 blk2(32, 8), grd2(nblk(n, 32), nblk(n, 8));
-
-    // F^{-1} v via the FP32 factor, with v scaled to unit norm first
-    auto solve_f = [&](const double *v, double vnorm, double *out) -> kfb_status {
-        const double sc = vnorm > 0.0 ? 1.0 / vnorm : 1.0;
-        scale_to_float_kernel<<<gb, 256, 0, s>>>(v, sc, n, f32v.as<float>());
+    // F^{-1} x via the FP32 factor, with x scaled to unit norm first
+    auto solve_f = [&](const double *x, double xnorm, double *out) -> kfb_status {
+        const double sc = xnorm > 0.0 ? 1.0 / xnorm : 1.0;
+        scale_to_float_kernel<<<gb, 256, 0, s>>>(x, sc, n, f32v.as<float>());
         KFB_TRY(rfp_potrs(F.ptr, f32v.ptr, n, 1, uplo, KFB_F32, s));
-        float_to_double_kernel<<<gb, 256, 0, s>>>(f32v.as<float>(), vnorm > 0.0 ? vnorm : 1.0, n,
+        float_to_double_kernel<<<gb, 256, 0, s>>>(f32v.as<float>(), xnorm > 0.0 ? xnorm : 1.0, n,
                                                   out);
         KFB_CUDA_TRY(cudaGetLastError());
         return KFB_OK;
     };
 
-    // One attempt at (K + lam I) alpha = y: FP32 factor (the shift starts at
-    // max(0, 2 u32 lam2 - lam) and grows 4x per failed factorisation), then
-    // preconditioned CG in FP64.  KFB_ERR_NOT_PD if CG meets a non-positive
-    // curvature p^T (K + lam I) p, i.e. K + lam I is indefinite at FP32 storage
-    // precision.
     auto attempt = [&](double lam) -> kfb_status {
         double shift = std::max(0.0, 2.0 * u32 * lam2 - lam);
         int finfo = 0;
         for (int a = 0; a < 12; ++a) {
-            rfp_deflate_kernel<<<grd2, blk2, 0, s>>>(k_rfp, n, uplo, dv.as<double>(), defl,
-                                                     F.as<float>());
+            rfp_deflate_kernel<<<grd2, blk2, 0, s>>>(B, n, uplo, v, fcoef, F.as<float>());
             KFB_CUDA_TRY(cudaGetLastError());
             KFB_TRY(rfp_potrf(F.ptr, n, lam + shift, uplo, KFB_F32, &finfo, s));
             if (finfo == 0) break;
@@ -535,9 +576,9 @@ kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2
         if (finfo != 0)
             return set_error(KFB_ERR_NOT_PD,
                              "FP32 RFP Cholesky failed even with shift %g (info=%d)", shift, finfo);
-        KFB_TRY(solve_f(dv.as<double>(), 1.0, dw.as<double>()));  // w = F^{-1} v
+        KFB_TRY(solve_f(v, 1.0, dw.as<double>()));  // w = F^{-1} v
         double vfv = 0.0;
-        KFB_TRY(dot(dv.as<double>(), dw.as<double>(), n, s, vfv));
+        KFB_TRY(dot(v, dw.as<double>(), n, s, vfv));
         const double sm_coef = defl / (1.0 + defl * vfv);
         // M^{-1} r = F^{-1} r - sm_coef (w . r) w
         auto precond = [&](const double *vec, double vnorm, double *out) -> kfb_status {
@@ -560,21 +601,19 @@ kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2
         KFB_TRY(dot(r.as<double>(), z.as<double>(), n, s, rz));
         int it = 0;
         for (; it < maxit; ++it) {
-            residual_kernel<<<gw, 256, 0, s>>>(Kd.as<float>(), p.as<double>(), nullptr, n, lam,
-                                               q.as<double>());  // q = -(K + lam I) p
+            KFB_TRY(A(p.as<double>(), lam, q.as<double>()));  // q = (A + lam I) p
             double pq = 0.0;
             KFB_TRY(dot(p.as<double>(), q.as<double>(), n, s, pq));
-            pq = -pq;
             if (!(pq > 0.0)) {
                 inf.iterations = it;
                 return set_error(KFB_ERR_NOT_PD,
-                                 "K + l2 I is indefinite at FP32 storage precision (p^T A p = "
-                                 "%.3e after %d CG iterations, l2 = %g); use a larger l2",
-                                 -pq, it, lam);
+                                 "the system is indefinite at the precision of its matrix (p^T A "
+                                 "p = %.3e after %d CG iterations, l2 = %g); use a larger l2",
+                                 pq, it, lam);
             }
             const double a = rz / pq;
             axpy_kernel<<<gb, 256, 0, s>>>(p.as<double>(), a, n, alpha);
-            axpy_kernel<<<gb, 256, 0, s>>>(q.as<double>(), a, n, r.as<double>());  // r -= a A p
+            axpy_kernel<<<gb, 256, 0, s>>>(q.as<double>(), -a, n, r.as<double>());
             double rr = 0.0;
             KFB_TRY(dot(r.as<double>(), r.as<double>(), n, s, rr));
             rn = std::sqrt(rr);
@@ -589,7 +628,10 @@ kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2
             rz = rz_new;
         }
         // true residual of the returned alpha
-        residual_kernel<<<gw, 256, 0, s>>>(Kd.as<float>(), alpha, y, n, lam, r.as<double>());
+        KFB_TRY(A(alpha, lam, q.as<double>()));
+        KFB_CUDA_TRY(cudaMemcpyAsync(r.ptr, y, (size_t)n * sizeof(double),
+                                     cudaMemcpyDeviceToDevice, s));
+        axpy_kernel<<<gb, 256, 0, s>>>(q.as<double>(), -1.0, n, r.as<double>());
         double rr = 0.0;
         KFB_TRY(dot(r.as<double>(), r.as<double>(), n, s, rr));
         inf.iterations = it;
@@ -609,27 +651,120 @@ kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2
         st = attempt(lam);
         inf.lambda_eff = lam;
         if (st != KFB_ERR_NOT_PD || !(flags & KFB_SOLVE_LAMBDA_FLOOR)) break;
-        // raise the regularisation until K + lam I is definite at FP32 precision
+        // raise the regularisation until A + lam I is definite at FP32 precision
         lam = (tries == 0) ? std::max(10.0 * l2, u32 * lam2) : lam * 10.0;
     }
+    return st;
+}
+
+}  // namespace
+
+// Kernel ridge: A = K (FP32 RFP input, expanded to a dense FP32 copy for the
+// FP64 residual products); the factor deflates K's dominant eigenpair.
+kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2,
+                           kfb_layout uplo, double tol, int maxit, int flags, double *alpha,
+                           kfb_solve_info *info, cudaStream_t s) {
+    kfb_solve_info inf{};
+    inf.lambda_eff = l2;
+    DevBuf Kd, dv, dw, dtmp;
+    KFB_TRY(Kd.alloc((size_t)n * n * sizeof(float), s));
+    KFB_TRY(rfp_to_full(k_rfp, n, uplo, KFB_F32, Kd.ptr, s));
+    KFB_TRY(dv.alloc((size_t)n * sizeof(double), s));
+    KFB_TRY(dw.alloc((size_t)n * sizeof(double), s));
+    KFB_TRY(dtmp.alloc((size_t)n * sizeof(double), s));
+    Dot dot;
+    KFB_TRY(dot.init(s));
+    const unsigned gw = nblk((long long)n * 32, 256);
+    ApplyFn A = [&](const double *x, double lam, double *out) -> kfb_status {
+        dense_apply_kernel<<<gw, 256, 0, s>>>(Kd.as<float>(), x, n, lam, out);
+        KFB_CUDA_TRY(cudaGetLastError());
+        return KFB_OK;
+    };
+    double ynorm2 = 0.0;
+    KFB_TRY(dot(y, y, n, s, ynorm2));
+    if (ynorm2 == 0.0) {
+        KFB_TRY(zero(alpha, (size_t)n * sizeof(double), s));
+        if (info) *info = inf;
+        return KFB_OK;
+    }
+    double mu = 0.0, lam2 = 0.0;
+    KFB_TRY(power_dominant(A, n, dv.as<double>(), dw.as<double>(), dtmp.as<double>(), dot, s, mu,
+                           lam2));
+    const double defl = std::max(0.0, mu - lam2);
+    const kfb_status st = mixed_core(A, k_rfp, n, uplo, dv.as<double>(), defl, defl, lam2, y, l2,
+                                     tol, maxit, flags, alpha, inf, dot, s);
+    if (info) *info = inf;
+    return st;
+}
+
+// Linear ridge on features: (Z^T Z + l2 I) w = Z^T y with Z (nm, d) FP32.  The
+// operator is applied matrix-free from Z (two FP64-accumulated passes), so the
+// refinement converges to the solution of the exact normal equations, not of
+// their FP32 rounding.  The FP32 factor is built from Z with the dominant
+// direction v projected out before the SYRK: Z^T Z's entries are dominated by
+// its top eigenvalue (the mode shared by all molecules), and forming Z1^T Z1
+// with Z1 = Z (I - v v^T) keeps the FP32 rounding at the scale of the
+// remaining spectrum.
+kfb_status ridge_solve_mixed(const float *zf, const double *y, int nm, int d, double l2,
+                             double tol, int maxit, int flags, double *w, kfb_solve_info *info,
+                             cudaStream_t s) {
+    kfb_solve_info inf{};
+    inf.lambda_eff = l2;
+    Handles *hd = nullptr;
+    KFB_TRY(get_handles(s, hd));
+    DevBuf t, rhs, dv, dw, dtmp;
+    KFB_TRY(t.alloc((size_t)nm * sizeof(double), s));
+    KFB_TRY(rhs.alloc((size_t)d * sizeof(double), s));
+    KFB_TRY(dv.alloc((size_t)d * sizeof(double), s));
+    KFB_TRY(dw.alloc((size_t)d * sizeof(double), s));
+    KFB_TRY(dtmp.alloc((size_t)d * sizeof(double), s));
+    Dot dot;
+    KFB_TRY(dot.init(s));
+    const int mchunk = 256;
+    const dim3 gty(nblk(d, 128), nblk(nm, mchunk));
+    const unsigned gzx = nblk((long long)nm * 32, 256);
+    ApplyFn A = [&](const double *x, double lam, double *out) -> kfb_status {
+        zx_kernel<<<gzx, 256, 0, s>>>(zf, x, nm, d, t.as<double>());
+        KFB_CUDA_TRY(cudaGetLastError());
+        KFB_TRY(zero(out, (size_t)d * sizeof(double), s));
+        zty_kernel<<<gty, 128, 0, s>>>(zf, t.as<double>(), nm, d, mchunk, out);
+        KFB_CUDA_TRY(cudaGetLastError());
+        if (lam != 0.0) axpy_kernel<<<nblk(d, 256), 256, 0, s>>>(x, lam, d, out);
+        KFB_CUDA_TRY(cudaGetLastError());
+        return KFB_OK;
+    };
+    KFB_TRY(zero(rhs.ptr, (size_t)d * sizeof(double), s));
+    zty_kernel<<<gty, 128, 0, s>>>(zf, y, nm, d, mchunk, rhs.as<double>());
+    KFB_CUDA_TRY(cudaGetLastError());
+    double mu = 0.0, lam2 = 0.0;
+    KFB_TRY(power_dominant(A, d, dv.as<double>(), dw.as<double>(), dtmp.as<double>(), dot, s, mu,
+                           lam2));
+    // B = Z1^T Z1 in RFP, Z1 = Z with v projected out
+    DevBuf z1, full, B;
+    KFB_TRY(z1.alloc((size_t)nm * d * sizeof(float), s));
+    zx_kernel<<<gzx, 256, 0, s>>>(zf, dv.as<double>(), nm, d, t.as<double>());
+    project_out_kernel<<<std::min<unsigned>(nblk((long long)nm * d, 256), 148u * 32), 256, 0, s>>>(
+        zf, t.as<double>(), dv.as<double>(), nm, d, z1.as<float>());
+    KFB_CUDA_TRY(cudaGetLastError());
+    KFB_TRY(full.alloc((size_t)d * d * sizeof(float), s));
+    const float one = 1.f, zero_f = 0.f;
+    KFB_BLAS_TRY(cublasSsyrk(hd->blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, d, nm, &one,
+                             z1.as<float>(), d, &zero_f, full.as<float>(), d));
+    z1.release();
+    KFB_TRY(B.alloc((size_t)d * (d + 1) / 2 * sizeof(float), s));
+    KFB_TRY(full_to_rfp(full.ptr, d, KFB_RFP_L, KFB_F32, B.ptr, s));
+    full.release();
+    const double defl = std::max(0.0, mu - lam2);
+    // F = B + lam2 v v^T (eigenvalue ~lam2 along v), M = F + defl v v^T ~ Z^T Z
+    const kfb_status st = mixed_core(A, B.as<float>(), d, KFB_RFP_L, dv.as<double>(), -lam2, defl,
+                                     lam2, rhs.as<double>(), l2, tol, maxit, flags, w, inf, dot,
+                                     s);
     if (info) *info = inf;
     return st;
 }
 
 // ---------------------------------------------------------------- normal equations
 namespace {
-
-// zty[c] = sum_m z[m][c] y[m] (FP64 accumulation), one thread per column,
-// molecules split over blockIdx.y and combined with atomics
-__global__ void zty_kernel(const float *__restrict__ z, const double *__restrict__ y, int nm,
-                           int d, int mchunk, double *__restrict__ zty) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= d) return;
-    const int m0 = blockIdx.y * mchunk, m1 = min(nm, m0 + mchunk);
-    double t = 0.0;
-    for (int m = m0; m < m1; ++m) t += (double)z[(size_t)m * d + c] * y[m];
-    atomicAdd(zty + c, t);
-}
 
 // mirror the upper triangle (row-major) of a symmetric d x d array into its lower
 __global__ void mirror_upper_kernel(float *a, int d) {

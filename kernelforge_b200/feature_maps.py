@@ -291,14 +291,33 @@ def _device_view(ptr, shape):
 
 # ------------------------------------------------------------------ ridge
 def fit_ridge(Z, y, l2, tol=1e-10, maxit=500, lambda_floor=True):
-    """Weights of the linear ridge model (Z^T Z + l2 I) w = Z^T y: FP32 SYRK in
-    RFP, then the mixed FP32-Cholesky / FP64-refinement solve.  Returns
-    (w float64, solve info)."""
-    from .cuda_global_kernels import krr_solve_mixed
-    from .cuda_rff_features import feature_gramian
-    ztz, zty = feature_gramian(Z, y, "L")
-    return krr_solve_mixed(ztz, zty, l2=l2, uplo="L", tol=tol, maxit=maxit,
-                           lambda_floor=lambda_floor)
+    """Weights of the linear ridge model (Z^T Z + l2 I) w = Z^T y (libkfb's
+    kfb_ridge_solve_mixed: FP32 factor, FP64 refinement against Z itself).
+    Returns (w float64 (d,), solve info dict)."""
+    require_cuda()
+    import torch
+    if Z.dtype != torch.float32 or not Z.is_cuda or Z.dim() != 2:
+        raise RuntimeError("Z must be a 2D float32 CUDA tensor")
+    Z = Z.contiguous()
+    nm, d = Z.shape
+    yd = y.to(device=Z.device, dtype=torch.float64).contiguous()
+    if yd.numel() != nm:
+        raise RuntimeError("y must have one value per row of Z")
+    w = torch.empty((d,), dtype=torch.float64, device=Z.device)
+    info = _lib.SolveInfo()
+    flags = _lib.KFB_SOLVE_LAMBDA_FLOOR if lambda_floor else 0
+    st = _lib.lib().kfb_ridge_solve_mixed(Z.data_ptr(), yd.data_ptr(), nm, d, float(l2),
+                                          float(tol), int(maxit), flags, w.data_ptr(),
+                                          ctypes.byref(info), stream_handle())
+    res = {"iterations": info.iterations, "factor_info": info.factor_info, "shift": info.shift,
+           "rel_residual": info.rel_residual, "used_cg": bool(info.used_cg),
+           "lambda_eff": info.lambda_eff}
+    if st == _lib.KFB_ERR_NOT_PD:
+        raise RuntimeError(_lib.lib().kfb_last_error().decode())
+    if st != _lib.KFB_OK and st != _lib.KFB_ERR_NO_CONVERGENCE:
+        _lib.check(st)
+    res["converged"] = st == _lib.KFB_OK
+    return w, res
 
 
 def predict_linear(Z, w):
