@@ -113,40 +113,96 @@ __global__ void transpose_f32_kernel(const float *__restrict__ src, int rows, in
 }
 
 // dst[c * ld_dst + r] = src[r][c] for a BF16 (rows, cols) array, and
-// colsum[c] += sum_r src[r][c] (FP32, optional).
+// colsum[c] += sum_r src[r][c] (FP32, optional).  64 x 64 tiles through shared
+// memory; bf16x2 loads along c and bf16x2 stores along r when cols, ld_dst and
+// the pointers allow it (128-byte accesses per warp), element-wise otherwise.
 __global__ void transpose_bf16_kernel(const bf16 *__restrict__ src, int rows, int cols,
                                       bf16 *__restrict__ dst, long long ld_dst,
-                                      float *__restrict__ colsum) {
-    __shared__ float tile[32][33];
-    const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
-    for (int rr = threadIdx.y; rr < 32; rr += blockDim.y) {
-        const int r = r0 + rr, c = c0 + threadIdx.x;
-        tile[rr][threadIdx.x] =
-            (r < rows && c < cols) ? __bfloat162float(src[(size_t)r * cols + c]) : 0.f;
+                                      float *__restrict__ colsum, int pairs) {
+    __shared__ float tile[64][65];
+    const int r0 = blockIdx.y * 64, c0 = blockIdx.x * 64;
+    const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+    for (int rr = ty; rr < 64; rr += 8) {
+        const int r = r0 + rr, c = c0 + 2 * tx;
+        float v0 = 0.f, v1 = 0.f;
+        if (r < rows) {
+            if (pairs && c + 1 < cols) {
+                const __nv_bfloat162 t =
+                    *reinterpret_cast<const __nv_bfloat162 *>(src + (size_t)r * cols + c);
+                v0 = __low2float(t);
+                v1 = __high2float(t);
+            } else {
+                if (c < cols) v0 = __bfloat162float(src[(size_t)r * cols + c]);
+                if (c + 1 < cols) v1 = __bfloat162float(src[(size_t)r * cols + c + 1]);
+            }
+        }
+        tile[rr][2 * tx] = v0;
+        tile[rr][2 * tx + 1] = v1;
     }
     __syncthreads();
-    for (int cc = threadIdx.y; cc < 32; cc += blockDim.y) {
-        const int c = c0 + cc, r = r0 + threadIdx.x;
-        const float v = tile[threadIdx.x][cc];
-        if (c < cols && r < rows) dst[(size_t)c * ld_dst + r] = src[(size_t)r * cols + c];
+    for (int cc = ty; cc < 64; cc += 8) {
+        const int c = c0 + cc, r = r0 + 2 * tx;
+        const float v0 = tile[2 * tx][cc], v1 = tile[2 * tx + 1][cc];
+        if (c < cols) {
+            bf16 *d = dst + (size_t)c * ld_dst + r;
+            if (pairs && r + 1 < rows) {
+                *reinterpret_cast<__nv_bfloat162 *>(d) = __floats2bfloat162_rn(v0, v1);
+            } else {
+                if (r < rows) d[0] = __float2bfloat16_rn(v0);
+                if (r + 1 < rows) d[1] = __float2bfloat16_rn(v1);
+            }
+        }
         if (colsum) {
-            float t = v;
+            float t = v0 + v1;
             for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-            if (threadIdx.x == 0 && c < cols) atomicAdd(colsum + c, t);
+            if (tx == 0 && c < cols) atomicAdd(colsum + c, t);
         }
     }
 }
 
-// out[r] = sum_c src[r][c] (BF16 rows, FP32 sums), one warp per row
+kfb_status transpose_bf16(const bf16 *src, int rows, int cols, bf16 *dst, long long ld_dst,
+                          float *colsum, cudaStream_t s) {
+    const bool pairs = cols % 2 == 0 && ld_dst % 2 == 0 &&
+                       (reinterpret_cast<uintptr_t>(src) & 3u) == 0 &&
+                       (reinterpret_cast<uintptr_t>(dst) & 3u) == 0;
+    transpose_bf16_kernel<<<dim3(nblk(cols, 64), nblk(rows, 64)), dim3(32, 8), 0, s>>>(
+        src, rows, cols, dst, ld_dst, colsum, pairs ? 1 : 0);
+    KFB_CUDA_TRY(cudaGetLastError());
+    return KFB_OK;
+}
+
+// out[r] = sum_c src[r][c] (BF16 rows, FP32 sums), one 256-thread block per
+// row, 16-byte loads when the row allows them
 __global__ void rowsum_bf16_kernel(const bf16 *__restrict__ src, int rows, int cols,
                                    float *__restrict__ out) {
-    const int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
+    const int r = blockIdx.x;
     if (r >= rows) return;
+    const bf16 *row = src + (size_t)r * cols;
     float t = 0.f;
-    for (int c = lane; c < cols; c += 32) t += __bfloat162float(src[(size_t)r * cols + c]);
+    const bool vec = cols % 8 == 0 && (reinterpret_cast<uintptr_t>(row) & 15u) == 0;
+    if (vec) {
+        const uint4 *v = reinterpret_cast<const uint4 *>(row);
+        for (int c = threadIdx.x; c < cols / 8; c += blockDim.x) {
+            const uint4 u = v[c];
+            const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const __nv_bfloat162 b2 = *reinterpret_cast<const __nv_bfloat162 *>(&w[q]);
+                t += __low2float(b2) + __high2float(b2);
+            }
+        }
+    } else {
+        for (int c = threadIdx.x; c < cols; c += blockDim.x) t += __bfloat162float(row[c]);
+    }
+    __shared__ float red[32];
     for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-    if (lane == 0) out[r] = t;
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float s = 0.f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+        out[r] = s;
+    }
 }
 
 // Exact pair-kernel values e_p = exp(-|x_i - x_j|^2 / (2 sigma^2)) (squared
@@ -178,55 +234,96 @@ __global__ void pair_gaussian_kernel(const T *__restrict__ x, long long nsrc,
     if (lane == 0) out[p] = (float)exp(c * t);
 }
 
+// sin and cos of x: reduce to r = x - 2 pi round(x / 2 pi) in [-pi, pi] (2 pi
+// split into a float head and tail so the product is exact to ~1e-7 for the
+// |x| < 1e3 the network produces), then the hardware approximation, whose
+// absolute error on [-pi, pi] is about 1e-6.
+__device__ __forceinline__ void sincos_reduced(float x, float &sn, float &cs) {
+    const float TWO_PI_HI = 6.28318548202514648f;     // float(2 pi)
+    const float TWO_PI_LO = -1.74845553e-07f;          // 2 pi - TWO_PI_HI
+    const float k = rintf(x * 0.159154943091895336f);  // x / (2 pi)
+    const float r = fmaf(-k, TWO_PI_LO, fmaf(-k, TWO_PI_HI, x));
+    __sincosf(r, &sn, &cs);
+}
+
 // Pair loss and the gradient at layer 2's pre-activation.  Rows p and p + Bp
 // of z2 are the two atoms of pair p.  With s2 = 2 / D:
 //   k_p = s2 sum_d cos z_i[d] cos z_j[d],  r_p = k_p - t_p,  loss += r_p^2
 //   dZ2_i[d] = -(2 r_p / npairs) s2 cos z_j[d] sin z_i[d]   (and i <-> j)
-// Padded pairs (p >= npairs) get zero gradient rows.
-__global__ void pair_loss_kernel(const float *__restrict__ z2, int Bp, int npairs, int D,
-                                 const float *__restrict__ target, float s2, float gscale,
-                                 bf16 *__restrict__ dz2, double *__restrict__ loss) {
+// Padded pairs (p >= npairs) get zero gradient rows.  One block of 256
+// threads per pair; each thread keeps its float4 slices of both rows in
+// registers between the dot product and the gradient (D <= 256 * 4 * VPT).
+constexpr int PL_THREADS = 256, PL_VPT = 4;
+__global__ void __launch_bounds__(PL_THREADS)
+    pair_loss_kernel(const float *__restrict__ z2, int Bp, int npairs, int D,
+                     const float *__restrict__ target, float s2, float gscale,
+                     bf16 *__restrict__ dz2, double *__restrict__ loss) {
     const int p = blockIdx.x;
-    const float *zi = z2 + (size_t)p * D, *zj = z2 + (size_t)(p + Bp) * D;
-    bf16 *di = dz2 + (size_t)p * D, *dj = dz2 + (size_t)(p + Bp) * D;
+    const float4 *zi = reinterpret_cast<const float4 *>(z2 + (size_t)p * D);
+    const float4 *zj = reinterpret_cast<const float4 *>(z2 + (size_t)(p + Bp) * D);
+    uint2 *di = reinterpret_cast<uint2 *>(dz2 + (size_t)p * D);
+    uint2 *dj = reinterpret_cast<uint2 *>(dz2 + (size_t)(p + Bp) * D);
+    const int n4 = D / 4;
     if (p >= npairs) {
-        for (int d = threadIdx.x; d < D; d += blockDim.x) {
-            di[d] = __float2bfloat16_rn(0.f);
-            dj[d] = __float2bfloat16_rn(0.f);
+        for (int k = threadIdx.x; k < n4; k += PL_THREADS) {
+            di[k] = make_uint2(0u, 0u);
+            dj[k] = make_uint2(0u, 0u);
         }
         return;
     }
+    // sin / cos of both rows once, kept in registers between the dot product
+    // and the gradient
+    float si[PL_VPT][4], ci[PL_VPT][4], sj[PL_VPT][4], cj[PL_VPT][4];
     float acc = 0.f;
-    for (int d = threadIdx.x; d < D; d += blockDim.x) acc += cosf(zi[d]) * cosf(zj[d]);
-    __shared__ float red[32];
+#pragma unroll
+    for (int u = 0; u < PL_VPT; ++u) {
+        const int k = threadIdx.x + u * PL_THREADS;
+        if (k < n4) {
+            const float4 a = zi[k], b = zj[k];
+            const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                sincos_reduced(av[c], si[u][c], ci[u][c]);
+                sincos_reduced(bv[c], sj[u][c], cj[u][c]);
+                acc = fmaf(ci[u][c], cj[u][c], acc);
+            }
+        }
+    }
+    __shared__ float red[PL_THREADS / 32];
     for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
     __syncthreads();
-    if (threadIdx.x < 32) {
-        float t = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.f;
-        for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-        if (threadIdx.x == 0) red[0] = t;
-    }
-    __syncthreads();
-    const float r = s2 * red[0] - target[p];
+    float tot = 0.f;
+#pragma unroll
+    for (int w = 0; w < PL_THREADS / 32; ++w) tot += red[w];
+    const float r = s2 * tot - target[p];
     if (threadIdx.x == 0) atomicAdd(loss, (double)r * (double)r);
     const float g = gscale * r * s2;
-    for (int d = threadIdx.x; d < D; d += blockDim.x) {
-        float si, ci, sj, cj;
-        sincosf(zi[d], &si, &ci);
-        sincosf(zj[d], &sj, &cj);
-        di[d] = __float2bfloat16_rn(-g * cj * si);
-        dj[d] = __float2bfloat16_rn(-g * ci * sj);
+#pragma unroll
+    for (int u = 0; u < PL_VPT; ++u) {
+        const int k = threadIdx.x + u * PL_THREADS;
+        if (k < n4) {
+            const __nv_bfloat162 x01 = __floats2bfloat162_rn(-g * cj[u][0] * si[u][0],
+                                                             -g * cj[u][1] * si[u][1]);
+            const __nv_bfloat162 x23 = __floats2bfloat162_rn(-g * cj[u][2] * si[u][2],
+                                                             -g * cj[u][3] * si[u][3]);
+            const __nv_bfloat162 y01 = __floats2bfloat162_rn(-g * ci[u][0] * sj[u][0],
+                                                             -g * ci[u][1] * sj[u][1]);
+            const __nv_bfloat162 y23 = __floats2bfloat162_rn(-g * ci[u][2] * sj[u][2],
+                                                             -g * ci[u][3] * sj[u][3]);
+            di[k] = make_uint2(*reinterpret_cast<const uint32_t *>(&x01),
+                               *reinterpret_cast<const uint32_t *>(&x23));
+            dj[k] = make_uint2(*reinterpret_cast<const uint32_t *>(&y01),
+                               *reinterpret_cast<const uint32_t *>(&y23));
+        }
     }
 }
 
-// Adam on one parameter tensor (rows x cols, row-major), refreshing the BF16
-// copy (pb) and the transposed BF16 copy (pbt, cols x rows) when given.
+// Adam on one parameter tensor (n values), refreshing its BF16 copy (pb)
+// when given.
 __global__ void adam_kernel(float *__restrict__ p, const float *__restrict__ g,
-                            float *__restrict__ m, float *__restrict__ v, int rows, int cols,
-                            float lr, float bc1, float bc2, bf16 *__restrict__ pb,
-                            bf16 *__restrict__ pbt) {
-    const long long n = (long long)rows * cols;
+                            float *__restrict__ m, float *__restrict__ v, long long n, float lr,
+                            float bc1, float bc2, bf16 *__restrict__ pb) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
         const float gi = g[i];
@@ -237,7 +334,6 @@ __global__ void adam_kernel(float *__restrict__ p, const float *__restrict__ g,
         const float pi = p[i] - lr * (mi / bc1) / (sqrtf(vi / bc2) + ADAM_EPS);
         p[i] = pi;
         if (pb) pb[i] = __float2bfloat16_rn(pi);
-        if (pbt) pbt[(i % cols) * rows + i / cols] = __float2bfloat16_rn(pi);
     }
 }
 
@@ -504,14 +600,12 @@ kfb_status cosmlp_step_t(kfb_cosmlp *h, int e, const T *x, long long nrows, cons
     }
     float *gw1 = h->grad[0].as<float>(), *gb1 = h->grad[1].as<float>();
     float *gw2 = h->grad[2].as<float>(), *gb2 = h->grad[3].as<float>();
-    pair_loss_kernel<<<Bp, 256, 0, s>>>(h->z2.as<float>(), Bp, npairs, D, target, 2.f / (float)D,
-                                        2.f / (float)npairs, h->dz2.as<bf16>(),
-                                        h->loss.as<double>());
+    pair_loss_kernel<<<Bp, PL_THREADS, 0, s>>>(h->z2.as<float>(), Bp, npairs, D, target,
+                                               2.f / (float)D, 2.f / (float)npairs,
+                                               h->dz2.as<bf16>(), h->loss.as<double>());
     KFB_CUDA_TRY(cudaGetLastError());
     KFB_TRY(zero(gb2, (size_t)D * sizeof(float), s));
-    transpose_bf16_kernel<<<dim3(nblk(D, 32), nblk(R, 32)), dim3(32, 8), 0, s>>>(
-        h->dz2.as<bf16>(), R, D, h->dz2t.as<bf16>(), R, gb2);
-    KFB_CUDA_TRY(cudaGetLastError());
+    KFB_TRY(transpose_bf16(h->dz2.as<bf16>(), R, D, h->dz2t.as<bf16>(), R, gb2, s));
     // dW2 = dZ2^T H  (D x H, contraction over the batch rows)
     {
         TcOperand A, B;
@@ -555,7 +649,8 @@ kfb_status cosmlp_step_t(kfb_cosmlp *h, int e, const T *x, long long nrows, cons
         ep.ld_t = R;
         KFB_TRY(tc_gemm_grouped(A, B, 1, true, {p}, ElemSink(), s, ep, err));
     }
-    // dW1 = dZ1^T X  (H x rep)
+    // dW1 = dZ1^T X  (H x rep): few output tiles, so the batch axis (K) is
+    // split over problems that add into a zeroed gradient
     {
         TcOperand A, B;
         A.hi = h->dz1t.ptr;
@@ -564,18 +659,28 @@ kfb_status cosmlp_step_t(kfb_cosmlp *h, int e, const T *x, long long nrows, cons
         B.hi = h->xbt.ptr;
         B.rows = rep;
         B.cols = R;
-        TcProb p{};
-        p.M = H;
-        p.N = rep;
-        p.K = R;
-        p.alpha = 1.0;
+        const int tiles = ((H + 127) / 128) * ((rep + 127) / 128);
+        const int want = std::max(1, std::min(device_sm_count() / std::max(tiles, 1), R / 256));
+        const int kc = (int)((R / want + 63) / 64 * 64);
+        std::vector<TcProb> probs;
+        for (int k0 = 0; k0 < R; k0 += kc) {
+            TcProb p{};
+            p.a_k0 = p.b_k0 = k0;
+            p.M = H;
+            p.N = rep;
+            p.K = std::min(kc, R - k0);
+            p.alpha = 1.0;
+            probs.push_back(p);
+        }
         TcEpi ep;
         ep.mode = EPI_DENSE;
         ep.zf32 = gw1;
         ep.ld = rep;
-        KFB_TRY(tc_gemm_grouped(A, B, 1, true, {p}, ElemSink(), s, ep, err));
+        ep.accumulate = probs.size() > 1 ? 1 : 0;
+        if (ep.accumulate) KFB_TRY(zero(gw1, (size_t)H * rep * sizeof(float), s));
+        KFB_TRY(tc_gemm_grouped(A, B, 1, true, probs, ElemSink(), s, ep, err));
     }
-    rowsum_bf16_kernel<<<nblk(H, 8), 256, 0, s>>>(h->dz1t.as<bf16>(), H, R, gb1);
+    rowsum_bf16_kernel<<<H, 256, 0, s>>>(h->dz1t.as<bf16>(), H, R, gb1);
     KFB_CUDA_TRY(cudaGetLastError());
     if (update) {
         const int t = ++h->steps[e];
@@ -595,10 +700,12 @@ kfb_status cosmlp_step_t(kfb_cosmlp *h, int e, const T *x, long long nrows, cons
         };
         for (const P &q : ps) {
             const size_t off = (size_t)e * q.rows * q.cols;
-            adam_kernel<<<nblk((long long)q.rows * q.cols, 256 * 4), 256, 0, s>>>(
+            const long long n = (long long)q.rows * q.cols;
+            adam_kernel<<<nblk(n, 256 * 4), 256, 0, s>>>(
                 q.p->as<float>() + off, h->grad[q.k].as<float>(), h->mom[q.k].as<float>() + off,
-                h->var[q.k].as<float>() + off, q.rows, q.cols, lr, bc1, bc2, q.pb, q.pbt);
+                h->var[q.k].as<float>() + off, n, lr, bc1, bc2, q.pb);
             KFB_CUDA_TRY(cudaGetLastError());
+            if (q.pbt) KFB_TRY(transpose_bf16(q.pb, q.rows, q.cols, q.pbt, q.rows, nullptr, s));
         }
     }
     int herr[2] = {0, 0};
@@ -697,6 +804,8 @@ kfb_status kfb_cosmlp_create(int nelem, int rep, int hidden, int d, int max_pair
         if (rep % 16 != 0 || hidden % 16 != 0 || d % 16 != 0)
             return set_error(KFB_ERR_UNSUPPORTED,
                              "cos-MLP: rep, hidden and D must be multiples of 16");
+        if (d > PL_THREADS * 4 * PL_VPT)
+            return set_error(KFB_ERR_UNSUPPORTED, "cos-MLP: D up to %d", PL_THREADS * 4 * PL_VPT);
         if (!device_is_sm100())
             return set_error(KFB_ERR_UNSUPPORTED, "cos-MLP needs an sm_100 (B200) device");
         auto *h = new kfb_cosmlp();
@@ -786,8 +895,10 @@ kfb_status kfb_cosmlp_sync(kfb_cosmlp *h, int reset_optimizer, void *stream) {
             nullptr);
         to_bf16_kernel<<<nblk((long long)D * H, 1024), 256, 0, s>>>(
             h->w2.as<float>() + (size_t)e * D * H, D, H, h->w2b.as<bf16>() + (size_t)e * D * H,
-            h->w2tb.as<bf16>() + (size_t)e * H * D);
+            nullptr);
         KFB_CUDA_TRY(cudaGetLastError());
+        KFB_TRY(transpose_bf16(h->w2b.as<bf16>() + (size_t)e * D * H, D, H,
+                               h->w2tb.as<bf16>() + (size_t)e * H * D, D, nullptr, s));
     }
     if (reset_optimizer) {
         const size_t sizes[4] = {(size_t)h->nelem * H * rep, (size_t)h->nelem * H,

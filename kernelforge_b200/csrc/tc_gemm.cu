@@ -227,19 +227,42 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                 const float alpha = (float)pb.alpha;
                 const bool vec = epi.vec && nvalid == 32;
                 if (epi.mode == EPI_DENSE) {
-                    if (nvalid <= 0 || !mvalid) continue;
+                    if (nvalid <= 0) continue;  // warp-uniform
+                    // bias: one coalesced load, then broadcast by shuffles
+                    const float bl = (epi.bias && lane < nvalid) ? epi.bias[gcol0 + lane] : 0.f;
                     float z[32];
 #pragma unroll
                     for (int j = 0; j < 32; ++j)
-                        z[j] = v[j] * alpha + ((epi.bias && j < nvalid) ? epi.bias[gcol0 + j] : 0.f);
-                    if (epi.zf32) {
-                        float *d = epi.zf32 + grow * epi.ld + gcol0;
-                        if (vec) {
+                        z[j] = v[j] * alpha + __shfl_sync(0xffffffffu, bl, j);
+                    float(*scr)[33] = molsum_scr[warp - EPI_WARP0];
+                    const long long grow0 = (long long)pb.row_off + tl.m0 + q * 32;
+                    const int mrows = min(32, pb.M - (tl.m0 + q * 32));  // valid rows of the chunk
+                    if (epi.zf32 && epi.accumulate) {
+                        if (mvalid) {
+                            float *d = epi.zf32 + grow * epi.ld + gcol0;
 #pragma unroll
-                            for (int j = 0; j < 32; j += 4)
-                                *reinterpret_cast<float4 *>(d + j) =
-                                    make_float4(z[j], z[j + 1], z[j + 2], z[j + 3]);
-                        } else {
+                            for (int j = 0; j < 32; ++j)
+                                if (j < nvalid) atomicAdd(d + j, z[j]);
+                        }
+                    } else if (epi.zf32) {
+                        if (vec) {
+                            // stage the 32 x 32 chunk, then 4 rows x 128 B per store
+#pragma unroll
+                            for (int j = 0; j < 32; ++j) scr[lane][j] = z[j];
+                            __syncwarp();
+                            const int rsub = lane >> 3, c4 = (lane & 7) * 4;
+#pragma unroll
+                            for (int rr = 0; rr < 8; ++rr) {
+                                const int row = rr * 4 + rsub;
+                                if (row < mrows)
+                                    *reinterpret_cast<float4 *>(epi.zf32 + (grow0 + row) * epi.ld +
+                                                                gcol0 + c4) =
+                                        make_float4(scr[row][c4], scr[row][c4 + 1],
+                                                    scr[row][c4 + 2], scr[row][c4 + 3]);
+                            }
+                            __syncwarp();
+                        } else if (mvalid) {
+                            float *d = epi.zf32 + grow * epi.ld + gcol0;
 #pragma unroll
                             for (int j = 0; j < 32; ++j)
                                 if (j < nvalid) d[j] = z[j];
@@ -249,24 +272,34 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
 #pragma unroll
                         for (int j = 0; j < 32; ++j) z[j] = cosf(z[j]);
                         if (epi.act) {
-                            __nv_bfloat16 *d = epi.act + grow * epi.ld + gcol0;
                             if (vec) {
+                                // stage, then 8 rows x 64 B per store (16 B per lane)
 #pragma unroll
-                                for (int j = 0; j < 32; j += 8) {
-                                    uint4 u;
-                                    u.x = pack_bf16(z[j], z[j + 1]);
-                                    u.y = pack_bf16(z[j + 2], z[j + 3]);
-                                    u.z = pack_bf16(z[j + 4], z[j + 5]);
-                                    u.w = pack_bf16(z[j + 6], z[j + 7]);
-                                    *reinterpret_cast<uint4 *>(d + j) = u;
+                                for (int j = 0; j < 32; ++j) scr[lane][j] = z[j];
+                                __syncwarp();
+                                const int rsub = lane >> 2, c8 = (lane & 3) * 8;
+#pragma unroll
+                                for (int rr = 0; rr < 4; ++rr) {
+                                    const int row = rr * 8 + rsub;
+                                    if (row < mrows) {
+                                        uint4 u;
+                                        u.x = pack_bf16(scr[row][c8], scr[row][c8 + 1]);
+                                        u.y = pack_bf16(scr[row][c8 + 2], scr[row][c8 + 3]);
+                                        u.z = pack_bf16(scr[row][c8 + 4], scr[row][c8 + 5]);
+                                        u.w = pack_bf16(scr[row][c8 + 6], scr[row][c8 + 7]);
+                                        *reinterpret_cast<uint4 *>(epi.act + (grow0 + row) * epi.ld +
+                                                                   gcol0 + c8) = u;
+                                    }
                                 }
-                            } else {
+                                __syncwarp();
+                            } else if (mvalid) {
+                                __nv_bfloat16 *d = epi.act + grow * epi.ld + gcol0;
 #pragma unroll
                                 for (int j = 0; j < 32; ++j)
                                     if (j < nvalid) d[j] = __float2bfloat16_rn(z[j]);
                             }
                         }
-                        if (epi.act_t) {
+                        if (epi.act_t && mvalid) {
                             // lanes hold consecutive rows: these stores coalesce
 #pragma unroll
                             for (int j = 0; j < 32; ++j)
@@ -302,10 +335,12 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                     // column through shared memory, one atomic add per (run, column)
                     float(*scr)[33] = molsum_scr[warp - EPI_WARP0];
                     const int mol = mvalid ? epi.mol[grow] : -1;
+                    const float bl =
+                        (epi.bias && lane < nvalid && nvalid > 0) ? epi.bias[gcol0 + lane] : 0.f;
 #pragma unroll
                     for (int j = 0; j < 32; ++j) {
                         const bool ok = mvalid && j < nvalid;
-                        const float bias = (ok && epi.bias) ? epi.bias[gcol0 + j] : 0.f;
+                        const float bias = __shfl_sync(0xffffffffu, bl, j);
                         scr[j][lane] = ok ? epi.scale * cosf(v[j] * alpha + bias) : 0.f;
                     }
                     __syncwarp();

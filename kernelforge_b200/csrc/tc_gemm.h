@@ -36,7 +36,7 @@ struct TcTile {
 // ElemSink.  The other modes serve the feature-map kernels; (row, col) is the
 // global position (row_off + m, col_off + n) and z = alpha * acc + bias[col]
 // (bias optional):
-//   EPI_DENSE      zf32[row * ld + col] = z                (FP32, optional)
+//   EPI_DENSE      zf32[row * ld + col] = z  (or += z, atomically, with accumulate)
 //                  act[row * ld + col] = bf16(cos z)       (optional)
 //                  act_t[col * ld_t + row] = bf16(cos z)   (optional)
 //   EPI_DSIN_T     act_t[col * ld_t + row] = bf16(-alpha * acc * sin(aux[row * ld + col]))
@@ -47,7 +47,8 @@ enum TcEpiMode : int { EPI_SINK = 0, EPI_DENSE = 1, EPI_DSIN_T = 2, EPI_COS_MOLS
 
 struct TcEpi {
     int mode = EPI_SINK;
-    int vec = 0;  // set by tc_gemm_grouped: 16-byte row stores allowed
+    int vec = 0;         // set by tc_gemm_grouped: 16-byte row stores allowed
+    int accumulate = 0;  // EPI_DENSE: zf32 += z (atomic; split-K problems)
     float *zf32 = nullptr;
     __nv_bfloat16 *act = nullptr;
     __nv_bfloat16 *act_t = nullptr;

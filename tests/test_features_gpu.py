@@ -132,13 +132,13 @@ def test_cosmlp_features_match_oracle():
     assert rel(Z, exact) <= 3e-2
 
 
-@pytest.mark.parametrize("npairs", [40, 8, 203])
+@pytest.mark.parametrize("npairs", [40, 8, 203, 2048])
 def test_cosmlp_gradients_match_oracle(npairs):
     import torch
     from kernelforge_b200.feature_maps import CosMLPFeatureMap
     rng = np.random.default_rng(npairs)
     rows = (rng.standard_normal((120, 48)) * 0.7).astype(np.float32)
-    fm = CosMLPFeatureMap(2, rep=48, hidden=32, d=144, sigma=2.0, seed=9, max_pairs=256,
+    fm = CosMLPFeatureMap(2, rep=48, hidden=32, d=144, sigma=2.0, seed=9, max_pairs=2048,
                           init_scale=0.3)
     pi = rng.integers(0, 120, npairs).astype(np.int32)
     pj = rng.integers(0, 120, npairs).astype(np.int32)
