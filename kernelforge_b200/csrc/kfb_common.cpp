@@ -1,6 +1,8 @@
 // Host-side helpers of libkfb: error reporting, scratch buffers, label
 // bucketing and derivative offsets.
 #include <algorithm>
+#include <chrono>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <set>
@@ -23,8 +25,33 @@ kfb_status set_error(kfb_status st, const char *fmt, ...) {
 
 const char *last_error() { return g_last_error.c_str(); }
 
+// The device's default memory pool returns unused memory to the driver at every
+// synchronisation unless told otherwise; the solves synchronise between
+// iterations, so their scratch (hundreds of MB) would be unmapped and mapped
+// again on every call.  Keep up to KFB_POOL_KEEP_GB (default 16) GB in the pool.
+static void keep_pool_memory() {
+    static std::mutex mu;
+    static bool done[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+    std::lock_guard<std::mutex> lk(mu);
+    if (done[dev]) return;
+    done[dev] = true;
+    const char *v = std::getenv("KFB_POOL_KEEP_GB");
+    const double gb = v ? std::atof(v) : 16.0;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return;
+    }
+    unsigned long long keep = (unsigned long long)((gb > 0 ? gb : 0.0) * (double)(1ull << 30));
+    if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess)
+        (void)cudaGetLastError();
+}
+
 kfb_status DevBuf::alloc(size_t nbytes, cudaStream_t s) {
     release();
+    keep_pool_memory();
     stream = s;
     bytes = nbytes ? nbytes : 16;
     cudaError_t e = cudaMallocAsync(&ptr, bytes, s);
@@ -142,6 +169,31 @@ bool device_is_sm100() {
     cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
     cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev);
     return major == 10 && minor == 0;
+}
+
+int trace_level() {
+    static const int lvl = [] {
+        const char *v = std::getenv("KFB_TRACE");
+        return v ? std::atoi(v) : 0;
+    }();
+    return lvl;
+}
+
+static double now_ms() {
+    using namespace std::chrono;
+    return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+TraceScope::TraceScope(const char *n, cudaStream_t s) : name(n), stream(s), level(trace_level()) {
+    if (level <= 0) return;
+    if (level >= 2) cudaStreamSynchronize(stream);
+    t0 = now_ms();
+}
+
+TraceScope::~TraceScope() {
+    if (level <= 0) return;
+    if (level >= 2) cudaStreamSynchronize(stream);
+    std::fprintf(stderr, "[kfb-trace] %-28s %9.3f ms\n", name, now_ms() - t0);
 }
 
 }  // namespace kfb

@@ -171,4 +171,17 @@ struct KernelTimer {
     void stop();
 };
 
+// Host-phase tracing (environment KFB_TRACE): 1 prints the host wall time of
+// each traced phase to stderr; 2 also synchronises the stream at both ends of
+// the phase, so the time includes the device work the phase enqueued.
+int trace_level();
+struct TraceScope {
+    const char *name;
+    cudaStream_t stream;
+    double t0 = 0.0;
+    int level = 0;
+    TraceScope(const char *n, cudaStream_t s);
+    ~TraceScope();
+};
+
 }  // namespace kfb

@@ -47,7 +47,9 @@ kfb_status run_simt(const ScalarProblem &p, const PairSink &sink, cudaStream_t s
     Buckets b1 = make_buckets(p.s1, labels);
     Buckets b2 = p.symmetric ? Buckets() : make_buckets(p.s2, labels);
     const Buckets &bb = p.symmetric ? b1 : b2;
-    std::vector<PairTile> tiles = make_pair_tiles(b1, bb, p.symmetric, ST, ST);
+    const int Dp_ = (p.rep + SK - 1) / SK * SK;
+    std::vector<PairTile> tiles =
+        make_pair_tiles(b1, bb, p.symmetric, ST, ST, (size_t)Dp_ * sizeof(T));
     if (tiles.empty()) return KFB_OK;
     const int Dp = (p.rep + SK - 1) / SK * SK;
     DevBuf pa, na, ma, pb, nb, mb, dt;
@@ -76,23 +78,39 @@ kfb_status run_simt(const ScalarProblem &p, const PairSink &sink, cudaStream_t s
 }  // namespace
 
 std::vector<PairTile> make_pair_tiles(const Buckets &a, const Buckets &b, bool symmetric,
-                                      int tm, int tn) {
+                                      int tm, int tn, size_t row_bytes) {
     std::vector<PairTile> out;
+    int group = 1 << 30;  // tiles per super-block side (unbounded: row-major order)
+    if (row_bytes > 0) {
+        int dev = 0, l2 = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev) != cudaSuccess || l2 <= 0)
+            l2 = 64 << 20;
+        const size_t tile_bytes = (size_t)std::max(tm, tn) * row_bytes;
+        group = (int)std::max<size_t>(4, std::min<size_t>(64, (size_t)l2 / 2 / (2 * tile_bytes)));
+    }
     const int L = (int)a.labels.size();
     for (int l = 0; l < L; ++l) {
         const int sa = a.lab_start[l], ea = a.lab_start[l + 1];
         const int sb = b.lab_start[l], eb = b.lab_start[l + 1];
         if (ea <= sa || eb <= sb) continue;
-        for (int i0 = sa; i0 < ea; i0 += tm) {
-            const int j_first = symmetric ? i0 : sb;
-            for (int j0 = j_first; j0 < eb; j0 += tn) {
-                PairTile t{};
-                t.a0 = i0;
-                t.a_end = ea;
-                t.b0 = j0;
-                t.b_end = eb;
-                t.diag = (symmetric && j0 == i0) ? 1 : 0;
-                out.push_back(t);
+        const int nti = (ea - sa + tm - 1) / tm, ntj = (eb - sb + tn - 1) / tn;
+        for (int bi = 0; bi < nti; bi += group) {
+            for (int bj = symmetric ? bi : 0; bj < ntj; bj += group) {
+                for (int ti = bi; ti < std::min(nti, bi + group); ++ti) {
+                    const int i0 = sa + ti * tm;
+                    for (int tj = bj; tj < std::min(ntj, bj + group); ++tj) {
+                        const int j0 = sb + tj * tn;
+                        if (symmetric && j0 < i0) continue;
+                        PairTile t{};
+                        t.a0 = i0;
+                        t.a_end = ea;
+                        t.b0 = j0;
+                        t.b_end = eb;
+                        t.diag = (symmetric && j0 == i0) ? 1 : 0;
+                        out.push_back(t);
+                    }
+                }
             }
         }
     }

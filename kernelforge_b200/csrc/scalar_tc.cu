@@ -25,6 +25,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <memory>
 #include <cmath>
 #include <mutex>
 
@@ -429,10 +430,16 @@ template <class Tin>
 kfb_status run_tc(const ScalarProblem &p, const PairSink &sink, cudaStream_t s) {
     std::vector<int> labels = collect_labels(p.s1, p.symmetric ? nullptr : &p.s2);
     if (labels.empty()) return KFB_OK;
+    TraceScope tr_all("scalar_tc", s);
+    auto tr_plan = std::make_unique<TraceScope>("scalar_tc:plan", s);
     Buckets b1 = make_buckets(p.s1, labels);
     Buckets b2 = p.symmetric ? Buckets() : make_buckets(p.s2, labels);
     const Buckets &bb = p.symmetric ? b1 : b2;
-    std::vector<PairTile> tiles = make_pair_tiles(b1, bb, p.symmetric, BM, BN);
+    // packed rows: hi + lo fp16 halves of Dp columns
+    const size_t packed_row_bytes = (size_t)((p.rep + 7) / 8 * 8) * 2 * sizeof(__half);
+    std::vector<PairTile> tiles = make_pair_tiles(b1, bb, p.symmetric, BM, BN, packed_row_bytes);
+    tr_plan.reset();
+    auto tr_pack = std::make_unique<TraceScope>("scalar_tc:pack", s);
     if (tiles.empty()) return KFB_OK;
     const int L = (int)labels.size();
     const int Dp = (p.rep + 7) / 8 * 8;
@@ -470,6 +477,8 @@ kfb_status run_tc(const ScalarProblem &p, const PairSink &sink, cudaStream_t s) 
 
     DevBuf dtiles, derr;
     KFB_TRY(upload(dtiles, tiles, s));
+    tr_pack.reset();
+    TraceScope tr_kern("scalar_tc:kernel+wait", s);
     KFB_TRY(derr.alloc(sizeof(int), s));
     KFB_TRY(zero(derr.ptr, sizeof(int), s));
 

@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cmath>
 #include <functional>
+#include <memory>
 #include <vector>
 
 #include "kernels_common.cuh"
@@ -348,18 +349,6 @@ __global__ void rfp_deflate_kernel(const float *K, int n, int layout, const doub
 
 inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 
-struct Dot {
-    DevBuf buf;
-    kfb_status init(cudaStream_t s) { return buf.alloc(sizeof(double), s); }
-    kfb_status operator()(const double *a, const double *b, int n, cudaStream_t s, double &out) {
-        KFB_TRY(zero(buf.ptr, sizeof(double), s));
-        dot_kernel<<<std::min(nblk(n, 256), 1184u), 256, 0, s>>>(a, b, n, buf.as<double>());
-        KFB_CUDA_TRY(cudaGetLastError());
-        KFB_CUDA_TRY(cudaMemcpyAsync(&out, buf.ptr, sizeof(double), cudaMemcpyDeviceToHost, s));
-        KFB_CUDA_TRY(cudaStreamSynchronize(s));
-        return KFB_OK;
-    }
-};
 
 }  // namespace
 
@@ -476,43 +465,146 @@ __global__ void project_out_kernel(const float *__restrict__ z, const double *__
     }
 }
 
-// The dominant eigenpair (mu, v) of a symmetric positive semi-definite
-// operator by power iteration, and lam2, an upper estimate of the norm of the
-// operator with that pair removed (a few power steps orthogonal to v; Rayleigh
-// quotients approach the norm from below, hence the factor 1.5).
-kfb_status power_dominant(const ApplyFn &A, int n, double *v, double *w, double *tmp, Dot &dot,
-                          cudaStream_t s, double &mu, double &lam2) {
-    const unsigned gb = nblk(n, 256);
-    mu = 0.0;
-    fill_kernel<<<gb, 256, 0, s>>>(v, 1.0 / std::sqrt((double)n), n);
-    for (int k = 0; k < 30; ++k) {
-        KFB_TRY(A(v, 0.0, tmp));
-        double vav = 0.0, tt = 0.0;
-        KFB_TRY(dot(v, tmp, n, s, vav));
-        KFB_TRY(dot(tmp, tmp, n, s, tt));
-        if (!(tt > 0.0)) break;
-        scale_copy_kernel<<<gb, 256, 0, s>>>(tmp, 1.0 / std::sqrt(tt), n, v);
-        const bool done = k > 2 && std::fabs(vav - mu) <= 1e-13 * std::fabs(vav);
-        mu = vav;
-        if (done) break;
+// ---- device-resident scalars of the iterative solves: the dot products,
+// step lengths and norms stay on the device, so an iteration enqueues its
+// kernels without waiting for the host; the host reads a pair (rr, flag)
+// once per CG iteration, one iteration behind, to stop.
+enum : int {
+    S_NRM = 0, S_VAV, S_WAW, S_WW, S_VW, S_LAM2, S_PQ, S_RZ0, S_RZ1, S_WR, S_Y2,
+    S_RR, S_FLAG,  // adjacent: copied to the host together
+    S_COUNT = 16
+};
+
+// out[slot] = 0 for the listed slots
+__global__ void zero_slots_kernel(double *sc, int a, int b, int c) {
+    if (threadIdx.x == 0) {
+        if (a >= 0) sc[a] = 0.0;
+        if (b >= 0) sc[b] = 0.0;
+        if (c >= 0) sc[c] = 0.0;
     }
-    lam2 = 0.0;
+}
+// out = a / sqrt(sc[i]) (a unchanged if sc[i] <= 0)
+__global__ void scale_rsqrt_kernel(const double *a, const double *sc, int i, int n, double *out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const double t = sc[i];
+    if (k < n) out[k] = t > 0.0 ? a[k] / sqrt(t) : a[k];
+}
+// y += mult * sc[i] * x
+__global__ void axpy_dev_kernel(const double *x, const double *sc, int i, double mult, int n,
+                                double *y) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) y[k] += mult * sc[i] * x[k];
+}
+// sc[LAM2] = max(sc[LAM2], sc[WAW] / sc[WW])
+__global__ void lam2_update_kernel(double *sc) {
+    if (threadIdx.x == 0) {
+        const double ww = sc[S_WW];
+        if (ww > 0.0) sc[S_LAM2] = fmax(sc[S_LAM2], sc[S_WAW] / ww);
+    }
+}
+// CG update with alpha = rz / pq from the device: x += alpha p, r -= alpha q.
+// A non-positive curvature with a nonzero residual raises the flag.
+__global__ void cg_update_kernel(const double *p, const double *q, double *x, double *r, int n,
+                                 double *sc, int rz_slot) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const double pq = sc[S_PQ], rz = sc[rz_slot];
+    const double a = pq > 0.0 ? rz / pq : 0.0;
+    if (k == 0 && !(pq > 0.0) && rz > 0.0) sc[S_FLAG] = 1.0;
+    if (k < n) {
+        x[k] += a * p[k];
+        r[k] -= a * q[k];
+    }
+}
+// out = (float)(a / sqrt(sc[i])) (unscaled if sc[i] <= 0)
+__global__ void scale_to_float_dev_kernel(const double *a, const double *sc, int i, int n,
+                                          float *out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const double t = sc[i];
+    if (k < n) out[k] = (float)(t > 0.0 ? a[k] / sqrt(t) : a[k]);
+}
+// out = sqrt(sc[i]) * (double)a
+__global__ void float_to_double_dev_kernel(const float *a, const double *sc, int i, int n,
+                                           double *out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const double t = sc[i];
+    if (k < n) out[k] = (t > 0.0 ? sqrt(t) : 1.0) * (double)a[k];
+}
+// p = z + beta p with beta = sc[new] / sc[old]
+__global__ void xpby_dev_kernel(const double *z, const double *sc, int new_slot, int old_slot,
+                                int n, double *p) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const double o = sc[old_slot];
+    const double beta = o > 0.0 ? sc[new_slot] / o : 0.0;
+    if (k < n) p[k] = z[k] + beta * p[k];
+}
+
+struct DevScalars {
+    DevBuf buf;
+    double *host = nullptr;  // pinned, 4 doubles: two (rr, flag) pairs
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    kfb_status init(cudaStream_t s) {
+        KFB_TRY(buf.alloc(S_COUNT * sizeof(double), s));
+        KFB_TRY(zero(buf.ptr, S_COUNT * sizeof(double), s));
+        // pinned host slots, allocated once per thread (cudaMallocHost synchronises)
+        static thread_local double *pinned = nullptr;
+        if (!pinned) KFB_CUDA_TRY(cudaMallocHost(&pinned, 4 * sizeof(double)));
+        host = pinned;
+        for (auto &e : ev) KFB_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        return KFB_OK;
+    }
+    ~DevScalars() {
+        for (auto &e : ev)
+            if (e) cudaEventDestroy(e);
+    }
+    double *sc() const { return buf.as<double>(); }
+    // sc[slot] += a . b (the slot is zeroed first), no host wait
+    kfb_status dot(const double *a, const double *b, int n, int slot, cudaStream_t s) {
+        zero_slots_kernel<<<1, 32, 0, s>>>(sc(), slot, -1, -1);
+        dot_kernel<<<std::min(nblk(n, 256), 1184u), 256, 0, s>>>(a, b, n, sc() + slot);
+        KFB_CUDA_TRY(cudaGetLastError());
+        return KFB_OK;
+    }
+    kfb_status read(int slot, double &out, cudaStream_t s) {
+        KFB_CUDA_TRY(cudaMemcpyAsync(&out, sc() + slot, sizeof(double), cudaMemcpyDeviceToHost, s));
+        KFB_CUDA_TRY(cudaStreamSynchronize(s));
+        return KFB_OK;
+    }
+};
+
+// The dominant eigenpair (mu, v) of a symmetric positive semi-definite
+// operator by 20 power steps, and lam2, an upper estimate of the norm of the
+// operator with that pair removed (8 power steps orthogonal to v; Rayleigh
+// quotients approach the norm from below, hence the factor 1.5).  All on the
+// device; one host read at the end.
+kfb_status power_dominant(const ApplyFn &A, int n, double *v, double *w, double *tmp,
+                          DevScalars &ds, cudaStream_t s, double &mu, double &lam2) {
+    const unsigned gb = nblk(n, 256);
+    double *sc = ds.sc();
+    fill_kernel<<<gb, 256, 0, s>>>(v, 1.0 / std::sqrt((double)n), n);
+    for (int k = 0; k < 20; ++k) {
+        KFB_TRY(A(v, 0.0, tmp));
+        KFB_TRY(ds.dot(v, tmp, n, S_VAV, s));
+        KFB_TRY(ds.dot(tmp, tmp, n, S_NRM, s));
+        scale_rsqrt_kernel<<<gb, 256, 0, s>>>(tmp, sc, S_NRM, n, v);
+    }
+    zero_slots_kernel<<<1, 32, 0, s>>>(sc, S_LAM2, -1, -1);
     fill_alt_kernel<<<gb, 256, 0, s>>>(w, 1.0 / std::sqrt((double)n), n);
     for (int k = 0; k < 8; ++k) {
-        double vw = 0.0;
-        KFB_TRY(dot(v, w, n, s, vw));
-        axpy_kernel<<<gb, 256, 0, s>>>(v, -vw, n, w);
+        KFB_TRY(ds.dot(v, w, n, S_VW, s));
+        axpy_dev_kernel<<<gb, 256, 0, s>>>(v, sc, S_VW, -1.0, n, w);
         KFB_TRY(A(w, 0.0, tmp));
-        double waw = 0.0, tt = 0.0, ww = 0.0;
-        KFB_TRY(dot(w, tmp, n, s, waw));
-        KFB_TRY(dot(w, w, n, s, ww));
-        KFB_TRY(dot(tmp, tmp, n, s, tt));
-        lam2 = std::max(lam2, waw / std::max(ww, 1e-300));
-        if (!(tt > 0.0)) break;
-        scale_copy_kernel<<<gb, 256, 0, s>>>(tmp, 1.0 / std::sqrt(tt), n, w);
+        KFB_TRY(ds.dot(w, tmp, n, S_WAW, s));
+        KFB_TRY(ds.dot(w, w, n, S_WW, s));
+        KFB_TRY(ds.dot(tmp, tmp, n, S_NRM, s));
+        lam2_update_kernel<<<1, 32, 0, s>>>(sc);
+        scale_rsqrt_kernel<<<gb, 256, 0, s>>>(tmp, sc, S_NRM, n, w);
     }
-    lam2 *= 1.5;
     KFB_CUDA_TRY(cudaGetLastError());
+    double h[S_COUNT];
+    KFB_CUDA_TRY(cudaMemcpyAsync(h, sc, sizeof(h), cudaMemcpyDeviceToHost, s));
+    KFB_CUDA_TRY(cudaStreamSynchronize(s));
+    mu = h[S_VAV];
+    lam2 = 1.5 * h[S_LAM2];
     return KFB_OK;
 }
 
@@ -531,7 +623,7 @@ kfb_status power_dominant(const ApplyFn &A, int n, double *v, double *w, double 
 kfb_status mixed_core(const ApplyFn &A, const float *B, int n, kfb_layout uplo, const double *v,
                       double fcoef, double defl, double lam2, const double *y, double l2,
                       double tol, int maxit, int flags, double *alpha, kfb_solve_info &inf,
-                      Dot &dot, cudaStream_t s) {
+                      DevScalars &ds, cudaStream_t s) {
     const size_t nt = (size_t)n * (n + 1) / 2;
     DevBuf F, r, z, p, q, f32v, dw;
     KFB_TRY(F.alloc(nt * sizeof(float), s));
@@ -544,19 +636,19 @@ kfb_status mixed_core(const ApplyFn &A, const float *B, int n, kfb_layout uplo, 
     const unsigned gb = nblk(n, 256);
     const dim3 blk2(32, 8), grd2(nblk(n, 32), nblk(n, 8));
     const double u32 = 5.960464477539063e-08;
+    double *sc = ds.sc();
+    KFB_TRY(ds.dot(y, y, n, S_Y2, s));
     double ynorm2 = 0.0;
-    KFB_TRY(dot(y, y, n, s, ynorm2));
+    KFB_TRY(ds.read(S_Y2, ynorm2, s));
     const double ynorm = std::sqrt(ynorm2);
     KFB_TRY(zero(alpha, (size_t)n * sizeof(double), s));
     if (ynorm == 0.0) return KFB_OK;
 
-    // F^{-1} x via the FP32 factor, with x scaled to unit norm first
-    auto solve_f = [&](const double *x, double xnorm, double *out) -> kfb_status {
-        const double sc = xnorm > 0.0 ? 1.0 / xnorm : 1.0;
-        scale_to_float_kernel<<<gb, 256, 0, s>>>(x, sc, n, f32v.as<float>());
+    // out = F^{-1} x, x scaled to unit norm by the device scalar sc[slot] = |x|^2
+    auto solve_f_dev = [&](const double *x, int slot, double *out) -> kfb_status {
+        scale_to_float_dev_kernel<<<gb, 256, 0, s>>>(x, sc, slot, n, f32v.as<float>());
         KFB_TRY(rfp_potrs(F.ptr, f32v.ptr, n, 1, uplo, KFB_F32, s));
-        float_to_double_kernel<<<gb, 256, 0, s>>>(f32v.as<float>(), xnorm > 0.0 ? xnorm : 1.0, n,
-                                                  out);
+        float_to_double_dev_kernel<<<gb, 256, 0, s>>>(f32v.as<float>(), sc, slot, n, out);
         KFB_CUDA_TRY(cudaGetLastError());
         return KFB_OK;
     };
@@ -564,6 +656,7 @@ kfb_status mixed_core(const ApplyFn &A, const float *B, int n, kfb_layout uplo, 
     auto attempt = [&](double lam) -> kfb_status {
         double shift = std::max(0.0, 2.0 * u32 * lam2 - lam);
         int finfo = 0;
+        auto tr_f = std::make_unique<TraceScope>("mixed:factor", s);
         for (int a = 0; a < 12; ++a) {
             rfp_deflate_kernel<<<grd2, blk2, 0, s>>>(B, n, uplo, v, fcoef, F.as<float>());
             KFB_CUDA_TRY(cudaGetLastError());
@@ -576,72 +669,114 @@ kfb_status mixed_core(const ApplyFn &A, const float *B, int n, kfb_layout uplo, 
         if (finfo != 0)
             return set_error(KFB_ERR_NOT_PD,
                              "FP32 RFP Cholesky failed even with shift %g (info=%d)", shift, finfo);
-        KFB_TRY(solve_f(v, 1.0, dw.as<double>()));  // w = F^{-1} v
+        tr_f.reset();
+        TraceScope tr_cg("mixed:cg", s);
+        // w = F^{-1} v (v has unit norm: slot S_NRM set to 1 for the scaling)
+        {
+            const double one = 1.0;
+            KFB_CUDA_TRY(cudaMemcpyAsync(sc + S_NRM, &one, sizeof(double), cudaMemcpyHostToDevice,
+                                         s));
+            KFB_TRY(solve_f_dev(v, S_NRM, dw.as<double>()));
+        }
         double vfv = 0.0;
-        KFB_TRY(dot(v, dw.as<double>(), n, s, vfv));
+        KFB_TRY(ds.dot(v, dw.as<double>(), n, S_VW, s));
+        KFB_TRY(ds.read(S_VW, vfv, s));
         const double sm_coef = defl / (1.0 + defl * vfv);
-        // M^{-1} r = F^{-1} r - sm_coef (w . r) w
-        auto precond = [&](const double *vec, double vnorm, double *out) -> kfb_status {
-            KFB_TRY(solve_f(vec, vnorm, out));
-            double wr = 0.0;
-            KFB_TRY(dot(dw.as<double>(), vec, n, s, wr));
-            axpy_kernel<<<gb, 256, 0, s>>>(dw.as<double>(), -sm_coef * wr, n, out);
+        // M^{-1} x = F^{-1} x - sm_coef (w . x) w, with |x|^2 in sc[slot]
+        auto precond = [&](const double *x, int slot, double *out) -> kfb_status {
+            KFB_TRY(solve_f_dev(x, slot, out));
+            KFB_TRY(ds.dot(dw.as<double>(), x, n, S_WR, s));
+            axpy_dev_kernel<<<gb, 256, 0, s>>>(dw.as<double>(), sc, S_WR, -sm_coef, n, out);
             KFB_CUDA_TRY(cudaGetLastError());
             return KFB_OK;
         };
-        // preconditioned conjugate gradients in FP64 from alpha = 0
+        // preconditioned conjugate gradients in FP64 from alpha = 0; when the
+        // recurrence residual meets the tolerance but the true one y - A alpha
+        // does not (their gap grows with the condition number), CG restarts
+        // from alpha with the true residual (at most 4 restarts)
         KFB_TRY(zero(alpha, (size_t)n * sizeof(double), s));
-        KFB_CUDA_TRY(cudaMemcpyAsync(r.ptr, y, (size_t)n * sizeof(double),
-                                     cudaMemcpyDeviceToDevice, s));
-        double rn = ynorm;
-        KFB_TRY(precond(r.as<double>(), rn, z.as<double>()));
-        KFB_CUDA_TRY(cudaMemcpyAsync(p.ptr, z.ptr, (size_t)n * sizeof(double),
-                                     cudaMemcpyDeviceToDevice, s));
-        double rz = 0.0;
-        KFB_TRY(dot(r.as<double>(), z.as<double>(), n, s, rz));
-        int it = 0;
-        for (; it < maxit; ++it) {
-            KFB_TRY(A(p.as<double>(), lam, q.as<double>()));  // q = (A + lam I) p
-            double pq = 0.0;
-            KFB_TRY(dot(p.as<double>(), q.as<double>(), n, s, pq));
-            if (!(pq > 0.0)) {
-                inf.iterations = it;
+        int total_it = 0;
+        double rel = 0.0;
+        for (int restart = 0; restart < 5; ++restart) {
+            // r = y - (A + lam I) alpha
+            KFB_CUDA_TRY(cudaMemcpyAsync(r.ptr, y, (size_t)n * sizeof(double),
+                                         cudaMemcpyDeviceToDevice, s));
+            if (restart > 0) {
+                KFB_TRY(A(alpha, lam, q.as<double>()));
+                axpy_kernel<<<gb, 256, 0, s>>>(q.as<double>(), -1.0, n, r.as<double>());
+            }
+            zero_slots_kernel<<<1, 32, 0, s>>>(sc, S_FLAG, -1, -1);
+            KFB_TRY(ds.dot(r.as<double>(), r.as<double>(), n, S_RR, s));
+            KFB_TRY(precond(r.as<double>(), S_RR, z.as<double>()));
+            KFB_CUDA_TRY(cudaMemcpyAsync(p.ptr, z.ptr, (size_t)n * sizeof(double),
+                                         cudaMemcpyDeviceToDevice, s));
+            KFB_TRY(ds.dot(r.as<double>(), z.as<double>(), n, S_RZ0, s));
+            int it = 0;
+            bool indefinite = false;
+            const int budget = maxit - total_it;
+            for (; it < budget; ++it) {
+                const int rz_cur = (it & 1) ? S_RZ1 : S_RZ0, rz_new = (it & 1) ? S_RZ0 : S_RZ1;
+                KFB_TRY(A(p.as<double>(), lam, q.as<double>()));  // q = (A + lam I) p
+                KFB_TRY(ds.dot(p.as<double>(), q.as<double>(), n, S_PQ, s));
+                cg_update_kernel<<<gb, 256, 0, s>>>(p.as<double>(), q.as<double>(), alpha,
+                                                    r.as<double>(), n, sc, rz_cur);
+                KFB_TRY(ds.dot(r.as<double>(), r.as<double>(), n, S_RR, s));
+                KFB_CUDA_TRY(cudaMemcpyAsync(ds.host + 2 * (it & 1), sc + S_RR,
+                                             2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+                KFB_CUDA_TRY(cudaEventRecord(ds.ev[it & 1], s));
+                KFB_TRY(precond(r.as<double>(), S_RR, z.as<double>()));
+                KFB_TRY(ds.dot(r.as<double>(), z.as<double>(), n, rz_new, s));
+                xpby_dev_kernel<<<gb, 256, 0, s>>>(z.as<double>(), sc, rz_new, rz_cur, n,
+                                                   p.as<double>());
+                KFB_CUDA_TRY(cudaGetLastError());
+                // stop test on the previous iteration's residual (the device runs one ahead)
+                const int chk = it - 1;
+                if (chk >= 0) {
+                    KFB_CUDA_TRY(cudaEventSynchronize(ds.ev[chk & 1]));
+                    const double rr = ds.host[2 * (chk & 1)], fl = ds.host[2 * (chk & 1) + 1];
+                    if (fl != 0.0) {
+                        indefinite = true;
+                        it = chk;
+                        break;
+                    }
+                    if (std::sqrt(rr) <= tol * ynorm) {
+                        ++it;
+                        break;
+                    }
+                }
+            }
+            if (!indefinite && it > 0 && it >= budget) {
+                KFB_CUDA_TRY(cudaEventSynchronize(ds.ev[(it - 1) & 1]));
+                if (ds.host[2 * ((it - 1) & 1) + 1] != 0.0) indefinite = true;
+            }
+            total_it += it;
+            if (indefinite) {
+                inf.iterations = total_it;
                 return set_error(KFB_ERR_NOT_PD,
-                                 "the system is indefinite at the precision of its matrix (p^T A "
-                                 "p = %.3e after %d CG iterations, l2 = %g); use a larger l2",
-                                 pq, it, lam);
+                                 "the system is indefinite at the precision of its matrix "
+                                 "(non-positive p^T A p after %d CG iterations, l2 = %g); use a "
+                                 "larger l2",
+                                 total_it, lam);
             }
-            const double a = rz / pq;
-            axpy_kernel<<<gb, 256, 0, s>>>(p.as<double>(), a, n, alpha);
-            axpy_kernel<<<gb, 256, 0, s>>>(q.as<double>(), -a, n, r.as<double>());
+            // true residual of alpha
+            KFB_TRY(A(alpha, lam, q.as<double>()));
+            KFB_CUDA_TRY(cudaMemcpyAsync(r.ptr, y, (size_t)n * sizeof(double),
+                                         cudaMemcpyDeviceToDevice, s));
+            axpy_kernel<<<gb, 256, 0, s>>>(q.as<double>(), -1.0, n, r.as<double>());
+            KFB_TRY(ds.dot(r.as<double>(), r.as<double>(), n, S_RR, s));
             double rr = 0.0;
-            KFB_TRY(dot(r.as<double>(), r.as<double>(), n, s, rr));
-            rn = std::sqrt(rr);
-            if (rn <= tol * ynorm) {
-                ++it;
-                break;
-            }
-            KFB_TRY(precond(r.as<double>(), rn, z.as<double>()));
-            double rz_new = 0.0;
-            KFB_TRY(dot(r.as<double>(), z.as<double>(), n, s, rz_new));
-            xpby_kernel<<<gb, 256, 0, s>>>(z.as<double>(), rz_new / rz, n, p.as<double>());
-            rz = rz_new;
+            KFB_TRY(ds.read(S_RR, rr, s));
+            rel = std::sqrt(rr) / ynorm;
+            if (rel <= tol || total_it >= maxit) break;
         }
-        // true residual of the returned alpha
-        KFB_TRY(A(alpha, lam, q.as<double>()));
-        KFB_CUDA_TRY(cudaMemcpyAsync(r.ptr, y, (size_t)n * sizeof(double),
-                                     cudaMemcpyDeviceToDevice, s));
-        axpy_kernel<<<gb, 256, 0, s>>>(q.as<double>(), -1.0, n, r.as<double>());
-        double rr = 0.0;
-        KFB_TRY(dot(r.as<double>(), r.as<double>(), n, s, rr));
-        inf.iterations = it;
+        inf.iterations = total_it;
         inf.used_cg = 1;
-        inf.rel_residual = std::sqrt(rr) / ynorm;
+        inf.rel_residual = rel;
         if (inf.rel_residual > tol)
             return set_error(KFB_ERR_NO_CONVERGENCE,
                              "refinement stopped at relative residual %.3e (tol %.1e) after %d "
                              "iterations",
-                             inf.rel_residual, tol, it);
+                             inf.rel_residual, tol, total_it);
         return KFB_OK;
     };
 
@@ -667,13 +802,14 @@ kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2
     kfb_solve_info inf{};
     inf.lambda_eff = l2;
     DevBuf Kd, dv, dw, dtmp;
+    TraceScope tr_all("krr_solve", s);
     KFB_TRY(Kd.alloc((size_t)n * n * sizeof(float), s));
     KFB_TRY(rfp_to_full(k_rfp, n, uplo, KFB_F32, Kd.ptr, s));
     KFB_TRY(dv.alloc((size_t)n * sizeof(double), s));
     KFB_TRY(dw.alloc((size_t)n * sizeof(double), s));
     KFB_TRY(dtmp.alloc((size_t)n * sizeof(double), s));
-    Dot dot;
-    KFB_TRY(dot.init(s));
+    DevScalars ds;
+    KFB_TRY(ds.init(s));
     const unsigned gw = nblk((long long)n * 32, 256);
     ApplyFn A = [&](const double *x, double lam, double *out) -> kfb_status {
         dense_apply_kernel<<<gw, 256, 0, s>>>(Kd.as<float>(), x, n, lam, out);
@@ -681,18 +817,23 @@ kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2
         return KFB_OK;
     };
     double ynorm2 = 0.0;
-    KFB_TRY(dot(y, y, n, s, ynorm2));
+    KFB_TRY(ds.dot(y, y, n, S_Y2, s));
+    KFB_TRY(ds.read(S_Y2, ynorm2, s));
     if (ynorm2 == 0.0) {
         KFB_TRY(zero(alpha, (size_t)n * sizeof(double), s));
         if (info) *info = inf;
         return KFB_OK;
     }
     double mu = 0.0, lam2 = 0.0;
-    KFB_TRY(power_dominant(A, n, dv.as<double>(), dw.as<double>(), dtmp.as<double>(), dot, s, mu,
-                           lam2));
+    {
+        TraceScope tr("krr_solve:power", s);
+        KFB_TRY(power_dominant(A, n, dv.as<double>(), dw.as<double>(), dtmp.as<double>(), ds, s,
+                               mu, lam2));
+    }
     const double defl = std::max(0.0, mu - lam2);
+    TraceScope tr_core("krr_solve:factor+cg", s);
     const kfb_status st = mixed_core(A, k_rfp, n, uplo, dv.as<double>(), defl, defl, lam2, y, l2,
-                                     tol, maxit, flags, alpha, inf, dot, s);
+                                     tol, maxit, flags, alpha, inf, ds, s);
     if (info) *info = inf;
     return st;
 }
@@ -718,8 +859,8 @@ kfb_status ridge_solve_mixed(const float *zf, const double *y, int nm, int d, do
     KFB_TRY(dv.alloc((size_t)d * sizeof(double), s));
     KFB_TRY(dw.alloc((size_t)d * sizeof(double), s));
     KFB_TRY(dtmp.alloc((size_t)d * sizeof(double), s));
-    Dot dot;
-    KFB_TRY(dot.init(s));
+    DevScalars ds;
+    KFB_TRY(ds.init(s));
     const int mchunk = 256;
     const dim3 gty(nblk(d, 128), nblk(nm, mchunk));
     const unsigned gzx = nblk((long long)nm * 32, 256);
@@ -737,7 +878,7 @@ kfb_status ridge_solve_mixed(const float *zf, const double *y, int nm, int d, do
     zty_kernel<<<gty, 128, 0, s>>>(zf, y, nm, d, mchunk, rhs.as<double>());
     KFB_CUDA_TRY(cudaGetLastError());
     double mu = 0.0, lam2 = 0.0;
-    KFB_TRY(power_dominant(A, d, dv.as<double>(), dw.as<double>(), dtmp.as<double>(), dot, s, mu,
+    KFB_TRY(power_dominant(A, d, dv.as<double>(), dw.as<double>(), dtmp.as<double>(), ds, s, mu,
                            lam2));
     // B = Z1^T Z1 in RFP, Z1 = Z with v projected out
     DevBuf z1, full, B;
@@ -757,7 +898,7 @@ kfb_status ridge_solve_mixed(const float *zf, const double *y, int nm, int d, do
     const double defl = std::max(0.0, mu - lam2);
     // F = B + lam2 v v^T (eigenvalue ~lam2 along v), M = F + defl v v^T ~ Z^T Z
     const kfb_status st = mixed_core(A, B.as<float>(), d, KFB_RFP_L, dv.as<double>(), -lam2, defl,
-                                     lam2, rhs.as<double>(), l2, tol, maxit, flags, w, inf, dot,
+                                     lam2, rhs.as<double>(), l2, tol, maxit, flags, w, inf, ds,
                                      s);
     if (info) *info = inf;
     return st;

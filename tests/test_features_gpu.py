@@ -254,7 +254,8 @@ def test_ridge_with_dominant_mode_below_fp32_resolution():
     ev = np.linalg.eigvalsh(A)
     assert ev[-1] / ev[0] > 1e9          # far beyond FP32
     l2 = 1e-3
-    w, info = fit_ridge(cuda(Zh), cuda(y), l2=l2, tol=1e-13, maxit=2000)
+    # the FP64 residual floor of this system is ~1e-12 relative (|A| |w| >> |Z^T y|)
+    w, info = fit_ridge(cuda(Zh), cuda(y), l2=l2, tol=1e-11, maxit=2000)
     ref = np.linalg.solve(A + l2 * np.eye(d), Zd.T @ y)
     assert info["converged"] and info["lambda_eff"] == l2, info
     assert rel(w.cpu().numpy(), ref) <= 1e-6
