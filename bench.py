@@ -544,10 +544,49 @@ def run_config3(args):
             torch.cuda.current_stream().cuda_stream))
         err = sub.double().cpu().numpy() - ref
         cpu["gpu_rel_frobenius_err"] = float(np.linalg.norm(err) / np.linalg.norm(ref))
+    # force prediction of an energy-trained KRR model on the 1,000 training
+    # molecules: E_b = sum_a alpha_a K(a, b), so F_b = -alpha^T K_jac[:, b]
+    # (K_jac = +dK/dR_b); tensor-core path (split-fp16 kernels, mixed solve)
+    # against the FP64 GPU path, both with lambda 1e-2 and the per-element
+    # energy baseline of the training molecules
+    from kernelforge_b200 import cuda_global_kernels as cgk
+    from kernelforge_b200 import cuda_local_kernels as clk
+    from kernelforge_b200 import kernelmath as km_ours
+    from kernelforge_b200 import local_kernels as lk_ours
+    from kernelforge_b200.feature_maps import element_baseline
+    lam3 = 1e-2
+    Qe1 = np.full(Q1.shape, -1, np.int32)
+    for k, z in enumerate((1, 6, 7, 8)):
+        Qe1[Q1 == z] = k
+    Qe1[np.arange(ma1)[None, :] >= N1[:, None]] = -1
+    coef, counts = element_baseline(Qe1, N1, tr.E, 4)
+    yres = tr.E - counts @ coef
+    ym3 = yres.mean()
+    Fte = np.concatenate([np.asarray(f).reshape(-1) for f in te.F])
+    Kt = clk.kernel_gaussian_symm_rfp(x1, Q1, N1, SIGMA)
+    a_tc, _ = cgk.krr_solve_mixed(Kt, torch.tensor(yres - ym3, device="cuda"), l2=lam3, uplo="L",
+                                  tol=TOL, lambda_floor=True)
+    make_step("split_f16")()
+    f_tc = -(a_tc.to(torch.float64) @ out.to(torch.float64)).cpu().numpy()
+    K64 = lk_ours.kernel_gaussian_symm_rfp(X1.astype(np.float64), Q1, N1, SIGMA)
+    a64 = km_ours.cho_solve_rfp(K64, yres - ym3, lam3)
+    x1d, x2d, dx2d = x1.double(), x2.double(), dx2.double()
+    J64 = torch.empty((nm1, naq2), dtype=torch.float64, device="cuda")
+    _lib.check(lib.kfb_kernel_gaussian_jacobian(
+        x1d.data_ptr(), x2d.data_ptr(), dx2d.data_ptr(), Q1.ctypes.data, Q2.ctypes.data,
+        N1.ctypes.data, N2.ctypes.data, nm1, nm2, ma1, ma2, rep, naq2, SIGMA, _lib.KFB_F64,
+        _lib.PREC["fp64"], J64.data_ptr(), torch.cuda.current_stream().cuda_stream))
+    f_64 = -(torch.tensor(a64, device="cuda") @ J64).cpu().numpy()
+    del x1d, x2d, dx2d, J64
+    force_mae = {"tensor_core": float(np.abs(f_tc - Fte).mean()),
+                 "fp64_gpu": float(np.abs(f_64 - Fte).mean()),
+                 "pred_rel_diff": float(np.linalg.norm(f_tc - f_64) / np.linalg.norm(f_64)),
+                 "lambda": lam3, "train": "energies of the 1,000 training molecules"}
     _line("FCHL19 local Jacobian kernel: entries/s", entries / (ms * 1e-3), "entries/s", ms, args,
           f"kernel_gaussian_jacobian {nm1} x {nm2} molecules (9-30 atoms), naq2={naq2}, "
           "v rows on CUDA cores + contraction on tcgen05 (split fp16)", "f16x3 / f32",
-          {"cpu_baseline": cpu, "shape": [nm1, naq2], "fp32_cuda_core_ms": ms_fp32})
+          {"cpu_baseline": cpu, "shape": [nm1, naq2], "fp32_cuda_core_ms": ms_fp32,
+           "force_prediction_mae": force_mae})
 
 
 def _full_asym(X1, dX1, Q1, N1, X2, dX2, Q2, N2, precision, dt):
@@ -740,8 +779,9 @@ def run_config5(args):
     from kernelforge_b200 import cuda_rff_features as crf
     from kernelforge_b200 import local_kernels as lk_ours
     from kernelforge_b200 import synthetic
-    from kernelforge_b200.feature_maps import (CosMLPFeatureMap, fit_ridge, judge_feature_model,
-                                               pair_targets, predict_linear, sample_pairs)
+    from kernelforge_b200.feature_maps import (CosMLPFeatureMap, element_baseline, fit_ridge,
+                                               judge_feature_model, pair_targets, predict_linear,
+                                               sample_pairs)
     nmol, npairs, epochs = args.c5_nmol, args.c5_pairs, args.c5_epochs
     D, H = 4096, 512
     t_data = time.perf_counter()
@@ -756,6 +796,11 @@ def run_config5(args):
     train = np.sort(perm[1000:])
     exact_train = np.sort(perm[1000:5000])
     X = torch.tensor(Xh, device="cuda")
+    # one per-element energy baseline (least squares on element counts, as the
+    # reference's models fit it) from the 49,000 training molecules, subtracted
+    # for every model; ym is then the mean of the residual energies
+    coef, counts = element_baseline(Qe, N, y, len(C5_ELEMENTS), molecules=train)
+    y = y - counts @ coef
     ym = y[train].mean()
     yd = torch.tensor(y - ym, device="cuda")
     itest = torch.tensor(test, device="cuda")
@@ -949,6 +994,8 @@ def run_config5(args):
                         "solve": info_e, "fp64_fit_predict_s": t_exact64,
                         "fp64_test_mae": mae_exact64},
            "judge_learned": judge, "judge_rff": judge_rff,
+           "energy_baseline": "per-element least squares on element counts (49,000 training "
+                              "molecules), the same for every model",
            "data_prep_s": t_data, "cpu_baseline": cpu})
 
 def main():

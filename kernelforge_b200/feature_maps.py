@@ -29,7 +29,7 @@ from . import _lib
 from ._device import host_i32, require_cuda, stream_handle
 
 __all__ = ["CosMLPFeatureMap", "sample_pairs", "pair_targets", "fit_ridge", "predict_linear",
-           "judge_feature_model"]
+           "judge_feature_model", "element_baseline"]
 
 
 def _x_dt(X):
@@ -324,6 +324,24 @@ def predict_linear(Z, w):
     """Z @ w in float64."""
     import torch
     return Z.to(torch.float64) @ w.to(device=Z.device, dtype=torch.float64)
+
+
+def element_baseline(Q, N, y, nelem, molecules=None):
+    """Per-element energy baseline as the reference's models fit it
+    (models/base.py:401-418): least squares of the energies on the element
+    counts of each molecule, no intercept.  Q holds element indices (-1 =
+    padding).  Returns (coef (nelem,), counts (nmol, nelem)); the baseline of
+    molecule m is counts[m] @ coef."""
+    q = host_i32(Q)
+    n = host_i32(N).reshape(-1)
+    nm, ma = q.shape
+    counts = np.zeros((nm, nelem))
+    valid = np.arange(ma)[None, :] < np.clip(n, 0, ma)[:, None]
+    for e in range(nelem):
+        counts[:, e] = np.sum((q == e) & valid, axis=1)
+    idx = np.arange(nm) if molecules is None else np.asarray(molecules)
+    coef, *_ = np.linalg.lstsq(counts[idx], np.asarray(y, np.float64)[idx], rcond=None)
+    return coef, counts
 
 
 def judge_feature_model(mae_feature, mae_exact, bound=1.01):
