@@ -55,7 +55,8 @@ def parse():
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the FP64-GPU fit and the accuracy check (profiling runs)")
     ap.add_argument("--workload", default="fit10k",
-                    choices=["fit10k", "config1", "config3", "config4", "config5"],
+                    choices=["fit10k", "config1", "config3", "config4", "config5",
+                             "cosmlp_step"],
                     help="fit10k (default): the 10,000-molecule kernel + solve; config1: FP64 "
                          "1,000-molecule fit+predict; config3: Jacobian kernel 1,000 x 1,000 "
                          "molecules; config4: energy+force kernel of 300 x 21-atom molecules "
@@ -998,11 +999,46 @@ def run_config5(args):
                               "molecules), the same for every model",
            "data_prep_s": t_data, "cpu_baseline": cpu})
 
+
+def run_cosmlp_step(args):
+    """The learned map's training step at the config-5 sizes (720 -> 512 ->
+    4096, 4 elements, 4,096 same-element pairs per step, Adam), on seeded
+    descriptor-like rows (40,000 x 720, FP32): the unit the config-5 training
+    loop repeats ~3,000 times.  Metric: tensor FLOP/s of the step's GEMMs."""
+    import torch
+
+    from kernelforge_b200.feature_maps import CosMLPFeatureMap
+    rng = np.random.default_rng(SEED + 60)
+    rows = torch.tensor((rng.standard_normal((40000, 720)) * 0.3).astype(np.float32),
+                        device="cuda")
+    fm = CosMLPFeatureMap(4, 720, 512, 4096, sigma=SIGMA, seed=SEED + 61, max_pairs=4096)
+    B = 4096
+    pi = torch.tensor(rng.integers(0, 40000, B).astype(np.int32), device="cuda")
+    pj = torch.tensor(rng.integers(0, 40000, B).astype(np.int32), device="cuda")
+    t = torch.tensor(rng.uniform(0, 1, B).astype(np.float32), device="cuda")
+    k = [0]
+
+    def step():
+        fm.step(k[0] % 4, rows, pi, pj, t)
+        k[0] += 1
+
+    ms = _events_ms(step, args.steps, max(args.warmup, 3))
+    flops = _mlp_flops_per_atom_eval() * 2 * B
+    _line("cos-MLP feature-map training step: tensor FLOP/s", flops / (ms * 1e-3) / 1e12,
+          "TFLOP/s", ms, args,
+          "cos-MLP 720-512-4096 x 4 elements, 4096 pairs per step (8192 atom rows), "
+          "BF16 GEMMs with FP32 accumulation + pair loss + Adam", "bf16 / f32",
+          {"flops_per_step": flops,
+           "roofline": {"bound": "tensor", "achieved": flops / (ms * 1e-3) / 1e12,
+                        "peak": load_peaks()[0]["bf16_tflops"], "unit": "TFLOP/s",
+                        "frac": flops / (ms * 1e-3) / 1e12 / load_peaks()[0]["bf16_tflops"],
+                        "traffic": None}})
+
 def main():
     args = parse()
     if args.workload != "fit10k":
         {"config1": run_config1, "config3": run_config3, "config4": run_config4,
-         "config5": run_config5}[args.workload](args)
+         "config5": run_config5, "cosmlp_step": run_cosmlp_step}[args.workload](args)
         return
     rank, world, local = dist_setup(args.gpus)
     try:

@@ -259,3 +259,47 @@ def test_ridge_with_dominant_mode_below_fp32_resolution():
     ref = np.linalg.solve(A + l2 * np.eye(d), Zd.T @ y)
     assert info["converged"] and info["lambda_eff"] == l2, info
     assert rel(w.cpu().numpy(), ref) <= 1e-6
+
+
+def test_training_gains_over_the_untrained_map():
+    """What the trained network gains over the method without it: on held-out
+    same-element pairs of FCHL19 atoms, the trained map's pair-kernel error is
+    several times below that of the untrained map (a random-Fourier-like map of
+    the same sigma) and below RFF at equal D."""
+    import torch
+    from kernelforge_b200 import cuda_rff_features as crf
+    from kernelforge_b200 import synthetic
+    from kernelforge_b200.feature_maps import CosMLPFeatureMap, pair_targets, sample_pairs
+    mols = synthetic.make_molecules(400, 9, 21, seed=31)
+    X, Qz, N = synthetic.fchl19_batched(mols, dtype=np.float32, device="cuda", chunk=128)
+    Qe = _elem_q(Qz, N)
+    Xd = cuda(X)
+    ma, D = X.shape[1], 1024
+    train = np.arange(300)
+    test = np.arange(300, 400)
+    pairs = sample_pairs(Qe, N, 4, 120000, seed=1, molecules=train)
+    targets = [pair_targets(Xd, pi, pj, 2.0) for pi, pj in pairs]
+    held = sample_pairs(Qe, N, 4, 8000, seed=2, molecules=test)
+    W = torch.randn((4, 720, D), generator=torch.Generator().manual_seed(3)).cuda() / 2.0
+    b = (torch.rand((4, D), generator=torch.Generator().manual_seed(4)) * 2 * np.pi).cuda()
+
+    def rmse(feat):
+        err = []
+        for e, (pi, pj) in enumerate(held):
+            if len(pi) == 0:
+                continue
+            def at(rows):
+                xa = Xd.reshape(-1, 1, 720)[torch.tensor(rows, device="cuda").long()].contiguous()
+                return feat(xa, np.full((len(rows), 1), e, np.int32), np.ones(len(rows), np.int32))
+            k = (at(pi) * at(pj)).sum(1)
+            err.append(((k - pair_targets(Xd, pi, pj, 2.0)) ** 2).double().cpu().numpy())
+        return float(np.sqrt(np.concatenate(err).mean()))
+
+    fm = CosMLPFeatureMap(4, 720, 256, D, sigma=2.0, seed=5, max_pairs=4096)
+    untrained = rmse(fm.features_elemental)
+    hist = fm.train(Xd, pairs, targets, epochs=4, lr=1e-3, batch=2048, seed=6)
+    trained = rmse(fm.features_elemental)
+    rff = rmse(lambda xa, q, n: crf.rff_features_elemental(xa, q, n, W, b))
+    assert hist[-1] < hist[0]
+    assert trained < untrained / 3, (trained, untrained)
+    assert trained < rff, (trained, rff)
