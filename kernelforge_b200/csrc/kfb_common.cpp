@@ -70,44 +70,75 @@ void DevBuf::release() {
     bytes = 0;
 }
 
+// Labels are nuclear charges or element indices: small non-negative integers
+// take a direct table, anything else a sorted set.
+static constexpr int LABEL_TABLE = 4096;
+
 std::vector<int> collect_labels(const SetView &a, const SetView *b) {
-    std::set<int> seen;
-    for (int m = 0; m < a.nm; ++m)
-        for (int i = 0; i < a.natoms(m); ++i) seen.insert(a.q[(size_t)m * a.ma + i]);
-    if (b)
-        for (int m = 0; m < b->nm; ++m)
-            for (int i = 0; i < b->natoms(m); ++i) seen.insert(b->q[(size_t)m * b->ma + i]);
-    return std::vector<int>(seen.begin(), seen.end());
+    std::vector<unsigned char> seen(LABEL_TABLE, 0);
+    std::set<int> other;
+    auto scan = [&](const SetView &v) {
+        for (int m = 0; m < v.nm; ++m) {
+            const int32_t *q = v.q + (size_t)m * v.ma;
+            const int na = v.natoms(m);
+            for (int i = 0; i < na; ++i) {
+                const int l = q[i];
+                if (l >= 0 && l < LABEL_TABLE) seen[l] = 1;
+                else other.insert(l);
+            }
+        }
+    };
+    scan(a);
+    if (b) scan(*b);
+    std::vector<int> out;
+    for (int l : other)
+        if (l < 0) out.push_back(l);
+    for (int l = 0; l < LABEL_TABLE; ++l)
+        if (seen[l]) out.push_back(l);
+    for (int l : other)
+        if (l >= LABEL_TABLE) out.push_back(l);
+    return out;  // ascending
 }
 
 Buckets make_buckets(const SetView &s, const std::vector<int> &labels) {
     Buckets bk;
     bk.labels = labels;
     const int L = (int)labels.size();
-    std::vector<int> count(L + 1, 0);
-    auto lidx = [&](int lbl) {
-        return (int)(std::lower_bound(labels.begin(), labels.end(), lbl) - labels.begin());
+    std::vector<int> table(LABEL_TABLE, -1);
+    for (int l = 0; l < L; ++l)
+        if (labels[l] >= 0 && labels[l] < LABEL_TABLE) table[labels[l]] = l;
+    auto lidx = [&](int lbl) -> int {
+        if (lbl >= 0 && lbl < LABEL_TABLE) return table[lbl];
+        const auto it = std::lower_bound(labels.begin(), labels.end(), lbl);
+        return (it != labels.end() && *it == lbl) ? (int)(it - labels.begin()) : -1;
     };
-    for (int m = 0; m < s.nm; ++m)
-        for (int i = 0; i < s.natoms(m); ++i) {
-            const int l = lidx(s.q[(size_t)m * s.ma + i]);
-            if (l < L && labels[l] == s.q[(size_t)m * s.ma + i]) count[l + 1]++;
+    // label of each active atom, counted in one pass
+    std::vector<int> count(L + 1, 0);
+    for (int m = 0; m < s.nm; ++m) {
+        const int32_t *q = s.q + (size_t)m * s.ma;
+        const int na = s.natoms(m);
+        for (int i = 0; i < na; ++i) {
+            const int l = lidx(q[i]);
+            if (l >= 0) count[l + 1]++;
         }
+    }
     bk.lab_start.assign(L + 1, 0);
     for (int l = 0; l < L; ++l) bk.lab_start[l + 1] = bk.lab_start[l] + count[l + 1];
     const int R = bk.lab_start[L];
     bk.src.resize(R);
     bk.mol.resize(R);
     std::vector<int> fill(bk.lab_start.begin(), bk.lab_start.end() - 1);
-    for (int m = 0; m < s.nm; ++m)
-        for (int i = 0; i < s.natoms(m); ++i) {
-            const int q = s.q[(size_t)m * s.ma + i];
-            const int l = lidx(q);
-            if (l >= L || labels[l] != q) continue;
+    for (int m = 0; m < s.nm; ++m) {
+        const int32_t *q = s.q + (size_t)m * s.ma;
+        const int na = s.natoms(m);
+        for (int i = 0; i < na; ++i) {
+            const int l = lidx(q[i]);
+            if (l < 0) continue;
             const int r = fill[l]++;
             bk.src[r] = m * s.ma + i;
             bk.mol[r] = m;
         }
+    }
     return bk;
 }
 

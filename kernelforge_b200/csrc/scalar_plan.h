@@ -19,4 +19,20 @@ namespace kfb {
 std::vector<PairTile> make_pair_tiles(const Buckets &a, const Buckets &b, bool symmetric, int tm,
                                       int tn, size_t row_bytes = 0);
 
+// The same tiles in the same order, described by their L2 super-blocks (a
+// few hundred entries instead of one entry per tile) and expanded into the
+// tile list by a device kernel: the host plans O(super-blocks) work and
+// uploads a few KB instead of building and copying ~10 MB per call.
+struct SuperBlock {
+    int sa, ea, sb, eb;  // bucket row ranges of the label
+    int bi, bj, g;       // first tile row / column, tiles per side
+    int nti, ntj;        // tiles of the label
+    int symmetric;
+    long long offset;    // index of the super-block's first tile in the list
+};
+std::vector<SuperBlock> make_super_blocks(const Buckets &a, const Buckets &b, bool symmetric,
+                                          int tm, int tn, size_t row_bytes, long long &ntiles);
+kfb_status expand_tiles(const std::vector<SuperBlock> &sbs, long long ntiles, int tm, int tn,
+                        DevBuf &tiles, cudaStream_t s);
+
 }  // namespace kfb

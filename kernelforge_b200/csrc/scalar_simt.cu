@@ -48,20 +48,21 @@ kfb_status run_simt(const ScalarProblem &p, const PairSink &sink, cudaStream_t s
     Buckets b2 = p.symmetric ? Buckets() : make_buckets(p.s2, labels);
     const Buckets &bb = p.symmetric ? b1 : b2;
     const int Dp_ = (p.rep + SK - 1) / SK * SK;
-    std::vector<PairTile> tiles =
-        make_pair_tiles(b1, bb, p.symmetric, ST, ST, (size_t)Dp_ * sizeof(T));
-    if (tiles.empty()) return KFB_OK;
+    long long ntiles_ll = 0;
+    const std::vector<SuperBlock> sbs =
+        make_super_blocks(b1, bb, p.symmetric, ST, ST, (size_t)Dp_ * sizeof(T), ntiles_ll);
+    if (ntiles_ll == 0) return KFB_OK;
     const int Dp = (p.rep + SK - 1) / SK * SK;
     DevBuf pa, na, ma, pb, nb, mb, dt;
     KFB_TRY((pack_set<Tin, T>(static_cast<const Tin *>(p.x1), b1, p.rep, Dp, pa, na, ma, s)));
     if (!p.symmetric)
         KFB_TRY((pack_set<Tin, T>(static_cast<const Tin *>(p.x2), b2, p.rep, Dp, pb, nb, mb, s)));
-    KFB_TRY(upload(dt, tiles, s));
+    KFB_TRY(expand_tiles(sbs, ntiles_ll, ST, ST, dt, s));
     const T coef = T(-1.0 / (2.0 * p.sigma * p.sigma));
     const DevBuf &PB = p.symmetric ? pa : pb, &NB = p.symmetric ? na : nb,
                  &MB = p.symmetric ? ma : mb;
     // grid-stride over tiles in launches of at most 2^31-1 blocks
-    const size_t ntiles = tiles.size();
+    const size_t ntiles = (size_t)ntiles_ll;
     KernelTimer timer(s);
     timer.start();
     for (size_t off = 0; off < ntiles; off += (size_t)1 << 30) {
@@ -77,40 +78,114 @@ kfb_status run_simt(const ScalarProblem &p, const PairSink &sink, cudaStream_t s
 
 }  // namespace
 
-std::vector<PairTile> make_pair_tiles(const Buckets &a, const Buckets &b, bool symmetric,
-                                      int tm, int tn, size_t row_bytes) {
-    std::vector<PairTile> out;
-    int group = 1 << 30;  // tiles per super-block side (unbounded: row-major order)
-    if (row_bytes > 0) {
-        int dev = 0, l2 = 0;
-        cudaGetDevice(&dev);
-        if (cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev) != cudaSuccess || l2 <= 0)
-            l2 = 64 << 20;
-        const size_t tile_bytes = (size_t)std::max(tm, tn) * row_bytes;
-        group = (int)std::max<size_t>(4, std::min<size_t>(64, (size_t)l2 / 2 / (2 * tile_bytes)));
-    }
+static int super_block_side(int tm, int tn, size_t row_bytes) {
+    if (row_bytes == 0) return 1 << 30;  // unbounded: plain row-major order
+    int dev = 0, l2 = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev) != cudaSuccess || l2 <= 0)
+        l2 = 64 << 20;
+    const size_t tile_bytes = (size_t)std::max(tm, tn) * row_bytes;
+    return (int)std::max<size_t>(4, std::min<size_t>(64, (size_t)l2 / 2 / (2 * tile_bytes)));
+}
+
+// columns [first, end) of tile row ti inside super-block sb
+__host__ __device__ inline void sb_row(const SuperBlock &sb, int ti, int &first, int &end) {
+    first = sb.bj;
+    if (sb.symmetric && ti > first) first = ti;
+    end = sb.bj + sb.g < sb.ntj ? sb.bj + sb.g : sb.ntj;
+}
+
+std::vector<SuperBlock> make_super_blocks(const Buckets &a, const Buckets &b, bool symmetric,
+                                          int tm, int tn, size_t row_bytes, long long &ntiles) {
+    std::vector<SuperBlock> out;
+    const int group = super_block_side(tm, tn, row_bytes);
+    ntiles = 0;
     const int L = (int)a.labels.size();
     for (int l = 0; l < L; ++l) {
         const int sa = a.lab_start[l], ea = a.lab_start[l + 1];
         const int sb = b.lab_start[l], eb = b.lab_start[l + 1];
         if (ea <= sa || eb <= sb) continue;
         const int nti = (ea - sa + tm - 1) / tm, ntj = (eb - sb + tn - 1) / tn;
-        for (int bi = 0; bi < nti; bi += group) {
+        for (int bi = 0; bi < nti; bi += group)
             for (int bj = symmetric ? bi : 0; bj < ntj; bj += group) {
+                SuperBlock s{sa, ea, sb, eb, bi, bj, group, nti, ntj, symmetric ? 1 : 0, ntiles};
+                long long cnt = 0;
                 for (int ti = bi; ti < std::min(nti, bi + group); ++ti) {
-                    const int i0 = sa + ti * tm;
-                    for (int tj = bj; tj < std::min(ntj, bj + group); ++tj) {
-                        const int j0 = sb + tj * tn;
-                        if (symmetric && j0 < i0) continue;
-                        PairTile t{};
-                        t.a0 = i0;
-                        t.a_end = ea;
-                        t.b0 = j0;
-                        t.b_end = eb;
-                        t.diag = (symmetric && j0 == i0) ? 1 : 0;
-                        out.push_back(t);
-                    }
+                    int f, e;
+                    sb_row(s, ti, f, e);
+                    if (e > f) cnt += e - f;
                 }
+                if (cnt == 0) continue;
+                out.push_back(s);
+                ntiles += cnt;
+            }
+    }
+    return out;
+}
+
+__global__ void expand_tiles_kernel(const SuperBlock *__restrict__ sbs, int nsb, long long ntiles,
+                                    int tm, int tn, PairTile *__restrict__ out) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= ntiles) return;
+    int lo = 0, hi = nsb - 1;  // last super-block with offset <= t
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (sbs[mid].offset <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    const SuperBlock sb = sbs[lo];
+    long long local = t - sb.offset;
+    const int ti_end = sb.bi + sb.g < sb.nti ? sb.bi + sb.g : sb.nti;
+    for (int ti = sb.bi; ti < ti_end; ++ti) {
+        int f, e;
+        sb_row(sb, ti, f, e);
+        const int c = e > f ? e - f : 0;
+        if (local < c) {
+            const int tj = f + (int)local;
+            PairTile pt{};
+            pt.a0 = sb.sa + ti * tm;
+            pt.a_end = sb.ea;
+            pt.b0 = sb.sb + tj * tn;
+            pt.b_end = sb.eb;
+            pt.diag = (sb.symmetric && ti == tj) ? 1 : 0;
+            out[t] = pt;
+            return;
+        }
+        local -= c;
+    }
+}
+
+kfb_status expand_tiles(const std::vector<SuperBlock> &sbs, long long ntiles, int tm, int tn,
+                        DevBuf &tiles, cudaStream_t s) {
+    KFB_TRY(tiles.alloc((size_t)std::max<long long>(ntiles, 1) * sizeof(PairTile), s));
+    if (ntiles == 0) return KFB_OK;
+    DevBuf dsb;
+    KFB_TRY(upload(dsb, sbs, s));
+    expand_tiles_kernel<<<(unsigned)((ntiles + 255) / 256), 256, 0, s>>>(
+        dsb.as<SuperBlock>(), (int)sbs.size(), ntiles, tm, tn, tiles.as<PairTile>());
+    KFB_CUDA_TRY(cudaGetLastError());
+    return KFB_OK;
+}
+
+std::vector<PairTile> make_pair_tiles(const Buckets &a, const Buckets &b, bool symmetric,
+                                      int tm, int tn, size_t row_bytes) {
+    std::vector<PairTile> out;
+    long long n = 0;
+    const std::vector<SuperBlock> sbs = make_super_blocks(a, b, symmetric, tm, tn, row_bytes, n);
+    out.reserve((size_t)n);
+    for (const SuperBlock &sb : sbs) {
+        const int ti_end = std::min(sb.nti, sb.bi + sb.g);
+        for (int ti = sb.bi; ti < ti_end; ++ti) {
+            int f, e;
+            sb_row(sb, ti, f, e);
+            for (int tj = f; tj < e; ++tj) {
+                PairTile t{};
+                t.a0 = sb.sa + ti * tm;
+                t.a_end = sb.ea;
+                t.b0 = sb.sb + tj * tn;
+                t.b_end = sb.eb;
+                t.diag = (sb.symmetric && ti == tj) ? 1 : 0;
+                out.push_back(t);
             }
         }
     }

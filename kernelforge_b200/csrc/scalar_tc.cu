@@ -25,6 +25,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <climits>
 #include <memory>
 #include <cmath>
 #include <mutex>
@@ -437,10 +438,13 @@ kfb_status run_tc(const ScalarProblem &p, const PairSink &sink, cudaStream_t s) 
     const Buckets &bb = p.symmetric ? b1 : b2;
     // packed rows: hi + lo fp16 halves of Dp columns
     const size_t packed_row_bytes = (size_t)((p.rep + 7) / 8 * 8) * 2 * sizeof(__half);
-    std::vector<PairTile> tiles = make_pair_tiles(b1, bb, p.symmetric, BM, BN, packed_row_bytes);
+    long long ntiles_ll = 0;
+    const std::vector<SuperBlock> sbs =
+        make_super_blocks(b1, bb, p.symmetric, BM, BN, packed_row_bytes, ntiles_ll);
     tr_plan.reset();
     auto tr_pack = std::make_unique<TraceScope>("scalar_tc:pack", s);
-    if (tiles.empty()) return KFB_OK;
+    if (ntiles_ll == 0) return KFB_OK;
+    if (ntiles_ll > INT_MAX) return set_error(KFB_ERR_UNSUPPORTED, "too many tiles (%lld)", ntiles_ll);
     const int L = (int)labels.size();
     const int Dp = (p.rep + 7) / 8 * 8;
     const double log2e = 1.4426950408889634;
@@ -476,7 +480,7 @@ kfb_status run_tc(const ScalarProblem &p, const PairSink &sink, cudaStream_t s) 
     KFB_TRY(make_map(&mb_lo, BB.lo.as<__half>(), bb.rows(), Dp, BN));
 
     DevBuf dtiles, derr;
-    KFB_TRY(upload(dtiles, tiles, s));
+    KFB_TRY(expand_tiles(sbs, ntiles_ll, BM, BN, dtiles, s));
     tr_pack.reset();
     TraceScope tr_kern("scalar_tc:kernel+wait", s);
     KFB_TRY(derr.alloc(sizeof(int), s));
@@ -488,7 +492,7 @@ kfb_status run_tc(const ScalarProblem &p, const PairSink &sink, cudaStream_t s) 
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_ALLOC));
         attr_set = true;
     }
-    const int ntiles = (int)tiles.size();
+    const int ntiles = (int)ntiles_ll;
     const int grid = std::min(ntiles, device_sm_count());
     KernelTimer timer(s);
     timer.start();
