@@ -399,7 +399,10 @@ kfb_status kfb_kernel_gaussian_full_symm(const void *x, const void *dx, const in
     ps.mode = OUT_SYMM;
     ps.layout = layout;
     ps.n = big;
-    KFB_TRY(scalar_dispatch(p, prec, ps, s));
+    {
+        TraceScope tr("full_symm:scalar", s);
+        KFB_TRY(scalar_dispatch(p, prec, ps, s));
+    }
     const DerivSet d = dset(x, dx, q, n, nm, ma);
     // jacobian block at rows [0, nm), columns [nm, big) and its mirror
     ElemSink sj;
@@ -409,7 +412,10 @@ kfb_status kfb_kernel_gaussian_full_symm(const void *x, const void *dx, const in
     sj.layout = layout;
     sj.ld = big;
     sj.col_base = nm;
-    KFB_TRY(jac_any(dt, prec, d, d, rep, sigma, 1.0, sj, s));
+    {
+        TraceScope tr("full_symm:jacobian", s);
+        KFB_TRY(jac_any(dt, prec, d, d, rep, sigma, 1.0, sj, s));
+    }
     ElemSink sh;
     sh.out = out;
     sh.f64 = dt == KFB_F64;
@@ -418,6 +424,7 @@ kfb_status kfb_kernel_gaussian_full_symm(const void *x, const void *dx, const in
     sh.ld = big;
     sh.row_base = nm;
     sh.col_base = nm;
+    TraceScope tr("full_symm:hessian", s);
     return hess_any(dt, prec, d, d, rep, sigma, true, sh, s);
 }
 

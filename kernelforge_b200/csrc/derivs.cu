@@ -17,6 +17,7 @@
 // (pair, i, 32-row slice of rep) (kernel 2) and H_ab = J_a^T Y by the grouped
 // GEMM (kernel 3).
 #include <algorithm>
+#include <memory>
 
 #include "derivs.h"
 #include "kernels_common.cuh"
@@ -454,17 +455,22 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
         const int np = (int)std::min<size_t>(batch, pairs.size() - p0);
         KFB_CUDA_TRY(cudaMemcpyAsync(dpairs.ptr, pairs.data() + p0, np * sizeof(HessPair),
                                      cudaMemcpyHostToDevice, s));
+        auto tr_t = std::make_unique<TraceScope>("hessian:t", s);
         hess_t_kernel<T><<<dim3(ma1, np), 128, rep * sizeof(T), s>>>(
             dpairs.as<HessPair>(), static_cast<const T *>(s1.x), static_cast<const T *>(s2.x),
             static_cast<const T *>(s2.dx), d_q1.as<int>(), d_q2.as<int>(), ma1, ma2, rep, c2,
             is2, is4, W.as<T>(), W2.as<T>(), Tt.as<T>());
         KFB_CUDA_TRY(cudaGetLastError());
+        tr_t.reset();
+        auto tr_y = std::make_unique<TraceScope>("hessian:y", s);
         if (tc) KFB_TRY(zero(yamax.ptr, sizeof(float), s));
         hess_y_kernel<T><<<dim3((rep + 31) / 32, ma1, np), 256, 0, s>>>(
             dpairs.as<HessPair>(), static_cast<const T *>(s1.x), static_cast<const T *>(s2.x),
             static_cast<const T *>(s2.dx), ma1, ma2, rep, W.as<T>(), W2.as<T>(), Tt.as<T>(),
             Y.as<T>(), tc ? yamax.as<float>() : nullptr);
         KFB_CUDA_TRY(cudaGetLastError());
+        tr_y.reset();
+        auto tr_g = std::make_unique<TraceScope>("hessian:split+gemm", s);
         if (tc) {
             float y_scale = 1.f;
             KFB_TRY(transpose_split_y<T>(Y.as<T>(), np, ma1, rep, ld2, yamax.as<float>(),
