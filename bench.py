@@ -47,7 +47,7 @@ CPU_SAMPLE_NMOL = 3000
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nmol", type=int, default=NMOL)
@@ -329,6 +329,20 @@ def run_ours(args, rank, world, local):
     ms = t0.elapsed_time(t1) / args.steps
     ms = max_over_ranks(ms, world)
     _lib.lib().kfb_set_timing(0)
+    # the same step with the FP32 factor (outside the timed region, for comparison)
+    Kc = clk.kernel_gaussian_symm_rfp(Xd, Qh, Nh, SIGMA)
+    solve_times = {}
+    for fac in ("fp64", "fp32"):
+        for _ in range(2):
+            cgk.krr_solve_mixed(Kc, yd, l2=L2, uplo="L", tol=TOL, factor=fac)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _, finfo = cgk.krr_solve_mixed(Kc, yd, l2=L2, uplo="L", tol=TOL, factor=fac)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        solve_times[fac] = {"ms": e0.elapsed_time(e1), "iterations": finfo["iterations"]}
+    del Kc
 
     # e2e (host buffers, copies inside the timed region)
     for _ in range(2):
@@ -377,7 +391,7 @@ def run_ours(args, rank, world, local):
         "vs_baseline": None, "dtype": "f16x3 (split fp16, fp32 accumulate) + f32/f64 solve",
         "data": "synthetic (seeded molecules, FCHL19 descriptors, Morse labels)",
         "config": {"workload": f"{nm}-molecule symmetric FCHL19 local kernel -> RFP (tcgen05 "
-                               "split-fp16) + FP32 RFP Cholesky / FP64 refinement solve",
+                               "split-fp16) + Cholesky-preconditioned FP64 refinement solve (FP64 dense factor; the FP32 factor variant in solve_by_factor)",
                    "molecules_per_gpu": nm, "atoms_per_gpu": int(np.clip(N, 0, None).sum()),
                    "rep": REP, "sigma": SIGMA, "l2": L2, "tol": TOL,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
@@ -386,6 +400,7 @@ def run_ours(args, rank, world, local):
         "kernel_ms": kms,
         "solve": {k: solve_info.get(k) for k in ("iterations", "shift", "rel_residual",
                                                   "used_cg")},
+        "solve_by_factor": solve_times,
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if peak else None, "traffic": traffic_per_launch(),
                      "peak_kind": f"{peak_kind} bf16 dense (f16 MMAs run at the same rate)",

@@ -221,6 +221,9 @@ typedef struct kfb_solve_info {
 #define KFB_SOLVE_LAMBDA_FLOOR 1  /* if K + l2 I is indefinite at FP32 storage
                                      precision, raise l2 (x10 steps) until it is
                                      not, and report it in lambda_eff */
+#define KFB_SOLVE_FP64_FACTOR 2   /* factor in FP64 (dense) instead of FP32; the
+                                     refinement then converges in one or two
+                                     steps */
 
 kfb_status kfb_krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2,
                                kfb_layout uplo, double tol, int maxit, int flags,

@@ -18,6 +18,7 @@ KFB_F32, KFB_F64 = 0, 1
 PREC = {"fp64": 0, "fp32": 1, "split_f16": 2}
 KFB_DENSE, KFB_RFP_U, KFB_RFP_L = 0, 1, 2
 KFB_SOLVE_LAMBDA_FLOOR = 1
+KFB_SOLVE_FP64_FACTOR = 2
 
 # every function declared in include/kfb.h
 EXPORTS = (

@@ -336,18 +336,32 @@ __global__ void scale_copy_kernel(const double *a, double s, int n, double *out)
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] = s * a[i];
 }
-// F = K - mu v v^T over the stored RFP triangle (FP64 arithmetic, FP32 result)
-__global__ void rfp_deflate_kernel(const float *K, int n, int layout, const double *v, double mu,
-                                   float *F) {
-    const long long i = blockIdx.y * (long long)blockDim.y + threadIdx.y;
-    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i < n && j < n && i <= j) {
-        const long long idx = sym_index((kfb_layout)layout, n, i, j);
-        F[idx] = (float)((double)K[idx] - mu * v[i] * v[j]);
+inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+// Dense column-major lower triangle of F = B - coef v v^T + diag I, B in RFP
+// (FP64 arithmetic, TD result); the upper triangle is not touched.
+template <class TD>
+__global__ void dense_deflate_kernel(const float *__restrict__ B, int n, int layout,
+                                     const double *__restrict__ v, double coef, double diag,
+                                     TD *__restrict__ F) {
+    const long long i = blockIdx.y * (long long)blockDim.y + threadIdx.y;  // row
+    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;  // column
+    if (i < n && j < n && i >= j) {
+        double f = (double)B[sym_index((kfb_layout)layout, n, i, j)] - coef * v[i] * v[j];
+        if (i == j) f += diag;
+        F[j * n + i] = (TD)f;
     }
 }
 
-inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+// RFP copy of a dense column-major lower Cholesky factor L: both RFP layouts
+// hold L(max(i,j), min(i,j)) at the symmetric position of (i, j) (UPLO='U'
+// stores U = L^T).
+__global__ void dense_lower_to_rfp_kernel(const float *__restrict__ L, int n, int layout,
+                                          float *__restrict__ arf) {
+    const long long i = blockIdx.y * (long long)blockDim.y + threadIdx.y;
+    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n && j < n && i <= j) arf[sym_index((kfb_layout)layout, n, i, j)] = L[i * n + j];
+}
 
 
 }  // namespace
@@ -634,7 +648,6 @@ kfb_status mixed_core(const ApplyFn &A, const float *B, int n, kfb_layout uplo, 
     KFB_TRY(dw.alloc((size_t)n * sizeof(double), s));
     KFB_TRY(f32v.alloc((size_t)n * sizeof(float), s));
     const unsigned gb = nblk(n, 256);
-    const dim3 blk2(32, 8), grd2(nblk(n, 32), nblk(n, 8));
     const double u32 = 5.960464477539063e-08;
     double *sc = ds.sc();
     KFB_TRY(ds.dot(y, y, n, S_Y2, s));
@@ -645,7 +658,56 @@ kfb_status mixed_core(const ApplyFn &A, const float *B, int n, kfb_layout uplo, 
     if (ynorm == 0.0) return KFB_OK;
 
     // out = F^{-1} x, x scaled to unit norm by the device scalar sc[slot] = |x|^2
+    // The factor: FP32 Cholesky of the dense lower triangle (one cuSOLVER call,
+    // faster at these sizes than the RFP block sequence), packed to RFP for the
+    // triangular solves; or, with KFB_SOLVE_FP64_FACTOR, an FP64 dense factor
+    // used as it is.
+    const bool f64 = (flags & KFB_SOLVE_FP64_FACTOR) != 0;
+    Handles *hd = nullptr;
+    KFB_TRY(get_handles(s, hd));
+    DevBuf Fd, ws, dinfo;
+    KFB_TRY(Fd.alloc((size_t)n * n * (f64 ? sizeof(double) : sizeof(float)), s));
+    KFB_TRY(dinfo.alloc(sizeof(int), s));
+    int lwork = 0;
+    if (f64)
+        KFB_SOLVER_TRY(cusolverDnDpotrf_bufferSize(hd->solver, CUBLAS_FILL_MODE_LOWER, n,
+                                                   Fd.as<double>(), n, &lwork));
+    else
+        KFB_SOLVER_TRY(cusolverDnSpotrf_bufferSize(hd->solver, CUBLAS_FILL_MODE_LOWER, n,
+                                                   Fd.as<float>(), n, &lwork));
+    KFB_TRY(ws.alloc((size_t)std::max(lwork, 1) * (f64 ? sizeof(double) : sizeof(float)), s));
+    auto factor = [&](double diag, int &finfo) -> kfb_status {
+        const dim3 b2(32, 8), g2(nblk(n, 32), nblk(n, 8));
+        KFB_TRY(zero(dinfo.ptr, sizeof(int), s));
+        if (f64) {
+            dense_deflate_kernel<double><<<g2, b2, 0, s>>>(B, n, uplo, v, fcoef, diag,
+                                                           Fd.as<double>());
+            KFB_CUDA_TRY(cudaGetLastError());
+            KFB_SOLVER_TRY(cusolverDnDpotrf(hd->solver, CUBLAS_FILL_MODE_LOWER, n, Fd.as<double>(),
+                                            n, ws.as<double>(), lwork, dinfo.as<int>()));
+        } else {
+            dense_deflate_kernel<float><<<g2, b2, 0, s>>>(B, n, uplo, v, fcoef, diag,
+                                                          Fd.as<float>());
+            KFB_CUDA_TRY(cudaGetLastError());
+            KFB_SOLVER_TRY(cusolverDnSpotrf(hd->solver, CUBLAS_FILL_MODE_LOWER, n, Fd.as<float>(),
+                                            n, ws.as<float>(), lwork, dinfo.as<int>()));
+        }
+        KFB_CUDA_TRY(cudaMemcpyAsync(&finfo, dinfo.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
+        KFB_CUDA_TRY(cudaStreamSynchronize(s));
+        if (finfo == 0 && !f64) {
+            dense_lower_to_rfp_kernel<<<g2, b2, 0, s>>>(Fd.as<float>(), n, uplo, F.as<float>());
+            KFB_CUDA_TRY(cudaGetLastError());
+        }
+        return KFB_OK;
+    };
     auto solve_f_dev = [&](const double *x, int slot, double *out) -> kfb_status {
+        if (f64) {
+            KFB_CUDA_TRY(cudaMemcpyAsync(out, x, (size_t)n * sizeof(double),
+                                         cudaMemcpyDeviceToDevice, s));
+            KFB_SOLVER_TRY(cusolverDnDpotrs(hd->solver, CUBLAS_FILL_MODE_LOWER, n, 1,
+                                            Fd.as<double>(), n, out, n, dinfo.as<int>()));
+            return KFB_OK;
+        }
         scale_to_float_dev_kernel<<<gb, 256, 0, s>>>(x, sc, slot, n, f32v.as<float>());
         KFB_TRY(rfp_potrs(F.ptr, f32v.ptr, n, 1, uplo, KFB_F32, s));
         float_to_double_dev_kernel<<<gb, 256, 0, s>>>(f32v.as<float>(), sc, slot, n, out);
@@ -658,9 +720,7 @@ kfb_status mixed_core(const ApplyFn &A, const float *B, int n, kfb_layout uplo, 
         int finfo = 0;
         auto tr_f = std::make_unique<TraceScope>("mixed:factor", s);
         for (int a = 0; a < 12; ++a) {
-            rfp_deflate_kernel<<<grd2, blk2, 0, s>>>(B, n, uplo, v, fcoef, F.as<float>());
-            KFB_CUDA_TRY(cudaGetLastError());
-            KFB_TRY(rfp_potrf(F.ptr, n, lam + shift, uplo, KFB_F32, &finfo, s));
+            KFB_TRY(factor(lam + shift, finfo));
             if (finfo == 0) break;
             shift = (shift == 0.0) ? std::max(u32 * lam2, 10.0 * lam) : shift * 4.0;
         }

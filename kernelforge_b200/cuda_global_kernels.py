@@ -60,14 +60,21 @@ def rfp_potrs(L_rfp, B, uplo="L"):
                                         _dt(L_rfp), stream_handle()))
 
 
-def krr_solve_mixed(K_rfp, y, l2=0.0, uplo="L", tol=1e-10, maxit=500, *, lambda_floor=False):
+def krr_solve_mixed(K_rfp, y, l2=0.0, uplo="L", tol=1e-10, maxit=500, *, lambda_floor=False,
+                    factor="fp64"):
     """(K + l2 I) alpha = y with an FP32 RFP kernel matrix (not modified): FP32
     Cholesky factor (dominant eigenpair deflated), FP64 conjugate-gradient
     refinement of residuals against K.  Returns (alpha float64, info dict).
 
     Raises RuntimeError if K + l2 I is indefinite at FP32 storage precision;
     with ``lambda_floor=True`` l2 is raised in x10 steps until it is not, and
-    info["lambda_eff"] reports the value used."""
+    info["lambda_eff"] reports the value used.
+
+    ``factor``: precision of the Cholesky factor behind the refinement.  On
+    B200 cuSOLVER's FP64 Cholesky runs as fast as the FP32 one (FP64 tensor
+    cores), and an FP64 factor leaves one or two refinement steps instead of
+    about ten latency-bound FP32 triangular-solve pairs, so "fp64" (default) is
+    the faster choice here; "fp32" keeps the factor in FP32 as well."""
     require_cuda()
     import torch
     if K_rfp.dtype != torch.float32 or not K_rfp.is_cuda or not K_rfp.is_contiguous():
@@ -78,7 +85,10 @@ def krr_solve_mixed(K_rfp, y, l2=0.0, uplo="L", tol=1e-10, maxit=500, *, lambda_
         raise RuntimeError("K_rfp must have n*(n+1)/2 elements")
     alpha = torch.empty((n,), dtype=torch.float64, device=K_rfp.device)
     info = _lib.SolveInfo()
-    flags = _lib.KFB_SOLVE_LAMBDA_FLOOR if lambda_floor else 0
+    if factor not in ("fp32", "fp64"):
+        raise ValueError("factor must be 'fp32' or 'fp64'")
+    flags = (_lib.KFB_SOLVE_LAMBDA_FLOOR if lambda_floor else 0) | \
+        (_lib.KFB_SOLVE_FP64_FACTOR if factor == "fp64" else 0)
     st = _lib.lib().kfb_krr_solve_mixed(K_rfp.data_ptr(), yd.data_ptr(), n, float(l2),
                                         _uplo(uplo), float(tol), int(maxit), flags,
                                         alpha.data_ptr(), ctypes.byref(info), stream_handle())

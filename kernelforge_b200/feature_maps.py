@@ -290,7 +290,7 @@ def _device_view(ptr, shape):
 
 
 # ------------------------------------------------------------------ ridge
-def fit_ridge(Z, y, l2, tol=1e-10, maxit=500, lambda_floor=True):
+def fit_ridge(Z, y, l2, tol=1e-10, maxit=500, lambda_floor=True, factor="fp64"):
     """Weights of the linear ridge model (Z^T Z + l2 I) w = Z^T y (libkfb's
     kfb_ridge_solve_mixed: FP32 factor, FP64 refinement against Z itself).
     Returns (w float64 (d,), solve info dict)."""
@@ -305,7 +305,10 @@ def fit_ridge(Z, y, l2, tol=1e-10, maxit=500, lambda_floor=True):
         raise RuntimeError("y must have one value per row of Z")
     w = torch.empty((d,), dtype=torch.float64, device=Z.device)
     info = _lib.SolveInfo()
-    flags = _lib.KFB_SOLVE_LAMBDA_FLOOR if lambda_floor else 0
+    if factor not in ("fp32", "fp64"):
+        raise ValueError("factor must be 'fp32' or 'fp64'")
+    flags = (_lib.KFB_SOLVE_LAMBDA_FLOOR if lambda_floor else 0) | \
+        (_lib.KFB_SOLVE_FP64_FACTOR if factor == "fp64" else 0)
     st = _lib.lib().kfb_ridge_solve_mixed(Z.data_ptr(), yd.data_ptr(), nm, d, float(l2),
                                           float(tol), int(maxit), flags, w.data_ptr(),
                                           ctypes.byref(info), stream_handle())

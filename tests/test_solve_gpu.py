@@ -120,3 +120,28 @@ def test_mixed_solve_matches_fp64_solution_when_well_conditioned():
     alpha, info = cgk.krr_solve_mixed(K, torch.tensor(y), l2=0.0, uplo="L", tol=1e-12)
     assert info["converged"], info
     np.testing.assert_allclose(alpha.cpu().numpy(), np.linalg.solve(A32, y), rtol=1e-9, atol=1e-11)
+
+
+@pytest.mark.parametrize("factor", ["fp32", "fp64"])
+def test_mixed_solve_factor_choice(factor):
+    """Both factor precisions converge to the FP64 solution of the FP32-stored
+    system; the FP64 factor needs at most two refinement steps."""
+    import torch
+
+    from kernelforge_b200 import cuda_global_kernels as cgk
+    from kernelforge_b200 import cuda_local_kernels as clk
+    from kernelforge_b200 import synthetic
+    mols = synthetic.make_molecules(400, 9, 21, seed=5)
+    X, Q, N = synthetic.fchl19_batched(mols, dtype=np.float32)
+    K = clk.kernel_gaussian_symm_rfp(torch.tensor(X, device="cuda"), Q, N, 2.0)
+    y = mols.E - mols.E.mean()
+    n = len(y)
+    alpha, info = cgk.krr_solve_mixed(K, torch.tensor(y), l2=1e-2, uplo="L", tol=1e-11,
+                                      factor=factor)
+    assert info["converged"], info
+    A32 = o.rfp_to_full(K.cpu().numpy().astype(np.float64), n, uplo_lower=True)
+    ref = np.linalg.solve(A32 + 1e-2 * np.eye(n), y)
+    np.testing.assert_allclose(alpha.cpu().numpy(), ref, rtol=1e-7,
+                               atol=1e-7 * np.abs(ref).max())
+    if factor == "fp64":
+        assert info["iterations"] <= 3, info
