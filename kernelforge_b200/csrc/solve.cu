@@ -885,7 +885,11 @@ kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2
         return KFB_OK;
     }
     double mu = 0.0, lam2 = 0.0;
-    {
+    if (flags & KFB_SOLVE_FP64_FACTOR) {
+        // an FP64 factor needs no deflation: its rounding (~1e-16 |K|) is far
+        // below any usable lambda
+        KFB_TRY(zero(dv.ptr, (size_t)n * sizeof(double), s));
+    } else {
         TraceScope tr("krr_solve:power", s);
         KFB_TRY(power_dominant(A, n, dv.as<double>(), dw.as<double>(), dtmp.as<double>(), ds, s,
                                mu, lam2));
