@@ -594,7 +594,22 @@ def run_config3(args):
         _lib.PREC["fp64"], J64.data_ptr(), torch.cuda.current_stream().cuda_stream))
     f_64 = -(torch.tensor(a64, device="cuda") @ J64).cpu().numpy()
     del x1d, x2d, dx2d, J64
-    force_mae = {"tensor_core": float(np.abs(f_tc - Fte).mean()),
+    # the same forces contracted (query = test molecules, alpha_F = 0): no
+    # training x test Jacobian matrix
+    a64d = torch.tensor(a64, device="cuda")
+    zero_ad = torch.zeros(X1.shape, dtype=torch.float64, device="cuda")
+
+    def contracted_forces():
+        return clk.kernel_gaussian_full_matvec(x2, dx2, Q2, N2, x1, Q1, N1, a64d, zero_ad,
+                                               SIGMA)[1]
+
+    c_ms = _events_ms(contracted_forces, 3, 1)
+    f_c = -contracted_forces().cpu().numpy()
+    force_mae = {"contracted_fp64": float(np.abs(f_c - Fte).mean()),
+                 "contracted_ms": c_ms,
+                 "contracted_rel_diff_vs_fp64": float(np.linalg.norm(f_c - f_64)
+                                                      / np.linalg.norm(f_64)),
+                 "tensor_core": float(np.abs(f_tc - Fte).mean()),
                  "fp64_gpu": float(np.abs(f_64 - Fte).mean()),
                  "pred_rel_diff": float(np.linalg.norm(f_tc - f_64) / np.linalg.norm(f_64)),
                  "lambda": lam3, "train": "energies of the 1,000 training molecules"}
@@ -671,6 +686,22 @@ def run_config4(args):
     Kt32 = _full_asym(xt, dxt, Qt, Nt, x, dx, Q, N, "split_f16", torch.float32)
     mae_e, mae_f = mae(Kt32, alpha)
     del Kt32
+
+    # contracted prediction (alpha_desc + J^T alpha matvec, FP64) of the same
+    # model: no test x train kernel matrix
+    def predict(a):
+        ad = clk.compute_alpha_desc(dx, N, a[nm:])
+        return clk.kernel_gaussian_full_matvec(xt, dxt, Qt, Nt, x, Q, N, a[:nm], ad, SIGMA)
+
+    pred_ms = _events_ms(lambda: predict(alpha), max(args.steps // 4, 3), 2)
+    full_pred_ms = _events_ms(
+        lambda: _full_asym(xt, dxt, Qt, Nt, x, dx, Q, N, "split_f16", torch.float32).double()
+        @ alpha, 2, 1)
+    Ec, Fc = (t.cpu().numpy() for t in predict(alpha))
+    contracted = {"predict_ms": pred_ms, "full_kernel_predict_ms": full_pred_ms,
+                  "fit_predict_ms": ms + pred_ms,
+                  "test_mae_energy": float(np.abs(Ec + em - te.E).mean()),
+                  "test_mae_force": float(np.abs(-Fc - Ft).mean())}
     # FP64 KRR on the same data (FP64 GPU kernels, which match the CPU oracle to 1e-10)
     x64, dx64 = x.double(), dx.double()
     t0 = time.perf_counter()
@@ -694,6 +725,12 @@ def run_config4(args):
         Kt64 = _full_asym(xt.double(), dxt.double(), Qt, Nt, x64, dx64, Q, N, "fp64",
                           torch.float64)
         fp64["test_mae_energy"], fp64["test_mae_force"] = mae(Kt64, a64)
+        # the contracted prediction against the FP64 test x train kernel product
+        p64 = (Kt64 @ a64).cpu().numpy()
+        del Kt64
+        Ec64, Fc64 = (t.cpu().numpy() for t in predict(a64))
+        contracted["rel_diff_vs_fp64_kernel_product"] = float(
+            np.linalg.norm(np.concatenate([Ec64, Fc64]) - p64) / np.linalg.norm(p64))
     cpu = None
     if not args.no_cpu_baseline:
         lk, km = _ref_modules()
@@ -711,8 +748,8 @@ def run_config4(args):
           f"mixed solve, lambda {lam}", "f32 kernel (split-fp16 scalar block) + f64 refinement",
           {"kernel_ms": kms, "solve": {k: info.get(k) for k in ("iterations", "shift",
                                                                  "rel_residual", "lambda_eff")},
-           "test_mae_energy": mae_e, "test_mae_force": mae_f, "fp64_krr": fp64,
-           "cpu_baseline": cpu})
+           "test_mae_energy": mae_e, "test_mae_force": mae_f,
+           "contracted_prediction": contracted, "fp64_krr": fp64, "cpu_baseline": cpu})
 
 
 def run_config1(args):

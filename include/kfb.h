@@ -317,6 +317,42 @@ kfb_status kfb_cosmlp_features_elemental(kfb_cosmlp *h, const void *x, const int
                                          kfb_dtype x_dt, float *z, void *stream);
 
 /* ---------------------------------------------------------------------- */
+/* Contracted energy / force prediction (the "J^T alpha" form)             */
+/* ---------------------------------------------------------------------- */
+
+/* alpha_desc (nm2, ma2, rep) double: alpha_desc[b, j] = dX2[b, j] (rep x 3 n_b)
+ * times alpha[off_b : off_b + 3 n_b] (off_b = 3 sum_{b' < b} n_b'), zero for
+ * padded atoms; dx2 (nm2, ma2, rep, 3 ma2) of element type x_dt, alpha (naq2,)
+ * double.  n2 host; q2 (host) may be NULL: the contraction does not depend
+ * on the labels.  Replaces
+ * local_kernels.kernel_gaussian_local_compute_alpha_desc
+ * (src/local_kernels_bindings.cpp:1179-1243, src/local_kernels.cpp:2821-2894). */
+kfb_status kfb_local_alpha_desc(const void *dx2, const int32_t *q2, const int32_t *n2, int nm2,
+                                int ma2, int rep, kfb_dtype x_dt, const double *alpha,
+                                double *alpha_desc, void *stream);
+
+/* Predictions of a model with coefficients [alpha_E; alpha_F] over the
+ * training set (x2, alpha_desc = kfb_local_alpha_desc of alpha_F) at the query
+ * set (x1, dx1), without forming the E+F kernel matrix:
+ *   e_out (nm1,)  = rows of kernel_gaussian_full(query, training) for the
+ *                   energies times [alpha_E; alpha_F],
+ *   f_out (naq1,) = the force rows (naq1 = 3 sum n1) times the same vector.
+ * alpha_e NULL drops the alpha_E terms: e_out is then
+ * kernel_gaussian_local_jacobian_t_matvec (src/local_kernels_bindings.cpp:
+ * 1358-1427, src/local_kernels.cpp:3155-3262) and f_out
+ * kernel_gaussian_local_hessian_matvec (:1246-1356, local_kernels.cpp:2895-3154);
+ * with alpha_e both are kernel_gaussian_local_full_matvec (:1429-1530,
+ * local_kernels.cpp:3263-3425).  e_out or f_out may be NULL (not
+ * computed); f_out needs dx1.  alpha_desc NULL means all-zero force
+ * coefficients.  x1, dx1, x2 of element type x_dt, everything else double;
+ * q / n host.  FP64 arithmetic (FP64 cuBLAS GEMMs for the pair products). */
+kfb_status kfb_local_matvec(const void *x1, const void *dx1, const void *x2,
+                            const double *alpha_desc, const double *alpha_e, const int32_t *q1,
+                            const int32_t *q2, const int32_t *n1, const int32_t *n2, int nm1,
+                            int nm2, int ma1, int ma2, int rep, double sigma, kfb_dtype x_dt,
+                            double *e_out, double *f_out, void *stream);
+
+/* ---------------------------------------------------------------------- */
 /* Allocation-free entry point                                             */
 /* ---------------------------------------------------------------------- */
 

@@ -48,6 +48,19 @@ kfb_status get_handles(cudaStream_t s, Handles *&out) {
     return KFB_OK;
 }
 
+}  // namespace
+
+// The per-device cuBLAS handle of this thread, bound to stream s (shared with
+// the prediction kernels).
+kfb_status blas_for_stream(cudaStream_t s, cublasHandle_t *out) {
+    Handles *h = nullptr;
+    KFB_TRY(get_handles(s, h));
+    *out = h->blas;
+    return KFB_OK;
+}
+
+namespace {
+
 #define KFB_BLAS_TRY(expr)                                                                  \
     do {                                                                                    \
         cublasStatus_t _b = (expr);                                                         \

@@ -23,6 +23,8 @@ __all__ = [
     "kernel_gaussian_jacobian", "kernel_gaussian_jacobian_t", "kernel_gaussian_hessian",
     "kernel_gaussian_hessian_symm", "kernel_gaussian_hessian_symm_rfp", "kernel_gaussian_full",
     "kernel_gaussian_full_symm", "kernel_gaussian_full_symm_rfp",
+    "kernel_gaussian_local_compute_alpha_desc", "kernel_gaussian_local_jacobian_t_matvec",
+    "kernel_gaussian_local_hessian_matvec", "kernel_gaussian_local_full_matvec",
 ]
 
 
@@ -348,3 +350,129 @@ def kernel_gaussian_full_symm_rfp(X, dX, Q, N, sigma, *, precision="fp64"):
     """Symmetric energy+force kernel in RFP (TRANSR='N', Fortran UPLO='U').
     Reference: src/local_kernels.cpp:2511-2815."""
     return _full_symm(X, dX, Q, N, sigma, precision, _lib.KFB_RFP_U)
+
+
+# --------------------------------------------------------------------------
+# contracted energy / force prediction ("J^T alpha")
+# --------------------------------------------------------------------------
+
+def kernel_gaussian_local_compute_alpha_desc(dX2, Q2, N2, alpha):
+    """alpha_desc[b, j, :] = dX2[b, j, :, :3 N2[b]] @ alpha[off_b : off_b + 3 N2[b]]
+    (zero for padded atoms), shape (nm2, max_atoms2, rep) float64.  Reference:
+    src/local_kernels_bindings.cpp:1179-1243, src/local_kernels.cpp:2821-2894."""
+    dX2 = np.asarray(dX2)
+    alpha = np.asarray(alpha)
+    Q2, N2 = host_i32(Q2), host_i32(N2)
+    if dX2.ndim != 4 or Q2.ndim != 2 or N2.ndim != 1 or alpha.ndim != 1:
+        raise ValueError("shape error")
+    nm2, ma2, rep = dX2.shape[0], dX2.shape[1], dX2.shape[2]
+    if dX2.shape[3] != 3 * ma2:
+        raise ValueError("dX2 shape mismatch")
+    if Q2.shape != (nm2, ma2):
+        raise ValueError("Q2 shape mismatch")
+    if N2.shape[0] != nm2:
+        raise ValueError("N2 length mismatch")
+    if nm2 <= 0 or ma2 <= 0 or rep <= 0:
+        raise ValueError("dimensions must be positive")
+    naq2 = _naq(N2, ma2)
+    if alpha.shape[0] < naq2:
+        raise ValueError("alpha length mismatch")
+    require_cuda()
+    import torch
+    dx2 = to_device(_f64(dX2), torch.float64)
+    al = to_device(_f64(alpha), torch.float64)
+    out = torch.empty((nm2, ma2, rep), dtype=torch.float64, device="cuda")
+    _lib.check(_lib.lib().kfb_local_alpha_desc(
+        dx2.data_ptr(), Q2.ctypes.data, N2.ctypes.data, nm2, ma2, rep, _lib.KFB_F64,
+        al.data_ptr(), out.data_ptr(), stream_handle()))
+    return out.cpu().numpy()
+
+
+def _check_matvec(X1, dX1, X2, ad, Q1, Q2, N1, N2, ad_name):
+    if X1.ndim != 3 or X2.ndim != 3 or ad.ndim != 3 or Q1.ndim != 2 or Q2.ndim != 2 \
+            or N1.ndim != 1 or N2.ndim != 1 or (dX1 is not None and dX1.ndim != 4):
+        raise ValueError("shape error")
+    nm1, ma1, rep = X1.shape
+    nm2, ma2 = X2.shape[0], X2.shape[1]
+    if dX1 is not None and dX1.shape != (nm1, ma1, rep, 3 * ma1):
+        raise ValueError("dX1 shape mismatch")
+    if X2.shape[2] != rep:
+        raise ValueError("X2 rep_size mismatch")
+    if ad.shape != (nm2, ma2, rep):
+        raise ValueError(f"{ad_name} shape mismatch")
+    if Q1.shape != (nm1, ma1):
+        raise ValueError("Q1 shape mismatch")
+    if Q2.shape != (nm2, ma2):
+        raise ValueError("Q2 shape mismatch")
+    if N1.shape[0] != nm1 or N2.shape[0] != nm2:
+        raise ValueError("N1/N2 length mismatch")
+
+
+def _matvec(X1, dX1, X2, ad, alpha_E, Q1, Q2, N1, N2, sigma, want_e, want_f):
+    """Shared body of the three matvecs: (E or None, F or None), float64."""
+    nm1, ma1, rep = X1.shape
+    nm2, ma2 = X2.shape[0], X2.shape[1]
+    naq1 = _naq(N1, ma1)
+    E = np.zeros(nm1) if want_e else None
+    F = np.zeros(naq1) if want_f else None
+    if nm1 == 0 or (want_f and not want_e and naq1 == 0):
+        return E, F
+    if nm2 <= 0 or ma1 <= 0 or ma2 <= 0 or rep <= 0:
+        raise ValueError("dimensions must be positive")
+    check_sigma(sigma)
+    require_cuda()
+    import torch
+    x1, x2 = to_device(_f64(X1), torch.float64), to_device(_f64(X2), torch.float64)
+    dx1 = to_device(_f64(dX1), torch.float64) if want_f else None
+    adt = to_device(_f64(ad), torch.float64)
+    ae = to_device(_f64(alpha_E), torch.float64) if alpha_E is not None else None
+    e = torch.empty(nm1, dtype=torch.float64, device="cuda") if want_e else None
+    f = torch.empty(max(naq1, 1), dtype=torch.float64, device="cuda") if want_f else None
+    _lib.check(_lib.lib().kfb_local_matvec(
+        x1.data_ptr(), dx1.data_ptr() if dx1 is not None else None, x2.data_ptr(),
+        adt.data_ptr(), ae.data_ptr() if ae is not None else None, Q1.ctypes.data,
+        Q2.ctypes.data, N1.ctypes.data, N2.ctypes.data, nm1, nm2, ma1, ma2, rep, float(sigma),
+        _lib.KFB_F64, e.data_ptr() if e is not None else None,
+        f.data_ptr() if f is not None else None, stream_handle()))
+    if want_e:
+        E = e.cpu().numpy()
+    if want_f:
+        F = f[:naq1].cpu().numpy()
+    return E, F
+
+
+def kernel_gaussian_local_jacobian_t_matvec(X1, X2, alpha_desc, Q1, Q2, N1, N2, sigma):
+    """Energies (nm1,) of force coefficients alpha (alpha_desc =
+    kernel_gaussian_local_compute_alpha_desc(dX2, Q2, N2, alpha)): the energy rows
+    of kernel_gaussian_full(query, training) times [0; alpha].  Reference:
+    src/local_kernels_bindings.cpp:1358-1427, src/local_kernels.cpp:3155-3262."""
+    X1, X2, ad = np.asarray(X1), np.asarray(X2), np.asarray(alpha_desc)
+    Q1, Q2, N1, N2 = host_i32(Q1), host_i32(Q2), host_i32(N1), host_i32(N2)
+    _check_matvec(X1, None, X2, ad, Q1, Q2, N1, N2, "alpha_desc")
+    return _matvec(X1, None, X2, ad, None, Q1, Q2, N1, N2, sigma, True, False)[0]
+
+
+def kernel_gaussian_local_hessian_matvec(X1, dX1, X2, alpha_desc, Q1, Q2, N1, N2, sigma):
+    """Forces (naq1,) = kernel_gaussian_hessian(X1, dX1, X2, dX2, ...) @ alpha, from
+    alpha_desc = kernel_gaussian_local_compute_alpha_desc(dX2, Q2, N2, alpha).
+    Reference: src/local_kernels_bindings.cpp:1246-1356, src/local_kernels.cpp:2895-3154."""
+    X1, X2, dX1, ad = map(np.asarray, (X1, X2, dX1, alpha_desc))
+    Q1, Q2, N1, N2 = host_i32(Q1), host_i32(Q2), host_i32(N1), host_i32(N2)
+    _check_matvec(X1, dX1, X2, ad, Q1, Q2, N1, N2, "alpha_desc")
+    return _matvec(X1, dX1, X2, ad, None, Q1, Q2, N1, N2, sigma, False, True)[1]
+
+
+def kernel_gaussian_local_full_matvec(X1, dX1, X2, alpha_desc_F, alpha_E, Q1, Q2, N1, N2,
+                                      sigma):
+    """(E (nm1,), F (naq1,)) = kernel_gaussian_full(query, training) @ [alpha_E; alpha_F]
+    with alpha_desc_F = kernel_gaussian_local_compute_alpha_desc(dX2, Q2, N2, alpha_F).
+    Reference: src/local_kernels_bindings.cpp:1429-1530, src/local_kernels.cpp:3263-3425."""
+    X1, X2, dX1, ad = map(np.asarray, (X1, X2, dX1, alpha_desc_F))
+    alpha_E = np.asarray(alpha_E)
+    Q1, Q2, N1, N2 = host_i32(Q1), host_i32(Q2), host_i32(N1), host_i32(N2)
+    if alpha_E.ndim != 1:
+        raise ValueError("shape error")
+    _check_matvec(X1, dX1, X2, ad, Q1, Q2, N1, N2, "alpha_desc_F")
+    if alpha_E.shape[0] != X2.shape[0]:
+        raise ValueError("alpha_E length mismatch")
+    return _matvec(X1, dX1, X2, ad, alpha_E, Q1, Q2, N1, N2, sigma, True, True)
