@@ -735,6 +735,10 @@ kfb_status mixed_core(const ApplyFn &A, const float *B, int n, kfb_layout uplo, 
         for (int a = 0; a < 12; ++a) {
             KFB_TRY(factor(lam + shift, finfo));
             if (finfo == 0) break;
+            // an FP64 factor that fails means A + lam I itself is indefinite at
+            // the precision A is held in: under the lambda floor, raise lam
+            // rather than shift a preconditioner for an indefinite system
+            if (f64 && (flags & KFB_SOLVE_LAMBDA_FLOOR)) break;
             shift = (shift == 0.0) ? std::max(u32 * lam2, 10.0 * lam) : shift * 4.0;
         }
         inf.factor_info = finfo;
@@ -859,7 +863,14 @@ kfb_status mixed_core(const ApplyFn &A, const float *B, int n, kfb_layout uplo, 
         st = attempt(lam);
         inf.lambda_eff = lam;
         if (st != KFB_ERR_NOT_PD || !(flags & KFB_SOLVE_LAMBDA_FLOOR)) break;
-        // raise the regularisation until A + lam I is definite at FP32 precision
+        // raise the regularisation until A + lam I is definite at FP32 precision;
+        // the first step goes to u32 lam2 (the FP64-factor path skipped the
+        // power steps, so it estimates lam2 now, with p, q, z as scratch)
+        if (tries == 0 && lam2 == 0.0) {
+            double mu_e = 0.0;
+            KFB_TRY(power_dominant(A, n, p.as<double>(), q.as<double>(), z.as<double>(), ds, s,
+                                   mu_e, lam2));
+        }
         lam = (tries == 0) ? std::max(10.0 * l2, u32 * lam2) : lam * 10.0;
     }
     return st;
