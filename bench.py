@@ -61,6 +61,8 @@ def parse():
                          "1,000-molecule fit+predict; config3: Jacobian kernel 1,000 x 1,000 "
                          "molecules; config4: energy+force kernel of 300 x 21-atom molecules "
                          "+ solve; config5: learned feature map vs RFF vs exact KRR")
+    ap.add_argument("--c4-nmol", type=int, default=300,
+                    help="config4 training molecules (smaller values: profiling cases)")
     ap.add_argument("--c5-nmol", type=int, default=50000)
     ap.add_argument("--c5-pairs", type=int, default=2000000)
     ap.add_argument("--c5-epochs", type=int, default=6)
@@ -651,7 +653,7 @@ def run_config4(args):
     from kernelforge_b200 import cuda_local_kernels as clk
     from kernelforge_b200 import synthetic
     lam = 1e-6
-    tr = synthetic.make_molecules(300, 21, 21, seed=SEED + 4)
+    tr = synthetic.make_molecules(args.c4_nmol, 21, 21, seed=SEED + 4)
     te = synthetic.make_molecules(100, 21, 21, seed=SEED + 40)
     X, dX, Q, N = synthetic.fchl19_batched_grad(tr, dtype=np.float32, device="cuda", chunk=16)
     Xt, dXt, Qt, Nt = synthetic.fchl19_batched_grad(te, dtype=np.float32, device="cuda", chunk=16)

@@ -143,103 +143,522 @@ __global__ void jac_v_kernel(const T *__restrict__ xo, const int *__restrict__ q
     }
 }
 
-// ------------------------------------------------------- Hessian kernel 1
-// Block per (pair p, atom i of a): for each same-label j of b,
-//   W[p,i,j] = e/sigma^2, W2[p,i,j] = e/sigma^4, Tt[p,i,j,:] = J_j^T (x_i - x_j)
-template <class T>
-__global__ void hess_t_kernel(const HessPair *__restrict__ pairs, const T *__restrict__ x1,
-                              const T *__restrict__ x2, const T *__restrict__ dx2,
-                              const int *__restrict__ q1, const int *__restrict__ q2, int ma1,
-                              int ma2, int rep, T c2, T is2, T is4, T *__restrict__ W,
-                              T *__restrict__ W2, T *__restrict__ Tt) {
-    extern __shared__ unsigned char hsm_raw[];
-    T *d = reinterpret_cast<T *>(hsm_raw);  // rep
-    __shared__ T red[32];
-    const HessPair pr = pairs[blockIdx.y];
-    const int i = blockIdx.x;
-    if (i >= pr.na) return;
-    const int ld2 = 3 * ma2;
-    const size_t wbase = ((size_t)blockIdx.y * ma1 + i) * ma2;
-    const int qi = q1[(size_t)pr.a * ma1 + i];
-    const T *xi = x1 + ((size_t)pr.a * ma1 + i) * rep;
-    for (int j = 0; j < pr.nb; ++j) {
-        if (q2[(size_t)pr.b * ma2 + j] != qi) {
-            if (threadIdx.x == 0) {
-                W[wbase + j] = T(0);
-                W2[wbase + j] = T(0);
-            }
-            continue;
+// Label groups of a molecule pair: for each run [x, y) of equal labels in a's
+// label order, the run [z, w) of the same label in b's (empty when b lacks
+// it).  Returns the number of groups (<= na).
+__device__ __forceinline__ int pair_label_groups(const int *la, const int *lb, int na, int nb,
+                                                 int4 *groups) {
+    int g = 0, t = 0;
+    for (int s0 = 0; s0 < na;) {
+        const int L = la[s0];
+        int s1 = s0 + 1;
+        while (s1 < na && la[s1] == L) ++s1;
+        while (t < nb && lb[t] < L) ++t;
+        int t1 = t;
+        while (t1 < nb && lb[t1] == L) ++t1;
+        groups[g++] = make_int4(s0, s1, t, t1);
+        s0 = s1;
+    }
+    return g;
+}
+
+// N consecutive values from p, which is aligned to min(16, N sizeof(T)) bytes.
+template <class T, int N>
+__device__ __forceinline__ void load_vec(const T *p, T (&v)[N]) {
+    if constexpr (sizeof(T) * N >= 16) {
+        constexpr int per = 16 / sizeof(T);
+#pragma unroll
+        for (int q = 0; q < N / per; ++q) {
+            const float4 f = reinterpret_cast<const float4 *>(p)[q];
+            const T *e = reinterpret_cast<const T *>(&f);
+#pragma unroll
+            for (int r = 0; r < per; ++r) v[q * per + r] = e[r];
         }
-        const T *xj = x2 + ((size_t)pr.b * ma2 + j) * rep;
-        T s = T(0);
-        for (int k = threadIdx.x; k < rep; k += blockDim.x) {
-            const T dk = xi[k] - xj[k];
-            d[k] = dk;
-            s = fma(dk, dk, s);
-        }
-        for (int off = 16; off; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
-        __syncthreads();
-        if (threadIdx.x < 32) {
-            T v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : T(0);
-            for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-            if (threadIdx.x == 0) red[0] = v;
-        }
-        __syncthreads();
-        const T e = kexp<T>(c2 * red[0]);
-        if (threadIdx.x == 0) {
-            W[wbase + j] = e * is2;
-            W2[wbase + j] = e * is4;
-        }
-        const T *Jj = dx2 + ((size_t)pr.b * ma2 + j) * rep * (size_t)ld2;
-        for (int c = threadIdx.x; c < 3 * pr.nb; c += blockDim.x) {
-            T acc = T(0);
-            for (int k = 0; k < rep; ++k) acc = fma(Jj[(size_t)k * ld2 + c], d[k], acc);
-            Tt[(wbase + j) * ld2 + c] = acc;
-        }
-        __syncthreads();
+    } else if constexpr (sizeof(T) * N == 8) {
+        const float2 f = *reinterpret_cast<const float2 *>(p);
+        const T *e = reinterpret_cast<const T *>(&f);
+#pragma unroll
+        for (int r = 0; r < N; ++r) v[r] = e[r];
+    } else {
+#pragma unroll
+        for (int r = 0; r < N; ++r) v[r] = p[r];
     }
 }
 
-// ------------------------------------------------------- Hessian kernel 2
-// Block per (pair p, atom i, 32-row slice of rep); thread (k, c):
-//   Y[p, i, k, c] = sum_j W[p,i,j] J_j[k,c] - W2[p,i,j] (x_i[k] - x_j[k]) Tt[p,i,j,c]
+// Size of the balanced chunks of a label group of n atoms (at most cap each).
+__device__ __forceinline__ int chunk_size(int n, int cap) {
+    const int nch = (n + cap - 1) / cap;
+    return (n + nch - 1) / nch;
+}
+
+// Smallest of 1, 2, 4, ... that is >= n.
+__device__ __forceinline__ int pow2_at_least(int n) {
+    int p = 1;
+    while (p < n) p <<= 1;
+    return p;
+}
+
+// ------------------------------------------------------- Hessian kernel 1
+// Block per molecule pair p = (a, b).  For every same-label atom pair (i, j):
+//   W[p, i, j] = e_ij / sigma^2,
+//   Tt[p, i, j, c] = (e_ij / sigma^4) (J_j^T (x_i - x_j))[c],  c < 3 n_b.
+// Other (i, j) entries are not written (never read).  The weights come first
+// (a warp per atom pair); then, per label group and balanced chunk of at most
+// HT_IG atoms i of a (descriptors staged in shared memory), a warp item is (32
+// columns, one partner j) accumulating the chunk's dot products over rep, so
+// each J_j load feeds one FMA per atom of the chunk.  With a non-null bound
+// the block raises *bound to an upper bound of |Y| (kernel 2's output) over
+// its pair:  max_i [max|J_b| sum_j w_ij + sum_j |x_i - x_j|_inf |t'_ij|_inf]
+// (|t'|_inf taken per 32-column slice and summed over the slices).
+template <class T> struct HtCfg { static constexpr int IG = 16; };
+template <> struct HtCfg<double> { static constexpr int IG = 8; };
+
+__host__ __device__ inline size_t hess_t_head(int ma1, int ma2) {
+    return ((size_t)ma1 * sizeof(int4) + (size_t)(ma1 + ma2 + ma1 + 1) * sizeof(int) +
+            (size_t)(2 * ma1 + ma1 * ma2) * sizeof(float) + 15) &
+           ~(size_t)15;
+}
+
 template <class T>
-__global__ void hess_y_kernel(const HessPair *__restrict__ pairs, const T *__restrict__ x1,
-                              const T *__restrict__ x2, const T *__restrict__ dx2, int ma1,
-                              int ma2, int rep, const T *__restrict__ W,
-                              const T *__restrict__ W2, const T *__restrict__ Tt,
-                              T *__restrict__ Y, float *__restrict__ amax) {
-    const HessPair pr = pairs[blockIdx.z];
-    const int i = blockIdx.y;
-    if (i >= pr.na) return;
-    float vmax = 0.f;
-    const int ld2 = 3 * ma2;
-    const int ncol = 3 * pr.nb;
-    const size_t wbase = ((size_t)blockIdx.z * ma1 + i) * ma2;
-    const T *xi = x1 + ((size_t)pr.a * ma1 + i) * rep;
-    T *Yi = Y + ((size_t)blockIdx.z * ma1 + i) * rep * (size_t)ld2;
-    for (int idx = threadIdx.x; idx < 32 * ncol; idx += blockDim.x) {
-        const int kl = idx / ncol, c = idx - kl * ncol;
-        const int k = blockIdx.x * 32 + kl;
-        if (k >= rep) continue;
-        const T xik = xi[k];
-        T acc = T(0);
-        for (int j = 0; j < pr.nb; ++j) {
-            const T wj = W[wbase + j];
-            if (wj == T(0)) continue;
-            const T jv = dx2[(((size_t)pr.b * ma2 + j) * rep + k) * ld2 + c];
-            const T dk = xik - x2[((size_t)pr.b * ma2 + j) * rep + k];
-            acc = fma(wj, jv, acc);
-            acc = fma(-W2[wbase + j] * dk, Tt[(wbase + j) * ld2 + c], acc);
+size_t hess_t_smem(int ma1, int ma2, int rep) {
+    return hess_t_head(ma1, ma2) +
+           ((size_t)HtCfg<T>::IG * ((rep + 7) & ~7) + (size_t)ma1 * ma2) * sizeof(T);
+}
+
+template <class T, int IGC, bool VEC>
+__device__ __forceinline__ void ht_chunk(const T *__restrict__ xs, int rep8, int rep,
+                                         const T *__restrict__ Jb, const T *__restrict__ xb,
+                                         const int *pa, const int *pb, int4 gr, int i0, int cnt,
+                                         int ncol, int ld2, size_t wbase, int ma2, const T *w2s,
+                                         const float *dinf, float *bterm, T *__restrict__ Tt,
+                                         T &jmax) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const int nchunk = (ncol + 31) / 32;
+    const int items = nchunk * (gr.w - gr.z);
+    for (int it = warp; it < items; it += nwarp) {
+        const int cc = it % nchunk, j = pb[gr.z + it / nchunk];
+        const int c = cc * 32 + lane;
+        const int cs = c < ncol ? c : 0;
+        const T *Jj = Jb + (size_t)j * rep * ld2 + cs;
+        const T *xj = xb + (size_t)j * rep;
+        T acc[IGC];
+#pragma unroll
+        for (int ii = 0; ii < IGC; ++ii) acc[ii] = T(0);
+        int k = 0;
+        if (VEC) {
+            for (; k + 8 <= rep; k += 8) {
+                T jv[8], xv[8];
+#pragma unroll
+                for (int r = 0; r < 8; ++r) jv[r] = Jj[(size_t)(k + r) * ld2];
+                load_vec<T, 8>(xj + k, xv);
+#pragma unroll
+                for (int r = 0; r < 8; ++r) jmax = fmax(jmax, fabs(jv[r]));
+#pragma unroll
+                for (int ii = 0; ii < IGC; ++ii) {
+                    T xi[8];
+                    load_vec<T, 8>(xs + ii * rep8 + k, xi);
+#pragma unroll
+                    for (int r = 0; r < 8; ++r) acc[ii] = fma(jv[r], xi[r] - xv[r], acc[ii]);
+                }
+            }
         }
-        Yi[(size_t)k * ld2 + c] = acc;
-        vmax = fmaxf(vmax, fabsf((float)acc));
+        for (; k < rep; ++k) {
+            const T jv = Jj[(size_t)k * ld2], xv = xj[k];
+            jmax = fmax(jmax, fabs(jv));
+#pragma unroll
+            for (int ii = 0; ii < IGC; ++ii) acc[ii] = fma(jv, xs[ii * rep8 + k] - xv, acc[ii]);
+        }
+#pragma unroll
+        for (int ii = 0; ii < IGC; ++ii) {
+            if (ii < cnt) {
+                const int i = pa[i0 + ii];
+                const T t = w2s[i * ma2 + j] * acc[ii];
+                if (c < ncol) Tt[(wbase + (size_t)i * ma2 + j) * ld2 + c] = t;
+                if (bterm) {
+                    float m = (c < ncol) ? fabsf((float)t) : 0.f;
+                    for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+                    if (lane == 0) atomicAdd(&bterm[i], dinf[i * ma2 + j] * m);
+                }
+            }
+        }
     }
-    if (amax) {
-        // largest |entry| written, for the power-of-two scale of the fp16 split
-        for (int o = 16; o; o >>= 1) vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
-        if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<int *>(amax), __float_as_int(vmax));
+}
+
+template <class T, bool VEC>
+__global__ void __launch_bounds__(256) hess_t_kernel(
+    const HessPair *__restrict__ pairs, const T *__restrict__ x1, const T *__restrict__ x2,
+    const T *__restrict__ dx2, const int *__restrict__ perm1, const int *__restrict__ lab1,
+    const int *__restrict__ perm2, const int *__restrict__ lab2, int ma1, int ma2, int rep,
+    T c2, T is2, T is4, T *__restrict__ W, T *__restrict__ Tt, float *__restrict__ bound) {
+    constexpr int IG = HtCfg<T>::IG;
+    extern __shared__ __align__(16) unsigned char ht_raw[];
+    int4 *groups = reinterpret_cast<int4 *>(ht_raw);  // ma1
+    int *pa = reinterpret_cast<int *>(groups + ma1);   // ma1
+    int *pb = pa + ma1;                                // ma2
+    int *gstart = pb + ma2;                            // ma1 + 1: prefix of pair counts
+    float *wsum = reinterpret_cast<float *>(gstart + ma1 + 1);  // ma1: sum_j w_ij
+    float *bterm = wsum + ma1;                                   // ma1
+    float *dinf = bterm + ma1;                                   // ma1 x ma2: |x_i - x_j|_inf
+    const int rep8 = (rep + 7) & ~7;
+    // xs first after the head: rows start on 16-byte boundaries (vector loads)
+    T *xs = reinterpret_cast<T *>(ht_raw + hess_t_head(ma1, ma2));  // [IG][rep8]
+    T *w2s = xs + (size_t)IG * rep8;                                  // [i][j] e / sigma^4
+    __shared__ float red[8];
+    __shared__ int ngroups;
+    const int p = blockIdx.x;
+    const HessPair pr = pairs[p];
+    const int ld2 = 3 * ma2, ncol = 3 * pr.nb;
+    const size_t wbase = (size_t)p * ma1 * ma2;
+    for (int e = threadIdx.x; e < pr.na; e += blockDim.x) {
+        pa[e] = perm1[(size_t)pr.a * ma1 + e];
+        wsum[e] = 0.f;
+        bterm[e] = 0.f;
+    }
+    for (int e = threadIdx.x; e < pr.nb; e += blockDim.x) pb[e] = perm2[(size_t)pr.b * ma2 + e];
+    if (threadIdx.x == 0) {
+        const int g = pair_label_groups(lab1 + (size_t)pr.a * ma1, lab2 + (size_t)pr.b * ma2,
+                                        pr.na, pr.nb, groups);
+        ngroups = g;
+        gstart[0] = 0;
+        for (int q = 0; q < g; ++q)
+            gstart[q + 1] = gstart[q] + (groups[q].y - groups[q].x) * (groups[q].w - groups[q].z);
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const T *xa = x1 + (size_t)pr.a * ma1 * rep, *xb = x2 + (size_t)pr.b * ma2 * rep;
+    // weights of all same-label pairs
+    for (int q = warp; q < gstart[ngroups]; q += nwarp) {
+        int g = 0;
+        while (gstart[g + 1] <= q) ++g;
+        const int4 gr = groups[g];
+        const int off = q - gstart[g], nbg = gr.w - gr.z;
+        const int i = pa[gr.x + off / nbg], j = pb[gr.z + off % nbg];
+        const T *xi = xa + (size_t)i * rep, *xj = xb + (size_t)j * rep;
+        T dd = T(0), dm = T(0);
+        for (int k = lane; k < rep; k += 32) {
+            const T d = xi[k] - xj[k];
+            dd = fma(d, d, dd);
+            dm = fmax(dm, fabs(d));
+        }
+        for (int o = 16; o; o >>= 1) {
+            dd += __shfl_xor_sync(0xffffffffu, dd, o);
+            dm = fmax(dm, __shfl_xor_sync(0xffffffffu, dm, o));
+        }
+        if (lane == 0) {
+            const T e = kexp<T>(c2 * dd);
+            W[wbase + (size_t)i * ma2 + j] = e * is2;
+            w2s[i * ma2 + j] = e * is4;
+            dinf[i * ma2 + j] = (float)dm;
+            if (bound) atomicAdd(&wsum[i], (float)(e * is2));
+        }
+    }
+    const T *Jb = dx2 + (size_t)pr.b * ma2 * rep * ld2;
+    T jmax = T(0);
+    float *bt = bound ? bterm : nullptr;
+    for (int g = 0; g < ngroups; ++g) {
+        const int4 gr = groups[g];
+        const int csz = chunk_size(gr.y - gr.x, IG);
+        for (int i0 = gr.x; i0 < gr.y; i0 += csz) {
+            const int cnt = min(csz, gr.y - i0);
+            const int igc = pow2_at_least(cnt);
+            __syncthreads();  // weights written / previous chunk's xs read
+            for (int row = warp; row < igc; row += nwarp)
+                for (int k = lane; k < rep8; k += 32)
+                    xs[row * rep8 + k] =
+                        (row < cnt && k < rep) ? xa[(size_t)pa[i0 + row] * rep + k] : T(0);
+            __syncthreads();
+            if (IG >= 16 && igc == 16)
+                ht_chunk<T, (IG >= 16 ? 16 : 8), VEC>(xs, rep8, rep, Jb, xb, pa, pb, gr, i0, cnt,
+                                                      ncol, ld2, wbase, ma2, w2s, dinf, bt, Tt,
+                                                      jmax);
+            else if (igc == 8)
+                ht_chunk<T, 8, VEC>(xs, rep8, rep, Jb, xb, pa, pb, gr, i0, cnt, ncol, ld2, wbase,
+                                    ma2, w2s, dinf, bt, Tt, jmax);
+            else if (igc == 4)
+                ht_chunk<T, 4, VEC>(xs, rep8, rep, Jb, xb, pa, pb, gr, i0, cnt, ncol, ld2, wbase,
+                                    ma2, w2s, dinf, bt, Tt, jmax);
+            else if (igc == 2)
+                ht_chunk<T, 2, VEC>(xs, rep8, rep, Jb, xb, pa, pb, gr, i0, cnt, ncol, ld2, wbase,
+                                    ma2, w2s, dinf, bt, Tt, jmax);
+            else
+                ht_chunk<T, 1, VEC>(xs, rep8, rep, Jb, xb, pa, pb, gr, i0, cnt, ncol, ld2, wbase,
+                                    ma2, w2s, dinf, bt, Tt, jmax);
+        }
+    }
+    if (!bound) return;
+    // block max of |J_b| over the loaded rows, then max_i of the bound
+    float jm = (float)jmax;
+    for (int o = 16; o; o >>= 1) jm = fmaxf(jm, __shfl_xor_sync(0xffffffffu, jm, o));
+    if (lane == 0) red[warp] = jm;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        float v = lane < nwarp ? red[lane] : 0.f;
+        for (int o = 16; o; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+        jm = v;
+        float bmax = 0.f;
+        for (int i = lane; i < pr.na; i += 32) bmax = fmaxf(bmax, jm * wsum[i] + bterm[i]);
+        for (int o = 16; o; o >>= 1) bmax = fmaxf(bmax, __shfl_xor_sync(0xffffffffu, bmax, o));
+        if (lane == 0) atomicMax(reinterpret_cast<int *>(bound), __float_as_int(bmax * 1.001f));
+    }
+}
+
+template <class T>
+kfb_status launch_hess_t(const HessPair *pairs, int np, const T *x1, const T *x2, const T *dx2,
+                         const int *perm1, const int *lab1, const int *perm2, const int *lab2,
+                         int ma1, int ma2, int rep, T c2, T is2, T is4, T *W, T *Tt,
+                         float *bound, cudaStream_t s) {
+    const size_t smem = hess_t_smem<T>(ma1, ma2, rep);
+    if (smem > 200 * 1024)
+        return set_error(KFB_ERR_INVALID_ARG, "max_atoms %d / %d, rep %d too large for the "
+                         "Hessian kernel", ma1, ma2, rep);
+    const bool vec = (rep % 8) == 0 && (reinterpret_cast<size_t>(x2) % 16) == 0;
+    auto kern = vec ? hess_t_kernel<T, true> : hess_t_kernel<T, false>;
+    if (smem > 48 * 1024)
+        KFB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem));
+    kern<<<np, 256, smem, s>>>(pairs, x1, x2, dx2, perm1, lab1, perm2, lab2, ma1, ma2, rep, c2,
+                               is2, is4, W, Tt, bound);
+    KFB_CUDA_TRY(cudaGetLastError());
+    return KFB_OK;
+}
+
+// ------------------------------------------------------- Hessian kernel 2
+// Y_i = sum_j (w_ij J_j - w'_ij d_ij t_ij^T) for all atoms i of a, written as
+//   Y_i[k, c] = sum_j (w_ij J_j[k, c] + x_j[k] t'_ij[c]) - x_i[k] r_i[c],
+//   t'_ij = w'_ij t_ij (kernel 1 writes it scaled),  r_i = sum_j t'_ij
+// over same-label atom pairs only.  Atoms of each molecule are visited in
+// label order (perm: sorted position -> atom), so one label group of a meets
+// one contiguous run of b.  Block per (pair, slice of kt rows of rep); each
+// warp owns one (32 columns c, 8 rows k) tile and keeps a chunk of up to
+// HY_IG atoms x 8 rows of Y in registers, so each J_j[k, c] load feeds two
+// FMAs per atom of the chunk.  w_ij and t'_ij of the chunk's atoms x HY_JT
+// partners are staged in shared memory by the whole block (t' with the atoms
+// innermost, read as vectors); the descriptor rows of the slice too.
+//   MODE 1: fp16 pair hi/lo of scale * Y, K-major rows (p, c) of (i, k)
+//   MODE 2: Y[p, i, k, c] in T
+// FULL: rep % 8 == 0 (no row guards).
+constexpr int HY_KR = 8, HY_JT = 8;
+template <class T> struct HyCfg { static constexpr int IG = 8, WARPS = 8; };
+template <> struct HyCfg<double> { static constexpr int IG = 4, WARPS = 8; };
+
+struct HyGeom {
+    int kt;      // rows of rep per block (multiple of 8)
+    int ldc;     // padded columns (multiple of 32)
+    int warps;   // (ldc / 32) * (kt / 8)
+    size_t smem;
+};
+
+template <class T>
+HyGeom hess_y_geom(int ma1, int ma2) {
+    HyGeom g;
+    const int nchunk = (3 * ma2 + 31) / 32;
+    const int kgroups = std::max(1, HyCfg<T>::WARPS / nchunk);
+    g.kt = 8 * kgroups;
+    g.ldc = 32 * nchunk;
+    g.warps = nchunk * kgroups;
+    const size_t head =
+        ((size_t)ma1 * sizeof(int4) + (size_t)(ma1 + ma2) * sizeof(int) + 15) & ~(size_t)15;
+    g.smem = head + ((size_t)(ma1 + ma2) * g.kt + (size_t)HyCfg<T>::IG * HY_JT +
+                     (size_t)HyCfg<T>::IG * HY_JT * g.ldc) * sizeof(T);
+    return g;
+}
+
+template <class T, int IGC, int MODE, bool FULL>
+__device__ __forceinline__ void hy_chunk(const HessPair &pr, int p, int4 gr, int i0, int cnt,
+                                         const int *pa, const int *pb, const T *xa_s,
+                                         const T *xb_s, T *ws, T *ts, int kt, int ldc, int ma1,
+                                         int ma2, int rep, int k0, int kk0, bool active,
+                                         const T *__restrict__ dx2, const T *__restrict__ W,
+                                         const T *__restrict__ Tt, float scale,
+                                         __half *__restrict__ yhi, __half *__restrict__ ylo,
+                                         T *__restrict__ Y) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const int nchunk = ldc / 32;
+    const int c = (warp % nchunk) * 32 + lane;
+    const int ld2 = 3 * ma2, ncol = 3 * pr.nb;
+    const int cs = c < ncol ? c : 0;
+    const size_t wbase = (size_t)p * ma1 * ma2;
+    T acc[IGC][HY_KR], rr[IGC];
+#pragma unroll
+    for (int ii = 0; ii < IGC; ++ii) {
+        rr[ii] = T(0);
+#pragma unroll
+        for (int r = 0; r < HY_KR; ++r) acc[ii][r] = T(0);
+    }
+    for (int j0 = gr.z; j0 < gr.w; j0 += HY_JT) {
+        const int jn = min(HY_JT, gr.w - j0);
+        __syncthreads();  // previous step's ws / ts fully read
+        for (int jj = warp; jj < HY_JT; jj += nwarp) {
+            const bool okj = jj < jn;
+            const int j = okj ? pb[j0 + jj] : 0;
+            for (int cx = lane; cx < ldc; cx += 32) {
+#pragma unroll
+                for (int ii = 0; ii < IGC; ++ii) {
+                    const bool ok = okj && ii < cnt && cx < ncol;
+                    ts[(jj * ldc + cx) * IGC + ii] =
+                        ok ? Tt[(wbase + (size_t)pa[i0 + ii] * ma2 + j) * ld2 + cx] : T(0);
+                }
+            }
+            if (lane < IGC)
+                ws[jj * IGC + lane] =
+                    (okj && lane < cnt) ? W[wbase + (size_t)pa[i0 + lane] * ma2 + j] : T(0);
+        }
+        __syncthreads();
+        if (!active) continue;  // warp-uniform
+        const T *Jb = dx2 + ((size_t)pr.b * ma2 * rep + k0) * (size_t)ld2 + cs;
+        for (int jj = 0; jj < jn; ++jj) {
+            T jv[HY_KR];
+            const T *Jj = Jb + (size_t)pb[j0 + jj] * rep * ld2;
+#pragma unroll
+            for (int r = 0; r < HY_KR; ++r)
+                jv[r] = (FULL || k0 + r < rep) ? Jj[(size_t)r * ld2] : T(0);
+            T xj[HY_KR], t[IGC], w[IGC];
+            load_vec<T, HY_KR>(xb_s + pb[j0 + jj] * kt + kk0, xj);
+            load_vec<T, IGC>(ts + (jj * ldc + c) * IGC, t);
+            load_vec<T, IGC>(ws + jj * IGC, w);
+#pragma unroll
+            for (int ii = 0; ii < IGC; ++ii) {
+                rr[ii] += t[ii];
+#pragma unroll
+                for (int r = 0; r < HY_KR; ++r)
+                    acc[ii][r] = fma(w[ii], jv[r], fma(xj[r], t[ii], acc[ii][r]));
+            }
+        }
+    }
+    if (!active || c >= ncol) return;
+#pragma unroll
+    for (int ii = 0; ii < IGC; ++ii) {
+        if (ii >= cnt) continue;
+        const int i = pa[i0 + ii];
+        T xi[HY_KR];
+        load_vec<T, HY_KR>(xa_s + i * kt + kk0, xi);
+#pragma unroll
+        for (int r = 0; r < HY_KR; ++r) acc[ii][r] = fma(-xi[r], rr[ii], acc[ii][r]);
+        if (MODE == 1) {
+            // rep % 16 == 0 on this path: 8 rows are 16 aligned bytes
+            unsigned hw[HY_KR / 2], lw[HY_KR / 2];
+#pragma unroll
+            for (int r = 0; r < HY_KR; r += 2) {
+                const float v0 = (float)acc[ii][r] * scale;
+                const float v1 = (float)acc[ii][r + 1] * scale;
+                const __half h0 = __float2half_rn(v0), h1 = __float2half_rn(v1);
+                const __half l0 = __float2half_rn(v0 - __half2float(h0));
+                const __half l1 = __float2half_rn(v1 - __half2float(h1));
+                hw[r / 2] =
+                    (unsigned)__half_as_ushort(h0) | ((unsigned)__half_as_ushort(h1) << 16);
+                lw[r / 2] =
+                    (unsigned)__half_as_ushort(l0) | ((unsigned)__half_as_ushort(l1) << 16);
+            }
+            const size_t o = (((size_t)p * ld2 + c) * ma1 + i) * (size_t)rep + k0;
+            *reinterpret_cast<uint4 *>(yhi + o) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+            *reinterpret_cast<uint4 *>(ylo + o) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+        } else {
+            T *Yi = Y + ((size_t)p * ma1 + i) * rep * (size_t)ld2 + c;
+#pragma unroll
+            for (int r = 0; r < HY_KR; ++r)
+                if (FULL || k0 + r < rep) Yi[(size_t)(k0 + r) * ld2] = acc[ii][r];
+        }
+    }
+}
+
+template <class T, int MODE, bool FULL>
+__global__ void __launch_bounds__(256, 2) hess_y_kernel(
+    const HessPair *__restrict__ pairs, const T *__restrict__ x1, const T *__restrict__ x2,
+    const T *__restrict__ dx2, const int *__restrict__ perm1, const int *__restrict__ lab1,
+    const int *__restrict__ perm2, const int *__restrict__ lab2, int ma1, int ma2, int rep,
+    int kt, int ldc, const T *__restrict__ W, const T *__restrict__ Tt, float scale,
+    __half *__restrict__ yhi, __half *__restrict__ ylo, T *__restrict__ Y) {
+    constexpr int IG = HyCfg<T>::IG;
+    extern __shared__ __align__(16) unsigned char hy_raw[];
+    int4 *groups = reinterpret_cast<int4 *>(hy_raw);  // ma1
+    int *pa = reinterpret_cast<int *>(groups + ma1);   // ma1
+    int *pb = pa + ma1;                                // ma2
+    T *xa_s = reinterpret_cast<T *>(
+        hy_raw + (((size_t)ma1 * sizeof(int4) + (size_t)(ma1 + ma2) * sizeof(int) + 15) & ~(size_t)15));
+    T *xb_s = xa_s + (size_t)ma1 * kt;  // [atom][row of the slice]
+    T *ws = xb_s + (size_t)ma2 * kt;    // [HY_JT][IGC]
+    T *ts = ws + IG * HY_JT;            // [HY_JT][ldc][IGC]
+    __shared__ int ngroups;
+    const int p = blockIdx.y;
+    const HessPair pr = pairs[p];
+    const int kbase = blockIdx.x * kt;
+    for (int e = threadIdx.x; e < pr.na; e += blockDim.x) pa[e] = perm1[(size_t)pr.a * ma1 + e];
+    for (int e = threadIdx.x; e < pr.nb; e += blockDim.x) pb[e] = perm2[(size_t)pr.b * ma2 + e];
+    for (int e = threadIdx.x; e < pr.na * kt; e += blockDim.x) {
+        const int i = e / kt, kk = e - i * kt;
+        xa_s[e] = (kbase + kk < rep) ? x1[((size_t)pr.a * ma1 + i) * rep + kbase + kk] : T(0);
+    }
+    for (int e = threadIdx.x; e < pr.nb * kt; e += blockDim.x) {
+        const int j = e / kt, kk = e - j * kt;
+        xb_s[e] = (kbase + kk < rep) ? x2[((size_t)pr.b * ma2 + j) * rep + kbase + kk] : T(0);
+    }
+    if (threadIdx.x == 0)  // atoms of a whose label b lacks get Y = 0 (written)
+        ngroups = pair_label_groups(lab1 + (size_t)pr.a * ma1, lab2 + (size_t)pr.b * ma2,
+                                    pr.na, pr.nb, groups);
+    __syncthreads();
+    const int warp = threadIdx.x >> 5;
+    const int nchunk = ldc / 32;
+    const int kk0 = (warp / nchunk) * HY_KR, k0 = kbase + kk0;
+    const bool active = k0 < rep;  // warp-uniform
+    for (int g = 0; g < ngroups; ++g) {
+        const int4 gr = groups[g];
+        const int csz = chunk_size(gr.y - gr.x, IG);
+        for (int i0 = gr.x; i0 < gr.y; i0 += csz) {
+            const int cnt = min(csz, gr.y - i0);
+            const int igc = pow2_at_least(cnt);
+#define KFB_HY_CHUNK(N)                                                                        \
+    hy_chunk<T, N, MODE, FULL>(pr, p, gr, i0, cnt, pa, pb, xa_s, xb_s, ws, ts, kt, ldc, ma1, ma2, \
+                               rep, k0, kk0, active, dx2, W, Tt, scale, yhi, ylo, Y)
+            if (IG >= 8 && igc == 8)
+                KFB_HY_CHUNK((IG >= 8 ? 8 : 4));
+            else if (igc == 4)
+                KFB_HY_CHUNK(4);
+            else if (igc == 2)
+                KFB_HY_CHUNK(2);
+            else
+                KFB_HY_CHUNK(1);
+#undef KFB_HY_CHUNK
+        }
+    }
+}
+
+template <class T, int MODE>
+kfb_status launch_hess_y(const HessPair *pairs, int np, const T *x1, const T *x2, const T *dx2,
+                         const int *perm1, const int *lab1, const int *perm2, const int *lab2,
+                         int ma1, int ma2, int rep, const T *W, const T *Tt, float scale,
+                         __half *yhi, __half *ylo, T *Y, cudaStream_t s) {
+    const HyGeom g = hess_y_geom<T>(ma1, ma2);
+    if (g.warps > 8 || g.smem > 100 * 1024)
+        return set_error(KFB_ERR_INVALID_ARG, "max_atoms %d / %d too large for the Hessian kernel",
+                         ma1, ma2);
+    const bool full = rep % 8 == 0;
+    auto kern = full ? hess_y_kernel<T, MODE, true> : hess_y_kernel<T, MODE, false>;
+    if (g.smem > 48 * 1024)
+        KFB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)g.smem));
+    const dim3 grid((unsigned)((rep + g.kt - 1) / g.kt), (unsigned)np);
+    kern<<<grid, 32 * g.warps, g.smem, s>>>(pairs, x1, x2, dx2, perm1, lab1, perm2, lab2, ma1,
+                                            ma2, rep, g.kt, g.ldc, W, Tt, scale, yhi, ylo, Y);
+    KFB_CUDA_TRY(cudaGetLastError());
+    return KFB_OK;
+}
+
+// Atoms of every molecule in label order: perm[m * ma + s] = atom at sorted
+// position s, lab[m * ma + s] its label (stable within a label).
+void label_order(const SetView &v, std::vector<int> &perm, std::vector<int> &lab) {
+    perm.assign((size_t)v.nm * v.ma, 0);
+    lab.assign((size_t)v.nm * v.ma, 0);
+    std::vector<int> idx;
+    for (int m = 0; m < v.nm; ++m) {
+        const int n = v.natoms(m);
+        const int32_t *q = v.q + (size_t)m * v.ma;
+        idx.resize(n);
+        for (int i = 0; i < n; ++i) idx[i] = i;
+        std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return q[x] < q[y]; });
+        for (int s2 = 0; s2 < n; ++s2) {
+            perm[(size_t)m * v.ma + s2] = idx[s2];
+            lab[(size_t)m * v.ma + s2] = q[idx[s2]];
+        }
     }
 }
 
@@ -403,34 +822,39 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
     std::vector<int> off1, off2;
     deriv_offsets(s1.v, off1);
     deriv_offsets(s2.v, off2);
+    // pairs ordered by b: the Y kernels stream molecule b's Jacobian, which
+    // then stays in L2 across the consecutive pairs that share it
     std::vector<HessPair> pairs;
-    for (int a = 0; a < s1.v.nm; ++a) {
-        const int na = s1.v.natoms(a);
-        if (na == 0) continue;
-        for (int b = symmetric ? a : 0; b < s2.v.nm; ++b) {
-            const int nb = s2.v.natoms(b);
-            if (nb == 0) continue;
+    for (int b = 0; b < s2.v.nm; ++b) {
+        const int nb = s2.v.natoms(b);
+        if (nb == 0) continue;
+        for (int a = 0; a < (symmetric ? b + 1 : s1.v.nm); ++a) {
+            const int na = s1.v.natoms(a);
+            if (na == 0) continue;
             pairs.push_back(HessPair{a, b, na, nb});
         }
     }
     if (pairs.empty()) return KFB_OK;
-    std::vector<int> q1(s1.v.q, s1.v.q + (size_t)s1.v.nm * s1.v.ma);
-    std::vector<int> q2(s2.v.q, s2.v.q + (size_t)s2.v.nm * s2.v.ma);
-    DevBuf d_q1, d_q2;
-    KFB_TRY(upload(d_q1, q1, s));
-    KFB_TRY(upload(d_q2, q2, s));
     const int ma1 = s1.v.ma, ma2 = s2.v.ma, ld1 = 3 * ma1, ld2 = 3 * ma2;
-    const size_t per_pair = ((size_t)ma1 * ma2 * (2 + ld2) + (size_t)ma1 * rep * ld2) * sizeof(T) +
-                            (tc ? (size_t)ma1 * rep * ld2 * 2 * sizeof(__half) : 0);
+    // scratch per pair: W, Tt, and Y (T) or its fp16 pair (tensor cores)
+    const size_t per_pair = (size_t)ma1 * ma2 * (1 + ld2) * sizeof(T) +
+                            (size_t)ma1 * rep * ld2 * (tc ? 2 * sizeof(__half) : sizeof(T));
     int batch = (int)std::max<size_t>(1, budget_bytes() / per_pair);
     batch = std::min<int>(batch, (int)pairs.size());
     batch = std::min(batch, 65535);
-    DevBuf W, W2, Tt, Y, dpairs;
+    DevBuf W, Tt, Y, dpairs;
     KFB_TRY(W.alloc((size_t)batch * ma1 * ma2 * sizeof(T), s));
-    KFB_TRY(W2.alloc((size_t)batch * ma1 * ma2 * sizeof(T), s));
     KFB_TRY(Tt.alloc((size_t)batch * ma1 * ma2 * ld2 * sizeof(T), s));
-    KFB_TRY(Y.alloc((size_t)batch * ma1 * rep * ld2 * sizeof(T), s));
+    if (!tc) KFB_TRY(Y.alloc((size_t)batch * ma1 * rep * ld2 * sizeof(T), s));
     KFB_TRY(dpairs.alloc((size_t)batch * sizeof(HessPair), s));
+    std::vector<int> perm1, lab1, perm2, lab2;
+    label_order(s1.v, perm1, lab1);
+    label_order(s2.v, perm2, lab2);
+    DevBuf d_perm1, d_lab1, d_perm2, d_lab2;
+    KFB_TRY(upload(d_perm1, perm1, s));
+    KFB_TRY(upload(d_lab1, lab1, s));
+    KFB_TRY(upload(d_perm2, perm2, s));
+    KFB_TRY(upload(d_lab2, lab2, s));
     DevBuf jth, jtl, yth, ytl, yamax;
     float jt_scale = 1.f;
     if (tc) {
@@ -455,26 +879,35 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
         const int np = (int)std::min<size_t>(batch, pairs.size() - p0);
         KFB_CUDA_TRY(cudaMemcpyAsync(dpairs.ptr, pairs.data() + p0, np * sizeof(HessPair),
                                      cudaMemcpyHostToDevice, s));
+        const T *x1p = static_cast<const T *>(s1.x), *x2p = static_cast<const T *>(s2.x);
+        const T *dx2p = static_cast<const T *>(s2.dx);
         auto tr_t = std::make_unique<TraceScope>("hessian:t", s);
-        hess_t_kernel<T><<<dim3(ma1, np), 128, rep * sizeof(T), s>>>(
-            dpairs.as<HessPair>(), static_cast<const T *>(s1.x), static_cast<const T *>(s2.x),
-            static_cast<const T *>(s2.dx), d_q1.as<int>(), d_q2.as<int>(), ma1, ma2, rep, c2,
-            is2, is4, W.as<T>(), W2.as<T>(), Tt.as<T>());
-        KFB_CUDA_TRY(cudaGetLastError());
+        // with tensor cores kernel 1 also bounds |Y| for the power-of-two
+        // scale of the fp16 split that kernel 2 writes
+        if (tc) KFB_TRY(zero(yamax.ptr, sizeof(float), s));
+        KFB_TRY(launch_hess_t<T>(dpairs.as<HessPair>(), np, x1p, x2p, dx2p, d_perm1.as<int>(),
+                                 d_lab1.as<int>(), d_perm2.as<int>(), d_lab2.as<int>(), ma1, ma2,
+                                 rep, c2, is2, is4, W.as<T>(), Tt.as<T>(),
+                                 tc ? yamax.as<float>() : nullptr, s));
         tr_t.reset();
         auto tr_y = std::make_unique<TraceScope>("hessian:y", s);
-        if (tc) KFB_TRY(zero(yamax.ptr, sizeof(float), s));
-        hess_y_kernel<T><<<dim3((rep + 31) / 32, ma1, np), 256, 0, s>>>(
-            dpairs.as<HessPair>(), static_cast<const T *>(s1.x), static_cast<const T *>(s2.x),
-            static_cast<const T *>(s2.dx), ma1, ma2, rep, W.as<T>(), W2.as<T>(), Tt.as<T>(),
-            Y.as<T>(), tc ? yamax.as<float>() : nullptr);
-        KFB_CUDA_TRY(cudaGetLastError());
+        float y_scale = 1.f;
+        if (tc) {
+            KFB_TRY(pow2_from_device(yamax.as<float>(), s, &y_scale));
+            KFB_TRY((launch_hess_y<T, 1>(dpairs.as<HessPair>(), np, x1p, x2p, dx2p,
+                                         d_perm1.as<int>(), d_lab1.as<int>(), d_perm2.as<int>(),
+                                         d_lab2.as<int>(), ma1, ma2, rep, W.as<T>(), Tt.as<T>(),
+                                         y_scale, yth.as<__half>(), ytl.as<__half>(), nullptr,
+                                         s)));
+        } else {
+            KFB_TRY((launch_hess_y<T, 2>(dpairs.as<HessPair>(), np, x1p, x2p, dx2p,
+                                         d_perm1.as<int>(), d_lab1.as<int>(), d_perm2.as<int>(),
+                                         d_lab2.as<int>(), ma1, ma2, rep, W.as<T>(), Tt.as<T>(),
+                                         1.f, nullptr, nullptr, Y.as<T>(), s)));
+        }
         tr_y.reset();
         auto tr_g = std::make_unique<TraceScope>("hessian:split+gemm", s);
         if (tc) {
-            float y_scale = 1.f;
-            KFB_TRY(transpose_split_y<T>(Y.as<T>(), np, ma1, rep, ld2, yamax.as<float>(),
-                                         yth.as<__half>(), ytl.as<__half>(), &y_scale, s));
             std::vector<TcProb> tprobs;
             tprobs.reserve(np);
             for (int k = 0; k < np; ++k) {

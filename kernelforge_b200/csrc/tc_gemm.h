@@ -83,6 +83,9 @@ kfb_status split_rows(const T *src, long long n, __half *hi, __half *lo, float *
 template <class T>
 kfb_status transpose_split_dx(const T *dx, int nm, int ma, int rep, const int *nat, __half *hi,
                               __half *lo, float *scale, cudaStream_t s);
+// Host copy of a power of two that brings the device float *dmax to about
+// 2^14 (synchronises the stream).
+kfb_status pow2_from_device(const float *dmax, cudaStream_t s, float *scale);
 template <class T>
 kfb_status transpose_split_y(const T *Y, int np, int ma1, int rep, int ld, const float *amax,
                              __half *hi, __half *lo, float *scale, cudaStream_t s);
