@@ -185,6 +185,24 @@ __device__ __forceinline__ void load_vec(const T *p, T (&v)[N]) {
     }
 }
 
+// Asynchronous global -> shared copies of one element (cp.async, L1-cached):
+// each lane fetches its own words ahead of use, so a warp can stream rows of
+// a Jacobian through a small ring without registers held for the prefetch.
+template <class T>
+__device__ __forceinline__ void cp_async_elem(T *smem, const T *gmem) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    if constexpr (sizeof(T) == 4)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(gmem));
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+constexpr int JRING = 3;  // stages of the per-warp Jacobian ring
+
 // Size of the balanced chunks of a label group of n atoms (at most cap each).
 __device__ __forceinline__ int chunk_size(int n, int cap) {
     const int nch = (n + cap - 1) / cap;
@@ -429,17 +447,22 @@ kfb_status launch_hess_t(const HessPair *pairs, int np, const T *x1, const T *x2
 // over same-label atom pairs only.  Atoms of each molecule are visited in
 // label order (perm: sorted position -> atom), so one label group of a meets
 // one contiguous run of b.  Block per (pair, slice of kt rows of rep); each
-// warp owns one (32 columns c, 8 rows k) tile and keeps a chunk of up to
-// HY_IG atoms x 8 rows of Y in registers, so each J_j[k, c] load feeds two
-// FMAs per atom of the chunk.  w_ij and t'_ij of the chunk's atoms x HY_JT
-// partners are staged in shared memory by the whole block (t' with the atoms
-// innermost, read as vectors); the descriptor rows of the slice too.
+// warp owns one (32 columns c, 8 rows k) tile and, for each label group and
+// balanced chunk of at most HY_IG atoms i, keeps the chunk's 8 rows of Y in
+// registers, so each J_j[k, c] load feeds two FMAs per atom of the chunk.
+// Per partner j the warp streams J_j's tile, t'_ij[c] of the chunk and w_ij
+// through a per-warp cp.async ring: no block-wide synchronisation after the
+// descriptor rows of the slice are staged.
 //   MODE 1: fp16 pair hi/lo of scale * Y, K-major rows (p, c) of (i, k)
 //   MODE 2: Y[p, i, k, c] in T
 // FULL: rep % 8 == 0 (no row guards).
-constexpr int HY_KR = 8, HY_JT = 8;
+constexpr int HY_KR = 8;
 template <class T> struct HyCfg { static constexpr int IG = 8, WARPS = 8; };
 template <> struct HyCfg<double> { static constexpr int IG = 4, WARPS = 8; };
+template <class T>
+constexpr int hy_stage() {  // ring stage: J rows, t' of the chunk, w of the chunk
+    return (HY_KR + HyCfg<T>::IG) * 32 + HyCfg<T>::IG;
+}
 
 struct HyGeom {
     int kt;      // rows of rep per block (multiple of 8)
@@ -458,23 +481,22 @@ HyGeom hess_y_geom(int ma1, int ma2) {
     g.warps = nchunk * kgroups;
     const size_t head =
         ((size_t)ma1 * sizeof(int4) + (size_t)(ma1 + ma2) * sizeof(int) + 15) & ~(size_t)15;
-    g.smem = head + ((size_t)(ma1 + ma2) * g.kt + (size_t)HyCfg<T>::IG * HY_JT +
-                     (size_t)HyCfg<T>::IG * HY_JT * g.ldc) * sizeof(T);
+    g.smem = head + ((size_t)(ma1 + ma2) * g.kt + (size_t)g.warps * JRING * hy_stage<T>()) *
+                        sizeof(T);
     return g;
 }
 
 template <class T, int IGC, int MODE, bool FULL>
 __device__ __forceinline__ void hy_chunk(const HessPair &pr, int p, int4 gr, int i0, int cnt,
                                          const int *pa, const int *pb, const T *xa_s,
-                                         const T *xb_s, T *ws, T *ts, int kt, int ldc, int ma1,
-                                         int ma2, int rep, int k0, int kk0, bool active,
+                                         const T *xb_s, T *ring, int kt, int ma1, int ma2,
+                                         int rep, int k0, int kk0, int c,
                                          const T *__restrict__ dx2, const T *__restrict__ W,
                                          const T *__restrict__ Tt, float scale,
                                          __half *__restrict__ yhi, __half *__restrict__ ylo,
                                          T *__restrict__ Y) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-    const int nchunk = ldc / 32;
-    const int c = (warp % nchunk) * 32 + lane;
+    constexpr int IG = HyCfg<T>::IG, SS = hy_stage<T>();
+    const int lane = threadIdx.x & 31;
     const int ld2 = 3 * ma2, ncol = 3 * pr.nb;
     const int cs = c < ncol ? c : 0;
     const size_t wbase = (size_t)p * ma1 * ma2;
@@ -485,47 +507,68 @@ __device__ __forceinline__ void hy_chunk(const HessPair &pr, int p, int4 gr, int
 #pragma unroll
         for (int r = 0; r < HY_KR; ++r) acc[ii][r] = T(0);
     }
-    for (int j0 = gr.z; j0 < gr.w; j0 += HY_JT) {
-        const int jn = min(HY_JT, gr.w - j0);
-        __syncthreads();  // previous step's ws / ts fully read
-        for (int jj = warp; jj < HY_JT; jj += nwarp) {
-            const bool okj = jj < jn;
-            const int j = okj ? pb[j0 + jj] : 0;
-            for (int cx = lane; cx < ldc; cx += 32) {
+    const T *Jb = dx2 + ((size_t)pr.b * ma2 * rep + k0) * (size_t)ld2 + cs;
+    const T *Tb = Tt + wbase * ld2 + cs;
+    const T *Wb = W + wbase;
+    const int nj = gr.w - gr.z;
+    auto issue = [&](int jj, int stage) {
+        if (jj < nj) {
+            const int j = pb[gr.z + jj];
+            T *dst = ring + stage * SS;
+            const T *Jj = Jb + (size_t)j * rep * ld2;
 #pragma unroll
-                for (int ii = 0; ii < IGC; ++ii) {
-                    const bool ok = okj && ii < cnt && cx < ncol;
-                    ts[(jj * ldc + cx) * IGC + ii] =
-                        ok ? Tt[(wbase + (size_t)pa[i0 + ii] * ma2 + j) * ld2 + cx] : T(0);
-                }
+            for (int r = 0; r < HY_KR; ++r) {
+                if (FULL || k0 + r < rep)
+                    cp_async_elem<T>(dst + r * 32 + lane, Jj + (size_t)r * ld2);
+                else
+                    dst[r * 32 + lane] = T(0);
             }
-            if (lane < IGC)
-                ws[jj * IGC + lane] =
-                    (okj && lane < cnt) ? W[wbase + (size_t)pa[i0 + lane] * ma2 + j] : T(0);
-        }
-        __syncthreads();
-        if (!active) continue;  // warp-uniform
-        const T *Jb = dx2 + ((size_t)pr.b * ma2 * rep + k0) * (size_t)ld2 + cs;
-        for (int jj = 0; jj < jn; ++jj) {
-            T jv[HY_KR];
-            const T *Jj = Jb + (size_t)pb[j0 + jj] * rep * ld2;
-#pragma unroll
-            for (int r = 0; r < HY_KR; ++r)
-                jv[r] = (FULL || k0 + r < rep) ? Jj[(size_t)r * ld2] : T(0);
-            T xj[HY_KR], t[IGC], w[IGC];
-            load_vec<T, HY_KR>(xb_s + pb[j0 + jj] * kt + kk0, xj);
-            load_vec<T, IGC>(ts + (jj * ldc + c) * IGC, t);
-            load_vec<T, IGC>(ws + jj * IGC, w);
 #pragma unroll
             for (int ii = 0; ii < IGC; ++ii) {
-                rr[ii] += t[ii];
-#pragma unroll
-                for (int r = 0; r < HY_KR; ++r)
-                    acc[ii][r] = fma(w[ii], jv[r], fma(xj[r], t[ii], acc[ii][r]));
+                if (ii < cnt)
+                    cp_async_elem<T>(dst + (HY_KR + ii) * 32 + lane,
+                                     Tb + ((size_t)pa[i0 + ii] * ma2 + j) * ld2);
+                else
+                    dst[(HY_KR + ii) * 32 + lane] = T(0);
+            }
+            if (lane < IGC) {
+                if (lane < cnt)
+                    cp_async_elem<T>(dst + (HY_KR + IG) * 32 + lane,
+                                     Wb + (size_t)pa[i0 + lane] * ma2 + j);
+                else
+                    dst[(HY_KR + IG) * 32 + lane] = T(0);
             }
         }
+        cp_async_commit();
+    };
+    issue(0, 0);
+    issue(1, 1);
+    int st = 0;
+    for (int jj = 0; jj < nj; ++jj) {
+        issue(jj + 2, st == 0 ? 2 : st - 1);
+        cp_async_wait<JRING - 1>();
+        __syncwarp();  // w of the stage was fetched by lanes 0..IGC-1
+        const T *src = ring + st * SS;
+        T jv[HY_KR], xj[HY_KR], t[IGC], w[IGC];
+#pragma unroll
+        for (int r = 0; r < HY_KR; ++r) jv[r] = src[r * 32 + lane];
+#pragma unroll
+        for (int ii = 0; ii < IGC; ++ii) {
+            t[ii] = src[(HY_KR + ii) * 32 + lane];
+            w[ii] = src[(HY_KR + IG) * 32 + ii];
+        }
+        load_vec<T, HY_KR>(xb_s + pb[gr.z + jj] * kt + kk0, xj);
+        st = st == JRING - 1 ? 0 : st + 1;
+#pragma unroll
+        for (int ii = 0; ii < IGC; ++ii) {
+            rr[ii] += t[ii];
+#pragma unroll
+            for (int r = 0; r < HY_KR; ++r)
+                acc[ii][r] = fma(w[ii], jv[r], fma(xj[r], t[ii], acc[ii][r]));
+        }
+        __syncwarp();  // every lane is done with the stage before it is refilled
     }
-    if (!active || c >= ncol) return;
+    if (c >= ncol) return;
 #pragma unroll
     for (int ii = 0; ii < IGC; ++ii) {
         if (ii >= cnt) continue;
@@ -575,9 +618,8 @@ __global__ void __launch_bounds__(256, 2) hess_y_kernel(
     int *pb = pa + ma1;                                // ma2
     T *xa_s = reinterpret_cast<T *>(
         hy_raw + (((size_t)ma1 * sizeof(int4) + (size_t)(ma1 + ma2) * sizeof(int) + 15) & ~(size_t)15));
-    T *xb_s = xa_s + (size_t)ma1 * kt;  // [atom][row of the slice]
-    T *ws = xb_s + (size_t)ma2 * kt;    // [HY_JT][IGC]
-    T *ts = ws + IG * HY_JT;            // [HY_JT][ldc][IGC]
+    T *xb_s = xa_s + (size_t)ma1 * kt;      // [atom][row of the slice]
+    T *jring = xb_s + (size_t)ma2 * kt;     // per warp [JRING][stage]
     __shared__ int ngroups;
     const int p = blockIdx.y;
     const HessPair pr = pairs[p];
@@ -596,19 +638,21 @@ __global__ void __launch_bounds__(256, 2) hess_y_kernel(
         ngroups = pair_label_groups(lab1 + (size_t)pr.a * ma1, lab2 + (size_t)pr.b * ma2,
                                     pr.na, pr.nb, groups);
     __syncthreads();
-    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nchunk = ldc / 32;
     const int kk0 = (warp / nchunk) * HY_KR, k0 = kbase + kk0;
-    const bool active = k0 < rep;  // warp-uniform
+    if (k0 >= rep) return;  // warp-uniform; no block-wide synchronisation follows
+    const int c = (warp % nchunk) * 32 + lane;
+    T *ring = jring + (size_t)warp * JRING * hy_stage<T>();
     for (int g = 0; g < ngroups; ++g) {
         const int4 gr = groups[g];
         const int csz = chunk_size(gr.y - gr.x, IG);
         for (int i0 = gr.x; i0 < gr.y; i0 += csz) {
             const int cnt = min(csz, gr.y - i0);
             const int igc = pow2_at_least(cnt);
-#define KFB_HY_CHUNK(N)                                                                        \
-    hy_chunk<T, N, MODE, FULL>(pr, p, gr, i0, cnt, pa, pb, xa_s, xb_s, ws, ts, kt, ldc, ma1, ma2, \
-                               rep, k0, kk0, active, dx2, W, Tt, scale, yhi, ylo, Y)
+#define KFB_HY_CHUNK(N)                                                                       \
+    hy_chunk<T, N, MODE, FULL>(pr, p, gr, i0, cnt, pa, pb, xa_s, xb_s, ring, kt, ma1, ma2, rep, \
+                               k0, kk0, c, dx2, W, Tt, scale, yhi, ylo, Y)
             if (IG >= 8 && igc == 8)
                 KFB_HY_CHUNK((IG >= 8 ? 8 : 4));
             else if (igc == 4)
