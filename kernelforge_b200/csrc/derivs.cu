@@ -1,11 +1,12 @@
-// Jacobian and Hessian FCHL19 local kernels on CUDA cores (FP64 / FP32).
+// Jacobian and Hessian FCHL19 local kernels (FP64 / FP32 arithmetic, with the
+// contractions on tcgen05 tensor cores or through cuBLAS).
 //
 // Jacobian (+dK/dR of the "inner" set, src/local_kernels.cpp:791-974):
 //   K[o, off_m + c] = sum_{j in m} v_{o,j} . J_j[:, c],
 //   v_{o,j} = sum_{i in o, q_i = q_j} (e_ij / sigma^2) (x_i - x_j)
 // The v rows are formed first (one warp per (o, j)), then contracted with the
-// Jacobians by a grouped GEMM, one problem per inner molecule m.  This costs
-// 2 rep 3 n_m per (o, j) instead of per atom pair.  The transposed Jacobian
+// Jacobians, one GEMM problem per inner molecule m.  This costs 2 rep 3 n_m
+// per (o, j) instead of per atom pair.  The transposed Jacobian
 // (src/local_kernels.cpp:991-1166) is the same contraction with the roles of
 // the sets swapped, negated and written transposed.
 //
@@ -13,11 +14,16 @@
 //   H_ab = sum_{i in a} J_i^T Y_i,
 //   Y_i  = sum_{j in b, q_j = q_i} (w_ij J_j - w'_ij d_ij (J_j^T d_ij)^T),
 //   d_ij = x_i - x_j, w = e/sigma^2, w' = e/sigma^4
-// t_ij = J_j^T d_ij is formed once per atom pair (kernel 1), Y_i per
-// (pair, i, 32-row slice of rep) (kernel 2) and H_ab = J_a^T Y by the grouped
-// GEMM (kernel 3).
+// t'_ij = w'_ij J_j^T d_ij is formed once per same-label atom pair (kernel 1,
+// block per molecule pair), Y_i per (pair, 8-row slice of rep) with the
+// atoms of a label group in registers (kernel 2), and H_ab = J_a^T Y by one
+// GEMM problem per pair (tcgen05 split-fp16, or cuBLAS).
+#include <cublas_v2.h>
+
 #include <algorithm>
 #include <memory>
+#include <numeric>
+#include <tuple>
 
 #include "derivs.h"
 #include "kernels_common.cuh"
@@ -25,76 +31,9 @@
 
 namespace kfb {
 
+kfb_status blas_for_stream(cudaStream_t s, cublasHandle_t *out);
+
 namespace {
-
-// ------------------------------------------------------------ grouped GEMM
-constexpr int GT = 64, GK = 16;
-
-template <class T>
-__global__ void __launch_bounds__(256) gemm_grouped_kernel(const GemmProb *__restrict__ probs,
-                                                           const GemmTile *__restrict__ tiles,
-                                                           ElemSink sink) {
-    __shared__ T As[GK][GT + 1];
-    __shared__ T Bs[GK][GT + 1];
-    const GemmTile tl = tiles[blockIdx.x];
-    const GemmProb pb = probs[tl.prob];
-    const T *A = static_cast<const T *>(pb.A);
-    const T *B = static_cast<const T *>(pb.B);
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-    T acc[4][4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = T(0);
-    for (int k0 = 0; k0 < pb.K; k0 += GK) {
-        if (pb.transA) {
-            const int k = tid >> 4, m = (tid & 15) * 4;
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int mm = tl.m0 + m + u, kk = k0 + k;
-                As[k][m + u] = (mm < pb.M && kk < pb.K) ? A[(size_t)kk * pb.lda + mm] : T(0);
-            }
-        } else {
-            const int m = tid >> 2, k = (tid & 3) * 4;
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int mm = tl.m0 + m, kk = k0 + k + u;
-                As[k + u][m] = (mm < pb.M && kk < pb.K) ? A[(size_t)mm * pb.lda + kk] : T(0);
-            }
-        }
-        {
-            const int k = tid >> 4, n = (tid & 15) * 4;
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int nn = tl.n0 + n + u, kk = k0 + k;
-                Bs[k][n + u] = (nn < pb.N && kk < pb.K) ? B[(size_t)kk * pb.ldb + nn] : T(0);
-            }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < GK; ++kk) {
-            T a[4], b[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = As[kk][ty * 4 + i];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx * 4 + j];
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int m = tl.m0 + ty * 4 + i, n = tl.n0 + tx * 4 + j;
-            if (m < pb.M && n < pb.N)
-                sink_store(sink, pb.row_off + m, pb.col_off + n, (double)acc[i][j] * pb.alpha,
-                           pb.diag);
-        }
-}
 
 // --------------------------------------------------------- Jacobian: v rows
 // One warp per (outer molecule o in [o0, o0+no), inner active atom u):
@@ -706,24 +645,102 @@ void label_order(const SetView &v, std::vector<int> &perm, std::vector<int> &lab
     }
 }
 
+// Contractions on CUDA cores through cuBLAS: problems of equal shape run as
+// one batched GEMM into a scratch array, then a scatter kernel writes each
+// result through the sink (alpha applied there).  Row-major
+// C (M x N) = A' (M x K) B (K x N) is the column-major C^T = B^T A'^T.
+template <class T> struct BlasBatched;
+template <> struct BlasBatched<float> {
+    static cublasStatus_t run(cublasHandle_t h, cublasOperation_t ta, cublasOperation_t tb, int m,
+                              int n, int k, const float *const A[], int lda,
+                              const float *const B[], int ldb, float *const C[], int ldc,
+                              int cnt) {
+        const float one = 1.f, zero = 0.f;
+        return cublasSgemmBatched(h, ta, tb, m, n, k, &one, A, lda, B, ldb, &zero, C, ldc, cnt);
+    }
+};
+template <> struct BlasBatched<double> {
+    static cublasStatus_t run(cublasHandle_t h, cublasOperation_t ta, cublasOperation_t tb, int m,
+                              int n, int k, const double *const A[], int lda,
+                              const double *const B[], int ldb, double *const C[], int ldc,
+                              int cnt) {
+        const double one = 1.0, zero = 0.0;
+        return cublasDgemmBatched(h, ta, tb, m, n, k, &one, A, lda, B, ldb, &zero, C, ldc, cnt);
+    }
+};
+
+struct ScatterProb {
+    long long coff;
+    int M, N, row_off, col_off, diag, pad;
+    double alpha;
+};
+
+template <class T>
+__global__ void scatter_sink_kernel(const ScatterProb *__restrict__ probs, const T *__restrict__ C,
+                                    ElemSink sink) {
+    const ScatterProb sp = probs[blockIdx.x];
+    for (int e = threadIdx.x; e < sp.M * sp.N; e += blockDim.x) {
+        const int m = e / sp.N, n = e - m * sp.N;
+        sink_store(sink, sp.row_off + m, sp.col_off + n, (double)C[sp.coff + e] * sp.alpha,
+                   sp.diag);
+    }
+}
+
 template <class T>
 kfb_status launch_gemm(const std::vector<GemmProb> &probs, const ElemSink &sink,
                        cudaStream_t s) {
-    if (probs.empty()) return KFB_OK;
-    std::vector<GemmTile> tiles;
-    for (int p = 0; p < (int)probs.size(); ++p)
-        for (int m0 = 0; m0 < probs[p].M; m0 += GT)
-            for (int n0 = 0; n0 < probs[p].N; n0 += GT) tiles.push_back(GemmTile{p, m0, n0, 0});
-    if (tiles.empty()) return KFB_OK;
-    DevBuf dp, dt;
-    KFB_TRY(upload(dp, probs, s));
-    KFB_TRY(upload(dt, tiles, s));
-    for (size_t off = 0; off < tiles.size(); off += (size_t)1 << 30) {
-        const unsigned nb = (unsigned)std::min<size_t>(tiles.size() - off, (size_t)1 << 30);
-        gemm_grouped_kernel<T><<<nb, 256, 0, s>>>(dp.as<GemmProb>(), dt.as<GemmTile>() + off,
-                                                  sink);
-        KFB_CUDA_TRY(cudaGetLastError());
+    const int n = (int)probs.size();
+    if (n == 0) return KFB_OK;
+    cublasHandle_t h = nullptr;
+    KFB_TRY(blas_for_stream(s, &h));
+    auto key = [&](int q) {
+        const GemmProb &g = probs[q];
+        return std::make_tuple(g.transA, g.M, g.N, g.K, g.lda, g.ldb);
+    };
+    std::vector<int> order(n);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return key(x) < key(y); });
+    std::vector<ScatterProb> sp(n);
+    long long total = 0;
+    for (int q = 0; q < n; ++q) {
+        const GemmProb &g = probs[order[q]];
+        sp[q] = ScatterProb{total, g.M, g.N, g.row_off, g.col_off, g.diag, 0, g.alpha};
+        total += (long long)g.M * g.N;
     }
+    DevBuf C, ptrs, dsp;
+    KFB_TRY(C.alloc((size_t)std::max<long long>(total, 1) * sizeof(T), s));
+    std::vector<const void *> pv(3 * (size_t)n);
+    for (int q = 0; q < n; ++q) {
+        const GemmProb &g = probs[order[q]];
+        pv[q] = g.A;
+        pv[n + q] = g.B;
+        pv[2 * n + q] = C.as<T>() + sp[q].coff;
+    }
+    KFB_TRY(upload(ptrs, pv, s));
+    KFB_TRY(upload(dsp, sp, s));
+    void **base = static_cast<void **>(ptrs.ptr);
+    const T *const *dA = reinterpret_cast<const T *const *>(base);
+    const T *const *dB = dA + n;
+    T *const *dC = reinterpret_cast<T *const *>(base + 2 * (size_t)n);
+    for (int q0 = 0; q0 < n;) {
+        int q1 = q0 + 1;
+        while (q1 < n && key(order[q1]) == key(order[q0])) ++q1;
+        const GemmProb &g = probs[order[q0]];
+        if (g.M > 0 && g.N > 0 && g.K > 0) {
+            const cublasStatus_t st = BlasBatched<T>::run(
+                h, CUBLAS_OP_N, g.transA ? CUBLAS_OP_T : CUBLAS_OP_N, g.N, g.M, g.K, dB + q0,
+                (int)g.ldb, dA + q0, (int)g.lda, dC + q0, g.N, q1 - q0);
+            if (st != CUBLAS_STATUS_SUCCESS)
+                return set_error(KFB_ERR_CUDA, "batched GEMM failed: cublas status %d", (int)st);
+        } else {
+            KFB_TRY(zero(C.as<T>() + sp[q0].coff,
+                         (size_t)(sp[q1 - 1].coff + (long long)sp[q1 - 1].M * sp[q1 - 1].N -
+                                  sp[q0].coff) * sizeof(T), s));
+        }
+        q0 = q1;
+    }
+    scatter_sink_kernel<T><<<n, 256, 0, s>>>(dsp.as<ScatterProb>(), C.as<T>(), sink);
+    KFB_CUDA_TRY(cudaGetLastError());
     return KFB_OK;
 }
 

@@ -30,10 +30,6 @@ struct GemmProb {
     int pad;
 };
 
-struct GemmTile {
-    int prob, m0, n0, pad;
-};
-
 struct HessPair {
     int a, b, na, nb;
 };
