@@ -148,6 +148,13 @@ __device__ __forceinline__ int chunk_size(int n, int cap) {
     return (n + nch - 1) / nch;
 }
 
+// Largest of 1, 2, 4, ... that is <= n (n >= 1).
+__device__ __forceinline__ int pow2_at_most(int n) {
+    int p = 1;
+    while (2 * p <= n) p <<= 1;
+    return p;
+}
+
 // Smallest of 1, 2, 4, ... that is >= n.
 __device__ __forceinline__ int pow2_at_least(int n) {
     int p = 1;
@@ -486,15 +493,17 @@ __device__ __forceinline__ void hy_chunk(const HessPair &pr, int p, int4 gr, int
     for (int jj = 0; jj < nj; ++jj) {
         issue(jj + 2, st == 0 ? 2 : st - 1);
         cp_async_wait<JRING - 1>();
-        __syncwarp();  // w of the stage was fetched by lanes 0..IGC-1
+        // every lane reads only the ring slots it filled itself; w_ij of the
+        // chunk (fetched by lanes 0..IGC-1) is broadcast by shuffles
         const T *src = ring + st * SS;
         T jv[HY_KR], xj[HY_KR], t[IGC], w[IGC];
 #pragma unroll
         for (int r = 0; r < HY_KR; ++r) jv[r] = src[r * 32 + lane];
+        const T wl = lane < IGC ? src[(HY_KR + IG) * 32 + lane] : T(0);
 #pragma unroll
         for (int ii = 0; ii < IGC; ++ii) {
             t[ii] = src[(HY_KR + ii) * 32 + lane];
-            w[ii] = src[(HY_KR + IG) * 32 + ii];
+            w[ii] = __shfl_sync(0xffffffffu, wl, ii);
         }
         load_vec<T, HY_KR>(xb_s + pb[gr.z + jj] * kt + kk0, xj);
         st = st == JRING - 1 ? 0 : st + 1;
@@ -505,7 +514,6 @@ __device__ __forceinline__ void hy_chunk(const HessPair &pr, int p, int4 gr, int
             for (int r = 0; r < HY_KR; ++r)
                 acc[ii][r] = fma(w[ii], jv[r], fma(xj[r], t[ii], acc[ii][r]));
         }
-        __syncwarp();  // every lane is done with the stage before it is refilled
     }
     if (c >= ncol) return;
 #pragma unroll
@@ -518,18 +526,17 @@ __device__ __forceinline__ void hy_chunk(const HessPair &pr, int p, int4 gr, int
         for (int r = 0; r < HY_KR; ++r) acc[ii][r] = fma(-xi[r], rr[ii], acc[ii][r]);
         if (MODE == 1) {
             // rep % 16 == 0 on this path: 8 rows are 16 aligned bytes
+            // packed conversions: two values per instruction
             unsigned hw[HY_KR / 2], lw[HY_KR / 2];
 #pragma unroll
             for (int r = 0; r < HY_KR; r += 2) {
-                const float v0 = (float)acc[ii][r] * scale;
-                const float v1 = (float)acc[ii][r + 1] * scale;
-                const __half h0 = __float2half_rn(v0), h1 = __float2half_rn(v1);
-                const __half l0 = __float2half_rn(v0 - __half2float(h0));
-                const __half l1 = __float2half_rn(v1 - __half2float(h1));
-                hw[r / 2] =
-                    (unsigned)__half_as_ushort(h0) | ((unsigned)__half_as_ushort(h1) << 16);
-                lw[r / 2] =
-                    (unsigned)__half_as_ushort(l0) | ((unsigned)__half_as_ushort(l1) << 16);
+                const float2 v = make_float2((float)acc[ii][r] * scale,
+                                             (float)acc[ii][r + 1] * scale);
+                const __half2 h = __float22half2_rn(v);
+                const float2 hf = __half22float2(h);
+                const __half2 l = __float22half2_rn(make_float2(v.x - hf.x, v.y - hf.y));
+                hw[r / 2] = *reinterpret_cast<const unsigned *>(&h);
+                lw[r / 2] = *reinterpret_cast<const unsigned *>(&l);
             }
             const size_t o = (((size_t)p * ld2 + c) * ma1 + i) * (size_t)rep + k0;
             *reinterpret_cast<uint4 *>(yhi + o) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
@@ -585,10 +592,10 @@ __global__ void __launch_bounds__(256, 2) hess_y_kernel(
     T *ring = jring + (size_t)warp * JRING * hy_stage<T>();
     for (int g = 0; g < ngroups; ++g) {
         const int4 gr = groups[g];
-        const int csz = chunk_size(gr.y - gr.x, IG);
-        for (int i0 = gr.x; i0 < gr.y; i0 += csz) {
-            const int cnt = min(csz, gr.y - i0);
-            const int igc = pow2_at_least(cnt);
+        // chunks of power-of-two sizes (largest first): no padded FMAs
+        for (int i0 = gr.x, cnt; i0 < gr.y; i0 += cnt) {
+            cnt = pow2_at_most(min(IG, gr.y - i0));
+            const int igc = cnt;
 #define KFB_HY_CHUNK(N)                                                                       \
     hy_chunk<T, N, MODE, FULL>(pr, p, gr, i0, cnt, pa, pb, xa_s, xb_s, ring, kt, ma1, ma2, rep, \
                                k0, kk0, c, dx2, W, Tt, scale, yhi, ylo, Y)
