@@ -406,8 +406,8 @@ constexpr int HY_KR = 8;
 template <class T> struct HyCfg { static constexpr int IG = 8, WARPS = 8; };
 template <> struct HyCfg<double> { static constexpr int IG = 4, WARPS = 8; };
 template <class T>
-constexpr int hy_stage() {  // ring stage: J rows, t' of the chunk, w of the chunk
-    return (HY_KR + HyCfg<T>::IG) * 32 + HyCfg<T>::IG;
+constexpr int hy_stage() {  // ring stage: J rows, t' of the chunk, w (one slot per lane)
+    return (HY_KR + HyCfg<T>::IG + 1) * 32;
 }
 
 struct HyGeom {
@@ -432,8 +432,9 @@ HyGeom hess_y_geom(int ma1, int ma2) {
     return g;
 }
 
+// One chunk of exactly IGC atoms (i0 .. i0 + IGC - 1 in label order) of group gr.
 template <class T, int IGC, int MODE, bool FULL>
-__device__ __forceinline__ void hy_chunk(const HessPair &pr, int p, int4 gr, int i0, int cnt,
+__device__ __forceinline__ void hy_chunk(const HessPair &pr, int p, int4 gr, int i0,
                                          const int *pa, const int *pb, const T *xa_s,
                                          const T *xb_s, T *ring, int kt, int ma1, int ma2,
                                          int rep, int k0, int kk0, int c,
@@ -470,20 +471,12 @@ __device__ __forceinline__ void hy_chunk(const HessPair &pr, int p, int4 gr, int
                     dst[r * 32 + lane] = T(0);
             }
 #pragma unroll
-            for (int ii = 0; ii < IGC; ++ii) {
-                if (ii < cnt)
-                    cp_async_elem<T>(dst + (HY_KR + ii) * 32 + lane,
-                                     Tb + ((size_t)pa[i0 + ii] * ma2 + j) * ld2);
-                else
-                    dst[(HY_KR + ii) * 32 + lane] = T(0);
-            }
-            if (lane < IGC) {
-                if (lane < cnt)
-                    cp_async_elem<T>(dst + (HY_KR + IG) * 32 + lane,
-                                     Wb + (size_t)pa[i0 + lane] * ma2 + j);
-                else
-                    dst[(HY_KR + IG) * 32 + lane] = T(0);
-            }
+            for (int ii = 0; ii < IGC; ++ii)
+                cp_async_elem<T>(dst + (HY_KR + ii) * 32 + lane,
+                                 Tb + ((size_t)pa[i0 + ii] * ma2 + j) * ld2);
+            // lane l fetches w of atom l mod IGC (no divergent branch)
+            cp_async_elem<T>(dst + (HY_KR + IG) * 32 + lane,
+                             Wb + (size_t)pa[i0 + (lane & (IGC - 1))] * ma2 + j);
         }
         cp_async_commit();
     };
@@ -499,7 +492,7 @@ __device__ __forceinline__ void hy_chunk(const HessPair &pr, int p, int4 gr, int
         T jv[HY_KR], xj[HY_KR], t[IGC], w[IGC];
 #pragma unroll
         for (int r = 0; r < HY_KR; ++r) jv[r] = src[r * 32 + lane];
-        const T wl = lane < IGC ? src[(HY_KR + IG) * 32 + lane] : T(0);
+        const T wl = src[(HY_KR + IG) * 32 + lane];
 #pragma unroll
         for (int ii = 0; ii < IGC; ++ii) {
             t[ii] = src[(HY_KR + ii) * 32 + lane];
@@ -518,7 +511,6 @@ __device__ __forceinline__ void hy_chunk(const HessPair &pr, int p, int4 gr, int
     if (c >= ncol) return;
 #pragma unroll
     for (int ii = 0; ii < IGC; ++ii) {
-        if (ii >= cnt) continue;
         const int i = pa[i0 + ii];
         T xi[HY_KR];
         load_vec<T, HY_KR>(xa_s + i * kt + kk0, xi);
@@ -597,7 +589,7 @@ __global__ void __launch_bounds__(256, 2) hess_y_kernel(
             cnt = pow2_at_most(min(IG, gr.y - i0));
             const int igc = cnt;
 #define KFB_HY_CHUNK(N)                                                                       \
-    hy_chunk<T, N, MODE, FULL>(pr, p, gr, i0, cnt, pa, pb, xa_s, xb_s, ring, kt, ma1, ma2, rep, \
+    hy_chunk<T, N, MODE, FULL>(pr, p, gr, i0, pa, pb, xa_s, xb_s, ring, kt, ma1, ma2, rep, \
                                k0, kk0, c, dx2, W, Tt, scale, yhi, ylo, Y)
             if (IG >= 8 && igc == 8)
                 KFB_HY_CHUNK((IG >= 8 ? 8 : 4));
