@@ -353,6 +353,34 @@ kfb_status kfb_local_matvec(const void *x1, const void *dx1, const void *x2,
                             double *e_out, double *f_out, void *stream);
 
 /* ---------------------------------------------------------------------- */
+/* FCHL19 descriptors and Jacobians                                        */
+/* ---------------------------------------------------------------------- */
+
+/* Descriptor length nelements nRs2 + nelements (nelements + 1) / 2 nRs3 2 nFourier
+ * (-1 for invalid sizes).  Replaces fchl19_repr.compute_rep_size
+ * (src/fchl19_repr_bindings.cpp:222-230; its nabasis is 2 nFourier). */
+int kfb_fchl19_rep_size(int nelements, int nRs2, int nRs3, int nFourier);
+
+/* FCHL19 descriptors of nm padded molecules: coords (nm, ma, 3) device, element
+ * indices elem (nm, ma) host int32 in [0, nelements) for the first natoms[m]
+ * atoms (host int32, clamped to [0, ma]); rep (nm, ma, rep_size) device and, when
+ * grad is not NULL, grad (nm, ma, rep_size, 3 ma) device = d rep[m, i, f] /
+ * d coords[m, a, t] at column 3 a + t (the layout of the kernels' dX; padded
+ * atoms are zero).  Element type of coords / rep / grad: dt; FP64 arithmetic.
+ * Hyper-parameters as fchl19_repr.generate_fchl_acsf (the three-body weight is
+ * scaled by sqrt(eta3 / pi) inside, as the reference's binding does); gradients
+ * need nFourier = 1.  Replaces fchl19_repr.generate_fchl_acsf /
+ * generate_fchl_acsf_and_gradients (src/fchl19_repr_bindings.cpp:52-216,
+ * src/fchl19_repr.cpp:89-781) and cuda_fchl19_repr.generate_fchl_acsf /
+ * generate_fchl_acsf_and_gradients (src/cuda_fchl19_repr_bindings.cpp:170-290). */
+kfb_status kfb_fchl19_repr(const void *coords, const int32_t *elem, const int32_t *natoms,
+                           int nm, int ma, int nelements, int nRs2, int nRs3, int nFourier,
+                           double eta2, double eta3, double zeta, double rcut, double acut,
+                           double two_body_decay, double three_body_decay,
+                           double three_body_weight, kfb_dtype dt, void *rep, void *grad,
+                           void *stream);
+
+/* ---------------------------------------------------------------------- */
 /* Allocation-free entry point                                             */
 /* ---------------------------------------------------------------------- */
 

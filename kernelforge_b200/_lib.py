@@ -31,7 +31,8 @@ EXPORTS = (
     "kfb_feature_gramian", "kfb_ridge_solve_mixed", "kfb_pair_gaussian", "kfb_cosmlp_create", "kfb_cosmlp_destroy",
     "kfb_cosmlp_params", "kfb_cosmlp_grads", "kfb_cosmlp_sync", "kfb_cosmlp_optimizer_state",
     "kfb_cosmlp_set_steps", "kfb_cosmlp_pair_step", "kfb_cosmlp_features_elemental",
-    "kfb_local_alpha_desc", "kfb_local_matvec", "kfb_kernel_gaussian_symm_noalloc",
+    "kfb_local_alpha_desc", "kfb_local_matvec", "kfb_fchl19_rep_size", "kfb_fchl19_repr",
+    "kfb_kernel_gaussian_symm_noalloc",
 )
 
 
@@ -93,6 +94,8 @@ _SIGS = {
     "kfb_cosmlp_features_elemental": (I, [P, P, P, P, I, I, I, I, P, P]),
     "kfb_local_alpha_desc": (I, [P, P, P, I, I, I, I, P, P, P]),
     "kfb_local_matvec": (I, [P, P, P, P, P, P, P, P, P, I, I, I, I, I, D, I, P, P, P]),
+    "kfb_fchl19_rep_size": (I, [I, I, I, I]),
+    "kfb_fchl19_repr": (I, [P, P, P, I, I, I, I, I, I, D, D, D, D, D, D, D, D, I, P, P, P]),
     "kfb_kernel_gaussian_symm_noalloc": (I, [P, P, P, I, I, I, D, I, I, P, P]),
 }
 
