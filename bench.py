@@ -56,7 +56,7 @@ def parse():
                     help="skip the FP64-GPU fit and the accuracy check (profiling runs)")
     ap.add_argument("--workload", default="fit10k",
                     choices=["fit10k", "config1", "config3", "config4", "config5",
-                             "cosmlp_step"],
+                             "cosmlp_step", "repr"],
                     help="fit10k (default): the 10,000-molecule kernel + solve; config1: FP64 "
                          "1,000-molecule fit+predict; config3: Jacobian kernel 1,000 x 1,000 "
                          "molecules; config4: energy+force kernel of 300 x 21-atom molecules "
@@ -1088,11 +1088,67 @@ def run_cosmlp_step(args):
                         "frac": flops / (ms * 1e-3) / 1e12 / load_peaks()[0]["bf16_tflops"],
                         "traffic": None}})
 
+def run_repr(args):
+    """FCHL19 descriptors + Jacobians on the GPU for the energy+force workload's
+    molecules (300 x 21 atoms, X and dX, FP32 storage, FP64 arithmetic), and
+    descriptors alone for 50,000 molecules of 9-30 atoms.  Metric: molecules/s of
+    the X + dX generation; the dominant cost is writing dX (HBM bound)."""
+    import torch
+
+    from kernelforge_b200 import fchl19_repr as fr
+    from kernelforge_b200 import synthetic
+
+    def padded(mols):
+        ma = max(len(z) for z in mols.Z)
+        C = np.zeros((mols.nm, ma, 3))
+        Z = np.zeros((mols.nm, ma), np.int32)
+        N = np.array([len(z) for z in mols.Z], np.int32)
+        for m in range(mols.nm):
+            C[m, :N[m]] = mols.R[m]
+            Z[m, :N[m]] = mols.Z[m]
+        return torch.tensor(C, dtype=torch.float32, device="cuda"), Z, N
+
+    tr = synthetic.make_molecules(300, 21, 21, seed=SEED + 4)
+    C, Z, N = padded(tr)
+    nm, ma = Z.shape
+    ms = _events_ms(lambda: fr.generate_batched(C, Z, N, gradients=True), args.steps,
+                    max(args.warmup, 3))
+    dx_bytes = nm * ma * 720 * 3 * ma * 4
+    big = synthetic.make_molecules(50000, 9, 30, seed=SEED + 5)
+    Cb, Zb, Nb = padded(big)
+    ms_big = _events_ms(lambda: fr.generate_batched(Cb, Zb, Nb), 3, 1)
+    peaks = load_peaks()[0]
+    cpu = None
+    if not args.no_cpu_baseline:
+        _, _ = _ref_modules()
+        import fchl19_repr as ref_fr  # noqa: E402  (reference build)
+        ns = 60
+        t0 = time.perf_counter()
+        for m in range(ns):
+            ref_fr.generate_fchl_acsf_and_gradients(tr.R[m], tr.Z[m])
+        dt = time.perf_counter() - t0
+        cpu = {"value": ns / dt, "unit": "molecules/s", "cores": os.cpu_count(),
+               "kind": "reference", "sample": f"{ns} of the 300 molecules, X + dX, FP64"}
+    _line("FCHL19 descriptor + Jacobian generation: molecules/s", nm / (ms * 1e-3),
+          "molecules/s", ms, args,
+          f"fchl19 X + dX of {nm} x {ma}-atom molecules (720 dims, FP32 storage, FP64 "
+          "arithmetic)", "f64 arithmetic / f32 storage",
+          {"dx_bytes": dx_bytes,
+           "roofline": {"bound": "hbm", "achieved": dx_bytes / (ms * 1e-3) / 1e9,
+                        "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                        "frac": dx_bytes / (ms * 1e-3) / 1e9 / peaks["hbm_gbs"],
+                        "traffic": None},
+           "descriptors_only_50k": {"ms": ms_big, "molecules_per_s": 50000 / (ms_big * 1e-3),
+                                    "atoms": int(Nb.sum())},
+           "cpu_baseline": cpu})
+
+
 def main():
     args = parse()
     if args.workload != "fit10k":
         {"config1": run_config1, "config3": run_config3, "config4": run_config4,
-         "config5": run_config5, "cosmlp_step": run_cosmlp_step}[args.workload](args)
+         "config5": run_config5, "cosmlp_step": run_cosmlp_step,
+         "repr": run_repr}[args.workload](args)
         return
     rank, world, local = dist_setup(args.gpus)
     try:

@@ -19,8 +19,10 @@
 // pair (i, o), three-body from the triples (i; o, q)): no atomics on dX.  The
 // centre's own columns follow from translation invariance of every term,
 //   dX[i, :, 3i + t] = -sum_{o != i} dX[i, :, 3o + t],
-// summed in shared memory.  In the three-body loop lane l owns radial channel
-// l and keeps its accumulators per partner element in registers.  Values of
+// summed in shared memory.  In the three-body loop the lanes first build the
+// geometry of 32 triples (one partner each) into shared slots, then lane l
+// takes radial channel l over the stored triples, with its accumulators per
+// partner element in registers.  Values of
 // the descriptor are summed in shared memory (each triple once, by its owner
 // o < q).  Arithmetic in FP64; outputs FP64 or FP32.
 #include <cmath>
@@ -165,6 +167,11 @@ __device__ inline Triple make_triple(const ReprParams &P, const Vec3 &Ri, const 
     return T;
 }
 
+struct TripleSlot {
+    Triple T;
+    int q, eq;  // partner atom (-1: empty slot) and its element
+};
+
 template <class TO, bool GRAD>
 __global__ void __launch_bounds__(REPR_WARPS * 32) fchl19_kernel(
     const TO *__restrict__ coords, const int *__restrict__ elem, const int *__restrict__ natoms,
@@ -173,7 +180,8 @@ __global__ void __launch_bounds__(REPR_WARPS * 32) fchl19_kernel(
     double *R = reinterpret_cast<double *>(rp_raw);  // [ma][3]
     double *xs = R + 3 * ma;                         // [rep] values of centre i
     double *gc = xs + P.rep;                         // [rep][3] centre columns (GRAD)
-    int *el = reinterpret_cast<int *>(gc + (GRAD ? 3 * P.rep : 0));  // [ma]
+    TripleSlot *tslots = reinterpret_cast<TripleSlot *>(gc + (GRAD ? 3 * P.rep : 0));  // [warps][32]
+    int *el = reinterpret_cast<int *>(tslots + REPR_WARPS * 32);                         // [ma]
     const int m = blockIdx.y, i = blockIdx.x;
     const int n = min(max(natoms[m], 0), ma);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -228,8 +236,11 @@ __global__ void __launch_bounds__(REPR_WARPS * 32) fchl19_kernel(
                 if (v != 0.0) atomicAdd(&xs[eo * P.nRs2 + k], v);
             }
         }
-        // ---- three-body: triples (i; o, q); lane owns radial channel l
+        // ---- three-body: triples (i; o, q).  Lanes first build the geometry of
+        // up to 32 partners q (one triple each) into the warp's shared slots,
+        // then lane l takes radial channel l over every stored triple.
         const bool o_in = r_io <= P.acut;
+        TripleSlot *slots = tslots + (size_t)warp * 32;
         for (int l0 = 0; l0 < P.nRs3; l0 += 32) {
             const int l = l0 + lane;
             const bool lv = l < P.nRs3;
@@ -241,19 +252,34 @@ __global__ void __launch_bounds__(REPR_WARPS * 32) fchl19_kernel(
                 for (int a = 0; a < 2; ++a)
 #pragma unroll
                     for (int t = 0; t < 3; ++t) acc[e][a][t] = 0.0;
-            if (o_in) {
-                for (int q = 0; q < n; ++q) {
-                    if (q == i || q == o) continue;
-                    const Vec3 Rq{R[3 * q], R[3 * q + 1], R[3 * q + 2]};
-                    const Vec3 diq = sub(Rq, Ri);
-                    const double r_iq = sqrt(dot(diq, diq));
-                    if (r_iq > P.acut) continue;
-                    const Triple T = make_triple(P, Ri, Ro, Rq, r_io, r_iq);
+            for (int q0 = 0; o_in && q0 < n; q0 += 32) {
+                {
+                    const int q = q0 + lane;
+                    TripleSlot &S = slots[lane];
+                    S.q = -1;
+                    if (q < n && q != i && q != o) {
+                        const Vec3 Rq{R[3 * q], R[3 * q + 1], R[3 * q + 2]};
+                        const Vec3 diq = sub(Rq, Ri);
+                        const double r_iq = sqrt(dot(diq, diq));
+                        if (r_iq <= P.acut) {
+                            S.T = make_triple(P, Ri, Ro, Rq, r_io, r_iq);
+                            S.q = q;
+                            S.eq = el[q];
+                        }
+                    }
+                }
+                __syncwarp();
+                const int qn = min(32, n - q0);
+                for (int sI = 0; sI < qn; ++sI) {
+                    const int q = slots[sI].q;
+                    if (q < 0) continue;  // warp-uniform
+                    const Triple &T = slots[sI].T;
+                    const int eq = slots[sI].eq;
                     const double dr = T.rbar - Rs3;
                     const double rad = exp(-P.eta3 * dr * dr);
                     double ang[16];
                     angular_basis(P, T.cos_i, T.sin_i, ang);
-                    const int ch = P.three_off + pair_channel(P.nelem, eo, el[q]) * npair_rows;
+                    const int ch = P.three_off + pair_channel(P.nelem, eo, eq) * npair_rows;
                     if (lv && o < q)
                         for (int a = 0; a < P.nab; ++a)
                             atomicAdd(&xs[ch + l * P.nab + a], ang[a] * rad * T.atm * T.dec);
@@ -262,7 +288,6 @@ __global__ void __launch_bounds__(REPR_WARPS * 32) fchl19_kernel(
                         const double drad = -P.eta3 * dr * rad;  // d rad / d r_io
                         const double wv = P.ang_w[0];
                         const double dang[2] = {wv * T.sin_i, -wv * T.cos_i};
-                        const int eq = el[q];
 #pragma unroll
                         for (int a = 0; a < 2; ++a) {
                             const double base = rad * T.dec;
@@ -283,6 +308,7 @@ __global__ void __launch_bounds__(REPR_WARPS * 32) fchl19_kernel(
                         }
                     }
                 }
+                __syncwarp();  // slots read by every lane before the next fill
             }
             if (GRAD) {
                 // write owner o's three-body columns for channel l (every pair block)
@@ -380,7 +406,7 @@ kfb_status kfb_fchl19_repr(const void *coords, const int32_t *elem, const int32_
     }
     const bool g = grad != nullptr;
     const size_t smem = (size_t)(3 * ma + P.rep + (g ? 3 * P.rep : 0)) * sizeof(double) +
-                        (size_t)ma * sizeof(int);
+                        (size_t)REPR_WARPS * 32 * sizeof(TripleSlot) + (size_t)ma * sizeof(int);
     if (smem > 200 * 1024)
         return set_error(KFB_ERR_INVALID_ARG, "descriptor too large for one block (%zu bytes)", smem);
     cudaStream_t s = static_cast<cudaStream_t>(stream);

@@ -127,13 +127,10 @@ def generate_batched(coords, Z, N, elements=DEFAULT_ELEMENTS, gradients=False,
     lut = np.full(max(max(elements), int(Zh.max(initial=0))) + 1, -1, np.int32)
     for k, e in enumerate(elements):
         lut[e] = k
-    idx = np.zeros((nm, ma), np.int32)
-    for m in range(nm):
-        n = min(max(int(Nh[m]), 0), ma)
-        e = lut[np.clip(Zh[m, :n], 0, None)]
-        if (e < 0).any() or (Zh[m, :n] < 0).any():
-            raise RuntimeError("nuclear_z contains an element not present in elements")
-        idx[m, :n] = e
+    valid = np.arange(ma)[None, :] < np.clip(Nh, 0, ma)[:, None]
+    idx = np.where(valid, lut[np.clip(Zh, 0, None)], 0).astype(np.int32)
+    if (valid & ((idx < 0) | (Zh < 0))).any():
+        raise RuntimeError("nuclear_z contains an element not present in elements")
     tdt = torch.float64 if dtype in ("float64", np.float64, torch.float64) else torch.float32
     kdt = _lib.KFB_F64 if tdt == torch.float64 else _lib.KFB_F32
     if isinstance(coords, torch.Tensor):
