@@ -246,6 +246,20 @@ kfb_status kfb_rff_features_elemental(const void *x, const int32_t *q, const int
                                       int ma, int rep, const float *w, const float *b, int nelem,
                                       int d, kfb_dtype x_dt, float *z, void *stream);
 
+/* Force features of the elemental RFF model: g (naq, d) device float32, row
+ * 3 off_m + 3 a + t = sqrt(2/d) sum_j sin(x_j W[e_j] + b[e_j]) (W[e_j]^T dX[m, j, :, 3 a + t])
+ * over the atoms j of molecule m, so that forces are F = g w.  x (nm, ma, rep) and
+ * dx (nm, ma, rep, 3 ma) device of type x_dt; q (element index, -1 = padding) and n
+ * host; w (nelem, rep, d), b (nelem, d) device float32; d a multiple of 8.  Tensor
+ * cores (split fp16, FP32 accumulation): the pre-activations, then the Jacobian rows
+ * times W with the sin weights and the per-molecule sums in the GEMM epilogue.
+ * Replaces rff_gradient_elemental_cuda (src/cuda_rff_features.hpp:55-63, the
+ * transpose of the CPU kf::rff::rff_gradient_elemental, src/rff_elemental.cpp:363-500). */
+kfb_status kfb_rff_gradient_elemental(const void *x, const void *dx, const int32_t *q,
+                                      const int32_t *n, int nm, int ma, int rep, const float *w,
+                                      const float *b, int nelem, int d, kfb_dtype x_dt, float *g,
+                                      void *stream);
+
 /* Normal equations of a linear ridge model on per-molecule features:
  * ztz = Z^T Z (d x d; KFB_DENSE both triangles, or RFP), zty = Z^T y (float64;
  * skipped when y is NULL).  z (nm, d) device float32, y (nm,) device float64.

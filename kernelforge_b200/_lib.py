@@ -28,7 +28,7 @@ EXPORTS = (
     "kfb_kernel_gaussian_full", "kfb_kernel_gaussian_full_symm", "kfb_full_to_rfp",
     "kfb_rfp_to_full", "kfb_rfp_add_diag", "kfb_rfp_potrf", "kfb_rfp_potrs",
     "kfb_cho_solve_rfp", "kfb_krr_solve_mixed", "kfb_rff_features_elemental",
-    "kfb_feature_gramian", "kfb_ridge_solve_mixed", "kfb_pair_gaussian", "kfb_cosmlp_create", "kfb_cosmlp_destroy",
+    "kfb_rff_gradient_elemental", "kfb_feature_gramian", "kfb_ridge_solve_mixed", "kfb_pair_gaussian", "kfb_cosmlp_create", "kfb_cosmlp_destroy",
     "kfb_cosmlp_params", "kfb_cosmlp_grads", "kfb_cosmlp_sync", "kfb_cosmlp_optimizer_state",
     "kfb_cosmlp_set_steps", "kfb_cosmlp_pair_step", "kfb_cosmlp_features_elemental",
     "kfb_local_alpha_desc", "kfb_local_matvec", "kfb_fchl19_rep_size", "kfb_fchl19_repr",
@@ -77,6 +77,7 @@ _SIGS = {
     "kfb_cho_solve_rfp": (I, [P, P, I, D, I, P, ctypes.POINTER(I), P]),
     "kfb_krr_solve_mixed": (I, [P, P, I, D, I, D, I, I, P, ctypes.POINTER(SolveInfo), P]),
     "kfb_rff_features_elemental": (I, [P, P, P, I, I, I, P, P, I, I, I, P, P]),
+    "kfb_rff_gradient_elemental": (I, [P, P, P, P, I, I, I, P, P, I, I, I, P, P]),
     "kfb_feature_gramian": (I, [P, P, I, I, I, P, P, P]),
     "kfb_ridge_solve_mixed": (I, [P, P, I, I, D, D, I, I, P, ctypes.POINTER(SolveInfo), P]),
     "kfb_pair_gaussian": (I, [P, ctypes.c_longlong, P, P, I, I, D, I, P, P]),

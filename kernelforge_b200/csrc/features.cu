@@ -383,6 +383,48 @@ size_t feature_budget() {
     return b;
 }
 
+// ---------------------------------------------------------------- RFF forces
+// K-padded operands for the force path (the tensor-core GEMM needs K % 16 == 0):
+// dst (rows, kpad) with dst[r][k] = src row r (stride src_ld) for k < rep, else 0.
+template <class T>
+__global__ void gather_pad_rows_kernel(const T *__restrict__ x, const int *__restrict__ idx,
+                                       int nrows, int rep, int kpad, float *__restrict__ out) {
+    const long long n = (long long)nrows * kpad;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(i / kpad), k = (int)(i % kpad);
+        out[i] = k < rep ? (float)x[(size_t)idx[r] * rep + k] : 0.f;
+    }
+}
+
+// wt (d, kpad) = W_e^T, zero beyond rep
+__global__ void transpose_pad_kernel(const float *__restrict__ w, int rep, int d, int kpad,
+                                     float *__restrict__ wt) {
+    __shared__ float tile[32][33];
+    const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int rr = r0 + r, cc = c0 + threadIdx.x;
+        tile[r][threadIdx.x] = (rr < rep && cc < d) ? w[(size_t)rr * d + cc] : 0.f;
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int cc = c0 + r, rr = r0 + threadIdx.x;  // output row cc (feature), column rr
+        if (cc < d && rr < kpad) wt[(size_t)cc * kpad + rr] = tile[threadIdx.x][r];
+    }
+}
+
+// Jacobian rows: out[r][k] = dx[(src[r] * rep + k) * ld + col[r]] (k < rep), 0 beyond
+template <class T>
+__global__ void jacobian_rows_kernel(const T *__restrict__ dx, const int *__restrict__ src,
+                                     const int *__restrict__ col, int nrows, int rep, int ld,
+                                     int kpad, float *__restrict__ out) {
+    const int r = blockIdx.x;
+    if (r >= nrows) return;
+    const T *base = dx + (size_t)src[r] * rep * ld + col[r];
+    for (int k = threadIdx.x; k < kpad; k += blockDim.x)
+        out[(size_t)r * kpad + k] = k < rep ? (float)base[(size_t)k * ld] : 0.f;
+}
+
 template <class T>
 kfb_status rff_features_t(const T *x, const int *q, const int *n, int nm, int ma, int rep,
                           const float *w, const float *b, int nelem, int d, float *z,
@@ -390,51 +432,52 @@ kfb_status rff_features_t(const T *x, const int *q, const int *n, int nm, int ma
     KFB_TRY(zero(z, (size_t)nm * d * sizeof(float), s));
     ElemRows er;
     KFB_TRY(elem_rows(q, n, nm, ma, nelem, er));
-    // W_e^T (d, rep) split once per element
+    // W_e^T (d, kpad) split once per element; K padded with zeros to a multiple of 16
+    const int kpad = (rep + 15) / 16 * 16;
     DevBuf wt, wh, wl;
-    KFB_TRY(wt.alloc((size_t)d * rep * sizeof(float), s));
-    KFB_TRY(wh.alloc((size_t)d * rep * sizeof(__half), s));
-    KFB_TRY(wl.alloc((size_t)d * rep * sizeof(__half), s));
-    const size_t row_bytes = (size_t)rep * (sizeof(float) + 2 * sizeof(__half));
+    KFB_TRY(wt.alloc((size_t)d * kpad * sizeof(float), s));
+    KFB_TRY(wh.alloc((size_t)d * kpad * sizeof(__half), s));
+    KFB_TRY(wl.alloc((size_t)d * kpad * sizeof(__half), s));
+    const size_t row_bytes = (size_t)kpad * (sizeof(float) + 2 * sizeof(__half));
     const int chunk = (int)std::max<size_t>(128, feature_budget() / row_bytes);
     DevBuf xr, xh, xl, didx, dmol;
     const float sc = std::sqrt(2.f / (float)d);
     for (int e = 0; e < nelem; ++e) {
         const int ne = (int)er.idx[e].size();
         if (ne == 0) continue;
-        transpose_f32_kernel<<<dim3(nblk(d, 32), nblk(rep, 32)), dim3(32, 8), 0, s>>>(
-            w + (size_t)e * rep * d, rep, d, wt.as<float>());
+        transpose_pad_kernel<<<dim3(nblk(d, 32), nblk(kpad, 32)), dim3(32, 8), 0, s>>>(
+            w + (size_t)e * rep * d, rep, d, kpad, wt.as<float>());
         KFB_CUDA_TRY(cudaGetLastError());
         float w_scale = 1.f;
-        KFB_TRY(split_rows<float>(wt.as<float>(), (long long)d * rep, wh.as<__half>(),
+        KFB_TRY(split_rows<float>(wt.as<float>(), (long long)d * kpad, wh.as<__half>(),
                                   wl.as<__half>(), &w_scale, s));
         KFB_TRY(upload(didx, er.idx[e], s));
         KFB_TRY(upload(dmol, er.mol[e], s));
         const int rows_max = std::min(ne, chunk);
-        KFB_TRY(xr.alloc((size_t)rows_max * rep * sizeof(float), s));
-        KFB_TRY(xh.alloc((size_t)rows_max * rep * sizeof(__half), s));
-        KFB_TRY(xl.alloc((size_t)rows_max * rep * sizeof(__half), s));
+        KFB_TRY(xr.alloc((size_t)rows_max * kpad * sizeof(float), s));
+        KFB_TRY(xh.alloc((size_t)rows_max * kpad * sizeof(__half), s));
+        KFB_TRY(xl.alloc((size_t)rows_max * kpad * sizeof(__half), s));
         for (int r0 = 0; r0 < ne; r0 += chunk) {
             const int nr = std::min(chunk, ne - r0);
-            gather_rows_f32_kernel<T><<<nblk((long long)nr * rep, 256 * 8), 256, 0, s>>>(
-                x, didx.as<int>() + r0, nr, rep, xr.as<float>());
+            gather_pad_rows_kernel<T><<<nblk((long long)nr * kpad, 256 * 8), 256, 0, s>>>(
+                x, didx.as<int>() + r0, nr, rep, kpad, xr.as<float>());
             KFB_CUDA_TRY(cudaGetLastError());
             float x_scale = 1.f;
-            KFB_TRY(split_rows<float>(xr.as<float>(), (long long)nr * rep, xh.as<__half>(),
+            KFB_TRY(split_rows<float>(xr.as<float>(), (long long)nr * kpad, xh.as<__half>(),
                                       xl.as<__half>(), &x_scale, s));
             TcOperand A, B;
             A.hi = xh.ptr;
             A.lo = xl.ptr;
             A.rows = nr;
-            A.cols = rep;
+            A.cols = kpad;
             B.hi = wh.ptr;
             B.lo = wl.ptr;
             B.rows = d;
-            B.cols = rep;
+            B.cols = kpad;
             TcProb p{};
             p.M = nr;
             p.N = d;
-            p.K = rep;
+            p.K = kpad;
             p.row_off = 0;
             p.alpha = 1.0 / ((double)x_scale * (double)w_scale);
             TcEpi epi;
@@ -442,6 +485,132 @@ kfb_status rff_features_t(const T *x, const int *q, const int *n, int nm, int ma
             epi.bias = b + (size_t)e * d;
             epi.mol = dmol.as<int>() + r0;
             epi.molsum = z;
+            epi.ld = d;
+            epi.scale = sc;
+            KFB_TRY(tc_gemm_grouped(A, B, 3, false, {p}, ElemSink(), s, epi));
+        }
+    }
+    return KFB_OK;
+}
+
+// G (naq, d) += rows 3 off_m + c: sqrt(2/d) sum_j sin(z_j) (W_e^T dX[m, j, :, c]), z_j the
+// pre-activation x_j W_e + b_e (src/rff_elemental.cpp:363-500 stores the transpose).
+template <class T>
+kfb_status rff_gradient_t(const T *x, const T *dx, const int *q, const int *n, int nm, int ma,
+                          int rep, const float *w, const float *b, int nelem, int d, float *g,
+                          cudaStream_t s) {
+    std::vector<int> offs(nm + 1, 0);
+    for (int m = 0; m < nm; ++m) offs[m + 1] = offs[m] + 3 * std::min(std::max(n[m], 0), ma);
+    KFB_TRY(zero(g, (size_t)std::max(offs[nm], 1) * d * sizeof(float), s));
+    ElemRows er;
+    KFB_TRY(elem_rows(q, n, nm, ma, nelem, er));
+    const int kpad = (rep + 15) / 16 * 16, ld = 3 * ma;
+    DevBuf wt, wh, wl;
+    KFB_TRY(wt.alloc((size_t)d * kpad * sizeof(float), s));
+    KFB_TRY(wh.alloc((size_t)d * kpad * sizeof(__half), s));
+    KFB_TRY(wl.alloc((size_t)d * kpad * sizeof(__half), s));
+    // per atom: one Z row (d floats) and up to 3 ma Jacobian rows (kpad wide, FP32 + pair)
+    const size_t atom_bytes = (size_t)d * sizeof(float) +
+                              (size_t)(1 + ld) * kpad * (sizeof(float) + 2 * sizeof(__half));
+    const int chunk = (int)std::max<size_t>(1, feature_budget() / atom_bytes);
+    const float sc = std::sqrt(2.f / (float)d);
+    DevBuf zpre, xr, xh, xl, jr, jh, jl, didx, dsrc, dcol, ddst, daux;
+    for (int e = 0; e < nelem; ++e) {
+        const int ne = (int)er.idx[e].size();
+        if (ne == 0) continue;
+        transpose_pad_kernel<<<dim3(nblk(d, 32), nblk(kpad, 32)), dim3(32, 8), 0, s>>>(
+            w + (size_t)e * rep * d, rep, d, kpad, wt.as<float>());
+        KFB_CUDA_TRY(cudaGetLastError());
+        float w_scale = 1.f;
+        KFB_TRY(split_rows<float>(wt.as<float>(), (long long)d * kpad, wh.as<__half>(),
+                                  wl.as<__half>(), &w_scale, s));
+        TcOperand B;
+        B.hi = wh.ptr;
+        B.lo = wl.ptr;
+        B.rows = d;
+        B.cols = kpad;
+        for (int a0 = 0; a0 < ne; a0 += chunk) {
+            const int na = std::min(chunk, ne - a0);
+            // rows of the chunk, ordered (molecule, c, atom): one destination per run
+            std::vector<int> src, col, dst, aux;
+            for (int t = 0; t < na;) {
+                const int m = er.mol[e][a0 + t];
+                int t1 = t;
+                while (t1 < na && er.mol[e][a0 + t1] == m) ++t1;
+                const int nc = offs[m + 1] - offs[m];
+                for (int c = 0; c < nc; ++c)
+                    for (int u = t; u < t1; ++u) {
+                        src.push_back(er.idx[e][a0 + u]);
+                        col.push_back(c);
+                        dst.push_back(offs[m] + c);
+                        aux.push_back(u);
+                    }
+                t = t1;
+            }
+            const int nr = (int)src.size();
+            std::vector<int> aidx(er.idx[e].begin() + a0, er.idx[e].begin() + a0 + na);
+            KFB_TRY(upload(didx, aidx, s));
+            KFB_TRY(upload(dsrc, src, s));
+            KFB_TRY(upload(dcol, col, s));
+            KFB_TRY(upload(ddst, dst, s));
+            KFB_TRY(upload(daux, aux, s));
+            // pre-activations Z = X_e W_e + b_e (na, d), FP32
+            KFB_TRY(zpre.alloc((size_t)na * d * sizeof(float), s));
+            KFB_TRY(xr.alloc((size_t)na * kpad * sizeof(float), s));
+            KFB_TRY(xh.alloc((size_t)na * kpad * sizeof(__half), s));
+            KFB_TRY(xl.alloc((size_t)na * kpad * sizeof(__half), s));
+            gather_pad_rows_kernel<T><<<nblk((long long)na * kpad, 256 * 8), 256, 0, s>>>(
+                x, didx.as<int>(), na, rep, kpad, xr.as<float>());
+            KFB_CUDA_TRY(cudaGetLastError());
+            float x_scale = 1.f;
+            KFB_TRY(split_rows<float>(xr.as<float>(), (long long)na * kpad, xh.as<__half>(),
+                                      xl.as<__half>(), &x_scale, s));
+            {
+                TcOperand A;
+                A.hi = xh.ptr;
+                A.lo = xl.ptr;
+                A.rows = na;
+                A.cols = kpad;
+                TcProb p{};
+                p.M = na;
+                p.N = d;
+                p.K = kpad;
+                p.alpha = 1.0 / ((double)x_scale * (double)w_scale);
+                TcEpi epi;
+                epi.mode = EPI_DENSE;
+                epi.zf32 = zpre.as<float>();
+                epi.bias = b + (size_t)e * d;
+                epi.ld = d;
+                KFB_TRY(tc_gemm_grouped(A, B, 3, false, {p}, ElemSink(), s, epi));
+            }
+            // Jacobian rows (nr, kpad) times W_e, weighted by sqrt(2/d) sin(Z) and
+            // summed into G per destination row
+            KFB_TRY(jr.alloc((size_t)nr * kpad * sizeof(float), s));
+            KFB_TRY(jh.alloc((size_t)nr * kpad * sizeof(__half), s));
+            KFB_TRY(jl.alloc((size_t)nr * kpad * sizeof(__half), s));
+            jacobian_rows_kernel<T><<<nr, 128, 0, s>>>(dx, dsrc.as<int>(), dcol.as<int>(), nr, rep,
+                                                       ld, kpad, jr.as<float>());
+            KFB_CUDA_TRY(cudaGetLastError());
+            float j_scale = 1.f;
+            KFB_TRY(split_rows<float>(jr.as<float>(), (long long)nr * kpad, jh.as<__half>(),
+                                      jl.as<__half>(), &j_scale, s));
+            TcOperand A;
+            A.hi = jh.ptr;
+            A.lo = jl.ptr;
+            A.rows = nr;
+            A.cols = kpad;
+            TcProb p{};
+            p.M = nr;
+            p.N = d;
+            p.K = kpad;
+            p.alpha = 1.0 / ((double)j_scale * (double)w_scale);
+            TcEpi epi;
+            epi.mode = EPI_SIN_RUNSUM;
+            epi.mol = ddst.as<int>();
+            epi.atom = daux.as<int>();
+            epi.aux = zpre.as<float>();
+            epi.ld_aux = d;
+            epi.molsum = g;
             epi.ld = d;
             epi.scale = sc;
             KFB_TRY(tc_gemm_grouped(A, B, 3, false, {p}, ElemSink(), s, epi));
@@ -751,9 +920,9 @@ kfb_status kfb_rff_features_elemental(const void *x, const int *q, const int *n,
             return set_error(KFB_ERR_INVALID_ARG, "null pointer argument");
         if (nm <= 0 || ma <= 0 || rep <= 0 || nelem <= 0 || d <= 0)
             return set_error(KFB_ERR_INVALID_ARG, "All dims must be positive.");
-        if (rep % 16 != 0 || d % 8 != 0)
+        if (d % 8 != 0)
             return set_error(KFB_ERR_UNSUPPORTED,
-                             "rff_features_elemental: rep must be a multiple of 16 and D of 8");
+                             "rff_features_elemental: D must be a multiple of 8");
         if (!device_is_sm100())
             return set_error(KFB_ERR_UNSUPPORTED, "feature maps need an sm_100 (B200) device");
         cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -762,6 +931,25 @@ kfb_status kfb_rff_features_elemental(const void *x, const int *q, const int *n,
                                           b, nelem, d, z, s);
         return rff_features_t<float>(static_cast<const float *>(x), q, n, nm, ma, rep, w, b,
                                      nelem, d, z, s);
+    });
+}
+
+kfb_status kfb_rff_gradient_elemental(const void *x, const void *dx, const int *q, const int *n,
+                                      int nm, int ma, int rep, const float *w, const float *b,
+                                      int nelem, int d, kfb_dtype x_dt, float *g, void *stream) {
+    return guarded([&]() -> kfb_status {
+        if (!x || !dx || !q || !n || !w || !b || !g)
+            return set_error(KFB_ERR_INVALID_ARG, "null pointer");
+        if (nm <= 0 || ma <= 0 || rep <= 0 || nelem <= 0 || d <= 0)
+            return set_error(KFB_ERR_INVALID_ARG, "dimensions must be positive");
+        if (d % 8 != 0) return set_error(KFB_ERR_INVALID_ARG, "D must be a multiple of 8");
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        if (x_dt == KFB_F64)
+            return rff_gradient_t<double>(static_cast<const double *>(x),
+                                          static_cast<const double *>(dx), q, n, nm, ma, rep, w,
+                                          b, nelem, d, g, s);
+        return rff_gradient_t<float>(static_cast<const float *>(x), static_cast<const float *>(dx),
+                                     q, n, nm, ma, rep, w, b, nelem, d, g, s);
     });
 }
 

@@ -330,18 +330,44 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                         if (j < nvalid)
                             epi.act_t[(gcol0 + j) * epi.ld_t + grow] =
                                 __float2bfloat16_rn(-v[j] * alpha * sinf(g[j]));
-                } else {  // EPI_COS_MOLSUM
-                    // rows of one molecule are consecutive: sum each run of rows per
-                    // column through shared memory, one atomic add per (run, column)
+                } else {  // EPI_COS_MOLSUM, EPI_SIN_RUNSUM
+                    // rows with one destination are consecutive: sum each run of rows
+                    // per column through shared memory, one atomic add per (run, column)
                     float(*scr)[33] = molsum_scr[warp - EPI_WARP0];
                     const int mol = mvalid ? epi.mol[grow] : -1;
-                    const float bl =
-                        (epi.bias && lane < nvalid && nvalid > 0) ? epi.bias[gcol0 + lane] : 0.f;
+                    if (epi.mode == EPI_SIN_RUNSUM) {
+                        // scale sin(aux[atom row, col]) times the product
+                        const float *a =
+                            epi.aux + (long long)(mvalid ? epi.atom[grow] : 0) * epi.ld_aux + gcol0;
+                        float g[32];
+                        if (vec) {
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        const bool ok = mvalid && j < nvalid;
-                        const float bias = __shfl_sync(0xffffffffu, bl, j);
-                        scr[j][lane] = ok ? epi.scale * cosf(v[j] * alpha + bias) : 0.f;
+                            for (int j = 0; j < 32; j += 4) {
+                                const float4 t4 = *reinterpret_cast<const float4 *>(a + j);
+                                g[j] = t4.x;
+                                g[j + 1] = t4.y;
+                                g[j + 2] = t4.z;
+                                g[j + 3] = t4.w;
+                            }
+                        } else {
+#pragma unroll
+                            for (int j = 0; j < 32; ++j) g[j] = (mvalid && j < nvalid) ? a[j] : 0.f;
+                        }
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) {
+                            const bool ok = mvalid && j < nvalid;
+                            scr[j][lane] = ok ? epi.scale * sinf(g[j]) * (v[j] * alpha) : 0.f;
+                        }
+                    } else {
+                        const float bl = (epi.bias && lane < nvalid && nvalid > 0)
+                                             ? epi.bias[gcol0 + lane]
+                                             : 0.f;
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) {
+                            const bool ok = mvalid && j < nvalid;
+                            const float bias = __shfl_sync(0xffffffffu, bl, j);
+                            scr[j][lane] = ok ? epi.scale * cosf(v[j] * alpha + bias) : 0.f;
+                        }
                     }
                     __syncwarp();
                     // lane l owns column n0 + l and walks the 32 rows by molecule runs
@@ -430,6 +456,7 @@ kfb_status launch(const TcOperand &A, const TcOperand &B, bool bf16,
     if (e.mode != EPI_SINK) {
         auto al = [](const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
         bool v = e.ld % 8 == 0 && al(e.zf32) && al(e.act) && al(e.aux);
+        if (e.mode == EPI_SIN_RUNSUM) v = v && e.ld_aux % 4 == 0;
         for (const TcProb &pb : probs) v = v && pb.col_off % 8 == 0;
         e.vec = v ? 1 : 0;
     }

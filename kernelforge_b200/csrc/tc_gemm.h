@@ -43,7 +43,16 @@ struct TcTile {
 //                  (back-propagation through a cos activation)
 //   EPI_COS_MOLSUM molsum[mol[row] * ld + col] += scale * cos z, each run of
 //                  rows of one molecule summed before its atomic add
-enum TcEpiMode : int { EPI_SINK = 0, EPI_DENSE = 1, EPI_DSIN_T = 2, EPI_COS_MOLSUM = 3 };
+//   EPI_SIN_RUNSUM molsum[mol[row] * ld + col] +=
+//                      scale * sin(aux[atom[row] * ld_aux + col]) * alpha * acc,
+//                  runs of rows with one destination summed as above
+enum TcEpiMode : int {
+    EPI_SINK = 0,
+    EPI_DENSE = 1,
+    EPI_DSIN_T = 2,
+    EPI_COS_MOLSUM = 3,
+    EPI_SIN_RUNSUM = 4
+};
 
 struct TcEpi {
     int mode = EPI_SINK;
@@ -55,8 +64,9 @@ struct TcEpi {
     const float *aux = nullptr;
     const float *bias = nullptr;
     const int *mol = nullptr;
+    const int *atom = nullptr;  // EPI_SIN_RUNSUM: row of aux for each output row
     float *molsum = nullptr;
-    long long ld = 0, ld_t = 0;
+    long long ld = 0, ld_t = 0, ld_aux = 0;
     float scale = 1.f;
 };
 

@@ -7,8 +7,10 @@ bench.py, never by the kernelforge_b200 package.
   Fourier features, restated from src/rff_elemental.hpp:7-24 and the steps of
   src/rff_elemental.cpp:30-135 (gather the atoms of element e, Z_e = X_e W_e,
   cos(Z_e + b_e) sqrt(2/D), scatter-add per molecule) and the normal equations
-  of src/rff_elemental.cpp:641-700 (Z^T Z, Z^T Y).  Pinned against the
-  reference's own kitchen_sinks module (tests/golden/golden_rff.npz).
+  of src/rff_elemental.cpp:641-700 (Z^T Z, Z^T Y); the force features
+  rff_gradient_elemental and the energy + force normal equations.  Pinned
+  against the reference's own kitchen_sinks module (tests/golden/golden_rff.npz,
+  golden_rff_force.npz).
 * The learned cos-MLP map (no reference counterpart): forward pass, the pair
   loss and its analytic FP64 gradient, the per-molecule feature sums.  The
   gradient is pinned by central finite differences in the CPU tests.
@@ -53,6 +55,39 @@ def rff_gramian(Z, Y):
 
 
 # ------------------------------------------------------------------ cos-MLP
+def rff_gradient_elemental(X, dX, Q, N, W, b):
+    """G (total_naq, D): row 3 off_m + 3 a + t (atom a of molecule m, axis t) is
+    sqrt(2/D) sum_j sin(x_j W[e_j] + b[e_j]) * (W[e_j]^T dX[m, j, :, 3 a + t]),
+    the force features with F = G w (src/rff_elemental.cpp:363-500, which stores
+    the transpose (D, ngrads)).  dX is (nm, ma, rep, 3 ma)."""
+    X = np.asarray(X, np.float64)
+    dX = np.asarray(dX, np.float64)
+    W = np.asarray(W, np.float64)
+    b = np.asarray(b, np.float64)
+    nm, ma, _ = X.shape
+    D = b.shape[1]
+    norm = np.sqrt(2.0 / D)
+    n = np.clip(np.asarray(N), 0, ma)
+    off = np.concatenate([[0], np.cumsum(3 * n)]).astype(int)
+    G = np.zeros((off[-1], D))
+    for m in range(nm):
+        nc = 3 * n[m]
+        for j in range(n[m]):
+            e = int(Q[m, j])
+            if e < 0:
+                continue
+            z = X[m, j] @ W[e] + b[e]
+            G[off[m]:off[m] + nc] += norm * (dX[m, j, :, :nc].T @ W[e]) * np.sin(z)[None, :]
+    return G
+
+
+def rff_full_gramian(Z, G, Y, F):
+    """Energy + force normal equations: [Z; G]^T [Z; G] and Z^T Y + G^T F
+    (src/rff_elemental.cpp:799-935)."""
+    A = np.concatenate([np.asarray(Z, np.float64), np.asarray(G, np.float64)])
+    return A.T @ A, A.T @ np.concatenate([np.ravel(Y), np.ravel(F)])
+
+
 def to_bf16(a):
     """Round to the nearest bfloat16 (ties to even), returned as float32."""
     a = np.ascontiguousarray(a, np.float32)

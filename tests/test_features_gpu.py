@@ -303,3 +303,41 @@ def test_training_gains_over_the_untrained_map():
     assert hist[-1] < hist[0]
     assert trained < untrained / 3, (trained, untrained)
     assert trained < rff, (trained, rff)
+
+
+@pytest.mark.parametrize("case", ["f", "r"])
+@pytest.mark.parametrize("xdtype", ["float32", "float64"])
+def test_rff_force_features_match_reference(case, xdtype):
+    """Force features G and the energy + force normal equations against the reference's
+    kitchen_sinks (tests/golden/golden_rff_force.npz) and the oracle on the same
+    float32 weights: split-fp16 products, FP32 accumulation."""
+    import torch
+    from kernelforge_b200 import cuda_rff_features as crf
+    g = load_golden("golden_rff_force.npz")
+    a = {k[2:]: g[k] for k in g if k.startswith(case + "_")}
+    dt = getattr(torch, xdtype)
+    X, dX = cuda(a["X"], dt), cuda(a["dX"], dt)
+    W, b = cuda(a["W"], torch.float32), cuda(a["b"], torch.float32)
+    G = crf.rff_gradient_elemental(X, dX, a["Q"], a["N"], W, b)
+    assert G.dtype == torch.float32 and tuple(G.shape) == a["G"].T.shape
+    ref32 = of.rff_gradient_elemental(np.asarray(X.cpu(), np.float64),
+                                      np.asarray(dX.cpu(), np.float64), a["Q"], a["N"],
+                                      a["W"].astype(np.float32), a["b"].astype(np.float32))
+    assert rel(G.cpu().numpy(), ref32) <= 2e-5
+    assert rel(G.cpu().numpy(), a["G"].T) <= 1e-4
+    # energy + force normal equations (RFP 'L' here, 'U' in the reference's CPU code)
+    ztz, zty = crf.rff_full_gramian_elemental_rfp(X, dX, a["Q"], a["N"], W, b,
+                                                  cuda(a["Y"], torch.float64),
+                                                  cuda(a["F"], torch.float64))
+    D = a["b"].shape[1]
+    got = o.rfp_to_full(ztz.cpu().numpy().astype(np.float64), D, uplo_lower=True)
+    ref = o.rfp_to_full(a["ZtZ_rfp"], D, uplo_lower=False)
+    assert rel(got, ref) <= 2e-4
+    assert rel(zty.cpu().numpy(), a["ZtY"]) <= 2e-4
+    # force predictions are G @ w
+    w = torch.tensor(np.random.default_rng(3).standard_normal(D), device="cuda")
+    Fp = crf.rff_predict_force_elemental(X, dX, a["Q"], a["N"], W, b, w)
+    np.testing.assert_allclose(Fp.cpu().numpy(), G.double().cpu().numpy() @ w.cpu().numpy(),
+                               rtol=1e-10, atol=1e-10)
+    Gt = crf.rff_gradient_elemental_col_major(X, dX, a["Q"], a["N"], W, b)
+    np.testing.assert_array_equal(Gt.cpu().numpy(), G.cpu().numpy().T)

@@ -87,3 +87,19 @@ def test_bf16_rounding_is_round_to_nearest_even():
     got = of.to_bf16(x)
     np.testing.assert_array_equal(got, np.array([1.0, 1.0, 1.0 + 2.0 ** -6, -2.5, 0.0],
                                                 np.float32))
+
+
+@pytest.mark.parametrize("tag", ["f", "r"])
+def test_oracle_rff_force_path_matches_reference(tag):
+    """The force features and the energy+force normal equations of the oracle
+    against the reference's kitchen_sinks (tests/golden/golden_rff_force.npz)."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "golden_rff_force.npz"))
+    a = {k[2:]: g[k] for k in g.files if k.startswith(tag + "_")}
+    G = of.rff_gradient_elemental(a["X"], a["dX"], a["Q"], a["N"], a["W"], a["b"])
+    np.testing.assert_allclose(G, a["G"].T, rtol=1e-11, atol=1e-12 * np.abs(G).max())
+    Z = of.rff_features_elemental(a["X"], a["Q"], a["N"], a["W"], a["b"])
+    A, rhs = of.rff_full_gramian(Z, G, a["Y"], a["F"])
+    np.testing.assert_allclose(rhs, a["ZtY"], rtol=1e-11, atol=1e-12 * np.abs(rhs).max())
+    np.testing.assert_allclose(o.full_to_rfp(A), a["ZtZ_rfp"], rtol=1e-11,
+                               atol=1e-12 * np.abs(A).max())
