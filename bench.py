@@ -56,7 +56,7 @@ def parse():
                     help="skip the FP64-GPU fit and the accuracy check (profiling runs)")
     ap.add_argument("--workload", default="fit10k",
                     choices=["fit10k", "config1", "config3", "config4", "config5",
-                             "cosmlp_step", "repr"],
+                             "cosmlp_step", "repr", "rff_force"],
                     help="fit10k (default): the 10,000-molecule kernel + solve; config1: FP64 "
                          "1,000-molecule fit+predict; config3: Jacobian kernel 1,000 x 1,000 "
                          "molecules; config4: energy+force kernel of 300 x 21-atom molecules "
@@ -1143,12 +1143,83 @@ def run_repr(args):
            "cpu_baseline": cpu})
 
 
+def run_rff_force(args):
+    """Energy + force random-Fourier-feature regression on the energy+force
+    workload's molecules (300 x 21 atoms train, 100 test; FCHL19 X and dX from the
+    GPU generator; D = 4096, W ~ N(0,1)/sigma, b ~ U(0, 2 pi)): features Z, force
+    features G (tensor cores), then the ridge solve on [Z; G] against [E; F].
+    Metric: fit time; test MAE of energies and forces beside it."""
+    import torch
+
+    from kernelforge_b200 import cuda_rff_features as crf
+    from kernelforge_b200 import fchl19_repr as fr
+    from kernelforge_b200 import synthetic
+    from kernelforge_b200.feature_maps import fit_ridge
+
+    def prep(mols):
+        N = np.array([len(z) for z in mols.Z], np.int32)
+        ma = int(N.max())
+        C = np.zeros((mols.nm, ma, 3))
+        Zn = np.zeros((mols.nm, ma), np.int32)
+        for m in range(mols.nm):
+            C[m, :N[m]], Zn[m, :N[m]] = mols.R[m], mols.Z[m]
+        X, dX = fr.generate_batched(C, Zn, N, gradients=True)
+        Q = np.full(Zn.shape, -1, np.int32)
+        for k, z in enumerate((1, 6, 7, 8)):
+            Q[Zn == z] = k
+        Q[np.arange(ma)[None, :] >= N[:, None]] = -1
+        return X, dX, Q, N, np.concatenate([np.asarray(f).ravel() for f in mols.F])
+
+    tr = synthetic.make_molecules(300, 21, 21, seed=SEED + 4)
+    te = synthetic.make_molecules(100, 21, 21, seed=SEED + 40)
+    X, dX, Q, N, F = prep(tr)
+    Xt, dXt, Qt, Nt, Ft = prep(te)
+    D = 4096
+    rng = np.random.default_rng(SEED + 70)
+    W = torch.tensor((rng.standard_normal((4, 720, D)) / SIGMA).astype(np.float32), device="cuda")
+    b = torch.tensor(rng.uniform(0, 2 * np.pi, (4, D)).astype(np.float32), device="cuda")
+    em = float(np.mean(tr.E))
+    y = torch.tensor(np.concatenate([tr.E - em, F]), device="cuda")
+    out = {}
+
+    def fit(l2):
+        Z = crf.rff_features_elemental(X, Q, N, W, b)
+        G = crf.rff_gradient_elemental(X, dX, Q, N, W, b)
+        return fit_ridge(torch.cat([Z, G]), y, l2)
+
+    g_ms = _events_ms(lambda: crf.rff_gradient_elemental(X, dX, Q, N, W, b), 3, 2)
+    rows = int(3 * N.sum())
+    # GEMM rows of the force features: every atom contributes the 3 n columns of
+    # its molecule's Jacobian (three fp16 products per multiply-add)
+    gemm_rows = int((3 * N.astype(np.int64) * N).sum())
+    g_flops = 3 * 2 * gemm_rows * 720 * D
+    for l2 in (1e-6, 1e-4, 1e-2):
+        w, info = fit(l2)
+        Ep = (crf.rff_features_elemental(Xt, Qt, Nt, W, b).double() @ w).cpu().numpy() + em
+        Fp = crf.rff_predict_force_elemental(Xt, dXt, Qt, Nt, W, b, w).cpu().numpy()
+        out[str(l2)] = {"test_mae_energy": float(np.abs(Ep - te.E).mean()),
+                        "test_mae_force": float(np.abs(Fp - Ft).mean()),
+                        "lambda_eff": info["lambda_eff"], "iterations": info["iterations"]}
+    best = min(out, key=lambda k: out[k]["test_mae_force"])
+    ms = _events_ms(lambda: fit(float(best)), max(args.steps // 4, 3), 2)
+    peaks = load_peaks()[0]
+    _line("RFF energy+force fit time (D = 4096)", ms * 1e-3, "s", ms, args,
+          f"elemental RFF D={D}, 300 x 21-atom molecules: Z, force features G ({rows} rows), "
+          "ridge solve on [Z; G]", "f16x3 / f32 features + f64 refinement",
+          {"higher_is_better": False, "lambda_scan": out, "lambda_best": float(best),
+           "force_features_ms": g_ms, "force_feature_gemm_rows": gemm_rows,
+           "roofline": {"bound": "tensor", "achieved": g_flops / (g_ms * 1e-3) / 1e12,
+                        "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
+                        "frac": g_flops / (g_ms * 1e-3) / 1e12 / peaks["bf16_tflops"],
+                        "traffic": None, "kernel": "force features (3 fp16 products)"}})
+
+
 def main():
     args = parse()
     if args.workload != "fit10k":
         {"config1": run_config1, "config3": run_config3, "config4": run_config4,
          "config5": run_config5, "cosmlp_step": run_cosmlp_step,
-         "repr": run_repr}[args.workload](args)
+         "repr": run_repr, "rff_force": run_rff_force}[args.workload](args)
         return
     rank, world, local = dist_setup(args.gpus)
     try:
