@@ -63,6 +63,8 @@ def parse():
                          "+ solve; config5: learned feature map vs RFF vs exact KRR")
     ap.add_argument("--c4-nmol", type=int, default=300,
                     help="config4 training molecules (smaller values: profiling cases)")
+    ap.add_argument("--c3-nmol", type=int, default=1000,
+                    help="config3 training and test molecules (smaller values: profiling cases)")
     ap.add_argument("--c5-nmol", type=int, default=50000)
     ap.add_argument("--c5-pairs", type=int, default=2000000)
     ap.add_argument("--c5-epochs", type=int, default=6)
@@ -517,8 +519,8 @@ def run_config3(args):
     import torch
 
     from kernelforge_b200 import _lib, synthetic
-    tr = synthetic.make_molecules(1000, 9, 30, seed=SEED + 3)
-    te = synthetic.make_molecules(1000, 9, 30, seed=SEED + 30)
+    tr = synthetic.make_molecules(args.c3_nmol, 9, 30, seed=SEED + 3)
+    te = synthetic.make_molecules(args.c3_nmol, 9, 30, seed=SEED + 30)
     X1, Q1, N1 = synthetic.fchl19_batched(tr, dtype=np.float32, device="cuda", chunk=64)
     X2, dX2, Q2, N2 = synthetic.fchl19_batched_grad(te, dtype=np.float32, device="cuda",
                                                    chunk=16)
@@ -562,6 +564,12 @@ def run_config3(args):
             torch.cuda.current_stream().cuda_stream))
         err = sub.double().cpu().numpy() - ref
         cpu["gpu_rel_frobenius_err"] = float(np.linalg.norm(err) / np.linalg.norm(ref))
+    if args.no_extras:
+        _line("FCHL19 local Jacobian kernel: entries/s", entries / (ms * 1e-3), "entries/s", ms,
+              args, f"kernel_gaussian_jacobian {nm1} x {nm2} molecules (9-30 atoms), "
+              f"naq2={naq2}", "f16x3 / f32",
+              {"cpu_baseline": cpu, "shape": [nm1, naq2], "fp32_cuda_core_ms": ms_fp32})
+        return
     # force prediction of an energy-trained KRR model on the 1,000 training
     # molecules: E_b = sum_a alpha_a K(a, b), so F_b = -alpha^T K_jac[:, b]
     # (K_jac = +dK/dR_b); tensor-core path (split-fp16 kernels, mixed solve)

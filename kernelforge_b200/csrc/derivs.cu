@@ -4,9 +4,10 @@
 // Jacobian (+dK/dR of the "inner" set, src/local_kernels.cpp:791-974):
 //   K[o, off_m + c] = sum_{j in m} v_{o,j} . J_j[:, c],
 //   v_{o,j} = sum_{i in o, q_i = q_j} (e_ij / sigma^2) (x_i - x_j)
-// The v rows are formed first (one warp per (o, j)), then contracted with the
-// Jacobians, one GEMM problem per inner molecule m.  This costs 2 rep 3 n_m
-// per (o, j) instead of per atom pair.  The transposed Jacobian
+// The v rows are formed first (label-major register tiles on the CUDA cores,
+// the squared distances from one dot-product GEMM per label), then contracted
+// with the Jacobians, one GEMM problem per inner molecule m.  This costs
+// 2 rep 3 n_m per (o, j) instead of per atom pair.  The transposed Jacobian
 // (src/local_kernels.cpp:991-1166) is the same contraction with the roles of
 // the sets swapped, negated and written transposed.
 //
@@ -36,51 +37,287 @@ kfb_status blas_for_stream(cudaStream_t s, cublasHandle_t *out);
 namespace {
 
 // --------------------------------------------------------- Jacobian: v rows
-// One warp per (outer molecule o in [o0, o0+no), inner active atom u):
 //   V[(o - o0) * NU + u, :] = sum_{i in o, q_i = q_u} w_iu (x_i - x_u)
+//                           = sum_i w_iu x_i - (sum_i w_iu) x_u,
+//   w_iu = exp(-|x_i - x_u|^2 / (2 sigma^2)) / sigma^2,
+//   |x_i - x_u|^2 = |x_i|^2 + |x_u|^2 - 2 x_i . x_u (the dot products come
+//   from one GEMM per label; the clamp at 0 absorbs rounding).
+// Both atom sets are gathered label-major: inner atoms in sorted order su
+// (runs [lab_start[l], lab_start[l+1])), outer atoms by (label, molecule),
+// orng[o * nlab + l] = (first sorted row, count) of molecule o's label-l atoms.
+
+// dst[r] = src[idx[r]] (rows of rep), norm[r] = |dst[r]|^2, *amax = max |dst|.
 template <class T>
-__global__ void jac_v_kernel(const T *__restrict__ xo, const int *__restrict__ qo,
-                             const int *__restrict__ no, int mao, int o0, int nout,
-                             const T *__restrict__ xi, const int *__restrict__ u_src,
-                             const int *__restrict__ u_lab, int NU, int rep, T c2, T is2,
-                             T *__restrict__ V) {
-    extern __shared__ unsigned char wsm_raw[];
-    T *wsm = reinterpret_cast<T *>(wsm_raw);
-    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + wib;
-    if (gw >= (long long)nout * NU) return;
-    const int ol = (int)(gw / NU), u = (int)(gw - (long long)ol * NU);
-    const int o = o0 + ol;
-    T *w = wsm + wib * mao;
-    const T *xu = xi + (size_t)u_src[u] * rep;
-    const int lab = u_lab[u];
-    const int na = min(max(no[o], 0), mao);
-    for (int i = 0; i < na; ++i) {
-        T wi = T(0);
-        if (qo[(size_t)o * mao + i] == lab) {
-            const T *xa = xo + ((size_t)o * mao + i) * rep;
-            T s = T(0);
-            for (int k = lane; k < rep; k += 32) {
-                const T d = xa[k] - xu[k];
-                s = fma(d, d, s);
-            }
-            for (int off = 16; off; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-            wi = kexp<T>(c2 * s) * is2;
-        }
-        if (lane == 0) w[i] = wi;
+__global__ void gather_rows_norm_kernel(const T *__restrict__ src, const int *__restrict__ idx,
+                                        int n, int rep, T *__restrict__ dst, T *__restrict__ norm,
+                                        float *amax) {
+    const int r = blockIdx.x;
+    if (r >= n) return;
+    const T *s = src + (size_t)idx[r] * rep;
+    T *d = dst + (size_t)r * rep;
+    T acc = T(0);
+    float m = 0.f;
+    for (int k = threadIdx.x; k < rep; k += blockDim.x) {
+        const T v = s[k];
+        d[k] = v;
+        acc = fma(v, v, acc);
+        m = fmaxf(m, fabsf((float)v));
     }
-    __syncwarp();
-    T *vrow = V + ((size_t)ol * NU + u) * rep;
-    for (int k = lane; k < rep; k += 32) {
-        const T xuk = xu[k];
-        T acc = T(0);
-        for (int i = 0; i < na; ++i) {
-            const T wi = w[i];
-            if (wi != T(0)) acc = fma(wi, xo[((size_t)o * mao + i) * rep + k] - xuk, acc);
+    __shared__ T red[8];
+    __shared__ float redm[8];
+    for (int o = 16; o; o >>= 1) {
+        acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    }
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        red[w] = acc;
+        redm[w] = m;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        T t = T(0);
+        float mm = 0.f;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
+            t += red[i];
+            mm = fmaxf(mm, redm[i]);
         }
-        vrow[k] = acc;
+        norm[r] = t;
+        // non-negative floats order like their bit patterns
+        atomicMax(reinterpret_cast<int *>(amax), __float_as_int(mm));
     }
 }
+
+// hi/lo[r][k] = fp16 pair of src[r][k] * scale for k < rep, zero for
+// rep <= k < kpad (K-major operands of the tensor-core dot products).
+template <class T>
+__global__ void split_pad_rows_kernel(const T *__restrict__ src, int rep, int kpad, float scale,
+                                      __half *__restrict__ hi, __half *__restrict__ lo) {
+    const size_t r = blockIdx.x;
+    for (int k = threadIdx.x; k < kpad; k += blockDim.x) {
+        const float v = k < rep ? (float)src[r * rep + k] * scale : 0.f;
+        const __half h = __float2half_rn(v);
+        hi[r * kpad + k] = h;
+        lo[r * kpad + k] = __float2half_rn(v - __half2float(h));
+    }
+}
+
+// Block per (outer molecule o = blockIdx.x, tile of up to JV_U sorted inner
+// atoms of one label = blockIdx.y; consecutive blocks share the tile, whose
+// rows then come from L2): 256 threads, each a 4 (atoms u) x 4 (consecutive
+// k) register tile of a 64-wide pass over rep.  The block's weights
+// (ns x JV_U, pre-multiplied by the output scale) and a slice of ks columns
+// of o's label-l rows (ns x ks, ks a multiple of 64) sit in shared memory.
+// Tiles of a label that o lacks write zero rows.  SPLIT writes the rows as
+// the scaled fp16 pair (hi, lo) of the tensor-core contraction instead of T.
+constexpr int JV_U = 64, JV_K = 64, JV_THREADS = 256;
+
+template <class T>
+__device__ __forceinline__ void ld4(const T *p, T (&v)[4]) {
+    if constexpr (sizeof(T) == 4) {
+        const float4 q = *reinterpret_cast<const float4 *>(p);
+        v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+    } else {
+        const double2 a = *reinterpret_cast<const double2 *>(p);
+        const double2 b = *reinterpret_cast<const double2 *>(p + 2);
+        v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+    }
+}
+
+template <class T>
+__device__ __forceinline__ void st4(T *p, const T (&v)[4]) {
+    if constexpr (sizeof(T) == 4) {
+        *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+    } else {
+        reinterpret_cast<double2 *>(p)[0] = make_double2(v[0], v[1]);
+        reinterpret_cast<double2 *>(p)[1] = make_double2(v[2], v[3]);
+    }
+}
+
+// (hi, lo) fp16 pairs of two values, hi = fp16(a), lo = fp16(a - hi)
+__device__ __forceinline__ void split2(float a, float b, __half2 &hi, __half2 &lo) {
+    hi = __floats2half2_rn(a, b);
+    const float2 back = __half22float2(hi);
+    lo = __floats2half2_rn(a - back.x, b - back.y);
+}
+
+template <class T, bool SPLIT>
+__global__ void __launch_bounds__(JV_THREADS, sizeof(T) == 4 ? 3 : 2) jac_v_kernel(
+    const int4 *__restrict__ tiles, const int2 *__restrict__ orng, int nlab, int o0,
+    const long long *__restrict__ cinfo,
+    const T *__restrict__ xo_s, const T *__restrict__ no_s, const T *__restrict__ xi_s,
+    const T *__restrict__ ni_s, const T *__restrict__ D, const int *__restrict__ u_sorted,
+    int NU, int rep, int lg_ks, T c2, T is2, T *__restrict__ V, __half *__restrict__ vh,
+    __half *__restrict__ vl) {
+    extern __shared__ __align__(16) unsigned char jv_raw[];
+    const int4 tl = tiles[blockIdx.y];
+    const int l = tl.x, u0 = tl.y, nu = tl.z - tl.y;
+    const int ol = blockIdx.x;
+    const int2 rg = orng[(size_t)(o0 + ol) * nlab + l];
+    const int ns = rg.y;
+    const int t = threadIdx.x;
+    const bool vec = (rep & 3) == 0;
+    if (ns == 0) {
+        // o has no atom of this label: zero rows
+        for (int uu = t >> 4; uu < nu; uu += JV_THREADS / 16) {
+            const size_t row = ((size_t)ol * NU + u_sorted[u0 + uu]) * rep;
+            for (int k = 4 * (t & 15); k < rep; k += 64) {
+                if (vec) {
+                    if constexpr (SPLIT) {
+                        *reinterpret_cast<uint2 *>(vh + row + k) = make_uint2(0u, 0u);
+                        *reinterpret_cast<uint2 *>(vl + row + k) = make_uint2(0u, 0u);
+                    } else {
+                        const T z[4] = {T(0), T(0), T(0), T(0)};
+                        st4(V + row + k, z);
+                    }
+                } else {
+                    for (int b = 0; b < 4 && k + b < rep; ++b) {
+                        if constexpr (SPLIT) {
+                            vh[row + k + b] = __float2half_rn(0.f);
+                            vl[row + k + b] = __float2half_rn(0.f);
+                        } else {
+                            V[row + k + b] = T(0);
+                        }
+                    }
+                }
+            }
+        }
+        return;
+    }
+    const int ks = 1 << lg_ks;
+    T *ws = reinterpret_cast<T *>(jv_raw);   // [ns][JV_U] weights
+    T *xs = ws + (size_t)ns * JV_U;          // [ns][ks] slice of o's label-l rows
+    T *wsum = xs + (size_t)ns * ks;          // [JV_U]
+    {
+        // dot products x_out . x_in: row (label block cinfo[l] + outer row offset),
+        // column su, row stride NU
+        const T *Dl = D + cinfo[l] + (long long)(rg.x - cinfo[nlab + l]) * NU + u0;
+        for (int e = t; e < ns * JV_U; e += JV_THREADS) {
+            const int r = e / JV_U, uu = e - r * JV_U;
+            T w = T(0);
+            if (uu < nu) {
+                const T d2 = no_s[rg.x + r] + ni_s[u0 + uu] - T(2) * Dl[(size_t)r * NU + uu];
+                w = kexp<T>(c2 * (d2 > T(0) ? d2 : T(0))) * is2;
+            }
+            ws[e] = w;
+        }
+        __syncthreads();
+        if (t < JV_U) {
+            T sum = T(0);
+            for (int r = 0; r < ns; ++r) sum += ws[r * JV_U + t];
+            wsum[t] = sum;
+        }
+        __syncthreads();
+    }
+    const int ug = t >> 4, kl = t & 15;   // atoms 4 ug .. 4 ug + 3, k = k0 + 4 kl ..
+    // this thread's output rows and weight sums
+    int urow[4];
+    T sws[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const int uu = 4 * ug + a;
+        urow[a] = uu < nu ? u_sorted[u0 + uu] : 0;
+        sws[a] = wsum[uu];
+    }
+    for (int s0 = 0; s0 < rep; s0 += ks) {
+        if (s0 > 0) __syncthreads();   // previous slice consumed
+        for (int e = t; e < (ns << lg_ks); e += JV_THREADS) {
+            const int r = e >> lg_ks, kk = e & (ks - 1);
+            xs[e] = (s0 + kk < rep) ? xo_s[(size_t)(rg.x + r) * rep + s0 + kk] : T(0);
+        }
+        __syncthreads();
+        for (int kp = 0; kp < ks && s0 + kp < rep; kp += JV_K) {
+            const int k = s0 + kp + 4 * kl;
+            const bool full = vec && k + 3 < rep;
+            // x_u of the epilogue, loaded ahead of the accumulation
+            T xuv[4][4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                const int uu = 4 * ug + a;
+                const T *xu = xi_s + (size_t)(u0 + uu) * rep + k;
+                if (uu < nu && full) {
+                    ld4(xu, xuv[a]);
+                } else {
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) xuv[a][b] = (uu < nu && k + b < rep) ? xu[b] : T(0);
+                }
+            }
+            T acc[4][4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) acc[a][b] = T(0);
+            const T *xr = xs + kp + 4 * kl;
+            const T *wr = ws + 4 * ug;
+            for (int r = 0; r < ns; ++r) {
+                T xv[4], wv[4];
+                ld4(xr + (size_t)r * ks, xv);
+                ld4(wr + r * JV_U, wv);
+#pragma unroll
+                for (int a = 0; a < 4; ++a)
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) acc[a][b] = fma(wv[a], xv[b], acc[a][b]);
+            }
+            if (k >= rep) continue;
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                const int uu = 4 * ug + a;
+                if (uu >= nu) continue;
+                const size_t row = ((size_t)ol * NU + urow[a]) * rep;
+                T v[4];
+#pragma unroll
+                for (int b = 0; b < 4; ++b) v[b] = fma(-sws[a], xuv[a][b], acc[a][b]);
+                if constexpr (SPLIT) {
+                    __half2 h01, l01, h23, l23;
+                    split2((float)v[0], (float)v[1], h01, l01);
+                    split2((float)v[2], (float)v[3], h23, l23);
+                    if (full) {
+                        uint2 hv, lv;
+                        hv.x = *reinterpret_cast<const unsigned *>(&h01);
+                        hv.y = *reinterpret_cast<const unsigned *>(&h23);
+                        lv.x = *reinterpret_cast<const unsigned *>(&l01);
+                        lv.y = *reinterpret_cast<const unsigned *>(&l23);
+                        *reinterpret_cast<uint2 *>(vh + row + k) = hv;
+                        *reinterpret_cast<uint2 *>(vl + row + k) = lv;
+                    } else {
+                        const __half hh[4] = {__low2half(h01), __high2half(h01), __low2half(h23),
+                                              __high2half(h23)};
+                        const __half ll[4] = {__low2half(l01), __high2half(l01), __low2half(l23),
+                                              __high2half(l23)};
+                        for (int b = 0; b < 4 && k + b < rep; ++b) {
+                            vh[row + k + b] = hh[b];
+                            vl[row + k + b] = ll[b];
+                        }
+                    }
+                } else {
+                    if (full) {
+                        st4(V + row + k, v);
+                    } else {
+                        for (int b = 0; b < 4 && k + b < rep; ++b) V[row + k + b] = v[b];
+                    }
+                }
+            }
+        }
+    }
+}
+
+template <class T> struct BlasGemm;
+template <> struct BlasGemm<float> {
+    static cublasStatus_t run(cublasHandle_t h, cublasOperation_t ta, cublasOperation_t tb, int m,
+                              int n, int k, const float *A, int lda, const float *B, int ldb,
+                              float *C, int ldc) {
+        const float one = 1.f, zero = 0.f;
+        return cublasSgemm(h, ta, tb, m, n, k, &one, A, lda, B, ldb, &zero, C, ldc);
+    }
+};
+template <> struct BlasGemm<double> {
+    static cublasStatus_t run(cublasHandle_t h, cublasOperation_t ta, cublasOperation_t tb, int m,
+                              int n, int k, const double *A, int lda, const double *B, int ldb,
+                              double *C, int ldc) {
+        const double one = 1.0, zero = 0.0;
+        return cublasDgemm(h, ta, tb, m, n, k, &one, A, lda, B, ldb, &zero, C, ldc);
+    }
+};
 
 // Label groups of a molecule pair: for each run [x, y) of equal labels in a's
 // label order, the run [z, w) of the same label in b's (empty when b lacks
@@ -772,21 +1009,127 @@ kfb_status jacobian_core(const DerivSet &outer, const DerivSet &inner, int rep, 
     }
     u_first[inner.v.nm] = (int)u_src.size();
     const int NU = (int)u_src.size();
-    if (NU == 0 || outer.v.nm == 0) return KFB_OK;
-    DevBuf d_usrc, d_ulab, d_qo, d_no;
-    KFB_TRY(upload(d_usrc, u_src, s));
-    KFB_TRY(upload(d_ulab, u_lab, s));
-    std::vector<int> qo(outer.v.q, outer.v.q + (size_t)outer.v.nm * outer.v.ma);
-    std::vector<int> no(outer.v.n, outer.v.n + outer.v.nm);
-    KFB_TRY(upload(d_qo, qo, s));
-    KFB_TRY(upload(d_no, no, s));
-    const size_t row_bytes = (size_t)NU * rep * (sizeof(T) + (tc ? 2 * sizeof(__half) : 0));
-    int chunk = (int)std::max<size_t>(1, budget_bytes() / std::max<size_t>(row_bytes, 1));
-    chunk = std::min(chunk, outer.v.nm);
-    DevBuf V, vh, vl, jth, jtl;
-    float jt_scale = 1.f;
-    KFB_TRY(V.alloc((size_t)chunk * NU * rep * sizeof(T), s));
+    const int nmo = outer.v.nm;
+    if (NU == 0 || nmo == 0) return KFB_OK;
+    // inner atoms sorted by label (runs lab_start), outer atoms by (label, molecule)
+    std::vector<int> labs(u_lab);
+    std::sort(labs.begin(), labs.end());
+    labs.erase(std::unique(labs.begin(), labs.end()), labs.end());
+    const int nlab = (int)labs.size();
+    std::vector<int> u_sorted(NU);
+    std::iota(u_sorted.begin(), u_sorted.end(), 0);
+    std::stable_sort(u_sorted.begin(), u_sorted.end(),
+                     [&](int a, int b) { return u_lab[a] < u_lab[b]; });
+    std::vector<int> lab_start(nlab + 1, 0), in_rows(NU);
+    for (int l = 0, u = 0; l < nlab; ++l) {
+        lab_start[l] = u;
+        while (u < NU && u_lab[u_sorted[u]] == labs[l]) ++u;
+        lab_start[l + 1] = u;
+    }
+    for (int su = 0; su < NU; ++su) in_rows[su] = u_src[u_sorted[su]];
+    std::vector<int> out_rows;
+    std::vector<int2> orng((size_t)nmo * nlab);
+    std::vector<int> out_lab_start(nlab + 1);
+    int ns_max = 0;
+    for (int l = 0; l < nlab; ++l) {
+        out_lab_start[l] = (int)out_rows.size();
+        for (int o = 0; o < nmo; ++o) {
+            const int start = (int)out_rows.size();
+            for (int i = 0; i < outer.v.natoms(o); ++i)
+                if (outer.v.q[(size_t)o * outer.v.ma + i] == labs[l])
+                    out_rows.push_back(o * outer.v.ma + i);
+            const int cnt = (int)out_rows.size() - start;
+            orng[(size_t)o * nlab + l] = make_int2(start, cnt);
+            ns_max = std::max(ns_max, cnt);
+        }
+    }
+    out_lab_start[nlab] = (int)out_rows.size();
+    const int NO = (int)out_rows.size();
+    // slice width of the staged outer rows: wide (fewer barriers) while the
+    // block stays small enough for several blocks per SM
+    int jv_lg = 8;   // 256 columns
+    auto jv_bytes = [&](int lg) { return ((size_t)ns_max * (JV_U + (1 << lg)) + JV_U) * sizeof(T); };
+    while (jv_lg > 6 && jv_bytes(jv_lg) > 72 * 1024) --jv_lg;
+    const size_t jv_smem = jv_bytes(jv_lg);
+    if (jv_smem > 200 * 1024)
+        return set_error(KFB_ERR_INVALID_ARG, "%d atoms of one element in a molecule: too many "
+                         "for the Jacobian kernel", ns_max);
+    if (jv_smem > 48 * 1024) {
+        KFB_CUDA_TRY(cudaFuncSetAttribute(jac_v_kernel<T, true>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)jv_smem));
+        KFB_CUDA_TRY(cudaFuncSetAttribute(jac_v_kernel<T, false>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)jv_smem));
+    }
+    // tiles of up to JV_U sorted inner atoms within one label
+    std::vector<int4> tiles;
+    for (int l = 0; l < nlab; ++l)
+        for (int u0 = lab_start[l]; u0 < lab_start[l + 1]; u0 += JV_U)
+            tiles.push_back(make_int4(l, u0, std::min(u0 + JV_U, lab_start[l + 1]), 0));
+    if (tiles.size() > 65535)
+        return set_error(KFB_ERR_INVALID_ARG, "%d inner atoms: too many for one Jacobian call", NU);
+    // gathered rows, norms and max |x|
+    DevBuf d_inrows, d_outrows, d_orng, d_usorted, d_tiles, amax, xi_s, ni_s, xo_s, no_s;
+    KFB_TRY(upload(d_inrows, in_rows, s));
+    KFB_TRY(upload(d_outrows, out_rows, s));
+    KFB_TRY(upload(d_orng, orng, s));
+    KFB_TRY(upload(d_usorted, u_sorted, s));
+    KFB_TRY(upload(d_tiles, tiles, s));
+    KFB_TRY(amax.alloc(2 * sizeof(float), s));
+    KFB_TRY(zero(amax.ptr, 2 * sizeof(float), s));
+    KFB_TRY(xi_s.alloc((size_t)NU * rep * sizeof(T), s));
+    KFB_TRY(ni_s.alloc((size_t)NU * sizeof(T), s));
+    KFB_TRY(xo_s.alloc(((size_t)NO * rep + 1) * sizeof(T), s));
+    KFB_TRY(no_s.alloc(((size_t)NO + 1) * sizeof(T), s));
+    {
+        TraceScope tr("jacobian:gather", s);
+        gather_rows_norm_kernel<T><<<NU, 256, 0, s>>>(static_cast<const T *>(inner.x),
+                                                      d_inrows.as<int>(), NU, rep, xi_s.as<T>(),
+                                                      ni_s.as<T>(), amax.as<float>());
+        KFB_CUDA_TRY(cudaGetLastError());
+        if (NO > 0) {
+            gather_rows_norm_kernel<T><<<NO, 256, 0, s>>>(
+                static_cast<const T *>(outer.x), d_outrows.as<int>(), NO, rep, xo_s.as<T>(),
+                no_s.as<T>(), amax.as<float>() + 1);
+            KFB_CUDA_TRY(cudaGetLastError());
+        }
+    }
+    // outer molecules per chunk: the v rows of a chunk (T, or the fp16 pair)
+    // stay resident for its contraction
+    const size_t row_bytes = (size_t)NU * rep * (tc ? 2 * sizeof(__half) : sizeof(T));
+    size_t budget = budget_bytes();
+    if (!getenv("KFB_WORKSPACE_GB")) {
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) == cudaSuccess)
+            budget = std::max(budget, std::min<size_t>(fr / 4, (size_t)16 << 30));
+    }
+    int chunk = (int)std::max<size_t>(1, budget / std::max<size_t>(row_bytes, 1));
+    chunk = std::min(chunk, nmo);
+    if (tc && chunk > 128) chunk -= chunk % 128;   // whole 128-row MMA tiles
+    // dot products of a chunk: a row per matched outer atom (label blocks one
+    // after the other), a column per sorted inner atom; only the label-diagonal
+    // blocks are formed and read
+    size_t d_elems = 1;
+    for (int o0 = 0; o0 < nmo; o0 += chunk) {
+        const int o1 = std::min(nmo, o0 + chunk);
+        size_t rows = 0;
+        for (int l = 0; l < nlab; ++l) {
+            const int r0 = orng[(size_t)o0 * nlab + l].x;
+            const int r1 = o1 < nmo ? orng[(size_t)o1 * nlab + l].x : out_lab_start[l + 1];
+            rows += (size_t)(r1 - r0);
+        }
+        d_elems = std::max(d_elems, rows * (size_t)NU);
+    }
+    // tensor-core dot products (FP32 inputs): K-major split copies of both sets
+    const bool tc_dots = tc && sizeof(T) == 4 && NO > 0;
+    const int kpad = (rep + 15) / 16 * 16;
+    float xi_scale = 1.f, xo_scale = 1.f;
+    DevBuf V, vh, vl, jth, jtl, Dd, d_cinfo, xih, xil, xoh, xol;
+    KFB_TRY(Dd.alloc(d_elems * sizeof(T), s));
+    float jt_scale = 1.f, v_scale = 1.f;
     const int ma_in = inner.v.ma;
+    const T c2 = T(-1.0 / (2.0 * sigma * sigma)), is2 = T(1.0 / (sigma * sigma));
     if (tc) {
         // inner Jacobians as K-major split rows: Jt[(m, c)][(j, k)]
         const size_t jt_elems = (size_t)inner.v.nm * 3 * ma_in * ma_in * rep;
@@ -796,28 +1139,120 @@ kfb_status jacobian_core(const DerivSet &outer, const DerivSet &inner, int rep, 
         for (int m = 0; m < inner.v.nm; ++m) nin[m] = inner.v.natoms(m);
         DevBuf d_nin;
         KFB_TRY(upload(d_nin, nin, s));
+        TraceScope tr("jacobian:split_dx", s);
         KFB_TRY(transpose_split_dx<T>(static_cast<const T *>(inner.dx), inner.v.nm, ma_in, rep,
                                       d_nin.as<int>(), jth.as<__half>(), jtl.as<__half>(),
                                       &jt_scale, s));
         KFB_TRY(vh.alloc((size_t)chunk * NU * rep * sizeof(__half), s));
         KFB_TRY(vl.alloc((size_t)chunk * NU * rep * sizeof(__half), s));
+        // |v| <= (sum_i w_iu) (max|x_out| + max|x_in|) <= ns_max / sigma^2 (...)
+        float am[2] = {0.f, 0.f};
+        KFB_CUDA_TRY(cudaMemcpyAsync(am, amax.ptr, sizeof(am), cudaMemcpyDeviceToHost, s));
+        KFB_CUDA_TRY(cudaStreamSynchronize(s));
+        const double bound = (double)ns_max / (sigma * sigma) * ((double)am[0] + (double)am[1]);
+        auto pow2_for = [](double mx) {
+            return (mx > 0.0 && std::isfinite(mx))
+                       ? (float)std::ldexp(1.0, 14 - (int)std::ceil(std::log2(mx)))
+                       : 1.f;
+        };
+        v_scale = pow2_for(bound);
+        if (tc_dots) {
+            xi_scale = pow2_for(am[0]);
+            xo_scale = pow2_for(am[1]);
+            KFB_TRY(xih.alloc((size_t)NU * kpad * sizeof(__half), s));
+            KFB_TRY(xil.alloc((size_t)NU * kpad * sizeof(__half), s));
+            KFB_TRY(xoh.alloc((size_t)NO * kpad * sizeof(__half), s));
+            KFB_TRY(xol.alloc((size_t)NO * kpad * sizeof(__half), s));
+            split_pad_rows_kernel<T><<<NU, 128, 0, s>>>(xi_s.as<T>(), rep, kpad, xi_scale,
+                                                        xih.as<__half>(), xil.as<__half>());
+            KFB_CUDA_TRY(cudaGetLastError());
+            split_pad_rows_kernel<T><<<NO, 128, 0, s>>>(xo_s.as<T>(), rep, kpad, xo_scale,
+                                                        xoh.as<__half>(), xol.as<__half>());
+            KFB_CUDA_TRY(cudaGetLastError());
+        }
+    } else {
+        KFB_TRY(V.alloc((size_t)chunk * NU * rep * sizeof(T), s));
     }
-    const T c2 = T(-1.0 / (2.0 * sigma * sigma)), is2 = T(1.0 / (sigma * sigma));
+    cublasHandle_t h = nullptr;
+    KFB_TRY(blas_for_stream(s, &h));
     const int ld_in = 3 * inner.v.ma;
-    for (int o0 = 0; o0 < outer.v.nm; o0 += chunk) {
-        const int nout = std::min(chunk, outer.v.nm - o0);
-        const long long nwarps = (long long)nout * NU;
-        const int wpb = 8;
-        jac_v_kernel<T><<<(unsigned)((nwarps + wpb - 1) / wpb), wpb * 32,
-                          wpb * outer.v.ma * sizeof(T), s>>>(
-            static_cast<const T *>(outer.x), d_qo.as<int>(), d_no.as<int>(), outer.v.ma, o0,
-            nout, static_cast<const T *>(inner.x), d_usrc.as<int>(), d_ulab.as<int>(), NU, rep,
-            c2, is2, V.as<T>());
-        KFB_CUDA_TRY(cudaGetLastError());
+    std::vector<long long> cinfo(2 * nlab);
+    for (int o0 = 0; o0 < nmo; o0 += chunk) {
+        const int nout = std::min(chunk, nmo - o0);
+        const int o1 = o0 + nout;
+        {
+            TraceScope tr_d("jacobian:dots", s);
+            int drow = 0;
+            std::vector<TcProb> dprobs;
+            for (int l = 0; l < nlab; ++l) {
+                const int r0 = orng[(size_t)o0 * nlab + l].x;
+                const int r1 = o1 < nmo ? orng[(size_t)o1 * nlab + l].x : out_lab_start[l + 1];
+                const int nin = lab_start[l + 1] - lab_start[l];
+                cinfo[l] = (long long)drow * NU;
+                cinfo[nlab + l] = r0;
+                if (r1 > r0 && nin > 0) {
+                    // D[drow + i][lab_start[l] + u] = x_out[r0 + i] . x_in[lab_start[l] + u]
+                    if (tc_dots) {
+                        TcProb p{};
+                        p.a_row0 = r0;
+                        p.b_row0 = lab_start[l];
+                        p.M = r1 - r0;
+                        p.N = nin;
+                        p.K = kpad;
+                        p.row_off = drow;
+                        p.col_off = lab_start[l];
+                        p.alpha = 1.0 / ((double)xo_scale * (double)xi_scale);
+                        dprobs.push_back(p);
+                    } else {
+                        const cublasStatus_t st = BlasGemm<T>::run(
+                            h, CUBLAS_OP_T, CUBLAS_OP_N, nin, r1 - r0, rep,
+                            xi_s.as<T>() + (size_t)lab_start[l] * rep, rep,
+                            xo_s.as<T>() + (size_t)r0 * rep, rep,
+                            Dd.as<T>() + (size_t)drow * NU + lab_start[l], NU);
+                        if (st != CUBLAS_STATUS_SUCCESS)
+                            return set_error(KFB_ERR_CUDA,
+                                             "dot-product GEMM failed: cublas status %d", (int)st);
+                    }
+                }
+                drow += r1 - r0;
+            }
+            if (!dprobs.empty()) {
+                TcOperand A, B;
+                A.hi = xoh.ptr;
+                A.lo = xol.ptr;
+                A.rows = NO;
+                A.cols = kpad;
+                B.hi = xih.ptr;
+                B.lo = xil.ptr;
+                B.rows = NU;
+                B.cols = kpad;
+                TcEpi epi;
+                epi.mode = EPI_DENSE;
+                epi.zf32 = reinterpret_cast<float *>(Dd.ptr);
+                epi.ld = NU;
+                KFB_TRY(tc_gemm_grouped(A, B, 3, false, dprobs, ElemSink(), s, epi));
+            }
+            KFB_TRY(upload(d_cinfo, cinfo, s));
+        }
+        {
+            TraceScope tr_v("jacobian:v", s);
+            const dim3 grid((unsigned)nout, (unsigned)tiles.size());
+            if (tc)
+                jac_v_kernel<T, true><<<grid, JV_THREADS, jv_smem, s>>>(
+                    d_tiles.as<int4>(), d_orng.as<int2>(), nlab, o0, d_cinfo.as<long long>(),
+                    xo_s.as<T>(), no_s.as<T>(), xi_s.as<T>(), ni_s.as<T>(),
+                    Dd.as<T>(), d_usorted.as<int>(), NU, rep, jv_lg, c2, T(is2 * (T)v_scale),
+                    nullptr, vh.as<__half>(), vl.as<__half>());
+            else
+                jac_v_kernel<T, false><<<grid, JV_THREADS, jv_smem, s>>>(
+                    d_tiles.as<int4>(), d_orng.as<int2>(), nlab, o0, d_cinfo.as<long long>(),
+                    xo_s.as<T>(), no_s.as<T>(), xi_s.as<T>(), ni_s.as<T>(),
+                    Dd.as<T>(), d_usorted.as<int>(), NU, rep, jv_lg, c2, is2, V.as<T>(), nullptr,
+                    nullptr);
+            KFB_CUDA_TRY(cudaGetLastError());
+        }
+        TraceScope tr_c("jacobian:gemm", s);
         if (tc) {
-            float v_scale = 1.f;
-            KFB_TRY(split_rows<T>(V.as<T>(), (long long)nout * NU * rep, vh.as<__half>(),
-                                  vl.as<__half>(), &v_scale, s));
             std::vector<TcProb> tprobs;
             for (int m = 0; m < inner.v.nm; ++m) {
                 const int nb = inner.v.natoms(m);

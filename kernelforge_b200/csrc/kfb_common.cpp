@@ -28,7 +28,9 @@ const char *last_error() { return g_last_error.c_str(); }
 // The device's default memory pool returns unused memory to the driver at every
 // synchronisation unless told otherwise; the solves synchronise between
 // iterations, so their scratch (hundreds of MB) would be unmapped and mapped
-// again on every call.  Keep up to KFB_POOL_KEEP_GB (default 16) GB in the pool.
+// again on every call, and the derivative kernels' chunk buffers (tens of GB on
+// a 180 GB device) would be remapped per call.  Keep up to KFB_POOL_KEEP_GB
+// (default 64) GB in the pool.
 static void keep_pool_memory() {
     static std::mutex mu;
     static bool done[64] = {};
@@ -38,7 +40,7 @@ static void keep_pool_memory() {
     if (done[dev]) return;
     done[dev] = true;
     const char *v = std::getenv("KFB_POOL_KEEP_GB");
-    const double gb = v ? std::atof(v) : 16.0;
+    const double gb = v ? std::atof(v) : 64.0;
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) {
         (void)cudaGetLastError();

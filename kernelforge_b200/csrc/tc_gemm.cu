@@ -522,13 +522,13 @@ __global__ void absmax_dx_kernel(const T *__restrict__ dx, int ma, int rep,
     const int ld = 3 * ma, nc = 3 * na;
     const long long n = (long long)na * rep * nc;
     const T *base = dx + (size_t)m * ma * rep * ld;
+    // warp per row (j, k), lanes over its 3 na columns
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const long long nrow = n / (nc > 0 ? nc : 1);
     float v = 0.f;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x) {
-        const long long row = i / nc;
-        const int c = (int)(i - row * nc);
-        v = fmaxf(v, fabsf((float)base[row * ld + c]));
-    }
+    for (long long row = (long long)blockIdx.x * nw + (threadIdx.x >> 5); row < nrow;
+         row += (long long)gridDim.x * nw)
+        for (int c = lane; c < nc; c += 32) v = fmaxf(v, fabsf((float)base[row * ld + c]));
     for (int o = 16; o; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
     if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<int *>(out), __float_as_int(v));
 }
@@ -545,11 +545,13 @@ __global__ void split_rows_kernel(const T *__restrict__ src, long long n, float 
     }
 }
 
-// Jt[(m, c)][(j, k)] = dX[m][j][k][c] for c < 3 ma (zero rows and columns
-// beyond the molecule's atoms are copied as they are: the padding is zero).
-// Tiles of 32 (j,k) x 32 c through shared memory.
+// Jt[(m, c)][(j, k)] = dX[m][j][k][c].  Tiles of 32 (j,k) x 32 c through
+// shared memory; tiles wholly beyond the molecule's atoms (j >= nat[m] or
+// c >= 3 nat[m]) are skipped: the GEMMs read (j, k) < nat rep only, and rows
+// c >= 3 nat only feed output columns they discard.
 template <class T>
-__global__ void transpose_split_dx_kernel(const T *__restrict__ dx, int ma, int rep, float scale,
+__global__ void transpose_split_dx_kernel(const T *__restrict__ dx, int ma, int rep,
+                                          const int *__restrict__ nat, float scale,
                                           __half *__restrict__ hi, __half *__restrict__ lo) {
     __shared__ float tile[32][33];
     const int m = blockIdx.z;
@@ -557,6 +559,8 @@ __global__ void transpose_split_dx_kernel(const T *__restrict__ dx, int ma, int 
     const long long kk_total = (long long)ma * rep;
     const long long kk0 = (long long)blockIdx.x * 32;
     const int c0 = blockIdx.y * 32;
+    const int na = min(max(nat[m], 0), ma);
+    if (kk0 >= (long long)na * rep || c0 >= 3 * na) return;
     const T *base = dx + (size_t)m * kk_total * ld;
     for (int r = threadIdx.y; r < 32; r += blockDim.y) {
         const long long kk = kk0 + r;
@@ -672,7 +676,7 @@ kfb_status transpose_split_dx(const T *dx, int nm, int ma, int rep, const int *n
         KFB_TRY(pow2_from_device(d.as<float>(), s, scale));
     }
     dim3 grid((unsigned)((kk + 31) / 32), (unsigned)((3 * ma + 31) / 32), (unsigned)nm);
-    transpose_split_dx_kernel<T><<<grid, dim3(32, 8), 0, s>>>(dx, ma, rep, *scale, hi, lo);
+    transpose_split_dx_kernel<T><<<grid, dim3(32, 8), 0, s>>>(dx, ma, rep, nat, *scale, hi, lo);
     KFB_CUDA_TRY(cudaGetLastError());
     return KFB_OK;
 }

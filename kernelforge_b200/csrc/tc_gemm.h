@@ -84,7 +84,8 @@ kfb_status tc_gemm_grouped(const TcOperand &A, const TcOperand &B, int nprod, bo
 // the two operands' scales.
 //   split_rows:         every entry of src is read;
 //   transpose_split_dx: nat (device int32, per molecule) limits the scale to
-//                       the real atoms, padding may hold anything;
+//                       the real atoms, padding may hold anything; 32 x 32
+//                       tiles wholly beyond the real atoms stay unwritten;
 //   transpose_split_y:  amax (device float) is the largest |entry| the
 //                       producer wrote (the rest of Y is never read).
 template <class T>
