@@ -25,7 +25,7 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 
 SOURCES = ["kfb_common.cpp", "scalar_simt.cu", "scalar_tc.cu", "derivs.cu", "solve.cu",
            "capi.cu", "scalar_noalloc.cu", "tc_gemm.cu", "features.cu",
-           "matvec.cu", "repr.cu"]
+           "matvec.cu", "repr.cu", "trsv.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
          "-fvisibility=hidden", "--expt-relaxed-constexpr", "-I", INCLUDE, "-I", CSRC]

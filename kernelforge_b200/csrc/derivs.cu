@@ -210,15 +210,17 @@ __global__ void __launch_bounds__(JV_THREADS, sizeof(T) == 4 ? 3 : 2) jac_v_kern
         __syncthreads();
     }
     const int ug = t >> 4, kl = t & 15;   // atoms 4 ug .. 4 ug + 3, k = k0 + 4 kl ..
-    // this thread's output rows and weight sums
-    int urow[4];
+    // this thread's output rows, x_u rows and weight sums
+    size_t orow[4];
     T sws[4];
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
         const int uu = 4 * ug + a;
-        urow[a] = uu < nu ? u_sorted[u0 + uu] : 0;
+        orow[a] = ((size_t)ol * NU + (uu < nu ? u_sorted[u0 + uu] : 0)) * rep;
         sws[a] = wsum[uu];
     }
+    const T *xu0 = xi_s + (size_t)(u0 + 4 * ug) * rep;
+    const int nu_t = min(max(nu - 4 * ug, 0), 4);   // rows of this thread in the tile
     for (int s0 = 0; s0 < rep; s0 += ks) {
         if (s0 > 0) __syncthreads();   // previous slice consumed
         for (int e = t; e < (ns << lg_ks); e += JV_THREADS) {
@@ -233,13 +235,12 @@ __global__ void __launch_bounds__(JV_THREADS, sizeof(T) == 4 ? 3 : 2) jac_v_kern
             T xuv[4][4];
 #pragma unroll
             for (int a = 0; a < 4; ++a) {
-                const int uu = 4 * ug + a;
-                const T *xu = xi_s + (size_t)(u0 + uu) * rep + k;
-                if (uu < nu && full) {
+                const T *xu = xu0 + (size_t)a * rep + k;
+                if (a < nu_t && full) {
                     ld4(xu, xuv[a]);
                 } else {
 #pragma unroll
-                    for (int b = 0; b < 4; ++b) xuv[a][b] = (uu < nu && k + b < rep) ? xu[b] : T(0);
+                    for (int b = 0; b < 4; ++b) xuv[a][b] = (a < nu_t && k + b < rep) ? xu[b] : T(0);
                 }
             }
             T acc[4][4];
@@ -249,10 +250,11 @@ __global__ void __launch_bounds__(JV_THREADS, sizeof(T) == 4 ? 3 : 2) jac_v_kern
                 for (int b = 0; b < 4; ++b) acc[a][b] = T(0);
             const T *xr = xs + kp + 4 * kl;
             const T *wr = ws + 4 * ug;
-            for (int r = 0; r < ns; ++r) {
+#pragma unroll 2
+            for (int r = 0; r < ns; ++r, xr += ks, wr += JV_U) {
                 T xv[4], wv[4];
-                ld4(xr + (size_t)r * ks, xv);
-                ld4(wr + r * JV_U, wv);
+                ld4(xr, xv);
+                ld4(wr, wv);
 #pragma unroll
                 for (int a = 0; a < 4; ++a)
 #pragma unroll
@@ -261,9 +263,8 @@ __global__ void __launch_bounds__(JV_THREADS, sizeof(T) == 4 ? 3 : 2) jac_v_kern
             if (k >= rep) continue;
 #pragma unroll
             for (int a = 0; a < 4; ++a) {
-                const int uu = 4 * ug + a;
-                if (uu >= nu) continue;
-                const size_t row = ((size_t)ol * NU + urow[a]) * rep;
+                if (a >= nu_t) continue;
+                const size_t row = orow[a] + k;
                 T v[4];
 #pragma unroll
                 for (int b = 0; b < 4; ++b) v[b] = fma(-sws[a], xuv[a][b], acc[a][b]);
@@ -277,23 +278,23 @@ __global__ void __launch_bounds__(JV_THREADS, sizeof(T) == 4 ? 3 : 2) jac_v_kern
                         hv.y = *reinterpret_cast<const unsigned *>(&h23);
                         lv.x = *reinterpret_cast<const unsigned *>(&l01);
                         lv.y = *reinterpret_cast<const unsigned *>(&l23);
-                        *reinterpret_cast<uint2 *>(vh + row + k) = hv;
-                        *reinterpret_cast<uint2 *>(vl + row + k) = lv;
+                        *reinterpret_cast<uint2 *>(vh + row) = hv;
+                        *reinterpret_cast<uint2 *>(vl + row) = lv;
                     } else {
                         const __half hh[4] = {__low2half(h01), __high2half(h01), __low2half(h23),
                                               __high2half(h23)};
                         const __half ll[4] = {__low2half(l01), __high2half(l01), __low2half(l23),
                                               __high2half(l23)};
                         for (int b = 0; b < 4 && k + b < rep; ++b) {
-                            vh[row + k + b] = hh[b];
-                            vl[row + k + b] = ll[b];
+                            vh[row + b] = hh[b];
+                            vl[row + b] = ll[b];
                         }
                     }
                 } else {
                     if (full) {
-                        st4(V + row + k, v);
+                        st4(V + row, v);
                     } else {
-                        for (int b = 0; b < 4 && k + b < rep; ++b) V[row + k + b] = v[b];
+                        for (int b = 0; b < 4 && k + b < rep; ++b) V[row + b] = v[b];
                     }
                 }
             }

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "kernels_common.cuh"
+#include "trsv.h"
 
 namespace kfb {
 
@@ -678,8 +679,10 @@ kfb_status mixed_core(const ApplyFn &A, const float *B, int n, kfb_layout uplo, 
     const bool f64 = (flags & KFB_SOLVE_FP64_FACTOR) != 0;
     Handles *hd = nullptr;
     KFB_TRY(get_handles(s, hd));
-    DevBuf Fd, ws, dinfo;
+    DevBuf Fd, ws, dinfo, ttmp;
+    TrsvPlan trsv;   // FP64 factor: blocked triangular solves
     KFB_TRY(Fd.alloc((size_t)n * n * (f64 ? sizeof(double) : sizeof(float)), s));
+    if (f64) KFB_TRY(ttmp.alloc((size_t)n * sizeof(double), s));
     KFB_TRY(dinfo.alloc(sizeof(int), s));
     int lwork = 0;
     if (f64)
@@ -711,16 +714,12 @@ kfb_status mixed_core(const ApplyFn &A, const float *B, int n, kfb_layout uplo, 
             dense_lower_to_rfp_kernel<<<g2, b2, 0, s>>>(Fd.as<float>(), n, uplo, F.as<float>());
             KFB_CUDA_TRY(cudaGetLastError());
         }
+        if (finfo == 0 && f64) KFB_TRY(trsv.prepare(Fd.as<double>(), n, s));
         return KFB_OK;
     };
     auto solve_f_dev = [&](const double *x, int slot, double *out) -> kfb_status {
-        if (f64) {
-            KFB_CUDA_TRY(cudaMemcpyAsync(out, x, (size_t)n * sizeof(double),
-                                         cudaMemcpyDeviceToDevice, s));
-            KFB_SOLVER_TRY(cusolverDnDpotrs(hd->solver, CUBLAS_FILL_MODE_LOWER, n, 1,
-                                            Fd.as<double>(), n, out, n, dinfo.as<int>()));
-            return KFB_OK;
-        }
+        TraceScope tr_s("mixed:potrs", s);
+        if (f64) return trsv.solve(Fd.as<double>(), x, ttmp.as<double>(), out, s);
         scale_to_float_dev_kernel<<<gb, 256, 0, s>>>(x, sc, slot, n, f32v.as<float>());
         KFB_TRY(rfp_potrs(F.ptr, f32v.ptr, n, 1, uplo, KFB_F32, s));
         float_to_double_dev_kernel<<<gb, 256, 0, s>>>(f32v.as<float>(), sc, slot, n, out);
@@ -748,20 +747,23 @@ kfb_status mixed_core(const ApplyFn &A, const float *B, int n, kfb_layout uplo, 
                              "FP32 RFP Cholesky failed even with shift %g (info=%d)", shift, finfo);
         tr_f.reset();
         TraceScope tr_cg("mixed:cg", s);
-        // w = F^{-1} v (v has unit norm: slot S_NRM set to 1 for the scaling)
-        {
+        // w = F^{-1} v (v has unit norm: slot S_NRM set to 1 for the scaling);
+        // without deflation (defl = 0) there is no correction to apply
+        double sm_coef = 0.0;
+        if (defl != 0.0) {
             const double one = 1.0;
             KFB_CUDA_TRY(cudaMemcpyAsync(sc + S_NRM, &one, sizeof(double), cudaMemcpyHostToDevice,
                                          s));
             KFB_TRY(solve_f_dev(v, S_NRM, dw.as<double>()));
+            double vfv = 0.0;
+            KFB_TRY(ds.dot(v, dw.as<double>(), n, S_VW, s));
+            KFB_TRY(ds.read(S_VW, vfv, s));
+            sm_coef = defl / (1.0 + defl * vfv);
         }
-        double vfv = 0.0;
-        KFB_TRY(ds.dot(v, dw.as<double>(), n, S_VW, s));
-        KFB_TRY(ds.read(S_VW, vfv, s));
-        const double sm_coef = defl / (1.0 + defl * vfv);
         // M^{-1} x = F^{-1} x - sm_coef (w . x) w, with |x|^2 in sc[slot]
         auto precond = [&](const double *x, int slot, double *out) -> kfb_status {
             KFB_TRY(solve_f_dev(x, slot, out));
+            if (sm_coef == 0.0) return KFB_OK;
             KFB_TRY(ds.dot(dw.as<double>(), x, n, S_WR, s));
             axpy_dev_kernel<<<gb, 256, 0, s>>>(dw.as<double>(), sc, S_WR, -sm_coef, n, out);
             KFB_CUDA_TRY(cudaGetLastError());
@@ -801,6 +803,21 @@ kfb_status mixed_core(const ApplyFn &A, const float *B, int n, kfb_layout uplo, 
                 KFB_CUDA_TRY(cudaMemcpyAsync(ds.host + 2 * (it & 1), sc + S_RR,
                                              2 * sizeof(double), cudaMemcpyDeviceToHost, s));
                 KFB_CUDA_TRY(cudaEventRecord(ds.ev[it & 1], s));
+                if (f64) {
+                    // an FP64 factor converges in one or two steps: test this
+                    // step's residual before paying for another preconditioner
+                    // solve (the FP32 path instead tests one step behind)
+                    KFB_CUDA_TRY(cudaEventSynchronize(ds.ev[it & 1]));
+                    const double rr = ds.host[2 * (it & 1)], fl = ds.host[2 * (it & 1) + 1];
+                    if (fl != 0.0) {
+                        indefinite = true;
+                        break;
+                    }
+                    if (std::sqrt(rr) <= tol * ynorm) {
+                        ++it;
+                        break;
+                    }
+                }
                 KFB_TRY(precond(r.as<double>(), S_RR, z.as<double>()));
                 KFB_TRY(ds.dot(r.as<double>(), z.as<double>(), n, rz_new, s));
                 xpby_dev_kernel<<<gb, 256, 0, s>>>(z.as<double>(), sc, rz_new, rz_cur, n,
@@ -808,7 +825,7 @@ kfb_status mixed_core(const ApplyFn &A, const float *B, int n, kfb_layout uplo, 
                 KFB_CUDA_TRY(cudaGetLastError());
                 // stop test on the previous iteration's residual (the device runs one ahead)
                 const int chk = it - 1;
-                if (chk >= 0) {
+                if (!f64 && chk >= 0) {
                     KFB_CUDA_TRY(cudaEventSynchronize(ds.ev[chk & 1]));
                     const double rr = ds.host[2 * (chk & 1)], fl = ds.host[2 * (chk & 1) + 1];
                     if (fl != 0.0) {
@@ -828,6 +845,7 @@ kfb_status mixed_core(const ApplyFn &A, const float *B, int n, kfb_layout uplo, 
             }
             total_it += it;
             if (indefinite) {
+                if (f64) KFB_TRY(trsv.check(s));
                 inf.iterations = total_it;
                 return set_error(KFB_ERR_NOT_PD,
                                  "the system is indefinite at the precision of its matrix "
@@ -846,6 +864,7 @@ kfb_status mixed_core(const ApplyFn &A, const float *B, int n, kfb_layout uplo, 
             rel = std::sqrt(rr) / ynorm;
             if (rel <= tol || total_it >= maxit) break;
         }
+        if (f64) KFB_TRY(trsv.check(s));
         inf.iterations = total_it;
         inf.used_cg = 1;
         inf.rel_residual = rel;
@@ -896,6 +915,7 @@ kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2
     KFB_TRY(ds.init(s));
     const unsigned gw = nblk((long long)n * 32, 256);
     ApplyFn A = [&](const double *x, double lam, double *out) -> kfb_status {
+        TraceScope tr_a("mixed:apply", s);
         dense_apply_kernel<<<gw, 256, 0, s>>>(Kd.as<float>(), x, n, lam, out);
         KFB_CUDA_TRY(cudaGetLastError());
         return KFB_OK;

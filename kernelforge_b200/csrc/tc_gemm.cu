@@ -545,38 +545,53 @@ __global__ void split_rows_kernel(const T *__restrict__ src, long long n, float 
     }
 }
 
-// Jt[(m, c)][(j, k)] = dX[m][j][k][c].  Tiles of 32 (j,k) x 32 c through
-// shared memory; tiles wholly beyond the molecule's atoms (j >= nat[m] or
-// c >= 3 nat[m]) are skipped: the GEMMs read (j, k) < nat rep only, and rows
-// c >= 3 nat only feed output columns they discard.
+// Jt[(m, c)][(j, k)] = dX[m][j][k][c].  Tiles of 64 (j,k) x 32 c through
+// shared memory (rows of dX read 128 bytes per warp, rows of Jt written as
+// fp16 pairs, 128 bytes per warp); tiles wholly beyond the molecule's atoms
+// (j >= nat[m] or c >= 3 nat[m]) are skipped: the GEMMs read (j, k) < nat rep
+// only, and rows c >= 3 nat only feed output columns they discard.
 template <class T>
-__global__ void transpose_split_dx_kernel(const T *__restrict__ dx, int ma, int rep,
-                                          const int *__restrict__ nat, float scale,
-                                          __half *__restrict__ hi, __half *__restrict__ lo) {
-    __shared__ float tile[32][33];
+__global__ void __launch_bounds__(256) transpose_split_dx_kernel(
+    const T *__restrict__ dx, int ma, int rep, const int *__restrict__ nat, float scale,
+    __half *__restrict__ hi, __half *__restrict__ lo) {
+    __shared__ float tile[64][33];
     const int m = blockIdx.z;
     const int ld = 3 * ma;
     const long long kk_total = (long long)ma * rep;
-    const long long kk0 = (long long)blockIdx.x * 32;
+    const long long kk0 = (long long)blockIdx.x * 64;
     const int c0 = blockIdx.y * 32;
     const int na = min(max(nat[m], 0), ma);
     if (kk0 >= (long long)na * rep || c0 >= 3 * na) return;
     const T *base = dx + (size_t)m * kk_total * ld;
-    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int r = warp; r < 64; r += 8) {
         const long long kk = kk0 + r;
-        const int c = c0 + threadIdx.x;
-        tile[r][threadIdx.x] = (kk < kk_total && c < ld) ? (float)base[kk * ld + c] : 0.f;
+        const int c = c0 + lane;
+        tile[r][lane] = (kk < kk_total && c < ld) ? (float)base[kk * ld + c] * scale : 0.f;
     }
     __syncthreads();
-    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const long long kk = kk0 + 2 * lane;
+    for (int r = warp; r < 32; r += 8) {
         const int c = c0 + r;
-        const long long kk = kk0 + threadIdx.x;
-        if (c < ld && kk < kk_total) {
-            const float v = tile[threadIdx.x][r] * scale;
-            const __half h = __float2half_rn(v);
-            const size_t o = ((size_t)m * ld + c) * kk_total + kk;
-            hi[o] = h;
-            lo[o] = __float2half_rn(v - __half2float(h));
+        if (c >= ld) break;
+        const size_t o = ((size_t)m * ld + c) * kk_total + kk;
+        __half2 h, l;
+        const float a0 = tile[2 * lane][r], a1 = tile[2 * lane + 1][r];
+        h = __floats2half2_rn(a0, a1);
+        const float2 back = __half22float2(h);
+        l = __floats2half2_rn(a0 - back.x, a1 - back.y);
+        if (kk + 1 < kk_total && (o & 1) == 0) {
+            *reinterpret_cast<__half2 *>(hi + o) = h;
+            *reinterpret_cast<__half2 *>(lo + o) = l;
+        } else {
+            if (kk < kk_total) {
+                hi[o] = __low2half(h);
+                lo[o] = __low2half(l);
+            }
+            if (kk + 1 < kk_total) {
+                hi[o + 1] = __high2half(h);
+                lo[o + 1] = __high2half(l);
+            }
         }
     }
 }
@@ -675,8 +690,8 @@ kfb_status transpose_split_dx(const T *dx, int nm, int ma, int rep, const int *n
         KFB_CUDA_TRY(cudaGetLastError());
         KFB_TRY(pow2_from_device(d.as<float>(), s, scale));
     }
-    dim3 grid((unsigned)((kk + 31) / 32), (unsigned)((3 * ma + 31) / 32), (unsigned)nm);
-    transpose_split_dx_kernel<T><<<grid, dim3(32, 8), 0, s>>>(dx, ma, rep, nat, *scale, hi, lo);
+    dim3 grid((unsigned)((kk + 63) / 64), (unsigned)((3 * ma + 31) / 32), (unsigned)nm);
+    transpose_split_dx_kernel<T><<<grid, 256, 0, s>>>(dx, ma, rep, nat, *scale, hi, lo);
     KFB_CUDA_TRY(cudaGetLastError());
     return KFB_OK;
 }

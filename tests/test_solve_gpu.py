@@ -145,3 +145,28 @@ def test_mixed_solve_factor_choice(factor):
                                atol=1e-7 * np.abs(ref).max())
     if factor == "fp64":
         assert info["iterations"] <= 3, info
+
+
+@pytest.mark.parametrize("factor", ["fp32", "fp64"])
+def test_mixed_solve_many_row_blocks(factor):
+    """Refinement at n = 9,700: for the FP64 factor, 152 row blocks of the
+    blocked triangular solves, more than one per CTA on a 148-SM device, and a
+    ragged last block."""
+    import torch
+
+    from kernelforge_b200 import cuda_global_kernels as cgk
+    n = 9700
+    rng = np.random.default_rng(21)
+    B = rng.normal(size=(n, 48))
+    A32 = (B @ B.T / 48.0 + 0.5 * np.eye(n)).astype(np.float32)
+    y = rng.normal(size=n)
+    K = torch.tensor(o.full_to_rfp(A32.astype(np.float64), uplo_lower=True).astype(np.float32),
+                     device="cuda")
+    alpha, info = cgk.krr_solve_mixed(K, torch.tensor(y), l2=1e-3, uplo="L", tol=1e-11,
+                                      factor=factor)
+    assert info["converged"], info
+    if factor == "fp64":
+        assert info["iterations"] <= 3, info
+    ref = np.linalg.solve(A32.astype(np.float64) + 1e-3 * np.eye(n), y)
+    np.testing.assert_allclose(alpha.cpu().numpy(), ref, rtol=1e-8,
+                               atol=1e-8 * np.abs(ref).max())
