@@ -107,6 +107,19 @@ kfb_status kfb_kernel_gaussian_symm(const void *x, const int32_t *q, const int32
                                     kfb_precision prec, kfb_layout layout, kfb_dtype out_dt,
                                     void *out, void *stream);
 
+/* kfb_kernel_gaussian_symm with X (nm, ma, rep) in HOST memory (page-locked
+ * for overlap) and `out` on the device.  With KFB_PREC_SPLIT_F16 the copy of
+ * X runs in chunks of molecules (KFB_H2D_CHUNKS, default 4) while the tensor
+ * cores work on the tiles whose molecules have arrived; each label is centred
+ * on the mean of its rows in the first chunk holding it, so the values differ
+ * from the device-input call at the split's rounding level.  Other
+ * precisions copy X once and run the device-input kernel.  Returns after the
+ * kernel has finished (the host buffer may be reused). */
+kfb_status kfb_kernel_gaussian_symm_host(const void *x_host, const int32_t *q, const int32_t *n,
+                                         int nm, int ma, int rep, double sigma, kfb_dtype x_dt,
+                                         kfb_precision prec, kfb_layout layout, kfb_dtype out_dt,
+                                         void *out, void *stream);
+
 /* ---------------------------------------------------------------------- */
 /* Derivative kernels (element type of x, dx and out: `dt`)                */
 /* ---------------------------------------------------------------------- */

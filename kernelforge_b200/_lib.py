@@ -23,6 +23,7 @@ KFB_SOLVE_FP64_FACTOR = 2
 # every function declared in include/kfb.h
 EXPORTS = (
     "kfb_last_error", "kfb_abi_version", "kfb_set_timing", "kfb_last_kernel_ms", "kfb_kernel_gaussian", "kfb_kernel_gaussian_symm",
+    "kfb_kernel_gaussian_symm_host",
     "kfb_kernel_gaussian_jacobian", "kfb_kernel_gaussian_jacobian_t",
     "kfb_kernel_gaussian_hessian", "kfb_kernel_gaussian_hessian_symm",
     "kfb_kernel_gaussian_full", "kfb_kernel_gaussian_full_symm", "kfb_full_to_rfp",
@@ -62,6 +63,7 @@ _SIGS = {
     "kfb_last_kernel_ms": (D, []),
     "kfb_kernel_gaussian": (I, [P, P, P, P, P, P, I, I, I, I, I, D, I, I, I, P, P]),
     "kfb_kernel_gaussian_symm": (I, [P, P, P, I, I, I, D, I, I, I, I, P, P]),
+    "kfb_kernel_gaussian_symm_host": (I, [P, P, P, I, I, I, D, I, I, I, I, P, P]),
     "kfb_kernel_gaussian_jacobian": (I, [P, P, P, P, P, P, P, I, I, I, I, I, I, D, I, I, P, P]),
     "kfb_kernel_gaussian_jacobian_t": (I, [P, P, P, P, P, P, P, I, I, I, I, I, I, D, I, I, P, P]),
     "kfb_kernel_gaussian_hessian": (I, [P, P, P, P, P, P, P, P, I, I, I, I, I, I, I, D, I, I, P,

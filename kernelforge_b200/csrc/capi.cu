@@ -195,6 +195,48 @@ kfb_status kfb_kernel_gaussian_symm(const void *x, const int32_t *q, const int32
     return scalar_dispatch(p, prec, sink, s);
 }
 
+kfb_status kfb_kernel_gaussian_symm_host(const void *x_host, const int32_t *q, const int32_t *n,
+                                         int nm, int ma, int rep, double sigma, kfb_dtype x_dt,
+                                         kfb_precision prec, kfb_layout layout, kfb_dtype out_dt,
+                                         void *out, void *stream) {
+    KFB_TRY(check_sigma(sigma));
+    KFB_TRY(check_prec(prec));
+    KFB_TRY(check_layout(layout));
+    KFB_TRY(check_set(x_host, q, n, nm, ma, "set"));
+    if (x_dt != KFB_F64 && x_dt != KFB_F32) return set_error(KFB_ERR_INVALID_ARG, "unknown dtype");
+    cudaStream_t s = as_stream(stream);
+    const size_t count = layout == KFB_DENSE ? (size_t)nm * nm : (size_t)nm * (nm + 1) / 2;
+    if (count == 0) return KFB_OK;
+    if (!out) return set_error(KFB_ERR_INVALID_ARG, "out is null");
+    if (prec != KFB_PREC_SPLIT_F16 || rep <= 0) {
+        // no pipelined path for these: one copy, then the device-input kernel
+        DevBuf xd;
+        const size_t bytes = (size_t)nm * ma * (rep > 0 ? rep : 0) * esize(x_dt);
+        KFB_TRY(xd.alloc(bytes, s));
+        if (bytes)
+            KFB_CUDA_TRY(cudaMemcpyAsync(xd.ptr, x_host, bytes, cudaMemcpyHostToDevice, s));
+        KFB_TRY(kfb_kernel_gaussian_symm(xd.ptr, q, n, nm, ma, rep, sigma, x_dt, prec, layout,
+                                         out_dt, out, stream));
+        KFB_CUDA_TRY(cudaStreamSynchronize(s));
+        return KFB_OK;
+    }
+    KFB_TRY(zero(out, count * esize(out_dt), s));
+    ScalarProblem p;
+    p.x1 = p.x2 = nullptr;
+    p.s1 = p.s2 = view(q, n, nm, ma);
+    p.rep = rep;
+    p.sigma = sigma;
+    p.x_dt = x_dt;
+    p.symmetric = true;
+    PairSink sink;
+    sink.out = out;
+    sink.out_f64 = out_dt == KFB_F64;
+    sink.mode = OUT_SYMM;
+    sink.layout = layout;
+    sink.n = nm;
+    return scalar_tc_from_host(p, x_host, sink, s);
+}
+
 kfb_status kfb_kernel_gaussian_jacobian(const void *x1, const void *x2, const void *dx2,
                                         const int32_t *q1, const int32_t *q2, const int32_t *n1,
                                         const int32_t *n2, int nm1, int nm2, int ma1, int ma2,

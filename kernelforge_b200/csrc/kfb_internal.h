@@ -153,6 +153,10 @@ struct ScalarProblem {
 kfb_status scalar_simt(const ScalarProblem &p, kfb_precision prec, const PairSink &sink,
                        cudaStream_t stream);
 kfb_status scalar_tc(const ScalarProblem &p, const PairSink &sink, cudaStream_t stream);
+// Symmetric split-fp16 kernel with X in host memory: chunked copies overlapped
+// with the tile waves whose rows have arrived (scalar_tc.cu).
+kfb_status scalar_tc_from_host(const ScalarProblem &p, const void *x_host, const PairSink &sink,
+                               cudaStream_t stream);
 
 // Zero an output region.
 kfb_status zero(void *ptr, size_t bytes, cudaStream_t s);

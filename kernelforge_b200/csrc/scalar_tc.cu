@@ -318,12 +318,14 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
 
 // Per-label mean of the set's active rows (FP64 partial sums, atomically
 // combined): the centre each bucket is shifted to before the fp16 split.
+// The rows of label l are [rs[l], re[l]) (the whole bucket, or the part of it
+// that one chunk of molecules holds).
 template <class Tin>
 __global__ void label_mean_kernel(const Tin *__restrict__ x, const int *__restrict__ src,
-                                  const int *__restrict__ lab_start, int rep, int nsplit,
-                                  double *__restrict__ mean) {
+                                  const int *__restrict__ rs, const int *__restrict__ re,
+                                  int rep, int nsplit, double *__restrict__ mean) {
     const int l = blockIdx.z;
-    const int s = lab_start[l], e = lab_start[l + 1];
+    const int s = rs[l], e = re[l];
     const int R = e - s;
     if (R <= 0) return;
     const int chunk = (R + nsplit - 1) / nsplit;
@@ -344,16 +346,18 @@ __global__ void label_mean_kernel(const Tin *__restrict__ x, const int *__restri
 }
 
 // Packed split rows: v = x - mean(label); hi = fp16(v); lo = fp16(v - hi);
-// norm = c * ||v||^2 (FP64 sum, stored as float).
+// norm = c * ||v||^2 (FP64 sum, stored as float).  Rows rows[i] for i < nrows
+// (rows null: rows 0 .. nrows-1).
 template <class Tin>
 __global__ void pack_split_kernel(const Tin *__restrict__ x, const int *__restrict__ src,
-                                  const int *__restrict__ lab_start, int L, int R, int rep, int Dp,
-                                  const double *__restrict__ mean, double c,
-                                  __half *__restrict__ hi, __half *__restrict__ lo,
+                                  const int *__restrict__ lab_start, int L, const int *rows,
+                                  int nrows, int rep, int Dp, const double *__restrict__ mean,
+                                  double c, __half *__restrict__ hi, __half *__restrict__ lo,
                                   float *__restrict__ norm) {
-    const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    if (r >= R) return;
+    if (i >= nrows) return;
+    const int r = rows ? rows[i] : i;
     int l = 0;
     while (l + 1 < L && r >= lab_start[l + 1]) ++l;
     const Tin *xr = x + (size_t)src[r] * rep;
@@ -421,8 +425,8 @@ kfb_status pack_split(const Tin *x, const Buckets &bk, int rep, int Dp, const do
     KFB_TRY(o.norm.alloc((size_t)std::max(R, 1) * sizeof(float), s));
     if (R > 0) {
         pack_split_kernel<Tin><<<(R + 7) / 8, 256, 0, s>>>(
-            x, o.src.as<int>(), o.lab.as<int>(), L, R, rep, Dp, mean, c, o.hi.as<__half>(),
-            o.lo.as<__half>(), o.norm.as<float>());
+            x, o.src.as<int>(), o.lab.as<int>(), L, nullptr, R, rep, Dp, mean, c,
+            o.hi.as<__half>(), o.lo.as<__half>(), o.norm.as<float>());
         KFB_CUDA_TRY(cudaGetLastError());
     }
     return KFB_OK;
@@ -463,8 +467,8 @@ kfb_status run_tc(const ScalarProblem &p, const PairSink &sink, cudaStream_t s) 
         const int nsplit = 16;
         dim3 g((p.rep + 31) / 32, nsplit, L);
         label_mean_kernel<Tin><<<g, 256, 0, s>>>(static_cast<const Tin *>(p.x1), src1.as<int>(),
-                                                 lab1.as<int>(), p.rep, nsplit,
-                                                 mean.as<double>());
+                                                 lab1.as<int>(), lab1.as<int>() + 1, p.rep,
+                                                 nsplit, mean.as<double>());
         KFB_CUDA_TRY(cudaGetLastError());
     }
     KFB_TRY(pack_split<Tin>(static_cast<const Tin *>(p.x1), b1, p.rep, Dp, mean.as<double>(), c,
@@ -510,7 +514,219 @@ kfb_status run_tc(const ScalarProblem &p, const PairSink &sink, cudaStream_t s) 
     return KFB_OK;
 }
 
+// One non-blocking copy stream per device for the pipelined host input.
+cudaStream_t h2d_stream() {
+    static std::mutex mu;
+    static cudaStream_t streams[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!streams[dev] && cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking) != cudaSuccess) {
+        (void)cudaGetLastError();
+        streams[dev] = nullptr;
+    }
+    return streams[dev];
+}
+
+struct EventSet {
+    std::vector<cudaEvent_t> ev;
+    ~EventSet() {
+        for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    }
+    kfb_status create(int n) {
+        ev.assign(n, nullptr);
+        for (int i = 0; i < n; ++i)
+            KFB_CUDA_TRY(cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming));
+        return KFB_OK;
+    }
+};
+
+// Symmetric kernel from descriptors in host memory.  The copy of X runs in
+// chunks of molecules on a copy stream while the tensor cores already work:
+// a chunk's rows are centred and split as soon as it lands, and the tiles run
+// in waves by the last chunk they need (rows are in molecule order inside a
+// label bucket, so a tile's last row names its chunk).  A label is centred on
+// the mean of its rows in the first chunk that has any.
+template <class Tin>
+kfb_status run_tc_from_host(const ScalarProblem &p, const Tin *xh, const PairSink &sink,
+                            cudaStream_t s) {
+    std::vector<int> labels = collect_labels(p.s1, nullptr);
+    if (labels.empty()) return KFB_OK;
+    TraceScope tr_all("scalar_tc_host", s);
+    const int nm = p.s1.nm, ma = p.s1.ma, rep = p.rep;
+    const size_t mol_elems = (size_t)ma * rep;
+    cudaStream_t cs = h2d_stream();
+    if (!cs) return set_error(KFB_ERR_CUDA, "could not create the copy stream");
+    DevBuf xd;
+    KFB_TRY(xd.alloc((size_t)nm * mol_elems * sizeof(Tin), s));
+    const char *env = getenv("KFB_H2D_CHUNKS");
+    const int C = std::max(1, std::min(env ? atoi(env) : 4, nm));
+    std::vector<int> m0(C + 1);
+    for (int c = 0; c <= C; ++c) m0[c] = (int)((long long)nm * c / C);
+    EventSet evs;
+    KFB_TRY(evs.create(C + 1));
+    // the copies start once the buffer exists on s; chunk 0 goes first, the
+    // plan is built while it runs, and the other chunks are queued after the
+    // plan's small uploads (copies from pageable memory would otherwise wait
+    // behind the whole of X in the copy engine)
+    KFB_CUDA_TRY(cudaEventRecord(evs.ev[C], s));
+    KFB_CUDA_TRY(cudaStreamWaitEvent(cs, evs.ev[C], 0));
+    // on every way out (errors included) the copies issued so far are waited
+    // for: s before it frees the device buffer, the host before the caller
+    // may reuse the host buffer
+    struct CopyGuard {
+        cudaStream_t s;
+        const std::vector<cudaEvent_t> &ev;
+        int issued = 0;
+        ~CopyGuard() {
+            for (int i = 0; i < issued; ++i) {
+                cudaStreamWaitEvent(s, ev[i], 0);
+                cudaEventSynchronize(ev[i]);
+            }
+        }
+    } guard{s, evs.ev};
+    auto copy_chunk = [&](int c) -> kfb_status {
+        const size_t off = (size_t)m0[c] * mol_elems;
+        KFB_CUDA_TRY(cudaMemcpyAsync(xd.as<Tin>() + off, xh + off,
+                                     (size_t)(m0[c + 1] - m0[c]) * mol_elems * sizeof(Tin),
+                                     cudaMemcpyHostToDevice, cs));
+        KFB_CUDA_TRY(cudaEventRecord(evs.ev[c], cs));
+        guard.issued = c + 1;
+        return KFB_OK;
+    };
+    KFB_TRY(copy_chunk(0));
+    // plan (host, while the first chunk is copied)
+    auto tr_plan = std::make_unique<TraceScope>("scalar_tc_host:plan", s);
+    const Buckets b1 = make_buckets(p.s1, labels);
+    const int L = (int)labels.size(), R = b1.rows();
+    std::vector<int> chunk_of(nm);
+    for (int c = 0; c < C; ++c)
+        for (int m = m0[c]; m < m0[c + 1]; ++m) chunk_of[m] = c;
+    // rows of each chunk; per chunk the row range of each label whose first
+    // chunk it is (the rows its mean is taken over), empty otherwise
+    std::vector<int> rows_all, rows_off(C + 1, 0), first(L, -1);
+    std::vector<std::vector<int>> rows_c(C);
+    std::vector<int> mrs((size_t)C * L, 0), mre((size_t)C * L, 0);
+    for (int l = 0; l < L; ++l)
+        for (int r = b1.lab_start[l]; r < b1.lab_start[l + 1];) {
+            const int c = chunk_of[b1.mol[r]];
+            int e = r;
+            while (e < b1.lab_start[l + 1] && chunk_of[b1.mol[e]] == c) rows_c[c].push_back(e++);
+            if (first[l] < 0) {
+                first[l] = c;
+                mrs[(size_t)c * L + l] = r;
+                mre[(size_t)c * L + l] = e;
+            }
+            r = e;
+        }
+    for (int c = 0; c < C; ++c) {
+        rows_off[c] = (int)rows_all.size();
+        rows_all.insert(rows_all.end(), rows_c[c].begin(), rows_c[c].end());
+    }
+    rows_off[C] = (int)rows_all.size();
+    // tiles, in waves by the chunk of their last row and column
+    const size_t packed_row_bytes = (size_t)((rep + 7) / 8 * 8) * 2 * sizeof(__half);
+    const std::vector<PairTile> tl = make_pair_tiles(b1, b1, true, BM, BN, packed_row_bytes);
+    if (tl.empty()) return KFB_OK;
+    if (tl.size() > (size_t)INT_MAX) return set_error(KFB_ERR_UNSUPPORTED, "too many tiles");
+    std::vector<int> wave(tl.size()), wstart(C + 1, 0);
+    for (size_t t = 0; t < tl.size(); ++t) {
+        const int ra = std::min(tl[t].a0 + BM, tl[t].a_end) - 1;
+        const int rb = std::min(tl[t].b0 + BN, tl[t].b_end) - 1;
+        wave[t] = std::max(chunk_of[b1.mol[ra]], chunk_of[b1.mol[rb]]);
+        ++wstart[wave[t] + 1];
+    }
+    for (int c = 0; c < C; ++c) wstart[c + 1] += wstart[c];
+    std::vector<PairTile> sorted(tl.size());
+    {
+        std::vector<int> pos(wstart.begin(), wstart.end() - 1);
+        for (size_t t = 0; t < tl.size(); ++t) sorted[pos[wave[t]]++] = tl[t];
+    }
+    tr_plan.reset();
+    const int Dp = (rep + 7) / 8 * 8;
+    const double log2e = 1.4426950408889634;
+    const double cexp = -log2e / (2.0 * p.sigma * p.sigma);
+    SplitSet A;
+    DevBuf mean, d_rows, d_mrs, d_mre, dtiles, derr;
+    KFB_TRY(upload(A.src, b1.src, s));
+    KFB_TRY(upload(A.mol, b1.mol, s));
+    KFB_TRY(upload(A.lab, b1.lab_start, s));
+    KFB_TRY(A.hi.alloc((size_t)std::max(R, 1) * Dp * sizeof(__half), s));
+    KFB_TRY(A.lo.alloc((size_t)std::max(R, 1) * Dp * sizeof(__half), s));
+    KFB_TRY(A.norm.alloc((size_t)std::max(R, 1) * sizeof(float), s));
+    KFB_TRY(upload(d_rows, rows_all, s));
+    KFB_TRY(upload(d_mrs, mrs, s));
+    KFB_TRY(upload(d_mre, mre, s));
+    KFB_TRY(upload(dtiles, sorted, s));
+    KFB_TRY(mean.alloc((size_t)L * rep * sizeof(double), s));
+    KFB_TRY(zero(mean.ptr, (size_t)L * rep * sizeof(double), s));
+    KFB_TRY(derr.alloc(sizeof(int), s));
+    KFB_TRY(zero(derr.ptr, sizeof(int), s));
+    for (int c = 1; c < C; ++c) KFB_TRY(copy_chunk(c));
+    CUtensorMap ma_hi, ma_lo;
+    KFB_TRY(make_map(&ma_hi, A.hi.as<__half>(), R, Dp, BM));
+    KFB_TRY(make_map(&ma_lo, A.lo.as<__half>(), R, Dp, BM));
+    static bool attr_set = false;
+    if (!attr_set) {
+        KFB_CUDA_TRY(cudaFuncSetAttribute(scalar_tc_kernel,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_ALLOC));
+        attr_set = true;
+    }
+    KernelTimer timer(s);
+    bool started = false;
+    for (int c = 0; c < C; ++c) {
+        KFB_CUDA_TRY(cudaStreamWaitEvent(s, evs.ev[c], 0));
+        bool new_label = false;
+        for (int l = 0; l < L; ++l) new_label |= first[l] == c;
+        if (new_label) {
+            const int nsplit = 16;
+            dim3 g((rep + 31) / 32, nsplit, L);
+            label_mean_kernel<Tin><<<g, 256, 0, s>>>(xd.as<Tin>(), A.src.as<int>(),
+                                                     d_mrs.as<int>() + (size_t)c * L,
+                                                     d_mre.as<int>() + (size_t)c * L, rep, nsplit,
+                                                     mean.as<double>());
+            KFB_CUDA_TRY(cudaGetLastError());
+        }
+        const int nr = rows_off[c + 1] - rows_off[c];
+        if (nr > 0) {
+            pack_split_kernel<Tin><<<(nr + 7) / 8, 256, 0, s>>>(
+                xd.as<Tin>(), A.src.as<int>(), A.lab.as<int>(), L, d_rows.as<int>() + rows_off[c],
+                nr, rep, Dp, mean.as<double>(), cexp, A.hi.as<__half>(), A.lo.as<__half>(),
+                A.norm.as<float>());
+            KFB_CUDA_TRY(cudaGetLastError());
+        }
+        const int nt = wstart[c + 1] - wstart[c];
+        if (nt == 0) continue;
+        if (!started) {
+            timer.start();
+            started = true;
+        }
+        const int grid = std::min(nt, device_sm_count());
+        scalar_tc_kernel<<<grid, NUM_THREADS, SMEM_ALLOC, s>>>(
+            ma_hi, ma_lo, ma_hi, ma_lo, rep, A.norm.as<float>(), A.norm.as<float>(),
+            A.mol.as<int>(), A.mol.as<int>(), dtiles.as<PairTile>() + wstart[c], nt,
+            (float)(-2.0 * cexp), sink, derr.as<int>());
+        KFB_CUDA_TRY(cudaGetLastError());
+    }
+    timer.stop();
+    int herr = 0;
+    KFB_CUDA_TRY(cudaMemcpyAsync(&herr, derr.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
+    KFB_CUDA_TRY(cudaStreamSynchronize(s));
+    if (herr) return set_error(KFB_ERR_TIMEOUT, "tensor-core scalar kernel: a pipeline wait timed out");
+    return KFB_OK;
+}
+
 }  // namespace
+
+kfb_status scalar_tc_from_host(const ScalarProblem &p, const void *x_host, const PairSink &sink,
+                               cudaStream_t s) {
+    if (!device_is_sm100())
+        return set_error(KFB_ERR_UNSUPPORTED,
+                         "the split-fp16 tensor-core path needs an sm_100 (B200) device");
+    if (!p.symmetric) return set_error(KFB_ERR_INVALID_ARG, "host input: symmetric kernel only");
+    if (p.x_dt == KFB_F64) return run_tc_from_host<double>(p, static_cast<const double *>(x_host), sink, s);
+    return run_tc_from_host<float>(p, static_cast<const float *>(x_host), sink, s);
+}
 
 kfb_status scalar_tc(const ScalarProblem &p, const PairSink &sink, cudaStream_t s) {
     if (!device_is_sm100())

@@ -66,6 +66,8 @@ def kernel_gaussian_rect(X_q, Q_q, N_q, X_t, Q_t, N_t, sigma, *, precision="spli
 def _symm(X, Q, N, sigma, precision, layout, out_dtype):
     require_cuda()
     import torch
+    if isinstance(X, torch.Tensor) and X.device.type == "cpu":
+        return _symm_host(X, Q, N, sigma, precision, layout, out_dtype)
     _check_x(X, "X")
     check_sigma(sigma)
     Qh, Nh = host_i32(Q), host_i32(N)
@@ -73,6 +75,25 @@ def _symm(X, Q, N, sigma, precision, layout, out_dtype):
     count = nm * nm if layout == _lib.KFB_DENSE else nm * (nm + 1) // 2
     out = torch.empty((count,), dtype=out_dtype, device=X.device)
     _lib.check(_lib.lib().kfb_kernel_gaussian_symm(
+        X.data_ptr(), Qh.ctypes.data, Nh.ctypes.data, nm, ma, rep, float(sigma), _lib.KFB_F32,
+        _prec(precision), layout, _lib.KFB_F64 if out_dtype == torch.float64 else _lib.KFB_F32,
+        out.data_ptr(), stream_handle()))
+    return out.view(nm, nm) if layout == _lib.KFB_DENSE else out
+
+
+def _symm_host(X, Q, N, sigma, precision, layout, out_dtype):
+    """X a float32 CPU tensor (page-locked for overlap): the library copies it
+    in chunks of molecules while the tensor cores start on the molecules that
+    have arrived; the output is on the current CUDA device."""
+    import torch
+    if X.dtype != torch.float32 or X.dim() != 3 or not X.is_contiguous():
+        raise RuntimeError("X must be a contiguous float32 tensor (nm, ma, rep)")
+    check_sigma(sigma)
+    Qh, Nh = host_i32(Q), host_i32(N)
+    nm, ma, rep = X.shape
+    count = nm * nm if layout == _lib.KFB_DENSE else nm * (nm + 1) // 2
+    out = torch.empty((count,), dtype=out_dtype, device="cuda")
+    _lib.check(_lib.lib().kfb_kernel_gaussian_symm_host(
         X.data_ptr(), Qh.ctypes.data, Nh.ctypes.data, nm, ma, rep, float(sigma), _lib.KFB_F32,
         _prec(precision), layout, _lib.KFB_F64 if out_dtype == torch.float64 else _lib.KFB_F32,
         out.data_ptr(), stream_handle()))

@@ -129,3 +129,33 @@ def test_tensor_core_path_is_deterministic_in_value():
     b = lk.kernel_gaussian_symm_rfp(X, Q, N, 2.0, precision="split_f16")
     # atomics may add in a different order: equal to FP32 rounding
     np.testing.assert_allclose(a, b, rtol=1e-6, atol=1e-6 * np.abs(a).max())
+
+
+@pytest.mark.parametrize("chunks", ["1", "3", "8"])
+@pytest.mark.parametrize("rep", [70, 720])
+def test_host_input_pipelined(chunks, rep, monkeypatch):
+    """X in (page-locked) host memory: copies in chunks of molecules overlapped
+    with the tile waves.  A label that first appears in a late chunk (oxygen
+    only in the last molecules) is centred on that chunk's rows; empty
+    molecules and clamped counts as in the device-input tests."""
+    import torch
+
+    from kernelforge_b200 import cuda_local_kernels as clk
+    monkeypatch.setenv("KFB_H2D_CHUNKS", chunks)
+    X, _, Q, N = make_set(90, 12, rep, 2, rep + 7, species=[1, 6])
+    X = (X * 0.3).astype(np.float32)
+    Q[80:, :3] = 8   # a label present only in the last chunk(s)
+    N[80:] = np.maximum(N[80:], 3)
+    N[5] = 0
+    N[7] = 40   # clamped to max_atoms
+    sig = 2.0
+    Xh = torch.from_numpy(X).pin_memory()
+    rfp = clk.kernel_gaussian_symm_rfp(Xh, Q, N, sig)
+    assert rfp.is_cuda and rfp.dtype == torch.float32
+    ref = o.kernel_gaussian_symm(X.astype(np.float64), Q, N, sig)
+    close32(rfp.cpu().numpy(), o.full_to_rfp(ref, uplo_lower=True))
+    dev = clk.kernel_gaussian_symm_rfp(torch.tensor(X, device="cuda"), Q, N, sig)
+    np.testing.assert_allclose(rfp.cpu().numpy(), dev.cpu().numpy(), rtol=2e-5,
+                               atol=2e-6 * float(dev.abs().max()))
+    Kd = clk.kernel_gaussian_symm(Xh, Q, N, sig)
+    close32(Kd.cpu().numpy(), ref)
