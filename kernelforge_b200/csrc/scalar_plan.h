@@ -16,8 +16,11 @@ namespace kfb {
 // CTAs working on neighbouring tiles at the same time reuse operand tiles from
 // L2 instead of streaming a whole label bucket from DRAM per tile row;
 // row_bytes = 0 keeps the plain row-major order.
+// merge > 1: `merge` consecutive column tiles of a super-block row form one
+// tile (wider MMA tiles); diag then marks a tile whose first column tile is
+// the diagonal one, and b_end stops at the tile's own columns.
 std::vector<PairTile> make_pair_tiles(const Buckets &a, const Buckets &b, bool symmetric, int tm,
-                                      int tn, size_t row_bytes = 0);
+                                      int tn, size_t row_bytes = 0, int merge = 1);
 
 // The same tiles in the same order, described by their L2 super-blocks (a
 // few hundred entries instead of one entry per tile) and expanded into the
@@ -33,6 +36,9 @@ struct SuperBlock {
 std::vector<SuperBlock> make_super_blocks(const Buckets &a, const Buckets &b, bool symmetric,
                                           int tm, int tn, size_t row_bytes, long long &ntiles);
 kfb_status expand_tiles(const std::vector<SuperBlock> &sbs, long long ntiles, int tm, int tn,
-                        DevBuf &tiles, cudaStream_t s);
+                        DevBuf &tiles, cudaStream_t s, int merge = 1);
+// Rewrite the offsets of sbs for tiles of `merge` column tiles; returns the
+// number of merged tiles.
+long long merge_offsets(std::vector<SuperBlock> &sbs, int merge);
 
 }  // namespace kfb

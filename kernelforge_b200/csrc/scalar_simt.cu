@@ -123,8 +123,12 @@ std::vector<SuperBlock> make_super_blocks(const Buckets &a, const Buckets &b, bo
     return out;
 }
 
+// Tile t of the list; `merge` consecutive column tiles of a super-block row
+// form one tile (the last one of a row may be narrower: b_end stops at the
+// row's own columns).  With merge > 1 the offsets of `sbs` count merged tiles
+// (merge_offsets).
 __global__ void expand_tiles_kernel(const SuperBlock *__restrict__ sbs, int nsb, long long ntiles,
-                                    int tm, int tn, PairTile *__restrict__ out) {
+                                    int tm, int tn, int merge, PairTile *__restrict__ out) {
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= ntiles) return;
     int lo = 0, hi = nsb - 1;  // last super-block with offset <= t
@@ -139,14 +143,16 @@ __global__ void expand_tiles_kernel(const SuperBlock *__restrict__ sbs, int nsb,
     for (int ti = sb.bi; ti < ti_end; ++ti) {
         int f, e;
         sb_row(sb, ti, f, e);
-        const int c = e > f ? e - f : 0;
+        const int c = e > f ? (e - f + merge - 1) / merge : 0;
         if (local < c) {
-            const int tj = f + (int)local;
+            const int tj = f + (int)local * merge;
+            const int ncol = min(merge, e - tj);
             PairTile pt{};
             pt.a0 = sb.sa + ti * tm;
             pt.a_end = sb.ea;
             pt.b0 = sb.sb + tj * tn;
-            pt.b_end = sb.eb;
+            pt.b_end = min(sb.eb, sb.sb + (tj + ncol) * tn);
+            if (merge == 1) pt.b_end = sb.eb;
             pt.diag = (sb.symmetric && ti == tj) ? 1 : 0;
             out[t] = pt;
             return;
@@ -155,20 +161,34 @@ __global__ void expand_tiles_kernel(const SuperBlock *__restrict__ sbs, int nsb,
     }
 }
 
+long long merge_offsets(std::vector<SuperBlock> &sbs, int merge) {
+    long long n = 0;
+    for (SuperBlock &sb : sbs) {
+        sb.offset = n;
+        const int ti_end = std::min(sb.nti, sb.bi + sb.g);
+        for (int ti = sb.bi; ti < ti_end; ++ti) {
+            int f, e;
+            sb_row(sb, ti, f, e);
+            if (e > f) n += (e - f + merge - 1) / merge;
+        }
+    }
+    return n;
+}
+
 kfb_status expand_tiles(const std::vector<SuperBlock> &sbs, long long ntiles, int tm, int tn,
-                        DevBuf &tiles, cudaStream_t s) {
+                        DevBuf &tiles, cudaStream_t s, int merge) {
     KFB_TRY(tiles.alloc((size_t)std::max<long long>(ntiles, 1) * sizeof(PairTile), s));
     if (ntiles == 0) return KFB_OK;
     DevBuf dsb;
     KFB_TRY(upload(dsb, sbs, s));
     expand_tiles_kernel<<<(unsigned)((ntiles + 255) / 256), 256, 0, s>>>(
-        dsb.as<SuperBlock>(), (int)sbs.size(), ntiles, tm, tn, tiles.as<PairTile>());
+        dsb.as<SuperBlock>(), (int)sbs.size(), ntiles, tm, tn, merge, tiles.as<PairTile>());
     KFB_CUDA_TRY(cudaGetLastError());
     return KFB_OK;
 }
 
 std::vector<PairTile> make_pair_tiles(const Buckets &a, const Buckets &b, bool symmetric,
-                                      int tm, int tn, size_t row_bytes) {
+                                      int tm, int tn, size_t row_bytes, int merge) {
     std::vector<PairTile> out;
     long long n = 0;
     const std::vector<SuperBlock> sbs = make_super_blocks(a, b, symmetric, tm, tn, row_bytes, n);
@@ -178,12 +198,13 @@ std::vector<PairTile> make_pair_tiles(const Buckets &a, const Buckets &b, bool s
         for (int ti = sb.bi; ti < ti_end; ++ti) {
             int f, e;
             sb_row(sb, ti, f, e);
-            for (int tj = f; tj < e; ++tj) {
+            for (int tj = f; tj < e; tj += merge) {
+                const int ncol = std::min(merge, e - tj);
                 PairTile t{};
                 t.a0 = sb.sa + ti * tm;
                 t.a_end = sb.ea;
                 t.b0 = sb.sb + tj * tn;
-                t.b_end = sb.eb;
+                t.b_end = merge == 1 ? sb.eb : std::min(sb.eb, sb.sb + (tj + ncol) * tn);
                 t.diag = (sb.symmetric && ti == tj) ? 1 : 0;
                 out.push_back(t);
             }

@@ -2,16 +2,17 @@
 //
 // Same-label atoms are packed per label bucket (molecules in order), centred
 // on the bucket mean and split into an fp16 pair x = hi + lo.  One persistent
-// CTA per SM walks a list of 128 x 128 same-label tiles:
+// CTA per SM walks a list of 128 x 256 same-label tiles (two 128-column tiles
+// of the L2-ordered plan merged, so each A slice feeds twice the MMA work):
 //
 //   warp 0      TMA producer: 64-wide K slices of A_hi, A_lo, B_hi, B_lo
-//               (128B-swizzled) into a 3-stage shared-memory ring;
+//               (128B-swizzled) into a 2-stage shared-memory ring (96 KB each);
 //   warp 1      MMA issuer: per K16 step, tcgen05.mma kind::f16
 //               hi*hi + hi*lo + lo*hi into an FP32 accumulator in TMEM
 //               (two accumulators, so the epilogue of tile t overlaps the
 //               MMAs of tile t+1);
 //   warp 2      TMEM allocator;
-//   warps 4..7  epilogue: tcgen05.ld of 32 x 32 accumulator blocks,
+//   warps 4..11 epilogue (two per TMEM lane quadrant): tcgen05.ld of 32 x 32 accumulator blocks,
 //               e_ij = exp2(c n_i + c n_j - 2c g_ij) with c = -log2(e)/(2 sigma^2),
 //               reduction over (molecule a) x (molecule b) rectangles in
 //               shared memory, one atomic add per rectangle into the output.
@@ -41,9 +42,11 @@ namespace {
 using namespace tc;
 
 constexpr int BM = 128;          // rows of A per tile (TMEM lanes)
-constexpr int BN = 128;          // rows of B per tile (TMEM columns per accumulator)
+constexpr int BN = 256;          // rows of B per tile (TMEM columns per accumulator)
+constexpr int TN = 128;          // column tiles of the plan; a tile merges BN / TN of them
+constexpr int MERGE = BN / TN;
 constexpr int BK = 64;           // fp16 elements per K slice (128 bytes: one swizzle row)
-constexpr int NSTAGE = 3;
+constexpr int NSTAGE = 2;        // 96 KB per stage
 constexpr int TILE_A_BYTES = BM * BK * 2;
 constexpr int TILE_B_BYTES = BN * BK * 2;
 constexpr int STAGE_BYTES = 2 * TILE_A_BYTES + 2 * TILE_B_BYTES;
@@ -78,6 +81,33 @@ __device__ __forceinline__ void umma_f16(uint32_t dtmem, uint64_t a, uint64_t b,
         : "memory");
 }
 // ------------------------------------------------------------------ kernel
+// emit_pair in FP32 arithmetic (the rectangle sums are FP32 already)
+__device__ __forceinline__ void emit_pair_f(const PairSink &s, int a, int b, float v, int diag) {
+    v *= (float)s.scale;
+    long long idx;
+    if (s.mode == OUT_RECT) {
+        idx = (long long)(a + s.row_off) * s.n + (b + s.col_off);
+    } else {
+        if (diag) {
+            if (a > b) return;
+        } else if (a == b) {
+            v *= 2.f;
+        }
+        const long long r = a + s.row_off, c = b + s.col_off;
+        if (s.layout == KFB_DENSE) {
+            if (r != c) {
+                if (s.out_f64) atomicAdd(static_cast<double *>(s.out) + c * s.n + r, (double)v);
+                else atomicAdd(static_cast<float *>(s.out) + c * s.n + r, v);
+            }
+            idx = r * s.n + c;
+        } else {
+            idx = sym_index((kfb_layout)s.layout, s.n, r, c);
+        }
+    }
+    if (s.out_f64) atomicAdd(static_cast<double *>(s.out) + idx, (double)v);
+    else atomicAdd(static_cast<float *>(s.out) + idx, v);
+}
+
 __global__ void __launch_bounds__(NUM_THREADS, 1)
     scalar_tc_kernel(const __grid_constant__ CUtensorMap tm_a_hi,
                      const __grid_constant__ CUtensorMap tm_a_lo,
@@ -256,8 +286,11 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                 const unsigned emask = __ballot_sync(0xffffffffu, cend);
                 float v[32];
                 tmem_ld32(tbase + (uint32_t)(c * 32), v);
-                // the self pair (same packed row) of a diagonal tile is exactly 1
-                const int self_j = (tl.diag && (row >> 5) == c) ? lane : -1;
+                // only the first TN columns of a diagonal tile are its diagonal
+                // block (the rest is the next, off-diagonal column tile); the
+                // self pair (same packed row) of a diagonal block is exactly 1
+                const int dg = (tl.diag && c * 32 < TN) ? 1 : 0;
+                const bool has_self = dg && c == q;   // warp-uniform
 #pragma unroll
                 for (int hh = 0; hh < 2; ++hh) {
                     const unsigned hmask = hh ? 0xFFFF0000u : 0x0000FFFFu;
@@ -269,17 +302,31 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                     // the run ends (run boundaries are the same for every lane)
                     float run_sum = 0.f;
                     int k = 0;
+                    if (has_self) {
 #pragma unroll
-                    for (int jj = 0; jj < 16; ++jj) {
-                        const int j = hh * 16 + jj;
-                        const float cnj = __shfl_sync(0xffffffffu, cn, j);
-                        float e = fast_exp2(fmaf(m2c, v[j], rn + cnj));
-                        if (j == self_j) e = 1.f;
-                        run_sum += e;
-                        if (emask & (1u << j)) {
-                            scr[k * SCR_LD + lane] = run_sum;
-                            ++k;
-                            run_sum = 0.f;
+                        for (int jj = 0; jj < 16; ++jj) {
+                            const int j = hh * 16 + jj;
+                            const float cnj = __shfl_sync(0xffffffffu, cn, j);
+                            float e = fast_exp2(fmaf(m2c, v[j], rn + cnj));
+                            if (j == lane) e = 1.f;
+                            run_sum += e;
+                            if (emask & (1u << j)) {
+                                scr[k * SCR_LD + lane] = run_sum;
+                                ++k;
+                                run_sum = 0.f;
+                            }
+                        }
+                    } else {
+#pragma unroll
+                        for (int jj = 0; jj < 16; ++jj) {
+                            const int j = hh * 16 + jj;
+                            const float cnj = __shfl_sync(0xffffffffu, cn, j);
+                            run_sum += fast_exp2(fmaf(m2c, v[j], rn + cnj));
+                            if (emask & (1u << j)) {
+                                scr[k * SCR_LD + lane] = run_sum;
+                                ++k;
+                                run_sum = 0.f;
+                            }
                         }
                     }
                     __syncwarp();
@@ -290,9 +337,15 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                         const int ci = p - ri * nc;
                         const int r0 = rstart[ri], r1 = rstart[ri + 1];
                         const float *col_sums = scr + ci * SCR_LD;
-                        float sum = 0.f;
-                        for (int r = r0; r < r1; ++r) sum += col_sums[r];
-                        emit_pair(sink, rmolr[ri], cmolr[ci], (double)sum, tl.diag);
+                        // two independent partial sums: the loads overlap
+                        float s0 = 0.f, s1 = 0.f;
+                        int r = r0;
+                        for (; r + 1 < r1; r += 2) {
+                            s0 += col_sums[r];
+                            s1 += col_sums[r + 1];
+                        }
+                        if (r < r1) s0 += col_sums[r];
+                        emit_pair_f(sink, rmolr[ri], cmolr[ci], s0 + s1, dg);
                     }
                 }
                 __syncwarp();
@@ -444,8 +497,9 @@ kfb_status run_tc(const ScalarProblem &p, const PairSink &sink, cudaStream_t s) 
     // packed rows: hi + lo fp16 halves of Dp columns
     const size_t packed_row_bytes = (size_t)((p.rep + 7) / 8 * 8) * 2 * sizeof(__half);
     long long ntiles_ll = 0;
-    const std::vector<SuperBlock> sbs =
-        make_super_blocks(b1, bb, p.symmetric, BM, BN, packed_row_bytes, ntiles_ll);
+    std::vector<SuperBlock> sbs =
+        make_super_blocks(b1, bb, p.symmetric, BM, TN, packed_row_bytes, ntiles_ll);
+    ntiles_ll = merge_offsets(sbs, MERGE);
     tr_plan.reset();
     auto tr_pack = std::make_unique<TraceScope>("scalar_tc:pack", s);
     if (ntiles_ll == 0) return KFB_OK;
@@ -485,7 +539,7 @@ kfb_status run_tc(const ScalarProblem &p, const PairSink &sink, cudaStream_t s) 
     KFB_TRY(make_map(&mb_lo, BB.lo.as<__half>(), bb.rows(), Dp, BN));
 
     DevBuf dtiles, derr;
-    KFB_TRY(expand_tiles(sbs, ntiles_ll, BM, BN, dtiles, s));
+    KFB_TRY(expand_tiles(sbs, ntiles_ll, BM, TN, dtiles, s, MERGE));
     tr_pack.reset();
     TraceScope tr_kern("scalar_tc:kernel+wait", s);
     KFB_TRY(derr.alloc(sizeof(int), s));
@@ -626,7 +680,8 @@ kfb_status run_tc_from_host(const ScalarProblem &p, const Tin *xh, const PairSin
     rows_off[C] = (int)rows_all.size();
     // tiles, in waves by the chunk of their last row and column
     const size_t packed_row_bytes = (size_t)((rep + 7) / 8 * 8) * 2 * sizeof(__half);
-    const std::vector<PairTile> tl = make_pair_tiles(b1, b1, true, BM, BN, packed_row_bytes);
+    const std::vector<PairTile> tl =
+        make_pair_tiles(b1, b1, true, BM, TN, packed_row_bytes, MERGE);
     if (tl.empty()) return KFB_OK;
     if (tl.size() > (size_t)INT_MAX) return set_error(KFB_ERR_UNSUPPORTED, "too many tiles");
     std::vector<int> wave(tl.size()), wstart(C + 1, 0);
@@ -663,9 +718,11 @@ kfb_status run_tc_from_host(const ScalarProblem &p, const Tin *xh, const PairSin
     KFB_TRY(derr.alloc(sizeof(int), s));
     KFB_TRY(zero(derr.ptr, sizeof(int), s));
     for (int c = 1; c < C; ++c) KFB_TRY(copy_chunk(c));
-    CUtensorMap ma_hi, ma_lo;
+    CUtensorMap ma_hi, ma_lo, mb_hi, mb_lo;
     KFB_TRY(make_map(&ma_hi, A.hi.as<__half>(), R, Dp, BM));
     KFB_TRY(make_map(&ma_lo, A.lo.as<__half>(), R, Dp, BM));
+    KFB_TRY(make_map(&mb_hi, A.hi.as<__half>(), R, Dp, BN));
+    KFB_TRY(make_map(&mb_lo, A.lo.as<__half>(), R, Dp, BN));
     static bool attr_set = false;
     if (!attr_set) {
         KFB_CUDA_TRY(cudaFuncSetAttribute(scalar_tc_kernel,
@@ -703,7 +760,7 @@ kfb_status run_tc_from_host(const ScalarProblem &p, const Tin *xh, const PairSin
         }
         const int grid = std::min(nt, device_sm_count());
         scalar_tc_kernel<<<grid, NUM_THREADS, SMEM_ALLOC, s>>>(
-            ma_hi, ma_lo, ma_hi, ma_lo, rep, A.norm.as<float>(), A.norm.as<float>(),
+            ma_hi, ma_lo, mb_hi, mb_lo, rep, A.norm.as<float>(), A.norm.as<float>(),
             A.mol.as<int>(), A.mol.as<int>(), dtiles.as<PairTile>() + wstart[c], nt,
             (float)(-2.0 * cexp), sink, derr.as<int>());
         KFB_CUDA_TRY(cudaGetLastError());
