@@ -109,7 +109,7 @@ kfb_status kfb_kernel_gaussian_symm(const void *x, const int32_t *q, const int32
 
 /* kfb_kernel_gaussian_symm with X (nm, ma, rep) in HOST memory (page-locked
  * for overlap) and `out` on the device.  With KFB_PREC_SPLIT_F16 the copy of
- * X runs in chunks of molecules (KFB_H2D_CHUNKS, default 4) while the tensor
+ * X runs in chunks of molecules (KFB_H2D_CHUNKS, default 8) while the tensor
  * cores work on the tiles whose molecules have arrived; each label is centred
  * on the mean of its rows in the first chunk holding it, so the values differ
  * from the device-input call at the split's rounding level.  Other

@@ -614,7 +614,7 @@ kfb_status run_tc_from_host(const ScalarProblem &p, const Tin *xh, const PairSin
     DevBuf xd;
     KFB_TRY(xd.alloc((size_t)nm * mol_elems * sizeof(Tin), s));
     const char *env = getenv("KFB_H2D_CHUNKS");
-    const int C = std::max(1, std::min(env ? atoi(env) : 4, nm));
+    const int C = std::max(1, std::min(env ? atoi(env) : 8, nm));
     std::vector<int> m0(C + 1);
     for (int c = 0; c <= C; ++c) m0[c] = (int)((long long)nm * c / C);
     EventSet evs;

@@ -265,25 +265,44 @@ __global__ void full_to_rfp_kernel(const T *A, int n, int layout, T *arf) {
     if (i < n && j < n && i <= j) arf[sym_index((kfb_layout)layout, n, i, j)] = A[i * n + j];
 }
 
-template <class Tin, class Tout>
-__global__ void rfp_to_full_kernel(const Tin *arf, int n, int layout, Tout *A) {
-    const long long i = blockIdx.y * (long long)blockDim.y + threadIdx.y;
-    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i < n && j < n) A[i * n + j] = (Tout)arf[sym_index((kfb_layout)layout, n, i, j)];
+// 32 x 32 tile (rows i0.., columns j0.., i0 >= j0) of an RFP array into
+// t[i - i0][j - j0] (FP64), reading along whichever index is contiguous in
+// the RFP storage of this tile (both occur: the two triangles of RFP are
+// stored transposed to each other).  Block (32, 8).
+template <class Tin>
+__device__ __forceinline__ void load_rfp_tile(const Tin *__restrict__ arf, int n, int layout,
+                                              int i0, int j0, double (*t)[33]) {
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int ib = min(i0 + 1, n - 1), jb = j0;
+    const bool along_i = ib > jb && sym_index((kfb_layout)layout, n, ib, jb) ==
+                                       sym_index((kfb_layout)layout, n, i0, jb) + 1;
+    for (int r = ty; r < 32; r += 8) {
+        const int i = along_i ? i0 + tx : i0 + r, j = along_i ? j0 + r : j0 + tx;
+        double v = 0.0;
+        if (i < n && j < n) v = (double)arf[sym_index((kfb_layout)layout, n, i, j)];
+        if (along_i) t[tx][r] = v;
+        else t[r][tx] = v;
+    }
 }
 
-// r = y - (K + l2 I) x with K dense FP32 (row-major, symmetric), FP64 vectors.
-__global__ void residual_kernel(const float *__restrict__ K, const double *__restrict__ x,
-                                const double *__restrict__ y, int n, double l2,
-                                double *__restrict__ r) {
-    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (row >= n) return;
-    const float *kr = K + (size_t)row * n;
-    double acc = 0.0;
-    for (int j = lane; j < n; j += 32) acc = fma((double)kr[j], x[j], acc);
-    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (lane == 0) r[row] = (y ? y[row] : 0.0) - acc - l2 * x[row];
+// Full symmetric row-major copy, one lower tile per block writing both
+// triangles with coalesced stores.
+template <class Tin, class Tout>
+__global__ void rfp_to_full_tiled_kernel(const Tin *__restrict__ arf, int n, int layout,
+                                         Tout *__restrict__ A) {
+    const int bi = blockIdx.y, bj = blockIdx.x;
+    if (bi < bj) return;
+    __shared__ double t[32][33];
+    const int i0 = bi * 32, j0 = bj * 32;
+    load_rfp_tile(arf, n, layout, i0, j0, t);
+    __syncthreads();
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    for (int r = ty; r < 32; r += 8) {
+        const int i = i0 + r, j = j0 + tx;   // A[i][j], along j
+        if (i < n && j < n) A[(size_t)i * n + j] = (Tout)t[r][tx];
+        const int i2 = j0 + r, j2 = i0 + tx;   // A[j0 + r][i0 + tx] = t[tx][r]
+        if (bi != bj && i2 < n && j2 < n) A[(size_t)i2 * n + j2] = (Tout)t[tx][r];
+    }
 }
 
 // out = sum_i a_i b_i  (FP64), one partial per block then atomically combined
@@ -302,39 +321,10 @@ __global__ void dot_kernel(const double *a, const double *b, int n, double *out)
     }
 }
 
-__global__ void scale_to_float_kernel(const double *a, double s, int n, float *out) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) out[i] = (float)(a[i] * s);
-}
-// x += s * (double)d
-__global__ void axpy_float_kernel(const float *d, double s, int n, double *x) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) x[i] += s * (double)d[i];
-}
 // y += s * x
 __global__ void axpy_kernel(const double *x, double s, int n, double *y) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) y[i] += s * x[i];
-}
-// p = z + beta * p
-__global__ void xpby_kernel(const double *z, double beta, int n, double *p) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) p[i] = z[i] + beta * p[i];
-}
-__global__ void float_to_double_kernel(const float *a, double s, int n, double *out) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) out[i] = s * (double)a[i];
-}
-// max_i sum_j |K_ij| (a Gershgorin bound on ||K||_2), one warp per row
-__global__ void max_rowsum_kernel(const float *K, int n, float *out) {
-    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (row >= n) return;
-    const float *kr = K + (size_t)row * n;
-    float acc = 0.f;
-    for (int j = lane; j < n; j += 32) acc += fabsf(kr[j]);
-    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (lane == 0) atomicMax(reinterpret_cast<int *>(out), __float_as_int(acc));
 }
 
 __global__ void fill_kernel(double *x, double v, int n) {
@@ -346,10 +336,7 @@ __global__ void fill_alt_kernel(double *x, double v, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) x[i] = (i % 3 == 0 ? -2.0 : 1.0) * v * (1.0 + 1e-3 * (i % 7));
 }
-__global__ void scale_copy_kernel(const double *a, double s, int n, double *out) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) out[i] = s * a[i];
-}
+
 inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 
 // Dense column-major lower triangle of F = B - coef v v^T + diag I, B in RFP
@@ -358,12 +345,23 @@ template <class TD>
 __global__ void dense_deflate_kernel(const float *__restrict__ B, int n, int layout,
                                      const double *__restrict__ v, double coef, double diag,
                                      TD *__restrict__ F) {
-    const long long i = blockIdx.y * (long long)blockDim.y + threadIdx.y;  // row
-    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;  // column
-    if (i < n && j < n && i >= j) {
-        double f = (double)B[sym_index((kfb_layout)layout, n, i, j)] - coef * v[i] * v[j];
+    // one lower 32 x 32 tile per block; column-major stores along i
+    const int bi = blockIdx.y, bj = blockIdx.x;
+    if (bi < bj) return;
+    __shared__ double t[32][33];
+    const int i0 = bi * 32, j0 = bj * 32;
+    load_rfp_tile(B, n, layout, i0, j0, t);
+    __syncthreads();
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int i = i0 + tx;
+    if (i >= n) return;
+    const double vi = v[i];
+    for (int r = ty; r < 32; r += 8) {
+        const int j = j0 + r;
+        if (j >= n || i < j) continue;
+        double f = t[tx][r] - coef * vi * v[j];
         if (i == j) f += diag;
-        F[j * n + i] = (TD)f;
+        F[(size_t)j * n + i] = (TD)f;
     }
 }
 
@@ -409,13 +407,13 @@ kfb_status full_to_rfp(const void *A, int n, kfb_layout uplo, kfb_dtype dt, void
 kfb_status rfp_to_full(const void *arf, int n, kfb_layout uplo, kfb_dtype dt, void *A,
                        cudaStream_t s) {
     if (n <= 0) return KFB_OK;
-    dim3 blk(32, 8), grd(nblk(n, 32), nblk(n, 8));
+    dim3 blk(32, 8), grd(nblk(n, 32), nblk(n, 32));
     if (dt == KFB_F64)
-        rfp_to_full_kernel<double, double><<<grd, blk, 0, s>>>(static_cast<const double *>(arf), n,
-                                                               uplo, static_cast<double *>(A));
+        rfp_to_full_tiled_kernel<double, double><<<grd, blk, 0, s>>>(
+            static_cast<const double *>(arf), n, uplo, static_cast<double *>(A));
     else
-        rfp_to_full_kernel<float, float><<<grd, blk, 0, s>>>(static_cast<const float *>(arf), n,
-                                                             uplo, static_cast<float *>(A));
+        rfp_to_full_tiled_kernel<float, float><<<grd, blk, 0, s>>>(
+            static_cast<const float *>(arf), n, uplo, static_cast<float *>(A));
     KFB_CUDA_TRY(cudaGetLastError());
     return KFB_OK;
 }
@@ -693,16 +691,16 @@ kfb_status mixed_core(const ApplyFn &A, const float *B, int n, kfb_layout uplo, 
                                                    Fd.as<float>(), n, &lwork));
     KFB_TRY(ws.alloc((size_t)std::max(lwork, 1) * (f64 ? sizeof(double) : sizeof(float)), s));
     auto factor = [&](double diag, int &finfo) -> kfb_status {
-        const dim3 b2(32, 8), g2(nblk(n, 32), nblk(n, 8));
+        const dim3 b2(32, 8), g2(nblk(n, 32), nblk(n, 8)), gt(nblk(n, 32), nblk(n, 32));
         KFB_TRY(zero(dinfo.ptr, sizeof(int), s));
         if (f64) {
-            dense_deflate_kernel<double><<<g2, b2, 0, s>>>(B, n, uplo, v, fcoef, diag,
+            dense_deflate_kernel<double><<<gt, b2, 0, s>>>(B, n, uplo, v, fcoef, diag,
                                                            Fd.as<double>());
             KFB_CUDA_TRY(cudaGetLastError());
             KFB_SOLVER_TRY(cusolverDnDpotrf(hd->solver, CUBLAS_FILL_MODE_LOWER, n, Fd.as<double>(),
                                             n, ws.as<double>(), lwork, dinfo.as<int>()));
         } else {
-            dense_deflate_kernel<float><<<g2, b2, 0, s>>>(B, n, uplo, v, fcoef, diag,
+            dense_deflate_kernel<float><<<gt, b2, 0, s>>>(B, n, uplo, v, fcoef, diag,
                                                           Fd.as<float>());
             KFB_CUDA_TRY(cudaGetLastError());
             KFB_SOLVER_TRY(cusolverDnSpotrf(hd->solver, CUBLAS_FILL_MODE_LOWER, n, Fd.as<float>(),

@@ -159,3 +159,28 @@ def test_host_input_pipelined(chunks, rep, monkeypatch):
                                atol=2e-6 * float(dev.abs().max()))
     Kd = clk.kernel_gaussian_symm(Xh, Q, N, sig)
     close32(Kd.cpu().numpy(), ref)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "split_f16"])
+def test_host_input_c_abi_f64(precision):
+    """kfb_kernel_gaussian_symm_host with FP64 descriptors in host memory: the
+    split-fp16 path pipelines the copy, the FP64 path copies once and runs the
+    device-input kernel; dense FP64 output against the oracle."""
+    import torch
+
+    from kernelforge_b200 import _lib
+    from kernelforge_b200._device import stream_handle
+    X, _, Q, N = make_set(40, 10, 70, 3, 11)
+    X = np.ascontiguousarray(X * 0.3)
+    nm, ma, rep = X.shape
+    out = torch.empty((nm * nm,), dtype=torch.float64, device="cuda")
+    _lib.check(_lib.lib().kfb_kernel_gaussian_symm_host(
+        X.ctypes.data, Q.ctypes.data, N.ctypes.data, nm, ma, rep, 2.0, _lib.KFB_F64,
+        _lib.PREC[precision], _lib.KFB_DENSE, _lib.KFB_F64, out.data_ptr(), stream_handle()))
+    torch.cuda.synchronize()
+    ref = o.kernel_gaussian_symm(X, Q, N, 2.0)
+    got = out.view(nm, nm).cpu().numpy()
+    if precision == "fp64":
+        np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-12)
+    else:
+        close32(got, ref)
