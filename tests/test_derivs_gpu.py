@@ -113,3 +113,32 @@ def test_tensor_core_contractions_match_oracle(rep):
           o.kernel_gaussian_full_symm_rfp(X1, dX1, Q1, N1, s), p)
     close(lk.kernel_gaussian_full(X1, dX1, X2, dX2, Q1, Q2, N1, N2, s, precision=p),
           o.kernel_gaussian_full(X1, dX1, X2, dX2, Q1, Q2, N1, N2, s), p)
+
+
+@pytest.mark.parametrize("precision,rep", [("fp64", 33), ("fp32", 33), ("split_f16", 48)])
+def test_jacobian_chunked_outer_molecules(precision, rep, monkeypatch):
+    """A workspace of a few kB splits the outer molecules into chunks (each with
+    its own dot-product block and label tiles).  Outer molecules lacking a label
+    (zero rows of V), an outer label the inner set lacks, empty molecules and
+    rep not a multiple of 4 (scalar row edges) on the CUDA-core paths."""
+    from kernelforge_b200 import local_kernels as lk
+    monkeypatch.setenv("KFB_WORKSPACE_GB", "0.00002")
+    X1, dX1, Q1, N1 = make_set(9, 7, rep, 3, 31)
+    X2, dX2, Q2, N2 = make_set(6, 5, rep, 3, 32)
+    sc = 1.0 / np.sqrt(rep)
+    X1 *= 2 * sc
+    X2 *= 2 * sc
+    dX1 *= sc
+    dX2 *= sc
+    Q1[2, :] = 1          # outer molecule with one label only
+    Q1[4, :2] = 9         # an outer label the inner set lacks
+    N1[6] = 0             # empty outer molecule
+    s = 2.0
+    if precision == "fp64":
+        close(lk.kernel_gaussian_jacobian(X1, X2, dX2, Q1, Q2, N1, N2, s),
+              o.kernel_gaussian_jacobian(X1, X2, dX2, Q1, Q2, N1, N2, s), "fp64")
+        close(lk.kernel_gaussian_jacobian_t(X2, dX2, X1, Q2, Q1, N2, N1, s),
+              o.kernel_gaussian_jacobian_t(X2, dX2, X1, Q2, Q1, N2, N1, s), "fp64")
+    else:
+        close(lk.kernel_gaussian_jacobian(X1, X2, dX2, Q1, Q2, N1, N2, s, precision=precision),
+              o.kernel_gaussian_jacobian(X1, X2, dX2, Q1, Q2, N1, N2, s), precision)
