@@ -25,6 +25,7 @@
 #include <memory>
 #include <numeric>
 #include <tuple>
+#include <type_traits>
 
 #include "derivs.h"
 #include "kernels_common.cuh"
@@ -622,6 +623,234 @@ kfb_status launch_hess_t(const HessPair *pairs, int np, const T *x1, const T *x2
                                is2, is4, W, Tt, bound);
     KFB_CUDA_TRY(cudaGetLastError());
     return KFB_OK;
+}
+
+// ------------------------------------------ Hessian kernel 1, GEMM form (FP32)
+// With tensor cores, J_j^T (x_i - x_j) comes from one product per batch of
+// molecules b:  P[(a, i)][(b, j, c)] = (x_i - mu_l) . J_j[:, c]  (split fp16,
+// tcgen05), and PB[(b, j, c)] = (x_j - mu_l) . J_j[:, c]  (FP64 sums), where
+// mu_l is the set-1 mean of the label l both atoms share:
+//   t_ij[c] = P[(a, i)][(b, j, c)] - PB[(b, j, c)].
+// The centring keeps the two terms close to |J| |x - x_j| so that their
+// difference loses little to cancellation.
+
+// sums[l][k] += x[atom][k] over atoms of label index l (lidx < 0: skipped).
+// Block (32 k, 8 atom groups); per-label partial sums in shared memory.
+template <class T>
+__global__ void __launch_bounds__(256) label_sums_kernel(const T *__restrict__ x,
+                                                         const int *__restrict__ lidx, int natoms,
+                                                         int rep, int L, double *__restrict__ sums) {
+    extern __shared__ double ls[];   // [L][8][32]
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int k = blockIdx.x * 32 + tx;
+    for (int e = threadIdx.x; e < L * 256; e += 256) ls[e] = 0.0;
+    __syncthreads();
+    for (int a = blockIdx.y * 8 + ty; a < natoms; a += gridDim.y * 8) {
+        const int l = lidx[a];
+        if (l >= 0 && k < rep) ls[(l * 8 + ty) * 32 + tx] += (double)x[(size_t)a * rep + k];
+    }
+    __syncthreads();
+    if (ty == 0 && k < rep)
+        for (int l = 0; l < L; ++l) {
+            double sum = 0.0;
+            for (int r = 0; r < 8; ++r) sum += ls[(l * 8 + r) * 32 + tx];
+            atomicAdd(&sums[(size_t)l * rep + k], sum);
+        }
+}
+
+// max |x - mu_l| over labelled atoms (FP32 bits, atomically)
+template <class T>
+__global__ void centred_absmax_kernel(const T *__restrict__ x, const int *__restrict__ lidx,
+                                      int natoms, int rep, const double *__restrict__ sums,
+                                      const double *__restrict__ inv_count, float *amax) {
+    float m = 0.f;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+         e < (long long)natoms * rep; e += (long long)gridDim.x * blockDim.x) {
+        const int a = (int)(e / rep), k = (int)(e - (long long)a * rep);
+        const int l = lidx[a];
+        if (l < 0) continue;
+        const double v = (double)x[e] - sums[(size_t)l * rep + k] * inv_count[l];
+        m = fmaxf(m, fabsf((float)v));
+    }
+    for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<int *>(amax), __float_as_int(m));
+}
+
+// hi/lo[a][k] = fp16 pair of (x[a][k] - mu_l[k]) * scale; unlabelled rows zero;
+// norm[a] = |x[a] - mu_l|^2 (FP64 sum).  Block (256) per row.
+template <class T>
+__global__ void __launch_bounds__(256) centred_split_kernel(
+    const T *__restrict__ x, const int *__restrict__ lidx, int rep,
+    const double *__restrict__ sums, const double *__restrict__ inv_count, float scale,
+    __half *__restrict__ hi, __half *__restrict__ lo, float *__restrict__ norm) {
+    const size_t a = blockIdx.x;
+    const int l = lidx[a];
+    double acc = 0.0;
+    for (int k = threadIdx.x; k < rep; k += blockDim.x) {
+        const double d = l < 0 ? 0.0 : (double)x[a * rep + k] - sums[(size_t)l * rep + k] *
+                                                                    inv_count[l];
+        acc = fma(d, d, acc);
+        const float v = (float)(d * scale);
+        const __half h = __float2half_rn(v);
+        hi[a * rep + k] = h;
+        lo[a * rep + k] = __float2half_rn(v - __half2float(h));
+    }
+    __shared__ double red[8];
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < 8; ++w) t += red[w];
+        norm[a] = (float)t;
+    }
+}
+
+// PB[(m, j)][c] = (x_j - mu_l) . J_j[:, c] (FP64 sums), block per atom (m, j)
+template <class T>
+__global__ void pb_kernel(const T *__restrict__ x2, const T *__restrict__ dx2,
+                          const int *__restrict__ lidx2, int ma2, int rep,
+                          const double *__restrict__ sums, const double *__restrict__ inv_count,
+                          float *__restrict__ PB) {
+    const size_t mj = blockIdx.x;
+    const int ld2 = 3 * ma2;
+    const int l = lidx2[mj];
+    const T *xj = x2 + mj * rep;
+    const T *J = dx2 + mj * rep * ld2;
+    for (int c = threadIdx.x; c < ld2; c += blockDim.x) {
+        double acc = 0.0;
+        if (l >= 0)
+            for (int k = 0; k < rep; ++k)
+                acc = fma((double)xj[k] - sums[(size_t)l * rep + k] * inv_count[l],
+                          (double)J[(size_t)k * ld2 + c], acc);
+        PB[mj * ld2 + c] = (float)acc;
+    }
+}
+
+// max |J_b| over the real atoms and columns of each molecule b
+template <class T>
+__global__ void jmax_per_mol_kernel(const T *__restrict__ dx, int ma, int rep,
+                                    const int *__restrict__ nat, float *__restrict__ out) {
+    const int m = blockIdx.x;
+    const int na = min(max(nat[m], 0), ma), ld = 3 * ma, nc = 3 * na;
+    const T *base = dx + (size_t)m * ma * rep * ld;
+    float v = 0.f;
+    const long long nrow = (long long)na * rep;
+    for (long long row = threadIdx.x >> 5; row < nrow; row += blockDim.x >> 5)
+        for (int c = threadIdx.x & 31; c < nc; c += 32)
+            v = fmaxf(v, fabsf((float)base[row * ld + c]));
+    for (int o = 16; o; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    __shared__ float red[32];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float mm = 0.f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) mm = fmaxf(mm, red[w]);
+        out[m] = mm;
+    }
+}
+
+// Kernel 1 with t from P: the same outputs as hess_t_kernel (W, Tt, bound);
+// weights from the centred dot products G[(a, i)][(b - b0) * ma2 + j] (row
+// length ldg) and the norms; t by a warp per (same-label pair, 32 columns).  P rows are set-1 padded atoms,
+// P columns ((b - b0) * ma2 + j) * ld2 + c with row length ldp.
+__global__ void __launch_bounds__(256) hess_t_p_kernel(
+    const HessPair *__restrict__ pairs, const float *__restrict__ G, long long ldg,
+    const float *__restrict__ n1, const float *__restrict__ n2, const int *__restrict__ perm1,
+    const int *__restrict__ lab1, const int *__restrict__ perm2, const int *__restrict__ lab2,
+    int ma1, int ma2, float c2, float is2, float is4, const float *__restrict__ P,
+    long long ldp, int b0, const float *__restrict__ PB, const float *__restrict__ jbmax,
+    float *__restrict__ W, float *__restrict__ Tt, float *__restrict__ bound) {
+    extern __shared__ __align__(16) unsigned char ht_raw[];
+    int4 *groups = reinterpret_cast<int4 *>(ht_raw);  // ma1
+    int *pa = reinterpret_cast<int *>(groups + ma1);   // ma1
+    int *pb = pa + ma1;                                // ma2
+    int *gstart = pb + ma2;                            // ma1 + 1
+    float *wsum = reinterpret_cast<float *>(gstart + ma1 + 1);  // ma1
+    float *bterm = wsum + ma1;                                   // ma1
+    float *dinf = bterm + ma1;                                   // ma1 x ma2
+    float *w2s = dinf + (size_t)ma1 * ma2;                       // ma1 x ma2
+    __shared__ int ngroups;
+    const int p = blockIdx.x;
+    const HessPair pr = pairs[p];
+    const int ld2 = 3 * ma2, ncol = 3 * pr.nb;
+    const size_t wbase = (size_t)p * ma1 * ma2;
+    for (int e = threadIdx.x; e < pr.na; e += blockDim.x) {
+        pa[e] = perm1[(size_t)pr.a * ma1 + e];
+        wsum[e] = 0.f;
+        bterm[e] = 0.f;
+    }
+    for (int e = threadIdx.x; e < pr.nb; e += blockDim.x) pb[e] = perm2[(size_t)pr.b * ma2 + e];
+    if (threadIdx.x == 0) {
+        const int g = pair_label_groups(lab1 + (size_t)pr.a * ma1, lab2 + (size_t)pr.b * ma2,
+                                        pr.na, pr.nb, groups);
+        ngroups = g;
+        gstart[0] = 0;
+        for (int q = 0; q < g; ++q)
+            gstart[q + 1] = gstart[q] + (groups[q].y - groups[q].x) * (groups[q].w - groups[q].z);
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const int npairs = gstart[ngroups];
+    auto pair_ij = [&](int q, int &i, int &j) {
+        int g = 0;
+        while (gstart[g + 1] <= q) ++g;
+        const int4 gr = groups[g];
+        const int off = q - gstart[g], nbg = gr.w - gr.z;
+        i = pa[gr.x + off / nbg];
+        j = pb[gr.z + off % nbg];
+    };
+    // weights of all same-label pairs (a thread per pair) from the centred dot
+    // products g = (x_i - mu) . (x_j - mu) and norms:  |d|^2 = n_i + n_j - 2 g
+    // (clamped at 0); |d|_2 bounds |d|_inf for the |Y| bound
+    const float *Ga = G + (size_t)pr.a * ma1 * ldg + (size_t)(pr.b - b0) * ma2;
+    for (int q = threadIdx.x; q < npairs; q += blockDim.x) {
+        int i, j;
+        pair_ij(q, i, j);
+        const float dd = fmaxf(n1[(size_t)pr.a * ma1 + i] + n2[(size_t)pr.b * ma2 + j] -
+                                   2.f * Ga[(size_t)i * ldg + j],
+                               0.f);
+        const float e = kexp<float>(c2 * dd);
+        W[wbase + (size_t)i * ma2 + j] = e * is2;
+        w2s[i * ma2 + j] = e * is4;
+        dinf[i * ma2 + j] = sqrtf(dd);
+        if (bound) atomicAdd(&wsum[i], e * is2);
+    }
+    __syncthreads();
+    // t'_ij = w'_ij (P - PB), a warp per (pair, 32 columns)
+    const int nchunk = (ncol + 31) / 32;
+    const float *Prow0 = P + (size_t)pr.a * ma1 * ldp + (size_t)(pr.b - b0) * ma2 * ld2;
+    const float *PBb = PB + (size_t)pr.b * ma2 * ld2;
+    for (int it = warp; it < npairs * nchunk; it += nwarp) {
+        const int q = it / nchunk, cc = it - q * nchunk;
+        int i, j;
+        pair_ij(q, i, j);
+        const int c = cc * 32 + lane;
+        float t = 0.f;
+        if (c < ncol)
+            t = w2s[i * ma2 + j] *
+                (Prow0[(size_t)i * ldp + (size_t)j * ld2 + c] - PBb[(size_t)j * ld2 + c]);
+        if (c < ncol) Tt[(wbase + (size_t)i * ma2 + j) * ld2 + c] = t;
+        if (bound) {
+            float m = fabsf(t);
+            for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+            if (lane == 0) atomicAdd(&bterm[i], dinf[i * ma2 + j] * m);
+        }
+    }
+    if (!bound) return;
+    __syncthreads();
+    const float jm = jbmax[pr.b];
+    if (warp == 0) {
+        float bmax = 0.f;
+        for (int i = lane; i < pr.na; i += 32) bmax = fmaxf(bmax, jm * wsum[i] + bterm[i]);
+        for (int o = 16; o; o >>= 1) bmax = fmaxf(bmax, __shfl_xor_sync(0xffffffffu, bmax, o));
+        if (lane == 0) atomicMax(reinterpret_cast<int *>(bound), __float_as_int(bmax * 1.001f));
+    }
+}
+
+size_t hess_t_p_smem(int ma1, int ma2) {
+    return (size_t)ma1 * sizeof(int4) + (size_t)(ma1 + ma2 + ma1 + 1) * sizeof(int) +
+           (size_t)(2 * ma1 + 2 * ma1 * ma2) * sizeof(float);
 }
 
 // ------------------------------------------------------- Hessian kernel 2
@@ -1371,8 +1600,125 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
     }
     const T c2 = T(-1.0 / (2.0 * sigma * sigma)), is2 = T(1.0 / (sigma * sigma));
     const T is4 = is2 * is2;
-    for (size_t p0 = 0; p0 < pairs.size(); p0 += batch) {
-        const int np = (int)std::min<size_t>(batch, pairs.size() - p0);
+    // Kernel 1 in GEMM form (tensor cores, FP32 inputs): P = (X1 - mu) Jr^T per
+    // batch of molecules b, with per-label centres mu of set 1.  Needs the P
+    // columns of one molecule b for every set-1 atom within half the workspace
+    // and at most 16 labels; otherwise kernel 1 forms J_j^T d_ij itself.
+    const long long Mrows = (long long)s1.v.nm * ma1, bcols = (long long)ma2 * ld2;
+    bool pform = false;
+    int bcap = 0;
+    float xs_scale = 1.f, jr_scale = 1.f;
+    DevBuf d_l1, d_l2, d_sums, d_invc, d_amx, xh1, xl1, jrh, jrl, d_pb, d_jbm, d_P, d_nat2,
+        d_n1, xh2, xl2, d_n2, d_G;
+    float xs2_scale = 1.f;
+    if constexpr (std::is_same<T, float>::value) {
+        const std::vector<int> labs1 = collect_labels(s1.v, nullptr);
+        const long long pbytes = Mrows * bcols * (long long)sizeof(float);
+        pform = tc && !labs1.empty() && labs1.size() <= 16 &&
+                pbytes <= (long long)(budget_bytes() / 2) && Mrows < INT_MAX &&
+                (long long)s2.v.nm * bcols < INT_MAX;
+        if (pform) {
+            TraceScope tr_p("hessian:p-setup", s);
+            const int L = (int)labs1.size();
+            auto lab_index = [&](int q) {
+                const auto it = std::lower_bound(labs1.begin(), labs1.end(), q);
+                return (it != labs1.end() && *it == q) ? (int)(it - labs1.begin()) : -1;
+            };
+            std::vector<int> l1((size_t)Mrows, -1), l2((size_t)s2.v.nm * ma2, -1), nat2(s2.v.nm);
+            std::vector<double> cnt(L, 0.0), invc(L, 0.0);
+            for (int m = 0; m < s1.v.nm; ++m)
+                for (int i = 0; i < s1.v.natoms(m); ++i) {
+                    const int l = lab_index(s1.v.q[(size_t)m * ma1 + i]);
+                    l1[(size_t)m * ma1 + i] = l;
+                    if (l >= 0) cnt[l] += 1.0;
+                }
+            for (int m = 0; m < s2.v.nm; ++m) {
+                nat2[m] = s2.v.natoms(m);
+                for (int j = 0; j < nat2[m]; ++j)
+                    l2[(size_t)m * ma2 + j] = lab_index(s2.v.q[(size_t)m * ma2 + j]);
+            }
+            for (int l = 0; l < L; ++l) invc[l] = cnt[l] > 0.0 ? 1.0 / cnt[l] : 0.0;
+            KFB_TRY(upload(d_l1, l1, s));
+            KFB_TRY(upload(d_l2, l2, s));
+            KFB_TRY(upload(d_invc, invc, s));
+            KFB_TRY(upload(d_nat2, nat2, s));
+            KFB_TRY(d_sums.alloc((size_t)L * rep * sizeof(double), s));
+            KFB_TRY(zero(d_sums.ptr, (size_t)L * rep * sizeof(double), s));
+            const float *x1f = static_cast<const float *>(s1.x);
+            const float *x2f = static_cast<const float *>(s2.x);
+            const float *dx2f = static_cast<const float *>(s2.dx);
+            label_sums_kernel<float><<<dim3((unsigned)((rep + 31) / 32), 16), 256,
+                                       (size_t)L * 256 * sizeof(double), s>>>(
+                x1f, d_l1.as<int>(), (int)Mrows, rep, L, d_sums.as<double>());
+            KFB_CUDA_TRY(cudaGetLastError());
+            KFB_TRY(d_amx.alloc(sizeof(float), s));
+            KFB_TRY(zero(d_amx.ptr, sizeof(float), s));
+            const unsigned ab = (unsigned)std::min<long long>((Mrows * rep + 255) / 256, 148LL * 8);
+            centred_absmax_kernel<float><<<ab, 256, 0, s>>>(x1f, d_l1.as<int>(), (int)Mrows, rep,
+                                                            d_sums.as<double>(),
+                                                            d_invc.as<double>(), d_amx.as<float>());
+            KFB_CUDA_TRY(cudaGetLastError());
+            KFB_TRY(pow2_from_device(d_amx.as<float>(), s, &xs_scale));
+            KFB_TRY(xh1.alloc((size_t)Mrows * rep * sizeof(__half), s));
+            KFB_TRY(xl1.alloc((size_t)Mrows * rep * sizeof(__half), s));
+            KFB_TRY(d_n1.alloc((size_t)Mrows * sizeof(float), s));
+            centred_split_kernel<float><<<(unsigned)Mrows, 256, 0, s>>>(
+                x1f, d_l1.as<int>(), rep, d_sums.as<double>(), d_invc.as<double>(), xs_scale,
+                xh1.as<__half>(), xl1.as<__half>(), d_n1.as<float>());
+            KFB_CUDA_TRY(cudaGetLastError());
+            // set 2, centred on the set-1 means of its labels (the same rows for
+            // a symmetric call)
+            const long long M2rows = (long long)s2.v.nm * ma2;
+            xs2_scale = xs_scale;
+            if (!symmetric) {
+                KFB_TRY(zero(d_amx.ptr, sizeof(float), s));
+                const unsigned ab2 =
+                    (unsigned)std::min<long long>((M2rows * rep + 255) / 256, 148LL * 8);
+                centred_absmax_kernel<float><<<ab2, 256, 0, s>>>(
+                    x2f, d_l2.as<int>(), (int)M2rows, rep, d_sums.as<double>(),
+                    d_invc.as<double>(), d_amx.as<float>());
+                KFB_CUDA_TRY(cudaGetLastError());
+                KFB_TRY(pow2_from_device(d_amx.as<float>(), s, &xs2_scale));
+                KFB_TRY(xh2.alloc((size_t)M2rows * rep * sizeof(__half), s));
+                KFB_TRY(xl2.alloc((size_t)M2rows * rep * sizeof(__half), s));
+                KFB_TRY(d_n2.alloc((size_t)M2rows * sizeof(float), s));
+                centred_split_kernel<float><<<(unsigned)M2rows, 256, 0, s>>>(
+                    x2f, d_l2.as<int>(), rep, d_sums.as<double>(), d_invc.as<double>(),
+                    xs2_scale, xh2.as<__half>(), xl2.as<__half>(), d_n2.as<float>());
+                KFB_CUDA_TRY(cudaGetLastError());
+            }
+            const size_t jr_elems = (size_t)s2.v.nm * bcols * rep;
+            KFB_TRY(jrh.alloc(jr_elems * sizeof(__half), s));
+            KFB_TRY(jrl.alloc(jr_elems * sizeof(__half), s));
+            KFB_TRY(transpose_split_dx_rows<float>(dx2f, s2.v.nm, ma2, rep, d_nat2.as<int>(),
+                                                   jrh.as<__half>(), jrl.as<__half>(),
+                                                   &jr_scale, s));
+            KFB_TRY(d_pb.alloc((size_t)s2.v.nm * bcols * sizeof(float), s));
+            pb_kernel<float><<<(unsigned)(s2.v.nm * ma2), 128, 0, s>>>(
+                x2f, dx2f, d_l2.as<int>(), ma2, rep, d_sums.as<double>(), d_invc.as<double>(),
+                d_pb.as<float>());
+            KFB_CUDA_TRY(cudaGetLastError());
+            KFB_TRY(d_jbm.alloc((size_t)s2.v.nm * sizeof(float), s));
+            jmax_per_mol_kernel<float><<<(unsigned)s2.v.nm, 256, 0, s>>>(
+                dx2f, ma2, rep, d_nat2.as<int>(), d_jbm.as<float>());
+            KFB_CUDA_TRY(cudaGetLastError());
+            bcap = (int)std::max<long long>(1, (long long)(budget_bytes() / 2) / pbytes);
+            int span_max = 1;
+            for (size_t q0 = 0; q0 < pairs.size(); q0 += batch) {
+                const size_t q1 = std::min(pairs.size(), q0 + batch) - 1;
+                span_max = std::max(span_max, pairs[q1].b - pairs[q0].b + 1);
+            }
+            bcap = std::min(bcap, span_max);
+            KFB_TRY(d_P.alloc((size_t)bcap * Mrows * bcols * sizeof(float), s));
+            KFB_TRY(d_G.alloc((size_t)bcap * Mrows * ma2 * sizeof(float), s));
+        }
+    }
+    const size_t smem_p = hess_t_p_smem(ma1, ma2);
+    for (size_t p0 = 0, npz = 0; p0 < pairs.size(); p0 += npz) {
+        int np = (int)std::min<size_t>(batch, pairs.size() - p0);
+        if (pform)  // the batch's molecules b fit the P buffer
+            while (np > 1 && pairs[p0 + np - 1].b - pairs[p0].b + 1 > bcap) --np;
+        npz = (size_t)np;
         KFB_CUDA_TRY(cudaMemcpyAsync(dpairs.ptr, pairs.data() + p0, np * sizeof(HessPair),
                                      cudaMemcpyHostToDevice, s));
         const T *x1p = static_cast<const T *>(s1.x), *x2p = static_cast<const T *>(s2.x);
@@ -1381,10 +1727,60 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
         // with tensor cores kernel 1 also bounds |Y| for the power-of-two
         // scale of the fp16 split that kernel 2 writes
         if (tc) KFB_TRY(zero(yamax.ptr, sizeof(float), s));
-        KFB_TRY(launch_hess_t<T>(dpairs.as<HessPair>(), np, x1p, x2p, dx2p, d_perm1.as<int>(),
-                                 d_lab1.as<int>(), d_perm2.as<int>(), d_lab2.as<int>(), ma1, ma2,
-                                 rep, c2, is2, is4, W.as<T>(), Tt.as<T>(),
-                                 tc ? yamax.as<float>() : nullptr, s));
+        if constexpr (std::is_same<T, float>::value) {
+            if (pform) {
+                const int bmin = pairs[p0].b, bmax = pairs[p0 + np - 1].b;
+                TcProb pp{};
+                pp.b_row0 = (int)((long long)bmin * bcols);
+                pp.M = (int)Mrows;
+                pp.N = (int)((long long)(bmax - bmin + 1) * bcols);
+                pp.K = rep;
+                pp.alpha = 1.0 / ((double)xs_scale * (double)jr_scale);
+                TcOperand A, B;
+                A.hi = xh1.ptr;
+                A.lo = xl1.ptr;
+                A.rows = Mrows;
+                A.cols = rep;
+                B.hi = jrh.ptr;
+                B.lo = jrl.ptr;
+                B.rows = (long long)s2.v.nm * bcols;
+                B.cols = rep;
+                TcEpi epi;
+                epi.mode = EPI_DENSE;
+                epi.zf32 = d_P.as<float>();
+                epi.ld = pp.N;
+                KFB_TRY(tc_gemm_grouped(A, B, 3, false, {pp}, ElemSink(), s, epi));
+                // centred dot products of the batch's atom pairs
+                TcProb pg{};
+                pg.b_row0 = bmin * ma2;
+                pg.M = (int)Mrows;
+                pg.N = (bmax - bmin + 1) * ma2;
+                pg.K = rep;
+                pg.alpha = 1.0 / ((double)xs_scale * (double)xs2_scale);
+                TcOperand B2;
+                B2.hi = symmetric ? xh1.ptr : xh2.ptr;
+                B2.lo = symmetric ? xl1.ptr : xl2.ptr;
+                B2.rows = (long long)s2.v.nm * ma2;
+                B2.cols = rep;
+                TcEpi eg;
+                eg.mode = EPI_DENSE;
+                eg.zf32 = d_G.as<float>();
+                eg.ld = pg.N;
+                KFB_TRY(tc_gemm_grouped(A, B2, 3, false, {pg}, ElemSink(), s, eg));
+                hess_t_p_kernel<<<np, 256, smem_p, s>>>(
+                    dpairs.as<HessPair>(), d_G.as<float>(), pg.N, d_n1.as<float>(),
+                    symmetric ? d_n1.as<float>() : d_n2.as<float>(), d_perm1.as<int>(),
+                    d_lab1.as<int>(), d_perm2.as<int>(), d_lab2.as<int>(), ma1, ma2, c2, is2, is4,
+                    d_P.as<float>(), pp.N, bmin, d_pb.as<float>(), d_jbm.as<float>(), W.as<T>(),
+                    Tt.as<T>(), yamax.as<float>());
+                KFB_CUDA_TRY(cudaGetLastError());
+            }
+        }
+        if (!pform)
+            KFB_TRY(launch_hess_t<T>(dpairs.as<HessPair>(), np, x1p, x2p, dx2p,
+                                     d_perm1.as<int>(), d_lab1.as<int>(), d_perm2.as<int>(),
+                                     d_lab2.as<int>(), ma1, ma2, rep, c2, is2, is4, W.as<T>(),
+                                     Tt.as<T>(), tc ? yamax.as<float>() : nullptr, s));
         tr_t.reset();
         auto tr_y = std::make_unique<TraceScope>("hessian:y", s);
         float y_scale = 1.f;

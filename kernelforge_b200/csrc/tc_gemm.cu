@@ -596,6 +596,37 @@ __global__ void __launch_bounds__(256) transpose_split_dx_kernel(
     }
 }
 
+// Jr[(m, j, c)][k] = dX[m][j][k][c] (one K-major row of rep per atom j and
+// coordinate column c).  Tiles of 32 k x 32 c of one atom through shared
+// memory; atoms j >= nat[m] and columns c >= 3 nat[m] are not written.
+template <class T>
+__global__ void __launch_bounds__(256) transpose_split_dx_rows_kernel(
+    const T *__restrict__ dx, int ma, int rep, const int *__restrict__ nat, float scale,
+    __half *__restrict__ hi, __half *__restrict__ lo) {
+    __shared__ float tile[32][33];
+    const int mj = blockIdx.x, m = mj / ma, j = mj - m * ma;
+    const int na = min(max(nat[m], 0), ma);
+    const int k0 = blockIdx.y * 32, c0 = blockIdx.z * 32;
+    const int ld = 3 * ma;
+    if (j >= na || c0 >= 3 * na) return;
+    const T *base = dx + (size_t)mj * rep * ld;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int r = warp; r < 32; r += 8) {
+        const int k = k0 + r, c = c0 + lane;
+        tile[r][lane] = (k < rep && c < ld) ? (float)base[(size_t)k * ld + c] * scale : 0.f;
+    }
+    __syncthreads();
+    for (int r = warp; r < 32; r += 8) {
+        const int c = c0 + r, k = k0 + lane;
+        if (c >= ld || k >= rep) continue;
+        const float v = tile[lane][r];
+        const __half h = __float2half_rn(v);
+        const size_t o = ((size_t)mj * ld + c) * rep + k;
+        hi[o] = h;
+        lo[o] = __float2half_rn(v - __half2float(h));
+    }
+}
+
 // Yt[(p, c)][(i, k)] = Y[p][i][k][c], Y with row stride ld (the Hessian's
 // per-pair Y blocks, ma1 x rep x ld each).
 template <class T>
@@ -697,6 +728,27 @@ kfb_status transpose_split_dx(const T *dx, int nm, int ma, int rep, const int *n
 }
 
 template <class T>
+kfb_status transpose_split_dx_rows(const T *dx, int nm, int ma, int rep, const int *nat,
+                                   __half *hi, __half *lo, float *scale, cudaStream_t s) {
+    *scale = 1.f;
+    if (nm <= 0) return KFB_OK;
+    {
+        DevBuf d;
+        KFB_TRY(d.alloc(sizeof(float), s));
+        KFB_TRY(zero(d.ptr, sizeof(float), s));
+        const long long per = (long long)ma * rep * 3 * ma;
+        const unsigned bx = (unsigned)std::min<long long>((per + 255) / 256, 64);
+        absmax_dx_kernel<T><<<dim3(bx, (unsigned)nm), 256, 0, s>>>(dx, ma, rep, nat, d.as<float>());
+        KFB_CUDA_TRY(cudaGetLastError());
+        KFB_TRY(pow2_from_device(d.as<float>(), s, scale));
+    }
+    dim3 grid((unsigned)(nm * ma), (unsigned)((rep + 31) / 32), (unsigned)((3 * ma + 31) / 32));
+    transpose_split_dx_rows_kernel<T><<<grid, 256, 0, s>>>(dx, ma, rep, nat, *scale, hi, lo);
+    KFB_CUDA_TRY(cudaGetLastError());
+    return KFB_OK;
+}
+
+template <class T>
 kfb_status transpose_split_y(const T *Y, int np, int ma1, int rep, int ld, const float *amax,
                              __half *hi, __half *lo, float *scale, cudaStream_t s) {
     const long long kk = (long long)ma1 * rep;
@@ -712,6 +764,8 @@ template kfb_status split_rows<float>(const float *, long long, __half *, __half
                                       cudaStream_t);
 template kfb_status split_rows<double>(const double *, long long, __half *, __half *, float *,
                                        cudaStream_t);
+template kfb_status transpose_split_dx_rows<float>(const float *, int, int, int, const int *,
+                                                   __half *, __half *, float *, cudaStream_t);
 template kfb_status transpose_split_dx<float>(const float *, int, int, int, const int *, __half *,
                                               __half *, float *, cudaStream_t);
 template kfb_status transpose_split_dx<double>(const double *, int, int, int, const int *,

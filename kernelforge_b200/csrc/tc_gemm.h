@@ -91,6 +91,12 @@ kfb_status tc_gemm_grouped(const TcOperand &A, const TcOperand &B, int nprod, bo
 template <class T>
 kfb_status split_rows(const T *src, long long n, __half *hi, __half *lo, float *scale,
                       cudaStream_t s);
+// Jr[(m, j, c)][k] = dX[m][j][k][c] as scaled fp16 pairs: a K-major row of rep
+// per (atom, coordinate column); rows of padding atoms and columns are not
+// written.
+template <class T>
+kfb_status transpose_split_dx_rows(const T *dx, int nm, int ma, int rep, const int *nat,
+                                   __half *hi, __half *lo, float *scale, cudaStream_t s);
 template <class T>
 kfb_status transpose_split_dx(const T *dx, int nm, int ma, int rep, const int *nat, __half *hi,
                               __half *lo, float *scale, cudaStream_t s);

@@ -142,3 +142,30 @@ def test_jacobian_chunked_outer_molecules(precision, rep, monkeypatch):
     else:
         close(lk.kernel_gaussian_jacobian(X1, X2, dX2, Q1, Q2, N1, N2, s, precision=precision),
               o.kernel_gaussian_jacobian(X1, X2, dX2, Q1, Q2, N1, N2, s), precision)
+
+
+@pytest.mark.parametrize("gb", ["0.0001", "4"])
+def test_hessian_tensor_core_batches(gb, monkeypatch):
+    """Tensor-core Hessians with kernel 1 in GEMM form: a workspace of ~100 kB
+    gives batches of a few molecule pairs spanning at most two molecules b (the
+    projection buffer's capacity), the default one batch; symmetric RFP,
+    asymmetric and full energy+force kernels against the oracle."""
+    from kernelforge_b200 import local_kernels as lk
+    monkeypatch.setenv("KFB_WORKSPACE_GB", gb)
+    rep = 48
+    X1, dX1, Q1, N1 = make_set(7, 6, rep, 3, 41)
+    X2, dX2, Q2, N2 = make_set(5, 6, rep, 3, 42)
+    sc = 1.0 / np.sqrt(rep)
+    X1 *= 2 * sc
+    X2 *= 2 * sc
+    dX1 *= sc
+    dX2 *= sc
+    Q2[1, :2] = 9   # a set-2 label set 1 lacks
+    s = 2.0
+    p = "split_f16"
+    close(lk.kernel_gaussian_hessian_symm_rfp(X1, dX1, Q1, N1, s, precision=p),
+          o.kernel_gaussian_hessian_symm_rfp(X1, dX1, Q1, N1, s), p)
+    close(lk.kernel_gaussian_hessian(X1, dX1, X2, dX2, Q1, Q2, N1, N2, s, precision=p),
+          o.kernel_gaussian_hessian(X1, dX1, X2, dX2, Q1, Q2, N1, N2, s), p)
+    close(lk.kernel_gaussian_full(X1, dX1, X2, dX2, Q1, Q2, N1, N2, s, precision=p),
+          o.kernel_gaussian_full(X1, dX1, X2, dX2, Q1, Q2, N1, N2, s), p)
