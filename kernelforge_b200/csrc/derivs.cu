@@ -1719,6 +1719,15 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
         if (pform)  // the batch's molecules b fit the P buffer
             while (np > 1 && pairs[p0 + np - 1].b - pairs[p0].b + 1 > bcap) --np;
         npz = (size_t)np;
+        const int bmin = pairs[p0].b, bmax = pairs[p0 + np - 1].b;
+        // tensor-core contraction: the batch's pairs by (a, b), so that pairs
+        // (a, b), (a, b + 1) of whole molecules b can share one GEMM problem
+        // (their rows of Y and their output columns are adjacent)
+        if (tc)
+            std::stable_sort(pairs.begin() + p0, pairs.begin() + p0 + np,
+                             [](const HessPair &x, const HessPair &y) {
+                                 return x.a != y.a ? x.a < y.a : x.b < y.b;
+                             });
         KFB_CUDA_TRY(cudaMemcpyAsync(dpairs.ptr, pairs.data() + p0, np * sizeof(HessPair),
                                      cudaMemcpyHostToDevice, s));
         const T *x1p = static_cast<const T *>(s1.x), *x2p = static_cast<const T *>(s2.x);
@@ -1729,7 +1738,6 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
         if (tc) KFB_TRY(zero(yamax.ptr, sizeof(float), s));
         if constexpr (std::is_same<T, float>::value) {
             if (pform) {
-                const int bmin = pairs[p0].b, bmax = pairs[p0 + np - 1].b;
                 TcProb pp{};
                 pp.b_row0 = (int)((long long)bmin * bcols);
                 pp.M = (int)Mrows;
@@ -1802,21 +1810,35 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
         if (tc) {
             std::vector<TcProb> tprobs;
             tprobs.reserve(np);
-            for (int k = 0; k < np; ++k) {
+            for (int k = 0; k < np;) {
                 const HessPair &pr = pairs[p0 + k];
+                const bool dg = symmetric && pr.a == pr.b;
+                // merge the following pairs (a, b + 1), ... while the previous
+                // molecule is whole (no padding rows between the Y blocks) and
+                // the columns fit one 128-wide tile
+                int k1 = k + 1, ncols = 3 * pr.nb;
+                while (!dg && k1 < np) {
+                    const HessPair &q = pairs[p0 + k1], &prev = pairs[p0 + k1 - 1];
+                    if (q.a != pr.a || q.b != prev.b + 1 || prev.nb != ma2 ||
+                        (symmetric && q.a == q.b) || ncols + 3 * q.nb > 128)
+                        break;
+                    ncols += 3 * q.nb;
+                    ++k1;
+                }
                 TcProb p{};
                 p.a_row0 = pr.a * ld1;
                 p.a_k0 = 0;
                 p.b_row0 = k * ld2;
                 p.b_k0 = 0;
                 p.M = 3 * pr.na;
-                p.N = 3 * pr.nb;
+                p.N = ncols;
                 p.K = pr.na * rep;
                 p.row_off = off1[pr.a];
                 p.col_off = off2[pr.b];
-                p.diag = (symmetric && pr.a == pr.b) ? 1 : 0;
+                p.diag = dg ? 1 : 0;
                 p.alpha = 1.0 / ((double)jt_scale * (double)y_scale);
                 tprobs.push_back(p);
+                k = k1;
             }
             TcOperand A, B;
             A.hi = jth.ptr;
