@@ -16,9 +16,12 @@
 //   Y_i  = sum_{j in b, q_j = q_i} (w_ij J_j - w'_ij d_ij (J_j^T d_ij)^T),
 //   d_ij = x_i - x_j, w = e/sigma^2, w' = e/sigma^4
 // t'_ij = w'_ij J_j^T d_ij is formed once per same-label atom pair (kernel 1,
-// block per molecule pair), Y_i per (pair, 8-row slice of rep) with the
-// atoms of a label group in registers (kernel 2), and H_ab = J_a^T Y by one
-// GEMM problem per pair (tcgen05 split-fp16, or cuBLAS).
+// block per molecule pair; with tensor cores and FP32 inputs J_j^T d_ij is a
+// difference of two projections of centred descriptors onto the Jacobian
+// rows, one of them a tcgen05 GEMM per batch), Y_i per (pair, 8-row slice of
+// rep) with the atoms of a label group in registers (kernel 2), and
+// H_ab = J_a^T Y by one GEMM problem per pair, or per run of pairs
+// (a, b), (a, b + 1), ... (tcgen05 split-fp16, or cuBLAS).
 #include <cublas_v2.h>
 
 #include <algorithm>
