@@ -730,7 +730,8 @@ __global__ void pb_kernel(const T *__restrict__ x2, const T *__restrict__ dx2,
     }
 }
 
-// max |J_b| over the real atoms and columns of each molecule b
+// max |J_b| over the real atoms and columns of each molecule b (out zeroed
+// first; blockIdx.y splits a molecule's rows, warps per row)
 template <class T>
 __global__ void jmax_per_mol_kernel(const T *__restrict__ dx, int ma, int rep,
                                     const int *__restrict__ nat, float *__restrict__ out) {
@@ -739,18 +740,14 @@ __global__ void jmax_per_mol_kernel(const T *__restrict__ dx, int ma, int rep,
     const T *base = dx + (size_t)m * ma * rep * ld;
     float v = 0.f;
     const long long nrow = (long long)na * rep;
-    for (long long row = threadIdx.x >> 5; row < nrow; row += blockDim.x >> 5)
+    const int nw = blockDim.x >> 5;
+    for (long long row = (long long)blockIdx.y * nw + (threadIdx.x >> 5); row < nrow;
+         row += (long long)gridDim.y * nw)
         for (int c = threadIdx.x & 31; c < nc; c += 32)
             v = fmaxf(v, fabsf((float)base[row * ld + c]));
     for (int o = 16; o; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
-    __shared__ float red[32];
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        float mm = 0.f;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) mm = fmaxf(mm, red[w]);
-        out[m] = mm;
-    }
+    // non-negative floats order like their bit patterns
+    if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<int *>(out + m), __float_as_int(v));
 }
 
 // Kernel 1 with t from P: the same outputs as hess_t_kernel (W, Tt, bound);
@@ -1702,7 +1699,8 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
                 d_pb.as<float>());
             KFB_CUDA_TRY(cudaGetLastError());
             KFB_TRY(d_jbm.alloc((size_t)s2.v.nm * sizeof(float), s));
-            jmax_per_mol_kernel<float><<<(unsigned)s2.v.nm, 256, 0, s>>>(
+            KFB_TRY(zero(d_jbm.ptr, (size_t)s2.v.nm * sizeof(float), s));
+            jmax_per_mol_kernel<float><<<dim3((unsigned)s2.v.nm, 32), 256, 0, s>>>(
                 dx2f, ma2, rep, d_nat2.as<int>(), d_jbm.as<float>());
             KFB_CUDA_TRY(cudaGetLastError());
             bcap = (int)std::max<long long>(1, (long long)(budget_bytes() / 2) / pbytes);
