@@ -550,6 +550,8 @@ __global__ void split_rows_kernel(const T *__restrict__ src, long long n, float 
 // fp16 pairs, 128 bytes per warp); tiles wholly beyond the molecule's atoms
 // (j >= nat[m] or c >= 3 nat[m]) are skipped: the GEMMs read (j, k) < nat rep
 // only, and rows c >= 3 nat only feed output columns they discard.
+constexpr int TDX_TILES = 8;
+
 template <class T>
 __global__ void __launch_bounds__(256) transpose_split_dx_kernel(
     const T *__restrict__ dx, int ma, int rep, const int *__restrict__ nat, float scale,
@@ -558,39 +560,43 @@ __global__ void __launch_bounds__(256) transpose_split_dx_kernel(
     const int m = blockIdx.z;
     const int ld = 3 * ma;
     const long long kk_total = (long long)ma * rep;
-    const long long kk0 = (long long)blockIdx.x * 64;
     const int c0 = blockIdx.y * 32;
     const int na = min(max(nat[m], 0), ma);
-    if (kk0 >= (long long)na * rep || c0 >= 3 * na) return;
-    const T *base = dx + (size_t)m * kk_total * ld;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int r = warp; r < 64; r += 8) {
-        const long long kk = kk0 + r;
-        const int c = c0 + lane;
-        tile[r][lane] = (kk < kk_total && c < ld) ? (float)base[kk * ld + c] * scale : 0.f;
-    }
-    __syncthreads();
-    const long long kk = kk0 + 2 * lane;
-    for (int r = warp; r < 32; r += 8) {
-        const int c = c0 + r;
-        if (c >= ld) break;
-        const size_t o = ((size_t)m * ld + c) * kk_total + kk;
-        __half2 h, l;
-        const float a0 = tile[2 * lane][r], a1 = tile[2 * lane + 1][r];
-        h = __floats2half2_rn(a0, a1);
-        const float2 back = __half22float2(h);
-        l = __floats2half2_rn(a0 - back.x, a1 - back.y);
-        if (kk + 1 < kk_total && (o & 1) == 0) {
-            *reinterpret_cast<__half2 *>(hi + o) = h;
-            *reinterpret_cast<__half2 *>(lo + o) = l;
-        } else {
-            if (kk < kk_total) {
-                hi[o] = __low2half(h);
-                lo[o] = __low2half(l);
-            }
-            if (kk + 1 < kk_total) {
-                hi[o + 1] = __high2half(h);
-                lo[o + 1] = __high2half(l);
+    const T *base = dx + (size_t)m * kk_total * ld;
+    // TDX_TILES consecutive 64-row tiles per block (fewer, longer blocks)
+    for (int tt = 0; tt < TDX_TILES; ++tt) {
+        const long long kk0 = ((long long)blockIdx.x * TDX_TILES + tt) * 64;
+        if (kk0 >= (long long)na * rep || c0 >= 3 * na) return;   // block-uniform
+        if (tt > 0) __syncthreads();   // previous tile consumed
+        for (int r = warp; r < 64; r += 8) {
+            const long long kk = kk0 + r;
+            const int c = c0 + lane;
+            tile[r][lane] = (kk < kk_total && c < ld) ? (float)base[kk * ld + c] * scale : 0.f;
+        }
+        __syncthreads();
+        const long long kk = kk0 + 2 * lane;
+        for (int r = warp; r < 32; r += 8) {
+            const int c = c0 + r;
+            if (c >= ld) break;
+            const size_t o = ((size_t)m * ld + c) * kk_total + kk;
+            __half2 h, l;
+            const float a0 = tile[2 * lane][r], a1 = tile[2 * lane + 1][r];
+            h = __floats2half2_rn(a0, a1);
+            const float2 back = __half22float2(h);
+            l = __floats2half2_rn(a0 - back.x, a1 - back.y);
+            if (kk + 1 < kk_total && (o & 1) == 0) {
+                *reinterpret_cast<__half2 *>(hi + o) = h;
+                *reinterpret_cast<__half2 *>(lo + o) = l;
+            } else {
+                if (kk < kk_total) {
+                    hi[o] = __low2half(h);
+                    lo[o] = __low2half(l);
+                }
+                if (kk + 1 < kk_total) {
+                    hi[o + 1] = __high2half(h);
+                    lo[o + 1] = __high2half(l);
+                }
             }
         }
     }
@@ -721,7 +727,8 @@ kfb_status transpose_split_dx(const T *dx, int nm, int ma, int rep, const int *n
         KFB_CUDA_TRY(cudaGetLastError());
         KFB_TRY(pow2_from_device(d.as<float>(), s, scale));
     }
-    dim3 grid((unsigned)((kk + 63) / 64), (unsigned)((3 * ma + 31) / 32), (unsigned)nm);
+    dim3 grid((unsigned)((kk + 64 * TDX_TILES - 1) / (64 * TDX_TILES)),
+              (unsigned)((3 * ma + 31) / 32), (unsigned)nm);
     transpose_split_dx_kernel<T><<<grid, 256, 0, s>>>(dx, ma, rep, nat, *scale, hi, lo);
     KFB_CUDA_TRY(cudaGetLastError());
     return KFB_OK;
