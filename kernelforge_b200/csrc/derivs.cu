@@ -1510,6 +1510,10 @@ kfb_status jacobian_core(const DerivSet &outer, const DerivSet &inner, int rep, 
             B.lo = jtl.ptr;
             B.rows = (long long)inner.v.nm * 3 * ma_in;
             B.cols = (long long)ma_in * rep;
+            // longest problems first: the persistent CTAs take tiles in list
+            // order, so the ragged ends of the K loops fall in the last wave
+            std::stable_sort(tprobs.begin(), tprobs.end(),
+                             [](const TcProb &x, const TcProb &y) { return x.K > y.K; });
             KFB_TRY(tc_gemm_grouped(A, B, 3, false, tprobs, sink, s));
             continue;
         }
