@@ -184,3 +184,17 @@ def test_host_input_c_abi_f64(precision):
         np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-12)
     else:
         close32(got, ref)
+
+
+def test_host_input_more_chunks_than_molecules(monkeypatch):
+    """Host-memory descriptors of 5 molecules with 8 chunks requested: one
+    molecule per chunk."""
+    import torch
+
+    from kernelforge_b200 import cuda_local_kernels as clk
+    monkeypatch.setenv("KFB_H2D_CHUNKS", "8")
+    X, _, Q, N = make_set(5, 9, 32, 2, 77, species=[1, 6])
+    X = (X * 0.3).astype(np.float32)
+    rfp = clk.kernel_gaussian_symm_rfp(torch.from_numpy(X).pin_memory(), Q, N, 2.0)
+    ref = o.kernel_gaussian_symm(X.astype(np.float64), Q, N, 2.0)
+    close32(rfp.cpu().numpy(), o.full_to_rfp(ref, uplo_lower=True))

@@ -170,3 +170,25 @@ def test_mixed_solve_many_row_blocks(factor):
     ref = np.linalg.solve(A32.astype(np.float64) + 1e-3 * np.eye(n), y)
     np.testing.assert_allclose(alpha.cpu().numpy(), ref, rtol=1e-8,
                                atol=1e-8 * np.abs(ref).max())
+
+
+@pytest.mark.parametrize("n", [5, 64, 65, 130])
+def test_mixed_solve_fp64_factor_small_orders(n):
+    """FP64-factor refinement at orders around the 64-row blocks of the
+    triangular sweeps (one block, exactly one, one plus a ragged row, two plus a
+    ragged block)."""
+    import torch
+
+    from kernelforge_b200 import cuda_global_kernels as cgk
+    rng = np.random.default_rng(100 + n)
+    B = rng.normal(size=(n, n))
+    A32 = (B @ B.T / n + 0.3 * np.eye(n)).astype(np.float32)
+    y = rng.normal(size=n)
+    K = torch.tensor(o.full_to_rfp(A32.astype(np.float64), uplo_lower=True).astype(np.float32),
+                     device="cuda")
+    alpha, info = cgk.krr_solve_mixed(K, torch.tensor(y), l2=1e-3, uplo="L", tol=1e-11,
+                                      factor="fp64")
+    assert info["converged"], info
+    ref = np.linalg.solve(A32.astype(np.float64) + 1e-3 * np.eye(n), y)
+    np.testing.assert_allclose(alpha.cpu().numpy(), ref, rtol=1e-8,
+                               atol=1e-8 * np.abs(ref).max())
