@@ -101,7 +101,7 @@ kfb_status run(const ScalarProblem &p, const PairSink &sink, cudaStream_t s) {
         static_cast<const Tin *>(p.x1), src, R, p.rep, Dp, packed, norm);
     KFB_CUDA_TRY(cudaGetLastError());
     const T coef = T(-1.0 / (2.0 * p.sigma * p.sigma));
-    simt::scalar_tile_kernel<T><<<(unsigned)tiles.size(), 256, 0, s>>>(
+    simt::scalar_tile_kernel<T><<<(unsigned)tiles.size(), simt::SIMT_THREADS, 0, s>>>(
         packed, packed, Dp, norm, norm, mol, mol, dtiles, coef, sink);
     KFB_CUDA_TRY(cudaGetLastError());
     // the host vectors above are read by the copies before cudaMemcpyAsync

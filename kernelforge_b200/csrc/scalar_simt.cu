@@ -67,9 +67,9 @@ kfb_status run_simt(const ScalarProblem &p, const PairSink &sink, cudaStream_t s
     timer.start();
     for (size_t off = 0; off < ntiles; off += (size_t)1 << 30) {
         const unsigned nb_ = (unsigned)std::min<size_t>(ntiles - off, (size_t)1 << 30);
-        scalar_tile_kernel<T><<<nb_, 256, 0, s>>>(pa.as<T>(), PB.as<T>(), Dp, na.as<T>(),
-                                                   NB.as<T>(), ma.as<int>(), MB.as<int>(),
-                                                   dt.as<PairTile>() + off, coef, sink);
+        scalar_tile_kernel<T><<<nb_, simt::SIMT_THREADS, 0, s>>>(
+            pa.as<T>(), PB.as<T>(), Dp, na.as<T>(), NB.as<T>(), ma.as<int>(), MB.as<int>(),
+            dt.as<PairTile>() + off, coef, sink);
         KFB_CUDA_TRY(cudaGetLastError());
     }
     timer.stop();

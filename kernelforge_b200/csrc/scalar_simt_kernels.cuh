@@ -29,8 +29,13 @@ __global__ void pack_rows_kernel(const Tin *__restrict__ x, const int *__restric
     if (lane == 0) norm[warp] = (T)s;
 }
 
+// 128 threads: thread (ty = tid / 16, tx = tid % 16) owns rows 8 ty .. 8 ty + 7
+// and columns 4 tx .. 4 tx + 3 of the 64 x 64 tile (12 shared loads per 32
+// FMAs in the K loop).
+constexpr int SIMT_THREADS = 128;
+
 template <class T>
-__global__ void __launch_bounds__(256) scalar_tile_kernel(
+__global__ void __launch_bounds__(SIMT_THREADS) scalar_tile_kernel(
     const T *__restrict__ A, const T *__restrict__ B, int Dp, const T *__restrict__ nA,
     const T *__restrict__ nB, const int *__restrict__ molA, const int *__restrict__ molB,
     const PairTile *__restrict__ tiles, T coef, PairSink sink) {
@@ -47,20 +52,20 @@ __global__ void __launch_bounds__(256) scalar_tile_kernel(
 
     const PairTile t = tiles[blockIdx.x];
     const int tid = threadIdx.x;
-    const int tx = tid & 15, ty = tid >> 4;
+    const int tx = tid & 15, ty = tid >> 4;   // ty < 8
     const int nra = min(ST, t.a_end - t.a0);
     const int nrb = min(ST, t.b_end - t.b0);
 
-    T acc[4][4];
+    T acc[8][4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < 8; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[i][j] = T(0);
 
-    const int lr = tid >> 2, lk = (tid & 3) * 4;  // loader: row, first k
+    const int lr = tid >> 1, lk = (tid & 1) * 8;  // loader: row, first k
     for (int k0 = 0; k0 < Dp; k0 += SK) {
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int u = 0; u < 8; ++u) {
             const int k = k0 + lk + u;
             As[lk + u][lr] = (lr < nra && k < Dp) ? A[(size_t)(t.a0 + lr) * Dp + k] : T(0);
             Bs[lk + u][lr] = (lr < nrb && k < Dp) ? B[(size_t)(t.b0 + lr) * Dp + k] : T(0);
@@ -68,13 +73,13 @@ __global__ void __launch_bounds__(256) scalar_tile_kernel(
         __syncthreads();
 #pragma unroll
         for (int kk = 0; kk < SK; ++kk) {
-            T a[4], b[4];
+            T a[8], b[4];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = As[kk][ty * 4 + i];
+            for (int i = 0; i < 8; ++i) a[i] = As[kk][ty * 8 + i];
 #pragma unroll
             for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx * 4 + j];
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
+            for (int i = 0; i < 8; ++i)
 #pragma unroll
                 for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
         }
@@ -83,8 +88,8 @@ __global__ void __launch_bounds__(256) scalar_tile_kernel(
 
     // e_ij into shared memory (zero outside the valid rows / columns)
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const int r = ty * 4 + i;
+    for (int i = 0; i < 8; ++i) {
+        const int r = ty * 8 + i;
         const T ni = r < nra ? nA[t.a0 + r] : T(0);
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
