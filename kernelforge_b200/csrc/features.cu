@@ -96,22 +96,6 @@ __global__ void gather_rows_f32_kernel(const T *__restrict__ x, const int *__res
     }
 }
 
-// dst[c][r] = src[r][c] for an FP32 (rows, cols) block
-__global__ void transpose_f32_kernel(const float *__restrict__ src, int rows, int cols,
-                                     float *__restrict__ dst) {
-    __shared__ float tile[32][33];
-    const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
-    for (int rr = threadIdx.y; rr < 32; rr += blockDim.y) {
-        const int r = r0 + rr, c = c0 + threadIdx.x;
-        tile[rr][threadIdx.x] = (r < rows && c < cols) ? src[(size_t)r * cols + c] : 0.f;
-    }
-    __syncthreads();
-    for (int cc = threadIdx.y; cc < 32; cc += blockDim.y) {
-        const int c = c0 + cc, r = r0 + threadIdx.x;
-        if (c < cols && r < rows) dst[(size_t)c * rows + r] = tile[threadIdx.x][cc];
-    }
-}
-
 // dst[c * ld_dst + r] = src[r][c] for a BF16 (rows, cols) array, and
 // colsum[c] += sum_r src[r][c] (FP32, optional).  64 x 64 tiles through shared
 // memory; bf16x2 loads along c and bf16x2 stores along r when cols, ld_dst and

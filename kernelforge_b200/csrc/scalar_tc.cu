@@ -241,7 +241,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
         const int h = e_id >> 2;
         float *scr = reinterpret_cast<float *>(smem + OFF_SCR) + e_id * SCR_FLOATS;
         int *runs = reinterpret_cast<int *>(smem + OFF_RUNS) + e_id * RUN_INTS;
-        int *rstart = runs, *cstart = runs + 33, *rmolr = runs + 66, *cmolr = runs + 99;
+        int *rstart = runs, *rmolr = runs + 66, *cmolr = runs + 99;   // 33 ints each
         const unsigned lt_mask = (1u << lane) - 1u;
         int acc = 0;
         uint32_t aph = 0;
