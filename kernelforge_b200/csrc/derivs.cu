@@ -750,7 +750,8 @@ __global__ void jmax_per_mol_kernel(const T *__restrict__ dx, int ma, int rep,
     if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<int *>(out + m), __float_as_int(v));
 }
 
-// Kernel 1 with t from P: the same outputs as hess_t_kernel (W, Tt, bound);
+// Kernel 1 with t from P: the same outputs as hess_t_kernel (W, Tt, bound;
+// without the rank term in Y (rank_in_y = 0) the bound is max|J_b| sum_j w_ij);
 // weights from the centred dot products G[(a, i)][(b - b0) * ma2 + j] (row
 // length ldg) and the norms; t by a warp per (same-label pair, 32 columns).  P rows are set-1 padded atoms,
 // P columns ((b - b0) * ma2 + j) * ld2 + c with row length ldp.
@@ -760,7 +761,7 @@ __global__ void __launch_bounds__(256) hess_t_p_kernel(
     const int *__restrict__ lab1, const int *__restrict__ perm2, const int *__restrict__ lab2,
     int ma1, int ma2, float c2, float is2, float is4, const float *__restrict__ P,
     long long ldp, int b0, const float *__restrict__ PB, const float *__restrict__ jbmax,
-    float *__restrict__ W, float *__restrict__ Tt, float *__restrict__ bound) {
+    int rank_in_y, float *__restrict__ W, float *__restrict__ Tt, float *__restrict__ bound) {
     extern __shared__ __align__(16) unsigned char ht_raw[];
     int4 *groups = reinterpret_cast<int4 *>(ht_raw);  // ma1
     int *pa = reinterpret_cast<int *>(groups + ma1);   // ma1
@@ -831,7 +832,7 @@ __global__ void __launch_bounds__(256) hess_t_p_kernel(
             t = w2s[i * ma2 + j] *
                 (Prow0[(size_t)i * ldp + (size_t)j * ld2 + c] - PBb[(size_t)j * ld2 + c]);
         if (c < ncol) Tt[(wbase + (size_t)i * ma2 + j) * ld2 + c] = t;
-        if (bound) {
+        if (bound && rank_in_y) {
             float m = fabsf(t);
             for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
             if (lane == 0) atomicAdd(&bterm[i], dinf[i * ma2 + j] * m);
@@ -868,6 +869,9 @@ size_t hess_t_p_smem(int ma1, int ma2) {
 // descriptor rows of the slice are staged.
 //   MODE 1: fp16 pair hi/lo of scale * Y, K-major rows (p, c) of (i, k)
 //   MODE 2: Y[p, i, k, c] in T
+//   MODE 3: as MODE 1 for Y_i = sum_j w_ij J_j alone (the rank term
+//           -sum_j d_ij t'_ij^T is added to the Hessian block by
+//           hess_rank_kernel after the contraction)
 // FULL: rep % 8 == 0 (no row guards).
 constexpr int HY_KR = 8;
 template <class T> struct HyCfg { static constexpr int IG = 8, WARPS = 8; };
@@ -910,6 +914,7 @@ __device__ __forceinline__ void hy_chunk(const HessPair &pr, int p, int4 gr, int
                                          __half *__restrict__ yhi, __half *__restrict__ ylo,
                                          T *__restrict__ Y) {
     constexpr int IG = HyCfg<T>::IG, SS = hy_stage<T>();
+    constexpr bool RANK = MODE != 3;
     const int lane = threadIdx.x & 31;
     const int ld2 = 3 * ma2, ncol = 3 * pr.nb;
     const int cs = c < ncol ? c : 0;
@@ -937,10 +942,12 @@ __device__ __forceinline__ void hy_chunk(const HessPair &pr, int p, int4 gr, int
                 else
                     dst[r * 32 + lane] = T(0);
             }
+            if (RANK) {
 #pragma unroll
-            for (int ii = 0; ii < IGC; ++ii)
-                cp_async_elem<T>(dst + (HY_KR + ii) * 32 + lane,
-                                 Tb + ((size_t)pa[i0 + ii] * ma2 + j) * ld2);
+                for (int ii = 0; ii < IGC; ++ii)
+                    cp_async_elem<T>(dst + (HY_KR + ii) * 32 + lane,
+                                     Tb + ((size_t)pa[i0 + ii] * ma2 + j) * ld2);
+            }
             // lane l fetches w of atom l mod IGC (no divergent branch)
             cp_async_elem<T>(dst + (HY_KR + IG) * 32 + lane,
                              Wb + (size_t)pa[i0 + (lane & (IGC - 1))] * ma2 + j);
@@ -962,28 +969,35 @@ __device__ __forceinline__ void hy_chunk(const HessPair &pr, int p, int4 gr, int
         const T wl = src[(HY_KR + IG) * 32 + lane];
 #pragma unroll
         for (int ii = 0; ii < IGC; ++ii) {
-            t[ii] = src[(HY_KR + ii) * 32 + lane];
+            if (RANK) t[ii] = src[(HY_KR + ii) * 32 + lane];
             w[ii] = __shfl_sync(0xffffffffu, wl, ii);
         }
-        load_vec<T, HY_KR>(xb_s + pb[gr.z + jj] * kt + kk0, xj);
+        if (RANK) load_vec<T, HY_KR>(xb_s + pb[gr.z + jj] * kt + kk0, xj);
         st = st == JRING - 1 ? 0 : st + 1;
 #pragma unroll
         for (int ii = 0; ii < IGC; ++ii) {
-            rr[ii] += t[ii];
+            if (RANK) {
+                rr[ii] += t[ii];
 #pragma unroll
-            for (int r = 0; r < HY_KR; ++r)
-                acc[ii][r] = fma(w[ii], jv[r], fma(xj[r], t[ii], acc[ii][r]));
+                for (int r = 0; r < HY_KR; ++r)
+                    acc[ii][r] = fma(w[ii], jv[r], fma(xj[r], t[ii], acc[ii][r]));
+            } else {
+#pragma unroll
+                for (int r = 0; r < HY_KR; ++r) acc[ii][r] = fma(w[ii], jv[r], acc[ii][r]);
+            }
         }
     }
     if (c >= ncol) return;
 #pragma unroll
     for (int ii = 0; ii < IGC; ++ii) {
         const int i = pa[i0 + ii];
-        T xi[HY_KR];
-        load_vec<T, HY_KR>(xa_s + i * kt + kk0, xi);
+        if (RANK) {
+            T xi[HY_KR];
+            load_vec<T, HY_KR>(xa_s + i * kt + kk0, xi);
 #pragma unroll
-        for (int r = 0; r < HY_KR; ++r) acc[ii][r] = fma(-xi[r], rr[ii], acc[ii][r]);
-        if (MODE == 1) {
+            for (int r = 0; r < HY_KR; ++r) acc[ii][r] = fma(-xi[r], rr[ii], acc[ii][r]);
+        }
+        if (MODE != 2) {
             // rep % 16 == 0 on this path: 8 rows are 16 aligned bytes
             // packed conversions: two values per instruction
             unsigned hw[HY_KR / 2], lw[HY_KR / 2];
@@ -1031,13 +1045,15 @@ __global__ void __launch_bounds__(256, 2) hess_y_kernel(
     const int kbase = blockIdx.x * kt;
     for (int e = threadIdx.x; e < pr.na; e += blockDim.x) pa[e] = perm1[(size_t)pr.a * ma1 + e];
     for (int e = threadIdx.x; e < pr.nb; e += blockDim.x) pb[e] = perm2[(size_t)pr.b * ma2 + e];
-    for (int e = threadIdx.x; e < pr.na * kt; e += blockDim.x) {
-        const int i = e / kt, kk = e - i * kt;
-        xa_s[e] = (kbase + kk < rep) ? x1[((size_t)pr.a * ma1 + i) * rep + kbase + kk] : T(0);
-    }
-    for (int e = threadIdx.x; e < pr.nb * kt; e += blockDim.x) {
-        const int j = e / kt, kk = e - j * kt;
-        xb_s[e] = (kbase + kk < rep) ? x2[((size_t)pr.b * ma2 + j) * rep + kbase + kk] : T(0);
+    if (MODE != 3) {  // descriptor rows of the slice (rank term)
+        for (int e = threadIdx.x; e < pr.na * kt; e += blockDim.x) {
+            const int i = e / kt, kk = e - i * kt;
+            xa_s[e] = (kbase + kk < rep) ? x1[((size_t)pr.a * ma1 + i) * rep + kbase + kk] : T(0);
+        }
+        for (int e = threadIdx.x; e < pr.nb * kt; e += blockDim.x) {
+            const int j = e / kt, kk = e - j * kt;
+            xb_s[e] = (kbase + kk < rep) ? x2[((size_t)pr.b * ma2 + j) * rep + kbase + kk] : T(0);
+        }
     }
     if (threadIdx.x == 0)  // atoms of a whose label b lacks get Y = 0 (written)
         ngroups = pair_label_groups(lab1 + (size_t)pr.a * ma1, lab2 + (size_t)pr.b * ma2,
@@ -1067,6 +1083,113 @@ __global__ void __launch_bounds__(256, 2) hess_y_kernel(
             else
                 KFB_HY_CHUNK(1);
 #undef KFB_HY_CHUNK
+        }
+    }
+}
+
+// ------------------------------------------------------- Hessian rank term
+// With Y_i = sum_j w_ij J_j (MODE 3) the contraction leaves out
+//   -sum_i J_i^T sum_j d_ij t'_ij^T = -sum_{i, j same label} s_ij t'_ij^T,
+//   s_ij[c'] = J_i[:, c'] . (x_i - x_j) = PB1[(a, i)][c'] - Q[(b - b0, j)][(a, i, c') - qc0],
+// PB1 = (x_i - mu_l) . J_i[:, c'] and Q = (x_j - mu_l) . J_i[:, c'] (one
+// projection GEMM per batch over its molecules b and the range of set-1 rows
+// from column qc0 that its molecules a cover; mu_l the label centre that also
+// centres P).  This kernel adds that term to the pair's Hessian block after
+// the contraction wrote it: block per (pair, 64 x 64 tile of (c', c)),
+// 256 threads of 4 x 4 register tiles, the same-label pairs in chunks of HR_Q
+// with their s and t' rows staged in shared memory.  Every output element
+// belongs to one thread of one block and the contraction ran before on the
+// same stream, so the adds need no atomics.  ma1, ma2 <= HR_MAXA.
+constexpr int HR_Q = 32, HR_T = 64, HR_MAXA = 64;
+__global__ void __launch_bounds__(256) hess_rank_kernel(
+    const HessPair *__restrict__ pairs, const int *__restrict__ perm1,
+    const int *__restrict__ lab1, const int *__restrict__ perm2, const int *__restrict__ lab2,
+    int ma1, int ma2, const float *__restrict__ Q, long long ldq, int b0, long long qc0,
+    const float *__restrict__ PB1, const float *__restrict__ Tt, const int *__restrict__ off1,
+    const int *__restrict__ off2, int symmetric, ElemSink sink) {
+    __shared__ int4 groups[HR_MAXA];
+    __shared__ int pa[HR_MAXA], pb[HR_MAXA], gstart[HR_MAXA + 1], qi[HR_Q], qj[HR_Q];
+    __shared__ int ngroups;
+    __shared__ __align__(16) float Ss[HR_Q][HR_T];
+    __shared__ __align__(16) float Ts[HR_Q][HR_T];
+    const int p = blockIdx.y;
+    const HessPair pr = pairs[p];
+    const int ld1 = 3 * ma1, ld2 = 3 * ma2, m1 = 3 * pr.na, n2 = 3 * pr.nb;
+    const int ntc = (ld2 + HR_T - 1) / HR_T;
+    const int r0 = (blockIdx.x / ntc) * HR_T, c0 = (blockIdx.x % ntc) * HR_T;
+    if (r0 >= m1 || c0 >= n2) return;  // block-uniform
+    const int tid = threadIdx.x;
+    for (int e = tid; e < pr.na; e += blockDim.x) pa[e] = perm1[(size_t)pr.a * ma1 + e];
+    for (int e = tid; e < pr.nb; e += blockDim.x) pb[e] = perm2[(size_t)pr.b * ma2 + e];
+    if (tid == 0) {
+        const int g = pair_label_groups(lab1 + (size_t)pr.a * ma1, lab2 + (size_t)pr.b * ma2,
+                                        pr.na, pr.nb, groups);
+        ngroups = g;
+        gstart[0] = 0;
+        for (int q = 0; q < g; ++q)
+            gstart[q + 1] = gstart[q] + (groups[q].y - groups[q].x) * (groups[q].w - groups[q].z);
+    }
+    __syncthreads();
+    const int npairs = gstart[ngroups];
+    const int ty = tid >> 4, tx = tid & 15;
+    const size_t arow = (size_t)pr.a * ma1;
+    const float *Qb = Q + (size_t)(pr.b - b0) * ma2 * ldq;
+    const float *Tp = Tt + (size_t)p * ma1 * ma2 * ld2;
+    float acc[4][4] = {};
+    for (int q0 = 0; q0 < npairs; q0 += HR_Q) {
+        if (tid < HR_Q) {
+            const int q = q0 + tid;
+            int i = -1, j = -1;
+            if (q < npairs) {
+                int g = 0;
+                while (gstart[g + 1] <= q) ++g;
+                const int4 gr = groups[g];
+                const int off = q - gstart[g], nbg = gr.w - gr.z;
+                i = pa[gr.x + off / nbg];
+                j = pb[gr.z + off % nbg];
+            }
+            qi[tid] = i;
+            qj[tid] = j;
+        }
+        __syncthreads();
+        for (int e = tid; e < HR_Q * HR_T; e += blockDim.x) {
+            const int qq = e / HR_T, r = e - qq * HR_T;
+            const int i = qi[qq], j = qj[qq];
+            float sv = 0.f, tv = 0.f;
+            if (i >= 0) {
+                const size_t col = (arow + i) * ld1;
+                if (r0 + r < m1)
+                    sv = PB1[col + r0 + r] - Qb[(size_t)j * ldq + (col - qc0) + r0 + r];
+                if (c0 + r < n2) tv = Tp[((size_t)i * ma2 + j) * ld2 + c0 + r];
+            }
+            Ss[qq][r] = sv;
+            Ts[qq][r] = tv;
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int qq = 0; qq < HR_Q; ++qq) {
+            const float4 sv = *reinterpret_cast<const float4 *>(&Ss[qq][ty * 4]);
+            const float4 tv = *reinterpret_cast<const float4 *>(&Ts[qq][tx * 4]);
+            const float sa[4] = {sv.x, sv.y, sv.z, sv.w}, ta[4] = {tv.x, tv.y, tv.z, tv.w};
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) acc[u][v] = fmaf(sa[u], ta[v], acc[u][v]);
+        }
+        __syncthreads();  // Ss, Ts, qi, qj reused
+    }
+    const int dg = (symmetric && pr.a == pr.b) ? 1 : 0;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int R = r0 + ty * 4 + u;
+        if (R >= m1) continue;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const int C = c0 + tx * 4 + v;
+            if (C >= n2) continue;
+            const double val = -(double)acc[u][v];
+            sink_positions(sink, (long long)off1[pr.a] + R, (long long)off2[pr.b] + C, dg,
+                           [&](long long idx) { sink_add(sink, idx, val); });
         }
     }
 }
@@ -1609,11 +1732,14 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
     // columns of one molecule b for every set-1 atom within half the workspace
     // and at most 16 labels; otherwise kernel 1 forms J_j^T d_ij itself.
     const long long Mrows = (long long)s1.v.nm * ma1, bcols = (long long)ma2 * ld2;
-    bool pform = false;
+    // With the GEMM form the rank term of Y moves to hess_rank_kernel (hrank):
+    // Q = (X2 - mu) Jr1^T per batch, set-1 Jacobian rows (a, i, c') as columns.
+    const long long Mq = (long long)s1.v.nm * ma1 * ld1;
+    bool pform = false, hrank = false;
     int bcap = 0;
-    float xs_scale = 1.f, jr_scale = 1.f;
+    float xs_scale = 1.f, jr_scale = 1.f, jr1_scale = 1.f;
     DevBuf d_l1, d_l2, d_sums, d_invc, d_amx, xh1, xl1, jrh, jrl, d_pb, d_jbm, d_P, d_nat2,
-        d_n1, xh2, xl2, d_n2, d_G;
+        d_n1, xh2, xl2, d_n2, d_G, jr1h, jr1l, d_pb1, d_Q, d_off1, d_off2, d_nat1;
     float xs2_scale = 1.f;
     if constexpr (std::is_same<T, float>::value) {
         const std::vector<int> labs1 = collect_labels(s1.v, nullptr);
@@ -1621,6 +1747,9 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
         pform = tc && !labs1.empty() && labs1.size() <= 16 &&
                 pbytes <= (long long)(budget_bytes() / 2) && Mrows < INT_MAX &&
                 (long long)s2.v.nm * bcols < INT_MAX;
+        const long long qbytes = Mq * ma2 * (long long)sizeof(float);
+        hrank = pform && ma1 <= HR_MAXA && ma2 <= HR_MAXA && Mq < INT_MAX &&
+                pbytes + qbytes <= (long long)(budget_bytes() / 2);
         if (pform) {
             TraceScope tr_p("hessian:p-setup", s);
             const int L = (int)labs1.size();
@@ -1707,7 +1836,30 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
             jmax_per_mol_kernel<float><<<dim3((unsigned)s2.v.nm, 32), 256, 0, s>>>(
                 dx2f, ma2, rep, d_nat2.as<int>(), d_jbm.as<float>());
             KFB_CUDA_TRY(cudaGetLastError());
-            bcap = (int)std::max<long long>(1, (long long)(budget_bytes() / 2) / pbytes);
+            if (hrank) {
+                // set-1 Jacobian rows and PB1 (the set-2 ones for a symmetric call)
+                jr1_scale = jr_scale;
+                if (!symmetric) {
+                    const float *dx1f = static_cast<const float *>(s1.dx);
+                    std::vector<int> nat1(s1.v.nm);
+                    for (int m = 0; m < s1.v.nm; ++m) nat1[m] = s1.v.natoms(m);
+                    KFB_TRY(upload(d_nat1, nat1, s));
+                    KFB_TRY(jr1h.alloc((size_t)Mq * rep * sizeof(__half), s));
+                    KFB_TRY(jr1l.alloc((size_t)Mq * rep * sizeof(__half), s));
+                    KFB_TRY(transpose_split_dx_rows<float>(dx1f, s1.v.nm, ma1, rep,
+                                                           d_nat1.as<int>(), jr1h.as<__half>(),
+                                                           jr1l.as<__half>(), &jr1_scale, s));
+                    KFB_TRY(d_pb1.alloc((size_t)Mq * sizeof(float), s));
+                    pb_kernel<float><<<(unsigned)Mrows, 128, 0, s>>>(
+                        x1f, dx1f, d_l1.as<int>(), ma1, rep, d_sums.as<double>(),
+                        d_invc.as<double>(), d_pb1.as<float>());
+                    KFB_CUDA_TRY(cudaGetLastError());
+                }
+                KFB_TRY(upload(d_off1, off1, s));
+                KFB_TRY(upload(d_off2, off2, s));
+            }
+            bcap = (int)std::max<long long>(
+                1, (long long)(budget_bytes() / 2) / (pbytes + (hrank ? qbytes : 0)));
             int span_max = 1;
             for (size_t q0 = 0; q0 < pairs.size(); q0 += batch) {
                 const size_t q1 = std::min(pairs.size(), q0 + batch) - 1;
@@ -1716,6 +1868,7 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
             bcap = std::min(bcap, span_max);
             KFB_TRY(d_P.alloc((size_t)bcap * Mrows * bcols * sizeof(float), s));
             KFB_TRY(d_G.alloc((size_t)bcap * Mrows * ma2 * sizeof(float), s));
+            if (hrank) KFB_TRY(d_Q.alloc((size_t)bcap * ma2 * Mq * sizeof(float), s));
         }
     }
     const size_t smem_p = hess_t_p_smem(ma1, ma2);
@@ -1784,8 +1937,8 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
                     dpairs.as<HessPair>(), d_G.as<float>(), pg.N, d_n1.as<float>(),
                     symmetric ? d_n1.as<float>() : d_n2.as<float>(), d_perm1.as<int>(),
                     d_lab1.as<int>(), d_perm2.as<int>(), d_lab2.as<int>(), ma1, ma2, c2, is2, is4,
-                    d_P.as<float>(), pp.N, bmin, d_pb.as<float>(), d_jbm.as<float>(), W.as<T>(),
-                    Tt.as<T>(), yamax.as<float>());
+                    d_P.as<float>(), pp.N, bmin, d_pb.as<float>(), d_jbm.as<float>(),
+                    hrank ? 0 : 1, W.as<T>(), Tt.as<T>(), yamax.as<float>());
                 KFB_CUDA_TRY(cudaGetLastError());
             }
         }
@@ -1799,11 +1952,18 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
         float y_scale = 1.f;
         if (tc) {
             KFB_TRY(pow2_from_device(yamax.as<float>(), s, &y_scale));
-            KFB_TRY((launch_hess_y<T, 1>(dpairs.as<HessPair>(), np, x1p, x2p, dx2p,
-                                         d_perm1.as<int>(), d_lab1.as<int>(), d_perm2.as<int>(),
-                                         d_lab2.as<int>(), ma1, ma2, rep, W.as<T>(), Tt.as<T>(),
-                                         y_scale, yth.as<__half>(), ytl.as<__half>(), nullptr,
-                                         s)));
+            if (hrank)
+                KFB_TRY((launch_hess_y<T, 3>(dpairs.as<HessPair>(), np, x1p, x2p, dx2p,
+                                             d_perm1.as<int>(), d_lab1.as<int>(),
+                                             d_perm2.as<int>(), d_lab2.as<int>(), ma1, ma2, rep,
+                                             W.as<T>(), Tt.as<T>(), y_scale, yth.as<__half>(),
+                                             ytl.as<__half>(), nullptr, s)));
+            else
+                KFB_TRY((launch_hess_y<T, 1>(dpairs.as<HessPair>(), np, x1p, x2p, dx2p,
+                                             d_perm1.as<int>(), d_lab1.as<int>(),
+                                             d_perm2.as<int>(), d_lab2.as<int>(), ma1, ma2, rep,
+                                             W.as<T>(), Tt.as<T>(), y_scale, yth.as<__half>(),
+                                             ytl.as<__half>(), nullptr, s)));
         } else {
             KFB_TRY((launch_hess_y<T, 2>(dpairs.as<HessPair>(), np, x1p, x2p, dx2p,
                                          d_perm1.as<int>(), d_lab1.as<int>(), d_perm2.as<int>(),
@@ -1855,6 +2015,45 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
             B.rows = (long long)np * ld2;
             B.cols = (long long)ma1 * rep;
             KFB_TRY(tc_gemm_grouped(A, B, 3, false, tprobs, sink, s));
+            tr_g.reset();
+            if constexpr (std::is_same<T, float>::value) {
+                if (hrank) {
+                    TraceScope tr_r("hessian:rank", s);
+                    // set-1 rows of the batch's molecules a (pairs sorted by a)
+                    const long long rows_a = (long long)ma1 * ld1;
+                    const int amin = pairs[p0].a, amax = pairs[p0 + np - 1].a;
+                    TcProb pq{};
+                    pq.a_row0 = bmin * ma2;
+                    pq.b_row0 = (int)(amin * rows_a);
+                    pq.M = (bmax - bmin + 1) * ma2;
+                    pq.N = (int)((amax - amin + 1) * rows_a);
+                    pq.K = rep;
+                    pq.alpha = 1.0 / ((double)xs2_scale * (double)jr1_scale);
+                    TcOperand Aq, Bq;
+                    Aq.hi = symmetric ? xh1.ptr : xh2.ptr;
+                    Aq.lo = symmetric ? xl1.ptr : xl2.ptr;
+                    Aq.rows = (long long)s2.v.nm * ma2;
+                    Aq.cols = rep;
+                    Bq.hi = symmetric ? jrh.ptr : jr1h.ptr;
+                    Bq.lo = symmetric ? jrl.ptr : jr1l.ptr;
+                    Bq.rows = Mq;
+                    Bq.cols = rep;
+                    TcEpi eq;
+                    eq.mode = EPI_DENSE;
+                    eq.zf32 = d_Q.as<float>();
+                    eq.ld = pq.N;
+                    KFB_TRY(tc_gemm_grouped(Aq, Bq, 3, false, {pq}, ElemSink(), s, eq));
+                    const unsigned tiles =
+                        (unsigned)(((ld1 + HR_T - 1) / HR_T) * ((ld2 + HR_T - 1) / HR_T));
+                    hess_rank_kernel<<<dim3(tiles, (unsigned)np), 256, 0, s>>>(
+                        dpairs.as<HessPair>(), d_perm1.as<int>(), d_lab1.as<int>(),
+                        d_perm2.as<int>(), d_lab2.as<int>(), ma1, ma2, d_Q.as<float>(), pq.N, bmin,
+                        (long long)pq.b_row0,
+                        symmetric ? d_pb.as<float>() : d_pb1.as<float>(), Tt.as<float>(),
+                        d_off1.as<int>(), d_off2.as<int>(), symmetric ? 1 : 0, sink);
+                    KFB_CUDA_TRY(cudaGetLastError());
+                }
+            }
             continue;
         }
         std::vector<GemmProb> probs;

@@ -69,6 +69,38 @@ __device__ __forceinline__ void sink_store(const ElemSink &s, long long R, long 
     }
 }
 
+__device__ __forceinline__ void sink_add(const ElemSink &s, long long idx, double v) {
+    if (s.f64)
+        static_cast<double *>(s.out)[idx] += v;
+    else
+        static_cast<float *>(s.out)[idx] += (float)v;
+}
+
+// Calls f(idx) for every output index that sink_store(s, R, C, v, diag)
+// writes (none, one, or the two mirrored entries of a dense symmetric sink).
+template <class F>
+__device__ __forceinline__ void sink_positions(const ElemSink &s, long long R, long long C,
+                                               int diag, F f) {
+    R += s.row_base;
+    C += s.col_base;
+    if (s.mode == EM_RECT) {
+        f(R * s.ld + C);
+    } else if (s.mode == EM_RECT_T) {
+        f(C * s.ld + R);
+    } else {
+        if (diag && R > C) return;
+        if (s.layout == KFB_DENSE) {
+            f(R * s.ld + C);
+            if (R != C) f(C * s.ld + R);
+        } else if (s.layout == LAYOUT_DENSE_LOWER) {
+            const long long hi = R > C ? R : C, lo = R > C ? C : R;
+            f(hi * s.ld + lo);
+        } else {
+            f(sym_index((kfb_layout)s.layout, s.ld, R, C));
+        }
+    }
+}
+
 // tc: run the contraction GEMMs on the tensor cores (split fp16, three
 // products); needs rep % 16 == 0 and an sm_100 device.
 template <class T>
