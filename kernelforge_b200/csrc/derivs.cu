@@ -767,10 +767,12 @@ __global__ void __launch_bounds__(256) hess_t_p_kernel(
     int *pa = reinterpret_cast<int *>(groups + ma1);   // ma1
     int *pb = pa + ma1;                                // ma2
     int *gstart = pb + ma2;                            // ma1 + 1
-    float *wsum = reinterpret_cast<float *>(gstart + ma1 + 1);  // ma1
-    float *bterm = wsum + ma1;                                   // ma1
-    float *dinf = bterm + ma1;                                   // ma1 x ma2
-    float *w2s = dinf + (size_t)ma1 * ma2;                       // ma1 x ma2
+    int *la = gstart + ma1 + 1;                        // ma1 (labels in sorted order)
+    int *lb = la + ma1;                                // ma2
+    float *wsum = reinterpret_cast<float *>(lb + ma2);  // ma1
+    float *bterm = wsum + ma1;                          // ma1
+    float *dinf = bterm + ma1;                          // ma1 x ma2
+    float *w2s = dinf + (size_t)ma1 * ma2;              // ma1 x ma2
     __shared__ int ngroups;
     const int p = blockIdx.x;
     const HessPair pr = pairs[p];
@@ -778,13 +780,17 @@ __global__ void __launch_bounds__(256) hess_t_p_kernel(
     const size_t wbase = (size_t)p * ma1 * ma2;
     for (int e = threadIdx.x; e < pr.na; e += blockDim.x) {
         pa[e] = perm1[(size_t)pr.a * ma1 + e];
+        la[e] = lab1[(size_t)pr.a * ma1 + e];
         wsum[e] = 0.f;
         bterm[e] = 0.f;
     }
-    for (int e = threadIdx.x; e < pr.nb; e += blockDim.x) pb[e] = perm2[(size_t)pr.b * ma2 + e];
+    for (int e = threadIdx.x; e < pr.nb; e += blockDim.x) {
+        pb[e] = perm2[(size_t)pr.b * ma2 + e];
+        lb[e] = lab2[(size_t)pr.b * ma2 + e];
+    }
+    __syncthreads();
     if (threadIdx.x == 0) {
-        const int g = pair_label_groups(lab1 + (size_t)pr.a * ma1, lab2 + (size_t)pr.b * ma2,
-                                        pr.na, pr.nb, groups);
+        const int g = pair_label_groups(la, lb, pr.na, pr.nb, groups);
         ngroups = g;
         gstart[0] = 0;
         for (int q = 0; q < g; ++q)
@@ -850,7 +856,7 @@ __global__ void __launch_bounds__(256) hess_t_p_kernel(
 }
 
 size_t hess_t_p_smem(int ma1, int ma2) {
-    return (size_t)ma1 * sizeof(int4) + (size_t)(ma1 + ma2 + ma1 + 1) * sizeof(int) +
+    return (size_t)ma1 * sizeof(int4) + (size_t)(2 * ma1 + 2 * ma2 + ma1 + 1) * sizeof(int) +
            (size_t)(2 * ma1 + 2 * ma1 * ma2) * sizeof(float);
 }
 
@@ -897,7 +903,7 @@ HyGeom hess_y_geom(int ma1, int ma2) {
     g.ldc = 32 * nchunk;
     g.warps = nchunk * kgroups;
     const size_t head =
-        ((size_t)ma1 * sizeof(int4) + (size_t)(ma1 + ma2) * sizeof(int) + 15) & ~(size_t)15;
+        ((size_t)ma1 * sizeof(int4) + (size_t)2 * (ma1 + ma2) * sizeof(int) + 15) & ~(size_t)15;
     g.smem = head + ((size_t)(ma1 + ma2) * g.kt + (size_t)g.warps * JRING * hy_stage<T>()) *
                         sizeof(T);
     return g;
@@ -1035,16 +1041,25 @@ __global__ void __launch_bounds__(256, 2) hess_y_kernel(
     int4 *groups = reinterpret_cast<int4 *>(hy_raw);  // ma1
     int *pa = reinterpret_cast<int *>(groups + ma1);   // ma1
     int *pb = pa + ma1;                                // ma2
+    int *la = pb + ma2;                                // ma1 (labels in sorted order)
+    int *lb = la + ma1;                                // ma2
     T *xa_s = reinterpret_cast<T *>(
-        hy_raw + (((size_t)ma1 * sizeof(int4) + (size_t)(ma1 + ma2) * sizeof(int) + 15) & ~(size_t)15));
+        hy_raw + (((size_t)ma1 * sizeof(int4) + (size_t)2 * (ma1 + ma2) * sizeof(int) + 15) &
+                  ~(size_t)15));
     T *xb_s = xa_s + (size_t)ma1 * kt;      // [atom][row of the slice]
     T *jring = xb_s + (size_t)ma2 * kt;     // per warp [JRING][stage]
     __shared__ int ngroups;
     const int p = blockIdx.y;
     const HessPair pr = pairs[p];
     const int kbase = blockIdx.x * kt;
-    for (int e = threadIdx.x; e < pr.na; e += blockDim.x) pa[e] = perm1[(size_t)pr.a * ma1 + e];
-    for (int e = threadIdx.x; e < pr.nb; e += blockDim.x) pb[e] = perm2[(size_t)pr.b * ma2 + e];
+    for (int e = threadIdx.x; e < pr.na; e += blockDim.x) {
+        pa[e] = perm1[(size_t)pr.a * ma1 + e];
+        la[e] = lab1[(size_t)pr.a * ma1 + e];
+    }
+    for (int e = threadIdx.x; e < pr.nb; e += blockDim.x) {
+        pb[e] = perm2[(size_t)pr.b * ma2 + e];
+        lb[e] = lab2[(size_t)pr.b * ma2 + e];
+    }
     if (MODE != 3) {  // descriptor rows of the slice (rank term)
         for (int e = threadIdx.x; e < pr.na * kt; e += blockDim.x) {
             const int i = e / kt, kk = e - i * kt;
@@ -1055,9 +1070,9 @@ __global__ void __launch_bounds__(256, 2) hess_y_kernel(
             xb_s[e] = (kbase + kk < rep) ? x2[((size_t)pr.b * ma2 + j) * rep + kbase + kk] : T(0);
         }
     }
+    __syncthreads();
     if (threadIdx.x == 0)  // atoms of a whose label b lacks get Y = 0 (written)
-        ngroups = pair_label_groups(lab1 + (size_t)pr.a * ma1, lab2 + (size_t)pr.b * ma2,
-                                    pr.na, pr.nb, groups);
+        ngroups = pair_label_groups(la, lb, pr.na, pr.nb, groups);
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nchunk = ldc / 32;
@@ -1108,7 +1123,8 @@ __global__ void __launch_bounds__(256) hess_rank_kernel(
     const float *__restrict__ PB1, const float *__restrict__ Tt, const int *__restrict__ off1,
     const int *__restrict__ off2, int symmetric, ElemSink sink) {
     __shared__ int4 groups[HR_MAXA];
-    __shared__ int pa[HR_MAXA], pb[HR_MAXA], gstart[HR_MAXA + 1], qi[HR_Q], qj[HR_Q];
+    __shared__ int pa[HR_MAXA], pb[HR_MAXA], la[HR_MAXA], lb[HR_MAXA], gstart[HR_MAXA + 1];
+    __shared__ int qi[HR_Q], qj[HR_Q];
     __shared__ int ngroups;
     __shared__ __align__(16) float Ss[HR_Q][HR_T];
     __shared__ __align__(16) float Ts[HR_Q][HR_T];
@@ -1119,11 +1135,17 @@ __global__ void __launch_bounds__(256) hess_rank_kernel(
     const int r0 = (blockIdx.x / ntc) * HR_T, c0 = (blockIdx.x % ntc) * HR_T;
     if (r0 >= m1 || c0 >= n2) return;  // block-uniform
     const int tid = threadIdx.x;
-    for (int e = tid; e < pr.na; e += blockDim.x) pa[e] = perm1[(size_t)pr.a * ma1 + e];
-    for (int e = tid; e < pr.nb; e += blockDim.x) pb[e] = perm2[(size_t)pr.b * ma2 + e];
+    for (int e = tid; e < pr.na; e += blockDim.x) {
+        pa[e] = perm1[(size_t)pr.a * ma1 + e];
+        la[e] = lab1[(size_t)pr.a * ma1 + e];
+    }
+    for (int e = tid; e < pr.nb; e += blockDim.x) {
+        pb[e] = perm2[(size_t)pr.b * ma2 + e];
+        lb[e] = lab2[(size_t)pr.b * ma2 + e];
+    }
+    __syncthreads();
     if (tid == 0) {
-        const int g = pair_label_groups(lab1 + (size_t)pr.a * ma1, lab2 + (size_t)pr.b * ma2,
-                                        pr.na, pr.nb, groups);
+        const int g = pair_label_groups(la, lb, pr.na, pr.nb, groups);
         ngroups = g;
         gstart[0] = 0;
         for (int q = 0; q < g; ++q)
