@@ -21,7 +21,10 @@
 // rows, one of them a tcgen05 GEMM per batch), Y_i per (pair, 8-row slice of
 // rep) with the atoms of a label group in registers (kernel 2), and
 // H_ab = J_a^T Y by one GEMM problem per pair, or per run of pairs
-// (a, b), (a, b + 1), ... (tcgen05 split-fp16, or cuBLAS).
+// (a, b), (a, b + 1), ... (tcgen05 split-fp16, or cuBLAS).  On that GEMM-form
+// path (FP32, at most 64 atoms per molecule) Y_i keeps only sum_j w_ij J_j;
+// the rank part -sum_ij (J_i^T d_ij) t'_ij^T is added to H_ab after the
+// contraction by hess_rank_kernel, J_i^T d_ij coming from a third projection.
 #include <cublas_v2.h>
 
 #include <algorithm>
