@@ -81,6 +81,15 @@ int kfb_abi_version(void);
 kfb_status kfb_set_timing(int enable);
 double kfb_last_kernel_ms(void);
 
+/* Code-path log of the calling thread.  Where a call chooses between several
+ * implementations of one step (the Hessian's CUDA-core t' kernel, its GEMM form
+ * with the rank term inside Y, or the separate rank kernel), it appends the
+ * name of the path it took; kfb_path_log_read copies the comma-separated log
+ * (NUL-terminated, truncated to len - 1 characters) and returns its full
+ * length.  No reference counterpart (the reference has one path per call). */
+kfb_status kfb_path_log_clear(void);
+int kfb_path_log_read(char *buf, int len);
+
 /* ---------------------------------------------------------------------- */
 /* Scalar kernels: K[a,b] = sum_{i in a, j in b, q_i = q_j}                */
 /*                          exp(-||x_i - x_j||^2 / (2 sigma^2))            */

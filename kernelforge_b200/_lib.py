@@ -33,7 +33,7 @@ EXPORTS = (
     "kfb_cosmlp_params", "kfb_cosmlp_grads", "kfb_cosmlp_sync", "kfb_cosmlp_optimizer_state",
     "kfb_cosmlp_set_steps", "kfb_cosmlp_pair_step", "kfb_cosmlp_features_elemental",
     "kfb_local_alpha_desc", "kfb_local_matvec", "kfb_fchl19_rep_size", "kfb_fchl19_repr",
-    "kfb_kernel_gaussian_symm_noalloc",
+    "kfb_kernel_gaussian_symm_noalloc", "kfb_path_log_clear", "kfb_path_log_read",
 )
 
 
@@ -100,6 +100,8 @@ _SIGS = {
     "kfb_fchl19_rep_size": (I, [I, I, I, I]),
     "kfb_fchl19_repr": (I, [P, P, P, I, I, I, I, I, I, D, D, D, D, D, D, D, D, I, P, P, P]),
     "kfb_kernel_gaussian_symm_noalloc": (I, [P, P, P, I, I, I, D, I, I, P, P]),
+    "kfb_path_log_clear": (I, []),
+    "kfb_path_log_read": (I, [ctypes.c_char_p, I]),
 }
 
 
@@ -117,6 +119,20 @@ def lib():
             fn.argtypes = args
         _lib = handle
     return _lib
+
+
+def path_log_clear() -> None:
+    """Empty this thread's code-path log (kfb_path_log_clear)."""
+    lib().kfb_path_log_clear()
+
+
+def path_log() -> list:
+    """The names of the paths taken since the last clear, in call order."""
+    n = lib().kfb_path_log_read(None, 0)
+    buf = ctypes.create_string_buffer(n + 1)
+    lib().kfb_path_log_read(buf, n + 1)
+    s = buf.value.decode()
+    return s.split(",") if s else []
 
 
 def check(status: int) -> None:

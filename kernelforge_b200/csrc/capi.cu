@@ -3,8 +3,10 @@
 // scalar, derivative and solver launchers.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <string>
 
 #include "derivs.h"
 #include "kfb_internal.h"
@@ -25,6 +27,8 @@ kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2
                            cudaStream_t s);
 double last_kernel_ms();
 void set_timing(bool on);
+void path_log_clear();
+const std::string &path_log();
 }  // namespace kfb
 
 using namespace kfb;
@@ -135,6 +139,21 @@ kfb_status kfb_set_timing(int enable) {
     return KFB_OK;
 }
 double kfb_last_kernel_ms(void) { return last_kernel_ms(); }
+
+kfb_status kfb_path_log_clear(void) {
+    path_log_clear();
+    return KFB_OK;
+}
+
+int kfb_path_log_read(char *buf, int len) {
+    const std::string &s = path_log();
+    if (buf && len > 0) {
+        const int n = std::min<int>(len - 1, (int)s.size());
+        std::memcpy(buf, s.data(), (size_t)n);
+        buf[n] = '\0';
+    }
+    return (int)s.size();
+}
 
 kfb_status kfb_kernel_gaussian(const void *x1, const void *x2, const int32_t *q1,
                                const int32_t *q2, const int32_t *n1, const int32_t *n2, int nm1,

@@ -1775,6 +1775,19 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
         const long long qbytes = Mq * ma2 * (long long)sizeof(float);
         hrank = pform && ma1 <= HR_MAXA && ma2 <= HR_MAXA && Mq < INT_MAX &&
                 pbytes + qbytes <= (long long)(budget_bytes() / 2);
+        if (hrank && !symmetric) {
+            // an asymmetric call also keeps set 1's split Jacobian rows and PB1
+            // resident (outside the batch budget): take the rank kernel only
+            // when they fit in free memory next to a full workspace, else keep
+            // the rank term inside Y
+            const long long r1bytes = Mq * (long long)rep * 2 * (long long)sizeof(__half) +
+                                      Mq * (long long)sizeof(float);
+            size_t free_b = 0, total_b = 0;
+            KFB_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+            hrank = r1bytes + (long long)budget_bytes() <= (long long)free_b;
+        }
+        note_path(!pform ? "hessian:cuda-core-t" : (hrank ? "hessian:rank-kernel"
+                                                           : "hessian:rank-in-y"));
         if (pform) {
             TraceScope tr_p("hessian:p-setup", s);
             const int L = (int)labs1.size();
@@ -1895,6 +1908,8 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
             KFB_TRY(d_G.alloc((size_t)bcap * Mrows * ma2 * sizeof(float), s));
             if (hrank) KFB_TRY(d_Q.alloc((size_t)bcap * ma2 * Mq * sizeof(float), s));
         }
+    } else {
+        note_path("hessian:cuda-core-t");
     }
     const size_t smem_p = hess_t_p_smem(ma1, ma2);
     for (size_t p0 = 0, npz = 0; p0 < pairs.size(); p0 += npz) {

@@ -212,6 +212,17 @@ int trace_level() {
     return lvl;
 }
 
+static thread_local std::string g_path_log;
+
+void note_path(const char *name) {
+    if (g_path_log.size() > 4096) return;
+    if (!g_path_log.empty()) g_path_log += ',';
+    g_path_log += name;
+}
+
+void path_log_clear() { g_path_log.clear(); }
+const std::string &path_log() { return g_path_log; }
+
 static double now_ms() {
     using namespace std::chrono;
     return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();

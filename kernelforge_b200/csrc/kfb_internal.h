@@ -179,6 +179,9 @@ struct KernelTimer {
 // each traced phase to stderr; 2 also synchronises the stream at both ends of
 // the phase, so the time includes the device work the phase enqueued.
 int trace_level();
+// Code-path log of this thread (kfb_path_log_*): the name of each path a call
+// chose where it picks one of several (capped at a few KB).
+void note_path(const char *name);
 struct TraceScope {
     const char *name;
     cudaStream_t stream;

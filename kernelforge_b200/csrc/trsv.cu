@@ -31,7 +31,7 @@ namespace {
 constexpr int TB = 64;                  // rows per block
 constexpr int TB_BATCH = 8;             // solution blocks staged per wait
 constexpr int TRSV_THREADS = 256;       // 64 rows x 4 column groups
-constexpr unsigned TRSV_WAIT_LIMIT = 1u << 24;   // polls of ~32 ns: about a second
+constexpr unsigned long long TRSV_WAIT_NS = 1000000000ull;   // one second of %globaltimer
 
 __device__ __forceinline__ int ld_acquire(const int *p) {
     int v;
@@ -43,13 +43,23 @@ __device__ __forceinline__ void st_release(int *p, int v) {
     asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+__device__ __forceinline__ unsigned long long trsv_clock_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 // Thread 0: wait until more than `need` blocks are published; returns the
-// published count, or -1 when the wait gave up (or another CTA gave up).
+// published count, or -1 when the wait gave up (or another CTA gave up).  The
+// limit is elapsed time on %globaltimer (one second), not a poll count:
+// __nanosleep is only a hint, so a count would not bound the wait's length.
 __device__ int wait_published(const int *done, int need, int *err) {
-    for (unsigned it = 0; it < TRSV_WAIT_LIMIT; ++it) {
+    const unsigned long long t0 = trsv_clock_ns();
+    while (true) {
         const int d = ld_acquire(done);
         if (d > need) return d;
         if (*reinterpret_cast<volatile int *>(err)) return -1;
+        if (trsv_clock_ns() - t0 > TRSV_WAIT_NS) break;
         __nanosleep(32);
     }
     atomicExch(err, 1);

@@ -13,7 +13,7 @@ stores inputs and outputs as compressed .npz files:
 * golden_fchl19_720.npz -- default 720-dim FCHL19 descriptors of a few
   molecules (no Jacobians) and the scalar kernels on them.
 
-Usage:  python tests/golden/make_golden.py [REFERENCE_ROOT]
+Usage:  python tests/golden/make_golden.py REFERENCE_ROOT   (or KERNELFORGE_REFERENCE_ROOT set)
 """
 import os
 import subprocess
@@ -28,7 +28,7 @@ sys.path.insert(0, ROOT)
 from kernelforge_b200 import synthetic  # noqa: E402
 
 
-def main(ref_root="/root/reference"):
+def main(ref_root):
     subprocess.check_call([os.path.join(ROOT, "oracle", "build_ref.sh"), ref_root])
     sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))
     import fchl19_repr as fr
@@ -131,4 +131,6 @@ def main(ref_root="/root/reference"):
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    sys.path.insert(0, HERE)
+    from _refroot import reference_root
+    main(reference_root(sys.argv[1:]))

@@ -9,7 +9,7 @@ kernel the predictions equal), on
 * the reduced-basis FCHL19 molecules of golden_fchl19.npz (real Jacobians).
 Output: tests/golden/golden_matvec.npz.
 
-Usage:  python tests/golden/make_golden_matvec.py [REFERENCE_ROOT]
+Usage:  python tests/golden/make_golden_matvec.py REFERENCE_ROOT   (or KERNELFORGE_REFERENCE_ROOT set)
 """
 import os
 import subprocess
@@ -40,7 +40,7 @@ def run_case(lk, out, tag, X1, dX1, Q1, N1, X2, dX2, Q2, N2, sigma, rng):
         X1, dX1, X2, dX2, Q1, Q2, N1, N2, sigma)
 
 
-def main(ref_root="/root/reference"):
+def main(ref_root):
     subprocess.check_call([os.path.join(ROOT, "oracle", "build_ref.sh"), ref_root])
     sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))
     import local_kernels as lk
@@ -73,4 +73,6 @@ def main(ref_root="/root/reference"):
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from _refroot import reference_root
+    main(reference_root(sys.argv[1:]))

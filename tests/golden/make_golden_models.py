@@ -10,7 +10,7 @@ descriptor (nRs2=8, nRs3=6) keep the fixture small.  Stores, per training mode,
 the test predictions and training scores, and the energy+force model as the
 reference saved it (tests/golden/ref_local_krr_ef.npz, re-compressed).
 
-Usage:  python tests/golden/make_golden_models.py [REFERENCE_ROOT]
+Usage:  python tests/golden/make_golden_models.py REFERENCE_ROOT   (or KERNELFORGE_REFERENCE_ROOT set)
 """
 import os
 import subprocess
@@ -48,7 +48,7 @@ def reference_models(ref_root):
     return krr
 
 
-def main(ref_root="/root/reference"):
+def main(ref_root):
     subprocess.check_call([os.path.join(ROOT, "oracle", "build_ref.sh"), ref_root])
     krr = reference_models(ref_root)
     from kernelforge_b200 import synthetic
@@ -81,4 +81,6 @@ def main(ref_root="/root/reference"):
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from _refroot import reference_root
+    main(reference_root(sys.argv[1:]))

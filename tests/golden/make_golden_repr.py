@@ -11,7 +11,7 @@ Builds the reference's CPU FP64 modules with oracle/build_ref.sh and evaluates
   harmonic only).
 Output: tests/golden/golden_repr.npz.
 
-Usage:  python tests/golden/make_golden_repr.py [REFERENCE_ROOT]
+Usage:  python tests/golden/make_golden_repr.py REFERENCE_ROOT   (or KERNELFORGE_REFERENCE_ROOT set)
 """
 import math
 import os
@@ -37,7 +37,7 @@ def molecule(rng, n, box, elements, p=None):
     return np.array(R), rng.choice(elements, size=n, p=p).astype(np.int32)
 
 
-def main(ref_root="/root/reference"):
+def main(ref_root):
     subprocess.check_call([os.path.join(ROOT, "oracle", "build_ref.sh"), ref_root])
     sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))
     import fchl19_repr as fr
@@ -63,4 +63,6 @@ def main(ref_root="/root/reference"):
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from _refroot import reference_root
+    main(reference_root(sys.argv[1:]))

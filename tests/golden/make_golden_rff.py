@@ -13,7 +13,7 @@ rff_features_elemental and rff_gramian_elemental_rfp on
 W ~ N(0, 1) / sigma and b ~ U(0, 2 pi) as in the reference's LocalRFFModel
 (models/rff.py:110-112).  Output: tests/golden/golden_rff.npz.
 
-Usage:  python tests/golden/make_golden_rff.py [REFERENCE_ROOT]
+Usage:  python tests/golden/make_golden_rff.py REFERENCE_ROOT   (or KERNELFORGE_REFERENCE_ROOT set)
 """
 import os
 import subprocess
@@ -25,7 +25,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 
 
-def main(ref_root="/root/reference"):
+def main(ref_root):
     subprocess.check_call([os.path.join(ROOT, "oracle", "build_ref.sh"), ref_root])
     sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))
     import kitchen_sinks as ks
@@ -72,4 +72,6 @@ def main(ref_root="/root/reference"):
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from _refroot import reference_root
+    main(reference_root(sys.argv[1:]))

@@ -9,7 +9,7 @@ Runs the reference's CPU FP64 `kitchen_sinks` module (oracle/build_ref.sh) on
   three element types, rep 24, D = 32.
 W ~ N(0, 1) / sigma, b ~ U(0, 2 pi).  Output: tests/golden/golden_rff_force.npz.
 
-Usage:  python tests/golden/make_golden_rff_force.py [REFERENCE_ROOT]
+Usage:  python tests/golden/make_golden_rff_force.py REFERENCE_ROOT   (or KERNELFORGE_REFERENCE_ROOT set)
 """
 import os
 import subprocess
@@ -36,7 +36,7 @@ def case(ks, out, tag, X, dX, Qe, N, D, sigma, rng):
     out[f"{tag}_ZtZ_rfp"], out[f"{tag}_ZtY"] = ztz, zty
 
 
-def main(ref_root="/root/reference"):
+def main(ref_root):
     subprocess.check_call([os.path.join(ROOT, "oracle", "build_ref.sh"), ref_root])
     sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))
     import kitchen_sinks as ks
@@ -65,4 +65,6 @@ def main(ref_root="/root/reference"):
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from _refroot import reference_root
+    main(reference_root(sys.argv[1:]))

@@ -144,12 +144,18 @@ def test_jacobian_chunked_outer_molecules(precision, rep, monkeypatch):
               o.kernel_gaussian_jacobian(X1, X2, dX2, Q1, Q2, N1, N2, s), precision)
 
 
-@pytest.mark.parametrize("gb", ["0.0001", "4"])
-def test_hessian_tensor_core_batches(gb, monkeypatch):
+@pytest.mark.parametrize("gb,path", [("0.00005", "hessian:rank-in-y"),
+                                      ("0.0001", "hessian:rank-kernel"),
+                                      ("4", "hessian:rank-kernel")])
+def test_hessian_tensor_core_batches(gb, path, monkeypatch):
     """Tensor-core Hessians with kernel 1 in GEMM form: a workspace of ~100 kB
     gives batches of a few molecule pairs spanning at most two molecules b (the
     projection buffer's capacity), the default one batch; symmetric RFP,
-    asymmetric and full energy+force kernels against the oracle."""
+    asymmetric and full energy+force kernels against the oracle.  At ~54 kB the
+    projection and rank buffers (18 kB each here) no longer fit half the
+    workspace together, so the rank term stays inside Y; the path log shows
+    which of the two forms each call took."""
+    from kernelforge_b200 import _lib
     from kernelforge_b200 import local_kernels as lk
     monkeypatch.setenv("KFB_WORKSPACE_GB", gb)
     rep = 48
@@ -163,9 +169,13 @@ def test_hessian_tensor_core_batches(gb, monkeypatch):
     Q2[1, :2] = 9   # a set-2 label set 1 lacks
     s = 2.0
     p = "split_f16"
+    _lib.path_log_clear()
     close(lk.kernel_gaussian_hessian_symm_rfp(X1, dX1, Q1, N1, s, precision=p),
           o.kernel_gaussian_hessian_symm_rfp(X1, dX1, Q1, N1, s), p)
+    assert _lib.path_log() == [path]
+    _lib.path_log_clear()
     close(lk.kernel_gaussian_hessian(X1, dX1, X2, dX2, Q1, Q2, N1, N2, s, precision=p),
           o.kernel_gaussian_hessian(X1, dX1, X2, dX2, Q1, Q2, N1, N2, s), p)
+    assert _lib.path_log() == [path]
     close(lk.kernel_gaussian_full(X1, dX1, X2, dX2, Q1, Q2, N1, N2, s, precision=p),
           o.kernel_gaussian_full(X1, dX1, X2, dX2, Q1, Q2, N1, N2, s), p)

@@ -11,6 +11,7 @@ import numpy as np
 import pytest
 
 from conftest import make_set
+from oracle import oracle as o
 
 pytestmark = pytest.mark.gpu
 
@@ -55,9 +56,17 @@ def test_noalloc_matches_the_allocating_entry_point_twice(layout_name):
     count = nm * nm if layout == _lib.KFB_DENSE else nm * (nm + 1) // 2
     x = torch.tensor(X, device="cuda")
     ref = _regular(lib, x, Q, N, 2.0, layout, count).cpu().numpy()
+    # the CPU oracle of the same layout pins both entry points
+    if layout == _lib.KFB_DENSE:
+        want = o.kernel_gaussian_symm(X, Q, N, 2.0).ravel()
+    else:
+        want = o.kernel_gaussian_symm_rfp(X, Q, N, 2.0,
+                                          uplo_lower=(layout == _lib.KFB_RFP_L))
+    np.testing.assert_allclose(ref, want, rtol=1e-12, atol=1e-12)
     for _ in range(2):
         got = _noalloc(lib, x, Q, N, 2.0, layout, count).cpu().numpy()
         np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-12)
+        np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-12)
     # a different problem in between: the scratch keeps the last call's contents
     X2, _, Q2, N2 = make_set(60, 7, 48, 2, seed=18)
     x2 = torch.tensor(X2 * 0.4, device="cuda")
