@@ -188,6 +188,23 @@ kfb_status kfb_kernel_gaussian_full_symm(const void *x, const void *dx, const in
                                          kfb_layout layout, void *out, void *stream);
 
 /* ---------------------------------------------------------------------- */
+/* FP64-class products on the int8 tensor cores                            */
+/* ---------------------------------------------------------------------- */
+
+/* C (m, n) = alpha A B^T (beta = 0) or C + alpha A B^T (beta = 1) for
+ * row-major FP64 A (m, k; lda), B (n, k; ldb), C (m, n; ldc).  Each row of A
+ * and B is cut into `slices` (2..7) planes of balanced base-128 int8 digits
+ * under a per-row power-of-two scale; the digit-plane products are exact int32
+ * sums on the int8 tensor cores (tcgen05 kind::i8) and are combined in FP64,
+ * so each operand keeps about 7 * slices - 1 significant bits (slices = 7:
+ * |error| <~ 2^-47 k max|A_i| max|B_j|).  k <= 65536.  Allocates scratch.
+ * No reference counterpart: the reference's FP64 products are BLAS dgemm calls
+ * (src/local_kernels.cpp:237,689,940,1394,2751,3053-3107). */
+kfb_status kfb_gemm_f64_i8(int m, int n, int k, double alpha, const double *a, int lda,
+                           const double *b, int ldb, double beta, double *c, int ldc, int slices,
+                           void *stream);
+
+/* ---------------------------------------------------------------------- */
 /* RFP storage and the Cholesky solve                                      */
 /* ---------------------------------------------------------------------- */
 

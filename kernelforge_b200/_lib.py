@@ -34,6 +34,7 @@ EXPORTS = (
     "kfb_cosmlp_set_steps", "kfb_cosmlp_pair_step", "kfb_cosmlp_features_elemental",
     "kfb_local_alpha_desc", "kfb_local_matvec", "kfb_fchl19_rep_size", "kfb_fchl19_repr",
     "kfb_kernel_gaussian_symm_noalloc", "kfb_path_log_clear", "kfb_path_log_read",
+    "kfb_gemm_f64_i8",
 )
 
 
@@ -102,6 +103,7 @@ _SIGS = {
     "kfb_kernel_gaussian_symm_noalloc": (I, [P, P, P, I, I, I, D, I, I, P, P]),
     "kfb_path_log_clear": (I, []),
     "kfb_path_log_read": (I, [ctypes.c_char_p, I]),
+    "kfb_gemm_f64_i8": (I, [I, I, I, D, P, I, P, I, D, P, I, I, P]),
 }
 
 

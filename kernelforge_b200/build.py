@@ -25,7 +25,7 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 
 SOURCES = ["kfb_common.cpp", "scalar_simt.cu", "scalar_tc.cu", "derivs.cu", "solve.cu",
            "capi.cu", "scalar_noalloc.cu", "tc_gemm.cu", "features.cu",
-           "matvec.cu", "repr.cu", "trsv.cu"]
+           "matvec.cu", "repr.cu", "trsv.cu", "ozaki.cu", "chol.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
          "-fvisibility=hidden", "--expt-relaxed-constexpr", "-I", INCLUDE, "-I", CSRC]
@@ -63,7 +63,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         list(ex.map(lambda s: _compile(s, verbose), stale))
     objs = [os.path.join(BUILD, s + ".o") for s in SOURCES]
     if stale or not os.path.exists(LIB):
-        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcublas", "-lcusolver",
+        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcublas",
                "-Xlinker", f"-rpath={CUDA_HOME}/lib64"]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:

@@ -17,6 +17,8 @@ kfb_status full_to_rfp(const void *A, int n, kfb_layout uplo, kfb_dtype dt, void
 kfb_status rfp_to_full(const void *arf, int n, kfb_layout uplo, kfb_dtype dt, void *A, cudaStream_t s);
 kfb_status rfp_potrf(void *arf, int n, double l2, kfb_layout uplo, kfb_dtype dt, int *info, cudaStream_t s);
 kfb_status rfp_potrs(const void *arf, void *B, int n, int nrhs, kfb_layout uplo, kfb_dtype dt, cudaStream_t s);
+kfb_status cho_solve_rfp_f64(double *arf, const double *y, int n, double l2, kfb_layout uplo,
+                             double *alpha, int *info, cudaStream_t s);
 kfb_status feature_gramian(const float *z, const double *y, int nm, int d, kfb_layout layout,
                            float *ztz, double *zty, cudaStream_t s);
 kfb_status ridge_solve_mixed(const float *zf, const double *y, int nm, int d, double l2,
@@ -531,10 +533,9 @@ kfb_status kfb_cho_solve_rfp(void *arf, const double *y, int n, double l2, kfb_l
     if (uplo != KFB_RFP_U && uplo != KFB_RFP_L)
         return set_error(KFB_ERR_INVALID_ARG, "uplo must be 'U' or 'L'");
     cudaStream_t s = as_stream(stream);
-    KFB_TRY(rfp_potrf(arf, n, l2, uplo, KFB_F64, info, s));
+    KFB_TRY(cho_solve_rfp_f64(static_cast<double *>(arf), y, n, l2, uplo, alpha, info, s));
     if (*info != 0) return set_error(KFB_ERR_NOT_PD, "DPFTRF failed, info=%d", *info);
-    KFB_CUDA_TRY(cudaMemcpyAsync(alpha, y, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    return rfp_potrs(arf, alpha, n, 1, uplo, KFB_F64, s);
+    return KFB_OK;
 }
 
 kfb_status kfb_krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2,

@@ -1,15 +1,16 @@
-// RFP storage kernels, the in-place RFP Cholesky factorisation / solve, and
-// the mixed-precision (FP32 factor, FP64 residual) KRR solve.
+// RFP storage kernels, the RFP Cholesky factorisation / solve (the drop-ins of
+// dpftrf / dpftrs and of the FP32 rfp_potrf / rfp_potrs), and the
+// mixed-precision KRR and ridge solves.
 //
-// The RFP Cholesky follows the LAPACK dpftrf / dpftrs block structure for
-// TRANSR='N' (an RFP array is a column-major (n+1) x n/2 or n x (n+1)/2 matrix
-// holding two triangles and one rectangle): potrf on the first triangle, trsm
-// on the rectangle, syrk into the second triangle, potrf on it.  The four
-// block operations are issued on the caller's stream with one host
-// synchronisation at the end (the reference's curfpSpftrf synchronises twice,
-// src/curfp_spftrf.cpp:259,281).
+// Every factorisation goes through chol_dense (chol.cu): the RFP array is
+// expanded to a dense column-major lower triangle, factored with the panel
+// solves and trailing updates on the int8 tensor cores (digit-sliced FP64
+// products), and packed back; solves use the blocked FP64 triangular sweeps of
+// trsv.cu.  (The reference factors an RFP array in place by LAPACK's
+// potrf / trsm / syrk / potrf sequence on its sub-blocks,
+// src/curfp_spftrf.cpp:182-292; the dense copy here costs n^2 doubles of HBM,
+// which B200 has to spare, and makes every O(n^3) part one tensor-core GEMM.)
 #include <cublas_v2.h>
-#include <cusolverDn.h>
 
 #include <algorithm>
 #include <cmath>
@@ -17,6 +18,7 @@
 #include <memory>
 #include <vector>
 
+#include "chol.h"
 #include "kernels_common.cuh"
 #include "trsv.h"
 
@@ -26,7 +28,6 @@ namespace {
 
 struct Handles {
     cublasHandle_t blas = nullptr;
-    cusolverDnHandle_t solver = nullptr;
     int device = -1;
 };
 
@@ -39,12 +40,9 @@ kfb_status get_handles(cudaStream_t s, Handles *&out) {
     if (!hd.blas) {
         if (cublasCreate(&hd.blas) != CUBLAS_STATUS_SUCCESS)
             return set_error(KFB_ERR_CUDA, "cublasCreate failed");
-        if (cusolverDnCreate(&hd.solver) != CUSOLVER_STATUS_SUCCESS)
-            return set_error(KFB_ERR_CUDA, "cusolverDnCreate failed");
         cublasSetMathMode(hd.blas, CUBLAS_PEDANTIC_MATH);  // no reduced-precision shortcuts
     }
     cublasSetStream(hd.blas, s);
-    cusolverDnSetStream(hd.solver, s);
     out = &hd;
     return KFB_OK;
 }
@@ -68,188 +66,6 @@ namespace {
         if (_b != CUBLAS_STATUS_SUCCESS)                                                    \
             return set_error(KFB_ERR_CUDA, "%s failed: cublas status %d", #expr, (int)_b);  \
     } while (0)
-#define KFB_SOLVER_TRY(expr)                                                                \
-    do {                                                                                    \
-        cusolverStatus_t _b = (expr);                                                       \
-        if (_b != CUSOLVER_STATUS_SUCCESS)                                                  \
-            return set_error(KFB_ERR_CUDA, "%s failed: cusolver status %d", #expr, (int)_b); \
-    } while (0)
-
-// -------------------------------------------------- typed BLAS / LAPACK shims
-template <class T> struct Blas;
-template <> struct Blas<float> {
-    static cublasStatus_t trsm(cublasHandle_t h, cublasSideMode_t sd, cublasFillMode_t u,
-                               cublasOperation_t t, int m, int n, const float *al, const float *A,
-                               int lda, float *B, int ldb) {
-        return cublasStrsm(h, sd, u, t, CUBLAS_DIAG_NON_UNIT, m, n, al, A, lda, B, ldb);
-    }
-    static cublasStatus_t syrk(cublasHandle_t h, cublasFillMode_t u, cublasOperation_t t, int n,
-                               int k, const float *al, const float *A, int lda, const float *be,
-                               float *C, int ldc) {
-        return cublasSsyrk(h, u, t, n, k, al, A, lda, be, C, ldc);
-    }
-    static cublasStatus_t gemm(cublasHandle_t h, cublasOperation_t ta, cublasOperation_t tb, int m,
-                               int n, int k, const float *al, const float *A, int lda,
-                               const float *B, int ldb, const float *be, float *C, int ldc) {
-        return cublasSgemm(h, ta, tb, m, n, k, al, A, lda, B, ldb, be, C, ldc);
-    }
-    static cusolverStatus_t potrf_ws(cusolverDnHandle_t h, cublasFillMode_t u, int n, float *A,
-                                     int lda, int *lw) {
-        return cusolverDnSpotrf_bufferSize(h, u, n, A, lda, lw);
-    }
-    static cusolverStatus_t potrf(cusolverDnHandle_t h, cublasFillMode_t u, int n, float *A,
-                                  int lda, float *ws, int lw, int *info) {
-        return cusolverDnSpotrf(h, u, n, A, lda, ws, lw, info);
-    }
-};
-template <> struct Blas<double> {
-    static cublasStatus_t trsm(cublasHandle_t h, cublasSideMode_t sd, cublasFillMode_t u,
-                               cublasOperation_t t, int m, int n, const double *al,
-                               const double *A, int lda, double *B, int ldb) {
-        return cublasDtrsm(h, sd, u, t, CUBLAS_DIAG_NON_UNIT, m, n, al, A, lda, B, ldb);
-    }
-    static cublasStatus_t syrk(cublasHandle_t h, cublasFillMode_t u, cublasOperation_t t, int n,
-                               int k, const double *al, const double *A, int lda,
-                               const double *be, double *C, int ldc) {
-        return cublasDsyrk(h, u, t, n, k, al, A, lda, be, C, ldc);
-    }
-    static cublasStatus_t gemm(cublasHandle_t h, cublasOperation_t ta, cublasOperation_t tb, int m,
-                               int n, int k, const double *al, const double *A, int lda,
-                               const double *B, int ldb, const double *be, double *C, int ldc) {
-        return cublasDgemm(h, ta, tb, m, n, k, al, A, lda, B, ldb, be, C, ldc);
-    }
-    static cusolverStatus_t potrf_ws(cusolverDnHandle_t h, cublasFillMode_t u, int n, double *A,
-                                     int lda, int *lw) {
-        return cusolverDnDpotrf_bufferSize(h, u, n, A, lda, lw);
-    }
-    static cusolverStatus_t potrf(cusolverDnHandle_t h, cublasFillMode_t u, int n, double *A,
-                                  int lda, double *ws, int lw, int *info) {
-        return cusolverDnDpotrf(h, u, n, A, lda, ws, lw, info);
-    }
-};
-
-// The three blocks of an RFP array (TRANSR='N'), as column-major sub-matrices.
-struct RfpBlocks {
-    long long t1, s, t2;  // offsets of T1 (lower-stored), S (rectangle), T2 (upper-stored)
-    int n1, n2, ld;       // T1 is n1 x n1, T2 is n2 x n2; S is n2 x n1 (lower) / n1 x n2 (upper)
-};
-
-RfpBlocks rfp_blocks(int n, bool lower) {
-    RfpBlocks b{};
-    if (n & 1) {
-        b.ld = n;
-        if (lower) {
-            b.n1 = n - n / 2;
-            b.n2 = n / 2;
-            b.t1 = 0;
-            b.s = b.n1;
-            b.t2 = n;
-        } else {
-            b.n1 = n / 2;
-            b.n2 = n - n / 2;
-            b.t1 = b.n2;
-            b.s = 0;
-            b.t2 = b.n1;
-        }
-    } else {
-        const int k = n / 2;
-        b.ld = n + 1;
-        b.n1 = b.n2 = k;
-        if (lower) {
-            b.t1 = 1;
-            b.s = k + 1;
-            b.t2 = 0;
-        } else {
-            b.t1 = k + 1;
-            b.s = 0;
-            b.t2 = k;
-        }
-    }
-    return b;
-}
-
-template <class T>
-kfb_status rfp_potrf_t(T *a, int n, bool lower, int *info, cudaStream_t s) {
-    *info = 0;
-    if (n == 0) return KFB_OK;
-    Handles *h = nullptr;
-    KFB_TRY(get_handles(s, h));
-    const RfpBlocks b = rfp_blocks(n, lower);
-    const T one = T(1), mone = T(-1);
-    int lw1 = 0, lw2 = 0;
-    KFB_SOLVER_TRY(Blas<T>::potrf_ws(h->solver, CUBLAS_FILL_MODE_LOWER, b.n1, a + b.t1, b.ld, &lw1));
-    if (b.n2 > 0)
-        KFB_SOLVER_TRY(
-            Blas<T>::potrf_ws(h->solver, CUBLAS_FILL_MODE_UPPER, b.n2, a + b.t2, b.ld, &lw2));
-    DevBuf ws, dinfo;
-    KFB_TRY(ws.alloc((size_t)std::max(std::max(lw1, lw2), 1) * sizeof(T), s));
-    KFB_TRY(dinfo.alloc(2 * sizeof(int), s));
-    KFB_TRY(zero(dinfo.ptr, 2 * sizeof(int), s));
-    int *di = dinfo.as<int>();
-    KFB_SOLVER_TRY(Blas<T>::potrf(h->solver, CUBLAS_FILL_MODE_LOWER, b.n1, a + b.t1, b.ld,
-                                  ws.as<T>(), lw1, di));
-    if (b.n2 > 0) {
-        if (lower) {
-            KFB_BLAS_TRY(Blas<T>::trsm(h->blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER,
-                                       CUBLAS_OP_T, b.n2, b.n1, &one, a + b.t1, b.ld, a + b.s,
-                                       b.ld));
-            KFB_BLAS_TRY(Blas<T>::syrk(h->blas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, b.n2, b.n1,
-                                       &mone, a + b.s, b.ld, &one, a + b.t2, b.ld));
-        } else {
-            KFB_BLAS_TRY(Blas<T>::trsm(h->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER,
-                                       CUBLAS_OP_N, b.n1, b.n2, &one, a + b.t1, b.ld, a + b.s,
-                                       b.ld));
-            KFB_BLAS_TRY(Blas<T>::syrk(h->blas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, b.n2, b.n1,
-                                       &mone, a + b.s, b.ld, &one, a + b.t2, b.ld));
-        }
-        KFB_SOLVER_TRY(Blas<T>::potrf(h->solver, CUBLAS_FILL_MODE_UPPER, b.n2, a + b.t2, b.ld,
-                                      ws.as<T>(), lw2, di + 1));
-    }
-    int hi[2] = {0, 0};
-    KFB_CUDA_TRY(cudaMemcpyAsync(hi, di, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
-    KFB_CUDA_TRY(cudaStreamSynchronize(s));
-    if (hi[0] > 0)
-        *info = hi[0];
-    else if (hi[1] > 0)
-        *info = hi[1] + b.n1;
-    else if (hi[0] < 0 || hi[1] < 0)
-        return set_error(KFB_ERR_CUDA, "potrf reported an invalid argument");
-    return KFB_OK;
-}
-
-template <class T>
-kfb_status rfp_potrs_t(const T *a, T *B, int n, int nrhs, bool lower, cudaStream_t s) {
-    if (n == 0 || nrhs == 0) return KFB_OK;
-    Handles *h = nullptr;
-    KFB_TRY(get_handles(s, h));
-    const RfpBlocks b = rfp_blocks(n, lower);
-    const T one = T(1), mone = T(-1);
-    T *B1 = B, *B2 = B + b.n1;
-    const int ldb = n;
-    const cublasSideMode_t L = CUBLAS_SIDE_LEFT;
-    const cublasFillMode_t LO = CUBLAS_FILL_MODE_LOWER, UP = CUBLAS_FILL_MODE_UPPER;
-    // forward: (L or U^T) y = b ; T1 lower-stored, T2 upper-stored in both cases
-    KFB_BLAS_TRY(Blas<T>::trsm(h->blas, L, LO, CUBLAS_OP_N, b.n1, nrhs, &one, a + b.t1, b.ld, B1, ldb));
-    if (b.n2 > 0) {
-        if (lower)
-            KFB_BLAS_TRY(Blas<T>::gemm(h->blas, CUBLAS_OP_N, CUBLAS_OP_N, b.n2, nrhs, b.n1, &mone,
-                                       a + b.s, b.ld, B1, ldb, &one, B2, ldb));
-        else
-            KFB_BLAS_TRY(Blas<T>::gemm(h->blas, CUBLAS_OP_T, CUBLAS_OP_N, b.n2, nrhs, b.n1, &mone,
-                                       a + b.s, b.ld, B1, ldb, &one, B2, ldb));
-        KFB_BLAS_TRY(Blas<T>::trsm(h->blas, L, UP, CUBLAS_OP_T, b.n2, nrhs, &one, a + b.t2, b.ld, B2, ldb));
-        // backward
-        KFB_BLAS_TRY(Blas<T>::trsm(h->blas, L, UP, CUBLAS_OP_N, b.n2, nrhs, &one, a + b.t2, b.ld, B2, ldb));
-        if (lower)
-            KFB_BLAS_TRY(Blas<T>::gemm(h->blas, CUBLAS_OP_T, CUBLAS_OP_N, b.n1, nrhs, b.n2, &mone,
-                                       a + b.s, b.ld, B2, ldb, &one, B1, ldb));
-        else
-            KFB_BLAS_TRY(Blas<T>::gemm(h->blas, CUBLAS_OP_N, CUBLAS_OP_N, b.n1, nrhs, b.n2, &mone,
-                                       a + b.s, b.ld, B2, ldb, &one, B1, ldb));
-    }
-    KFB_BLAS_TRY(Blas<T>::trsm(h->blas, L, LO, CUBLAS_OP_T, b.n1, nrhs, &one, a + b.t1, b.ld, B1, ldb));
-    return KFB_OK;
-}
 
 // ------------------------------------------------------------ small kernels
 template <class T>
@@ -365,14 +181,46 @@ __global__ void dense_deflate_kernel(const float *__restrict__ B, int n, int lay
     }
 }
 
+// Dense column-major lower FP64 copy of an RFP matrix (FP32 or FP64) with l2
+// added to its diagonal; the upper triangle is not touched.  Block (32, 8),
+// one lower 32 x 32 tile per block, stores along i.
+template <class Tin>
+__global__ void rfp_to_dense_lower_kernel(const Tin *__restrict__ B, int n, int layout,
+                                          double l2, double *__restrict__ F) {
+    const int bi = blockIdx.y, bj = blockIdx.x;
+    if (bi < bj) return;
+    __shared__ double t[32][33];
+    const int i0 = bi * 32, j0 = bj * 32;
+    load_rfp_tile(B, n, layout, i0, j0, t);
+    __syncthreads();
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int i = i0 + tx;
+    if (i >= n) return;
+    for (int r = ty; r < 32; r += 8) {
+        const int j = j0 + r;
+        if (j >= n || i < j) continue;
+        F[(size_t)j * n + i] = t[tx][r] + (i == j ? l2 : 0.0);
+    }
+}
+
 // RFP copy of a dense column-major lower Cholesky factor L: both RFP layouts
 // hold L(max(i,j), min(i,j)) at the symmetric position of (i, j) (UPLO='U'
 // stores U = L^T).
-__global__ void dense_lower_to_rfp_kernel(const float *__restrict__ L, int n, int layout,
-                                          float *__restrict__ arf) {
+template <class Tout>
+__global__ void dense_lower_to_rfp_kernel(const double *__restrict__ L, int n, int layout,
+                                          Tout *__restrict__ arf) {
     const long long i = blockIdx.y * (long long)blockDim.y + threadIdx.y;
     const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i < n && j < n && i <= j) arf[sym_index((kfb_layout)layout, n, i, j)] = L[i * n + j];
+    if (i < n && j < n && i <= j) arf[sym_index((kfb_layout)layout, n, i, j)] = (Tout)L[i * n + j];
+}
+
+__global__ void f32_to_f64_kernel(const float *a, int n, double *b) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = (double)a[i];
+}
+__global__ void f64_to_f32_kernel(const double *a, int n, float *b) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = (float)a[i];
 }
 
 
@@ -418,20 +266,80 @@ kfb_status rfp_to_full(const void *arf, int n, kfb_layout uplo, kfb_dtype dt, vo
     return KFB_OK;
 }
 
-kfb_status rfp_potrf(void *arf, int n, double l2, kfb_layout uplo, kfb_dtype dt, int *info,
-                     cudaStream_t s) {
-    KFB_TRY(rfp_add_diag(arf, n, l2, uplo, dt, s));
-    if (dt == KFB_F64) return rfp_potrf_t<double>(static_cast<double *>(arf), n, uplo == KFB_RFP_L, info, s);
-    return rfp_potrf_t<float>(static_cast<float *>(arf), n, uplo == KFB_RFP_L, info, s);
+// Digit planes of the tensor-core Cholesky updates for a factor held in dt:
+// 7 (FP64-class) for an FP64 matrix, 4 (about 27 significant bits, FP32-class)
+// for an FP32 one.
+inline int chol_slices(kfb_dtype dt) { return dt == KFB_F64 ? 7 : 4; }
+
+// Dense column-major lower FP64 copy of an RFP array plus l2 on the diagonal.
+kfb_status rfp_to_dense_lower(const void *arf, int n, kfb_layout uplo, kfb_dtype dt, double l2,
+                              double *F, cudaStream_t s) {
+    const dim3 b2(32, 8), gt(nblk(n, 32), nblk(n, 32));
+    if (dt == KFB_F64)
+        rfp_to_dense_lower_kernel<double><<<gt, b2, 0, s>>>(static_cast<const double *>(arf), n,
+                                                            uplo, l2, F);
+    else
+        rfp_to_dense_lower_kernel<float><<<gt, b2, 0, s>>>(static_cast<const float *>(arf), n,
+                                                           uplo, l2, F);
+    KFB_CUDA_TRY(cudaGetLastError());
+    return KFB_OK;
 }
 
+kfb_status dense_lower_to_rfp(const double *L, int n, kfb_layout uplo, kfb_dtype dt, void *arf,
+                              cudaStream_t s) {
+    const dim3 b2(32, 8), g2(nblk(n, 32), nblk(n, 8));
+    if (dt == KFB_F64)
+        dense_lower_to_rfp_kernel<double><<<g2, b2, 0, s>>>(L, n, uplo, static_cast<double *>(arf));
+    else
+        dense_lower_to_rfp_kernel<float><<<g2, b2, 0, s>>>(L, n, uplo, static_cast<float *>(arf));
+    KFB_CUDA_TRY(cudaGetLastError());
+    return KFB_OK;
+}
+
+// In-place RFP Cholesky of (A + l2 I): the RFP array is expanded to a dense
+// column-major FP64 lower triangle, factored by chol_dense (tensor-core panel
+// solves and trailing updates) and packed back into the same RFP layout and
+// element type.  On a non-positive pivot *info is set and arf is unchanged.
+kfb_status rfp_potrf(void *arf, int n, double l2, kfb_layout uplo, kfb_dtype dt, int *info,
+                     cudaStream_t s) {
+    *info = 0;
+    if (n <= 0) return KFB_OK;
+    TraceScope tr("rfp_potrf", s);
+    DevBuf F;
+    KFB_TRY(F.alloc((size_t)n * n * sizeof(double), s));
+    KFB_TRY(rfp_to_dense_lower(arf, n, uplo, dt, l2, F.as<double>(), s));
+    KFB_TRY(chol_dense(F.as<double>(), n, n, chol_slices(dt), info, s));
+    if (*info != 0) return KFB_OK;
+    return dense_lower_to_rfp(F.as<double>(), n, uplo, dt, arf, s);
+}
+
+// Solve with an RFP factor: the factor is expanded to a dense FP64 lower
+// triangle and each right-hand side goes through the two blocked triangular
+// sweeps of trsv.cu (in FP64; FP32 right-hand sides are widened and narrowed).
 kfb_status rfp_potrs(const void *arf, void *B, int n, int nrhs, kfb_layout uplo, kfb_dtype dt,
                      cudaStream_t s) {
-    if (dt == KFB_F64)
-        return rfp_potrs_t<double>(static_cast<const double *>(arf), static_cast<double *>(B), n,
-                                   nrhs, uplo == KFB_RFP_L, s);
-    return rfp_potrs_t<float>(static_cast<const float *>(arf), static_cast<float *>(B), n, nrhs,
-                              uplo == KFB_RFP_L, s);
+    if (n <= 0 || nrhs <= 0) return KFB_OK;
+    TraceScope tr("rfp_potrs", s);
+    DevBuf F, x, tmp;
+    KFB_TRY(F.alloc((size_t)n * n * sizeof(double), s));
+    KFB_TRY(rfp_to_dense_lower(arf, n, uplo, dt, 0.0, F.as<double>(), s));
+    TrsvPlan plan;
+    KFB_TRY(plan.prepare(F.as<double>(), n, s));
+    KFB_TRY(tmp.alloc((size_t)n * sizeof(double), s));
+    if (dt == KFB_F32) KFB_TRY(x.alloc((size_t)n * sizeof(double), s));
+    for (int c = 0; c < nrhs; ++c) {
+        if (dt == KFB_F64) {
+            double *b = static_cast<double *>(B) + (size_t)c * n;
+            KFB_TRY(plan.solve(F.as<double>(), b, tmp.as<double>(), b, s));
+        } else {
+            float *b = static_cast<float *>(B) + (size_t)c * n;
+            f32_to_f64_kernel<<<nblk(n, 256), 256, 0, s>>>(b, n, x.as<double>());
+            KFB_TRY(plan.solve(F.as<double>(), x.as<double>(), tmp.as<double>(), x.as<double>(), s));
+            f64_to_f32_kernel<<<nblk(n, 256), 256, 0, s>>>(x.as<double>(), n, b);
+            KFB_CUDA_TRY(cudaGetLastError());
+        }
+    }
+    return plan.check(s);
 }
 
 namespace {
@@ -439,13 +347,15 @@ namespace {
 // (A + lam I) x of the operator a mixed solve refines against, FP64 vectors
 using ApplyFn = std::function<kfb_status(const double *x, double lam, double *out)>;
 
-// out = (K + l2 I) x with K dense FP32 (row-major, symmetric), one warp per row
-__global__ void dense_apply_kernel(const float *__restrict__ K, const double *__restrict__ x,
+// out = (K + l2 I) x with K dense FP32 or FP64 (row-major, symmetric), one
+// warp per row, FP64 accumulation
+template <class TK>
+__global__ void dense_apply_kernel(const TK *__restrict__ K, const double *__restrict__ x,
                                    int n, double l2, double *__restrict__ out) {
     const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (row >= n) return;
-    const float *kr = K + (size_t)row * n;
+    const TK *kr = K + (size_t)row * n;
     double acc = 0.0;
     for (int j = lane; j < n; j += 32) acc = fma((double)kr[j], x[j], acc);
     for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -540,20 +450,6 @@ __global__ void cg_update_kernel(const double *p, const double *q, double *x, do
         x[k] += a * p[k];
         r[k] -= a * q[k];
     }
-}
-// out = (float)(a / sqrt(sc[i])) (unscaled if sc[i] <= 0)
-__global__ void scale_to_float_dev_kernel(const double *a, const double *sc, int i, int n,
-                                          float *out) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const double t = sc[i];
-    if (k < n) out[k] = (float)(t > 0.0 ? a[k] / sqrt(t) : a[k]);
-}
-// out = sqrt(sc[i]) * (double)a
-__global__ void float_to_double_dev_kernel(const float *a, const double *sc, int i, int n,
-                                           double *out) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const double t = sc[i];
-    if (k < n) out[k] = (t > 0.0 ? sqrt(t) : 1.0) * (double)a[k];
 }
 // p = z + beta p with beta = sc[new] / sc[old]
 __global__ void xpby_dev_kernel(const double *z, const double *sc, int new_slot, int old_slot,
@@ -650,15 +546,12 @@ kfb_status mixed_core(const ApplyFn &A, const float *B, int n, kfb_layout uplo, 
                       double fcoef, double defl, double lam2, const double *y, double l2,
                       double tol, int maxit, int flags, double *alpha, kfb_solve_info &inf,
                       DevScalars &ds, cudaStream_t s) {
-    const size_t nt = (size_t)n * (n + 1) / 2;
-    DevBuf F, r, z, p, q, f32v, dw;
-    KFB_TRY(F.alloc(nt * sizeof(float), s));
+    DevBuf r, z, p, q, dw;
     KFB_TRY(r.alloc((size_t)n * sizeof(double), s));
     KFB_TRY(z.alloc((size_t)n * sizeof(double), s));
     KFB_TRY(p.alloc((size_t)n * sizeof(double), s));
     KFB_TRY(q.alloc((size_t)n * sizeof(double), s));
     KFB_TRY(dw.alloc((size_t)n * sizeof(double), s));
-    KFB_TRY(f32v.alloc((size_t)n * sizeof(float), s));
     const unsigned gb = nblk(n, 256);
     const double u32 = 5.960464477539063e-08;
     double *sc = ds.sc();
@@ -669,60 +562,30 @@ kfb_status mixed_core(const ApplyFn &A, const float *B, int n, kfb_layout uplo, 
     KFB_TRY(zero(alpha, (size_t)n * sizeof(double), s));
     if (ynorm == 0.0) return KFB_OK;
 
-    // out = F^{-1} x, x scaled to unit norm by the device scalar sc[slot] = |x|^2
-    // The factor: FP32 Cholesky of the dense lower triangle (one cuSOLVER call,
-    // faster at these sizes than the RFP block sequence), packed to RFP for the
-    // triangular solves; or, with KFB_SOLVE_FP64_FACTOR, an FP64 dense factor
-    // used as it is.
+    // The factor: the dense lower triangle of F factored by chol_dense (panel
+    // solves and trailing updates on the int8 tensor cores) with 4 digit planes
+    // (FP32-class: the north-star precision of the preconditioner) or, with
+    // KFB_SOLVE_FP64_FACTOR, 7 (FP64-class); held in FP64 either way, so the
+    // preconditioner out = F^{-1} x is the pair of blocked FP64 sweeps of
+    // trsv.cu.
     const bool f64 = (flags & KFB_SOLVE_FP64_FACTOR) != 0;
-    Handles *hd = nullptr;
-    KFB_TRY(get_handles(s, hd));
-    DevBuf Fd, ws, dinfo, ttmp;
-    TrsvPlan trsv;   // FP64 factor: blocked triangular solves
-    KFB_TRY(Fd.alloc((size_t)n * n * (f64 ? sizeof(double) : sizeof(float)), s));
-    if (f64) KFB_TRY(ttmp.alloc((size_t)n * sizeof(double), s));
-    KFB_TRY(dinfo.alloc(sizeof(int), s));
-    int lwork = 0;
-    if (f64)
-        KFB_SOLVER_TRY(cusolverDnDpotrf_bufferSize(hd->solver, CUBLAS_FILL_MODE_LOWER, n,
-                                                   Fd.as<double>(), n, &lwork));
-    else
-        KFB_SOLVER_TRY(cusolverDnSpotrf_bufferSize(hd->solver, CUBLAS_FILL_MODE_LOWER, n,
-                                                   Fd.as<float>(), n, &lwork));
-    KFB_TRY(ws.alloc((size_t)std::max(lwork, 1) * (f64 ? sizeof(double) : sizeof(float)), s));
+    DevBuf Fd, ttmp;
+    TrsvPlan trsv;
+    KFB_TRY(Fd.alloc((size_t)n * n * sizeof(double), s));
+    KFB_TRY(ttmp.alloc((size_t)n * sizeof(double), s));
     auto factor = [&](double diag, int &finfo) -> kfb_status {
-        const dim3 b2(32, 8), g2(nblk(n, 32), nblk(n, 8)), gt(nblk(n, 32), nblk(n, 32));
-        KFB_TRY(zero(dinfo.ptr, sizeof(int), s));
-        if (f64) {
-            dense_deflate_kernel<double><<<gt, b2, 0, s>>>(B, n, uplo, v, fcoef, diag,
-                                                           Fd.as<double>());
-            KFB_CUDA_TRY(cudaGetLastError());
-            KFB_SOLVER_TRY(cusolverDnDpotrf(hd->solver, CUBLAS_FILL_MODE_LOWER, n, Fd.as<double>(),
-                                            n, ws.as<double>(), lwork, dinfo.as<int>()));
-        } else {
-            dense_deflate_kernel<float><<<gt, b2, 0, s>>>(B, n, uplo, v, fcoef, diag,
-                                                          Fd.as<float>());
-            KFB_CUDA_TRY(cudaGetLastError());
-            KFB_SOLVER_TRY(cusolverDnSpotrf(hd->solver, CUBLAS_FILL_MODE_LOWER, n, Fd.as<float>(),
-                                            n, ws.as<float>(), lwork, dinfo.as<int>()));
-        }
-        KFB_CUDA_TRY(cudaMemcpyAsync(&finfo, dinfo.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
-        KFB_CUDA_TRY(cudaStreamSynchronize(s));
-        if (finfo == 0 && !f64) {
-            dense_lower_to_rfp_kernel<<<g2, b2, 0, s>>>(Fd.as<float>(), n, uplo, F.as<float>());
-            KFB_CUDA_TRY(cudaGetLastError());
-        }
-        if (finfo == 0 && f64) KFB_TRY(trsv.prepare(Fd.as<double>(), n, s));
+        const dim3 b2(32, 8), gt(nblk(n, 32), nblk(n, 32));
+        dense_deflate_kernel<double><<<gt, b2, 0, s>>>(B, n, uplo, v, fcoef, diag,
+                                                       Fd.as<double>());
+        KFB_CUDA_TRY(cudaGetLastError());
+        KFB_TRY(chol_dense(Fd.as<double>(), n, n, f64 ? 7 : 4, &finfo, s));
+        if (finfo == 0) KFB_TRY(trsv.prepare(Fd.as<double>(), n, s));
         return KFB_OK;
     };
     auto solve_f_dev = [&](const double *x, int slot, double *out) -> kfb_status {
+        (void)slot;
         TraceScope tr_s("mixed:potrs", s);
-        if (f64) return trsv.solve(Fd.as<double>(), x, ttmp.as<double>(), out, s);
-        scale_to_float_dev_kernel<<<gb, 256, 0, s>>>(x, sc, slot, n, f32v.as<float>());
-        KFB_TRY(rfp_potrs(F.ptr, f32v.ptr, n, 1, uplo, KFB_F32, s));
-        float_to_double_dev_kernel<<<gb, 256, 0, s>>>(f32v.as<float>(), sc, slot, n, out);
-        KFB_CUDA_TRY(cudaGetLastError());
-        return KFB_OK;
+        return trsv.solve(Fd.as<double>(), x, ttmp.as<double>(), out, s);
     };
 
     auto attempt = [&](double lam) -> kfb_status {
@@ -742,7 +605,8 @@ kfb_status mixed_core(const ApplyFn &A, const float *B, int n, kfb_layout uplo, 
         inf.shift = shift;
         if (finfo != 0)
             return set_error(KFB_ERR_NOT_PD,
-                             "FP32 RFP Cholesky failed even with shift %g (info=%d)", shift, finfo);
+                             "the preconditioner's Cholesky failed even with shift %g (info=%d)",
+                             shift, finfo);
         tr_f.reset();
         TraceScope tr_cg("mixed:cg", s);
         // w = F^{-1} v (v has unit norm: slot S_NRM set to 1 for the scaling);
@@ -843,7 +707,7 @@ kfb_status mixed_core(const ApplyFn &A, const float *B, int n, kfb_layout uplo, 
             }
             total_it += it;
             if (indefinite) {
-                if (f64) KFB_TRY(trsv.check(s));
+                KFB_TRY(trsv.check(s));
                 inf.iterations = total_it;
                 return set_error(KFB_ERR_NOT_PD,
                                  "the system is indefinite at the precision of its matrix "
@@ -862,7 +726,7 @@ kfb_status mixed_core(const ApplyFn &A, const float *B, int n, kfb_layout uplo, 
             rel = std::sqrt(rr) / ynorm;
             if (rel <= tol || total_it >= maxit) break;
         }
-        if (f64) KFB_TRY(trsv.check(s));
+        KFB_TRY(trsv.check(s));
         inf.iterations = total_it;
         inf.used_cg = 1;
         inf.rel_residual = rel;
@@ -895,6 +759,50 @@ kfb_status mixed_core(const ApplyFn &A, const float *B, int n, kfb_layout uplo, 
 
 }  // namespace
 
+namespace {
+// r = y - r
+__global__ void rsub_kernel(const double *y, int n, double *r) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) r[i] = y[i] - r[i];
+}
+}  // namespace
+
+// FP64 kernel ridge solve behind kernelmath.cho_solve_rfp: the FP64-class
+// tensor-core Cholesky (7 digit planes) of K + l2 I, the two blocked triangular
+// sweeps, and two steps of iterative refinement against K itself (residual
+// y - (K + l2 I) alpha from a dense FP64 copy of K), which bring alpha to the
+// accuracy of an FP64 LAPACK solve; the factor is then written over the RFP
+// input in its layout, as dpftrf does (src/math.cpp:134-171).
+kfb_status cho_solve_rfp_f64(double *arf, const double *y, int n, double l2, kfb_layout uplo,
+                             double *alpha, int *info, cudaStream_t s) {
+    *info = 0;
+    if (n <= 0) return KFB_OK;
+    TraceScope tr("cho_solve_rfp", s);
+    DevBuf D, F, r, tmp;
+    KFB_TRY(D.alloc((size_t)n * n * sizeof(double), s));
+    KFB_TRY(F.alloc((size_t)n * n * sizeof(double), s));
+    KFB_TRY(r.alloc((size_t)n * sizeof(double), s));
+    KFB_TRY(tmp.alloc((size_t)n * sizeof(double), s));
+    KFB_TRY(rfp_to_full(arf, n, uplo, KFB_F64, D.ptr, s));
+    KFB_TRY(rfp_to_dense_lower(arf, n, uplo, KFB_F64, l2, F.as<double>(), s));
+    KFB_TRY(chol_dense(F.as<double>(), n, n, 7, info, s));
+    if (*info != 0) return KFB_OK;
+    TrsvPlan plan;
+    KFB_TRY(plan.prepare(F.as<double>(), n, s));
+    KFB_TRY(plan.solve(F.as<double>(), y, tmp.as<double>(), alpha, s));
+    const unsigned gw = nblk((long long)n * 32, 256), gb = nblk(n, 256);
+    for (int it = 0; it < 2; ++it) {
+        dense_apply_kernel<double><<<gw, 256, 0, s>>>(D.as<double>(), alpha, n, l2, r.as<double>());
+        rsub_kernel<<<gb, 256, 0, s>>>(y, n, r.as<double>());
+        KFB_CUDA_TRY(cudaGetLastError());
+        KFB_TRY(plan.solve(F.as<double>(), r.as<double>(), tmp.as<double>(), r.as<double>(), s));
+        axpy_kernel<<<gb, 256, 0, s>>>(r.as<double>(), 1.0, n, alpha);
+        KFB_CUDA_TRY(cudaGetLastError());
+    }
+    KFB_TRY(plan.check(s));
+    return dense_lower_to_rfp(F.as<double>(), n, uplo, KFB_F64, arf, s);
+}
+
 // Kernel ridge: A = K (FP32 RFP input, expanded to a dense FP32 copy for the
 // FP64 residual products); the factor deflates K's dominant eigenpair.
 kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2,
@@ -914,7 +822,7 @@ kfb_status krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2
     const unsigned gw = nblk((long long)n * 32, 256);
     ApplyFn A = [&](const double *x, double lam, double *out) -> kfb_status {
         TraceScope tr_a("mixed:apply", s);
-        dense_apply_kernel<<<gw, 256, 0, s>>>(Kd.as<float>(), x, n, lam, out);
+        dense_apply_kernel<float><<<gw, 256, 0, s>>>(Kd.as<float>(), x, n, lam, out);
         KFB_CUDA_TRY(cudaGetLastError());
         return KFB_OK;
     };
