@@ -3,17 +3,18 @@
 //
 // Kernel roles (one persistent CTA per SM over a tile list, 384 threads):
 //   warp 0      TMA producer: per 64-byte K slice, the S digit planes of the
-//               A tile (128 rows) and of the B tile (64 rows), 64-byte swizzle,
-//               into a 2-stage shared-memory ring (S x 12 KB per stage);
+//               A tile (128 rows) and of the B tile (BN = 128 rows for S <= 4,
+//               else 64), 64-byte swizzle, into a shared-memory ring of 2-4
+//               stages;
 //   warp 1      MMA issuer: per K32 step, for every level L = 2 .. S+1 and every
-//               digit pair p + q = L, tcgen05.mma kind::i8 (M=128, N=64, K=32,
-//               s32 accumulation) into level L's TMEM accumulator (64 columns
+//               digit pair p + q = L, tcgen05.mma kind::i8 (M=128, N=BN, K=32,
+//               s32 accumulation) into level L's TMEM accumulator (BN columns
 //               each, S accumulators side by side);
 //   warp 2      TMEM allocator (512 columns);
-//   warps 4..11 epilogue, two per TMEM lane quadrant (32 columns each): load the
-//               S int32 levels, combine them in FP64 (Horner in 2^-7), release
-//               TMEM to the MMA issuer, then scale by 2^(e_a + e_b - 14) alpha
-//               and store / accumulate the FP64 outputs.
+//   warps 4..11 epilogue, two per TMEM lane quadrant (32-column chunks): load
+//               the S int32 levels, combine them in FP64 (Horner in 2^-7),
+//               release TMEM to the MMA issuer, then scale by 2^(e_a + e_b -
+//               14) alpha and store / accumulate the FP64 outputs.
 // Every mbarrier wait is bounded (%globaltimer); a wait that gives up raises
 // the error flag instead of trapping.  No TMA multicast.
 #include <cuda.h>
@@ -33,20 +34,28 @@ namespace {
 
 using namespace tc;
 
-constexpr int BM = OZ_BM, BN = OZ_BN, BK = OZ_BK;
-constexpr int TILE_A = BM * BK, TILE_B = BN * BK;   // bytes per digit plane
-constexpr int NSTAGE = 2;
+constexpr int BM = OZ_BM, BK = OZ_BK;
+constexpr int TILE_A = BM * BK;   // bytes per digit plane of an A tile
 constexpr int EPI_WARP0 = 4, NUM_EPI_WARPS = 8;
 constexpr int NUM_THREADS = 32 * (EPI_WARP0 + NUM_EPI_WARPS);
 constexpr int TMEM_COLS = 512;
 
+// S digit planes, BN output columns per tile (S BN <= 512 TMEM columns), as
+// many pipeline stages (up to 4) as fit in 200 KB of shared memory.
 template <int S>
 struct OzCfg {
+    static constexpr int BN = oz_bn(S);
+    static constexpr int TILE_B = BN * BK;
     static constexpr int STAGE = S * (TILE_A + TILE_B);
+    static constexpr int NSTAGE = (200 * 1024 / STAGE) < 4 ? (200 * 1024 / STAGE) : 4;
     static constexpr int OFF_BARS = NSTAGE * STAGE;
     static constexpr int NBARS = 2 * NSTAGE + 3;   // full, empty, tmem_full, tmem_empty, done
     static constexpr int OFF_TMEM = OFF_BARS + NBARS * 8;
     static constexpr int SMEM = OFF_TMEM + 16 + 1024;
+    // instruction descriptor, kind::i8: signed A and B (K-major), s32 accumulator
+    static constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) |
+                                      ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+    static_assert(NSTAGE >= 2, "pipeline depth");
     static_assert(S * BN <= TMEM_COLS, "TMEM columns");
     static_assert(SMEM <= 227 * 1024, "shared memory budget");
 };
@@ -58,27 +67,28 @@ __device__ __forceinline__ uint64_t sdesc64(uint32_t saddr) {
            ((uint64_t)(512 >> 4) << 32) | ((uint64_t)1 << 46) | ((uint64_t)4 << 61);
 }
 
-// Instruction descriptor, kind::i8: signed A and B (K-major), s32 accumulator.
-constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
-                           ((uint32_t)(BM >> 4) << 24);
-
-__device__ __forceinline__ void umma_i8(uint32_t dtmem, uint64_t a, uint64_t b, uint32_t acc) {
+__device__ __forceinline__ void umma_i8(uint32_t dtmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                        uint32_t acc) {
     asm volatile(
         "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
         " tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n" ::"r"(dtmem),
-        "l"(a), "l"(b), "r"(IDESC), "r"(acc)
+        "l"(a), "l"(b), "r"(idesc), "r"(acc)
         : "memory");
 }
 
-// Tile t of a generated tile set (see OzGen).  Lower mode: row tile ti holds
-// min(ntc, 2 ti + 2) column tiles (BM = 2 BN), the ones with some j <= i.
-__host__ __device__ __forceinline__ OzTile gen_tile(const OzGen &g, long long ldr,
+// Column tiles of row tile ti in lower mode: the ones holding some j <= i.
+__host__ __device__ __forceinline__ int lower_tiles(int ti, int ntc, int BN) {
+    return min(ntc, ((ti + 1) * BM + BN - 1) / BN);
+}
+
+// Tile t of a generated tile set (see OzGen), BN columns per tile.
+__host__ __device__ __forceinline__ OzTile gen_tile(const OzGen &g, int BN, long long ldr,
                                                     long long ldc, int t) {
     const int ntc = (g.N + BN - 1) / BN;
     int ti = 0, tj = t;
     if (g.mode == OZ_GEN_LOWER) {
         while (true) {
-            const int cnt = min(ntc, 2 * ti + 2);
+            const int cnt = lower_tiles(ti, ntc, BN);
             if (tj < cnt) break;
             tj -= cnt;
             ++ti;
@@ -98,6 +108,16 @@ __host__ __device__ __forceinline__ OzTile gen_tile(const OzGen &g, long long ld
     return tl;
 }
 
+// 3-D tile load: box (x, y, z) of the tensor map into shared memory.
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map, int x, int y,
+                                            int z, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(bar)
+        : "memory");
+}
+
 __device__ __forceinline__ void tmem_ld32_i(uint32_t taddr, int (&v)[32]) {
     float f[32];
     tmem_ld32(taddr, f);
@@ -112,6 +132,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                    const int *__restrict__ eb, const OzTile *__restrict__ tiles, OzGen gen,
                    int ntiles, OzEpi epi, int *err) {
     using C = OzCfg<S>;
+    constexpr int BN = C::BN, TILE_B = C::TILE_B, NSTAGE = C::NSTAGE;
     if (epi.skip && *(volatile const int *)epi.skip) return;   // block-uniform
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>(
@@ -155,7 +176,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             uint32_t ph = 0;
             bool ok = true;
             for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-                const OzTile tl = tiles ? tiles[t] : gen_tile(gen, epi.ldr, epi.ldc, t);
+                const OzTile tl = tiles ? tiles[t] : gen_tile(gen, BN, epi.ldr, epi.ldc, t);
                 for (int kb = 0; kb < nkb; ++kb) {
                     if (!mbar_wait(empty_bar(stage), ph ^ 1u, err)) {
                         ok = false;
@@ -163,13 +184,9 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                     }
                     const uint32_t sa = s_base + stage * C::STAGE;
                     mbar_expect_tx(full_bar(stage), C::STAGE);
-#pragma unroll
-                    for (int sl = 0; sl < S; ++sl) {
-                        tma_load_2d(sa + sl * TILE_A, &tm_a, kb * BK,
-                                    (int)(sl * a_rows + tl.a0), full_bar(stage));
-                        tma_load_2d(sa + S * TILE_A + sl * TILE_B, &tm_b, kb * BK,
-                                    (int)(sl * b_rows + tl.b0), full_bar(stage));
-                    }
+                    // all S planes of each operand tile in one 3-D box
+                    tma_load_3d(sa, &tm_a, kb * BK, tl.a0, 0, full_bar(stage));
+                    tma_load_3d(sa + S * TILE_A, &tm_b, kb * BK, tl.b0, 0, full_bar(stage));
                     if (++stage == NSTAGE) {
                         stage = 0;
                         ph ^= 1u;
@@ -205,7 +222,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                                 const uint64_t db =
                                     sdesc64(sa + S * TILE_A + (q - 1) * TILE_B + ks * 32);
                                 const bool first = kb == 0 && ks == 0 && p == 1;
-                                umma_i8(dtm, da, db, first ? 0u : 1u);
+                                umma_i8(dtm, da, db, C::IDESC, first ? 0u : 1u);
                             }
                         }
                     }
@@ -223,50 +240,77 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             mbar_wait(done_bar, 0, err);
         }
     } else if (warp >= EPI_WARP0) {
+        // warp (q, h): TMEM lane quadrant q (tile rows 32 q ..), 32-column
+        // chunks h, h + 2, ... of each level
         const int q = warp & 3;
-        const int h = (warp - EPI_WARP0) >> 2;   // column half: 32 columns of each level
+        const int h = (warp - EPI_WARP0) >> 2;
+        constexpr int NCH = BN / 64;
         uint32_t aph = 0;
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-            const OzTile tl = tiles ? tiles[t] : gen_tile(gen, epi.ldr, epi.ldc, t);
+            const OzTile tl = tiles ? tiles[t] : gen_tile(gen, BN, epi.ldr, epi.ldc, t);
             const int i = q * 32 + lane;
             const bool got = mbar_wait(tfull_bar, aph, err);
             if (!__all_sync(0xffffffffu, got)) break;
             tc_fence_after();
-            const uint32_t tb = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(h * 32);
-            double acc[32];
-            {
-                int v[32];
-                tmem_ld32_i(tb + (uint32_t)((S - 1) * BN), v);
 #pragma unroll
-                for (int j = 0; j < 32; ++j) acc[j] = (double)v[j];
-            }
+            for (int ch = 0; ch < NCH; ++ch) {
+                const int col0 = (h + 2 * ch) * 32;
+                const uint32_t tb = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)col0;
+                double acc[32];
+                {
+                    int v[32];
+                    tmem_ld32_i(tb + (uint32_t)((S - 1) * BN), v);
 #pragma unroll
-            for (int l = S - 2; l >= 0; --l) {
-                int v[32];
-                tmem_ld32_i(tb + (uint32_t)(l * BN), v);
+                    for (int j = 0; j < 32; ++j) acc[j] = (double)v[j];
+                }
 #pragma unroll
-                for (int j = 0; j < 32; ++j) acc[j] = fma(acc[j], 0.0078125, (double)v[j]);
-            }
-            // the levels are in registers: hand TMEM back to the MMA issuer
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(tempty_bar);
-            aph ^= 1u;
-            if (i < tl.m) {
-                const int er = ea[tl.a0 + i] - 14;
-                double *crow = epi.c + tl.c_off + (long long)i * epi.ldr;
-                const int lim = tl.lower ? tl.a0 + i + tl.lower_shift - tl.b0 : INT_MAX;
+                for (int l = S - 2; l >= 0; --l) {
+                    int v[32];
+                    tmem_ld32_i(tb + (uint32_t)(l * BN), v);
 #pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    const int jj = h * 32 + j;
-                    if (jj < tl.n && jj <= lim) {
-                        const double val = epi.alpha * ldexp(acc[j], er + eb[tl.b0 + jj]);
-                        double *dst = crow + (long long)jj * epi.ldc;
-                        if (epi.mode == OZ_ADD) *dst += val;
-                        else *dst = val;
+                    for (int j = 0; j < 32; ++j) acc[j] = fma(acc[j], 0.0078125, (double)v[j]);
+                }
+                if (ch == NCH - 1) {
+                    // every level of this warp's chunks is in registers: hand
+                    // TMEM back to the MMA issuer
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(tempty_bar);
+                }
+                if (i < tl.m) {
+                    // columns col0 .. col0 + 31 of row i; nv of them are inside
+                    // the tile (and on or below the diagonal in lower mode)
+                    const int er = ea[tl.a0 + i] - 14;
+                    double *crow = epi.c + tl.c_off + (long long)i * epi.ldr +
+                                   (long long)col0 * epi.ldc;
+                    const int *ebh = eb + tl.b0 + col0;
+                    int nv = min(tl.n - col0, 32);
+                    if (tl.lower) nv = min(nv, tl.a0 + i + tl.lower_shift - tl.b0 - col0 + 1);
+#pragma unroll
+                    for (int j = 0; j < 32; ++j)
+                        if (j < nv) acc[j] = epi.alpha * oz_scale2(acc[j], er + ebh[j]);
+                    if (epi.mode == OZ_ADD) {
+                        // the loads of 16 old values first, then their stores: two
+                        // memory latencies per chunk row instead of one per column
+#pragma unroll
+                        for (int hh = 0; hh < 32; hh += 16) {
+                            double old[16];
+#pragma unroll
+                            for (int j = 0; j < 16; ++j)
+                                if (hh + j < nv) old[j] = crow[(long long)(hh + j) * epi.ldc];
+#pragma unroll
+                            for (int j = 0; j < 16; ++j)
+                                if (hh + j < nv)
+                                    crow[(long long)(hh + j) * epi.ldc] = old[j] + acc[hh + j];
+                        }
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j)
+                            if (j < nv) crow[(long long)j * epi.ldc] = acc[j];
                     }
                 }
             }
+            aph ^= 1u;
         }
     }
     tc_fence_before();
@@ -280,24 +324,6 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
 }
 
 // ------------------------------------------------------------------ slicing
-// Balanced base-128 digits of v = a 2^-e (|v| < 1/2): t = 128 v, d = rint(t),
-// v = t - d, S times (every step exact in FP64).
-template <int S>
-__device__ __forceinline__ void digits(double v, int8_t (&d)[S]) {
-#pragma unroll
-    for (int s = 0; s < S; ++s) {
-        const double t = v * 128.0;
-        const double r = rint(t);
-        d[s] = (int8_t)(int)r;
-        v = t - r;
-    }
-}
-
-__device__ __forceinline__ int row_exponent(double amax) {
-    // smallest e with amax < 2^(e-1): amax = m 2^x, m in [1,2) -> e = x + 2
-    return amax > 0.0 ? ilogb(amax) + 2 : 0;
-}
-
 // One warp per row of a row-major source; lanes over groups of 4 columns.
 template <class T, int S>
 __global__ void slice_rows_kernel(const T *__restrict__ src, long long rows, int K, long long ld,
@@ -309,7 +335,7 @@ __global__ void slice_rows_kernel(const T *__restrict__ src, long long rows, int
     double m = 0.0;
     for (int k = lane; k < K; k += 32) m = fmax(m, fabs((double)row[k]));
     for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    const int ex = row_exponent(m);
+    const int ex = oz_row_exponent(m);
     if (lane == 0) e[r] = ex;
     const long long plane = rows * (long long)kp;
     for (int k0 = lane * 4; k0 < kp; k0 += 128) {
@@ -318,7 +344,7 @@ __global__ void slice_rows_kernel(const T *__restrict__ src, long long rows, int
         for (int c = 0; c < 4; ++c) {
             const int k = k0 + c;
             const double v = k < K ? ldexp((double)row[k], -ex) : 0.0;
-            digits<S>(v, dg[c]);
+            oz_digits<S>(v, dg[c]);
         }
 #pragma unroll
         for (int s = 0; s < S; ++s) {
@@ -339,9 +365,23 @@ __global__ void slice_cols_kernel(const double *__restrict__ src, long long rows
     extern __shared__ double tile[];   // [K][33]
     const long long r0 = (long long)blockIdx.x * 32;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int k = warp; k < K; k += nw) {
+    {
+        // eight independent column loads in flight per warp, then the stores
         const long long r = r0 + lane;
-        tile[k * 33 + lane] = r < rows ? src[(long long)k * ld + r] : 0.0;
+        const bool ok = r < rows;
+        for (int k0 = warp; k0 < K; k0 += 8 * nw) {
+            double v[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int k = k0 + u * nw;
+                v[u] = (ok && k < K) ? src[(long long)k * ld + r] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int k = k0 + u * nw;
+                if (k < K) tile[k * 33 + lane] = v[u];
+            }
+        }
     }
     __syncthreads();
     const long long plane = rows * (long long)kp;
@@ -351,7 +391,7 @@ __global__ void slice_cols_kernel(const double *__restrict__ src, long long rows
         double m = 0.0;
         for (int k = lane; k < K; k += 32) m = fmax(m, fabs(tile[k * 33 + rl]));
         for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-        const int ex = row_exponent(m);
+        const int ex = oz_row_exponent(m);
         if (lane == 0) e[r] = ex;
         for (int k0 = lane * 4; k0 < kp; k0 += 128) {
             int8_t dg[4][S];
@@ -359,7 +399,7 @@ __global__ void slice_cols_kernel(const double *__restrict__ src, long long rows
             for (int c = 0; c < 4; ++c) {
                 const int k = k0 + c;
                 const double v = k < K ? ldexp(tile[k * 33 + rl], -ex) : 0.0;
-                digits<S>(v, dg[c]);
+                oz_digits<S>(v, dg[c]);
             }
 #pragma unroll
             for (int s = 0; s < S; ++s) {
@@ -387,16 +427,19 @@ PFN_cuTensorMapEncodeTiled_v12000 oz_encoder() {
     return fn;
 }
 
-// The S digit planes of an operand as one 2-D int8 tensor (kp x S rows),
-// box 64 bytes x box_rows, 64-byte swizzle.
+// The S digit planes of an operand as one 3-D int8 tensor (kp x rows x S),
+// box 64 bytes x box_rows x S (all planes of a tile, stacked in shared
+// memory as S tiles of box_rows x 64 bytes), 64-byte swizzle; rows beyond the
+// operand read as zero.
 kfb_status map_slices(CUtensorMap *m, const OzSlices &o, int box_rows) {
     auto enc = oz_encoder();
     if (!enc) return set_error(KFB_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
-    cuuint64_t gdim[2] = {(cuuint64_t)o.kp, (cuuint64_t)(o.S * std::max<long long>(o.rows, 1))};
-    cuuint64_t gstride[1] = {(cuuint64_t)o.kp};
-    cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
-    cuuint32_t estr[2] = {1, 1};
-    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, o.d, gdim, gstride, box, estr,
+    const cuuint64_t rows = (cuuint64_t)std::max<long long>(o.rows, 1);
+    cuuint64_t gdim[3] = {(cuuint64_t)o.kp, rows, (cuuint64_t)o.S};
+    cuuint64_t gstride[2] = {(cuuint64_t)o.kp, (cuuint64_t)o.kp * rows};
+    cuuint32_t box[3] = {(cuuint32_t)BK, (cuuint32_t)box_rows, (cuuint32_t)o.S};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, o.d, gdim, gstride, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS)
@@ -410,7 +453,7 @@ kfb_status launch(const OzSlices &A, const OzSlices &B, const OzTile *tiles, con
     using C = OzCfg<S>;
     CUtensorMap ta, tb;
     KFB_TRY(map_slices(&ta, A, BM));
-    KFB_TRY(map_slices(&tb, B, BN));
+    KFB_TRY(map_slices(&tb, B, C::BN));
     static bool attr[OZ_MAXS + 1] = {};
     if (!attr[S]) {
         KFB_CUDA_TRY(cudaFuncSetAttribute(oz_gemm_kernel<S>,
@@ -469,7 +512,7 @@ kfb_status oz_slice_cols(const double *src, long long rows, int K, long long ld,
                          const OzSlices &o, cudaStream_t s) {
     KFB_TRY(oz_check(o, K));
     if (rows <= 0) return KFB_OK;
-    if (K > 256) return set_error(KFB_ERR_INVALID_ARG, "column-major slicing takes K <= 256");
+    if (K > 512) return set_error(KFB_ERR_INVALID_ARG, "column-major slicing takes K <= 512");
     const unsigned g = (unsigned)((rows + 31) / 32);
     const size_t sm = (size_t)std::max(K, 1) * 33 * sizeof(double);
     switch (o.S) {
@@ -479,7 +522,7 @@ kfb_status oz_slice_cols(const double *src, long long rows, int K, long long ld,
         if (!a) {                                                                             \
             KFB_CUDA_TRY(cudaFuncSetAttribute(slice_cols_kernel<SS>,                           \
                                               cudaFuncAttributeMaxDynamicSharedMemorySize,    \
-                                              256 * 33 * (int)sizeof(double)));               \
+                                              512 * 33 * (int)sizeof(double)));               \
             a = true;                                                                         \
         }                                                                                     \
         slice_cols_kernel<SS><<<g, 256, sm, s>>>(src, rows, K, ld, o.kp, o.d, o.e);           \
@@ -499,12 +542,13 @@ kfb_status oz_slice_cols(const double *src, long long rows, int K, long long ld,
     return KFB_OK;
 }
 
-int oz_gen_tiles(const OzGen &g) {
+int oz_gen_tiles(const OzGen &g, int S) {
     if (g.M <= 0 || g.N <= 0) return 0;
+    const int BN = oz_bn(S);
     const int ntr = (g.M + BM - 1) / BM, ntc = (g.N + BN - 1) / BN;
     if (g.mode != OZ_GEN_LOWER) return ntr * ntc;
     int n = 0;
-    for (int ti = 0; ti < ntr; ++ti) n += std::min(ntc, 2 * ti + 2);
+    for (int ti = 0; ti < ntr; ++ti) n += lower_tiles(ti, ntc, BN);
     return n;
 }
 
@@ -553,12 +597,13 @@ kfb_status oz_gemm(const OzSlices &A, const OzSlices &B, const OzTile *tiles, in
 
 kfb_status oz_gemm_gen(const OzSlices &A, const OzSlices &B, const OzGen &g, const OzEpi &epi,
                        int *err, cudaStream_t s) {
-    return oz_gemm_core(A, B, nullptr, g, oz_gen_tiles(g), epi, err, s);
+    return oz_gemm_core(A, B, nullptr, g, oz_gen_tiles(g, A.S), epi, err, s);
 }
 
 kfb_status oz_gemm_dense(const OzSlices &A, const OzSlices &B, int M, int N, const OzEpi &epi,
                          cudaStream_t s) {
     std::vector<OzTile> tiles;
+    const int BN = oz_bn(A.S);
     for (int m0 = 0; m0 < M; m0 += BM)
         for (int n0 = 0; n0 < N; n0 += BN) {
             OzTile t{};

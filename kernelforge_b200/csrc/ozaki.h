@@ -27,7 +27,8 @@ namespace kfb {
 
 constexpr int OZ_MAXS = 7;
 constexpr int OZ_BM = 128;   // output rows per tile (TMEM lanes)
-constexpr int OZ_BN = 64;    // output columns per tile (TMEM columns per level)
+// output columns per tile (TMEM columns per level): S levels x BN <= 512
+__host__ __device__ constexpr int oz_bn(int S) { return S <= 4 ? 128 : 64; }
 constexpr int OZ_BK = 64;    // K bytes per pipeline stage (one 64-byte swizzle row)
 
 // Sliced operand: S digit planes d[s][rows][kp] (kp a multiple of OZ_BK, the
@@ -47,12 +48,12 @@ inline int oz_kp(int k) { return (k + OZ_BK - 1) / OZ_BK * OZ_BK; }
 template <class T>
 kfb_status oz_slice_rows(const T *src, long long rows, int K, long long ld, const OzSlices &out,
                          cudaStream_t s);
-// Slice rows of a column-major source: a[r][k] = src[k * ld + r].
+// Slice rows of a column-major source: a[r][k] = src[k * ld + r] (K <= 512).
 kfb_status oz_slice_cols(const double *src, long long rows, int K, long long ld,
                          const OzSlices &out, cudaStream_t s);
 
 // One output tile: rows a0 .. a0 + m - 1 of A against rows b0 .. b0 + n - 1 of
-// B (m <= OZ_BM, n <= OZ_BN).  Output element (i, j) goes to
+// B (m <= OZ_BM, n <= oz_bn(S)).  Output element (i, j) goes to
 //     c[c_off + i * ldr + j * ldc]
 // and, with lower != 0, only where a0 + i + lower_shift >= b0 + j.
 struct OzTile {
@@ -91,7 +92,7 @@ struct OzGen {
     int a_base = 0, b_base = 0;
     long long c_off = 0;
 };
-int oz_gen_tiles(const OzGen &g);
+int oz_gen_tiles(const OzGen &g, int S);
 kfb_status oz_gemm_gen(const OzSlices &A, const OzSlices &B, const OzGen &g, const OzEpi &epi,
                        int *err, cudaStream_t s);
 
@@ -99,5 +100,33 @@ kfb_status oz_gemm_gen(const OzSlices &A, const OzSlices &B, const OzGen &g, con
 // C[i * ldr + j * ldc] (tile list built and uploaded here).
 kfb_status oz_gemm_dense(const OzSlices &A, const OzSlices &B, int M, int N, const OzEpi &epi,
                          cudaStream_t s);
+
+#ifdef __CUDACC__
+// Balanced base-128 digits of v = a 2^-e (|v| < 1/2): t = 128 v, d = rint(t),
+// v = t - d, S times (every step exact in FP64; |d| <= 64).
+template <int S>
+__device__ __forceinline__ void oz_digits(double v, int8_t (&d)[S]) {
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        const double t = v * 128.0;
+        const double r = rint(t);
+        d[s] = (int8_t)(int)r;
+        v = t - r;
+    }
+}
+
+// Row exponent e of a row with max |a| = amax: the smallest e with
+// amax < 2^(e-1) (amax = m 2^x, m in [1, 2) -> e = x + 2), so |a 2^-e| < 1/2.
+__device__ __forceinline__ int oz_row_exponent(double amax) {
+    return amax > 0.0 ? ilogb(amax) + 2 : 0;
+}
+
+// x 2^p, exact: a multiplication by the power of two built from its exponent
+// bits when 2^p is a normal double, ldexp otherwise.
+__device__ __forceinline__ double oz_scale2(double x, int p) {
+    if (p >= -1022 && p <= 1023) return x * __longlong_as_double((long long)(p + 1023) << 52);
+    return ldexp(x, p);
+}
+#endif
 
 }  // namespace kfb
