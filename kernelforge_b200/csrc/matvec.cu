@@ -12,34 +12,30 @@
 //   F_(a,c) = sum_{i in a} J_i[:, c] . g_i,
 //   g_i     = sum_j w Ad_j + sum_j v_ij d,  v_ij = -w alpha_E[b] - w2 (d . Ad_j)
 //           = W Ad + rowsum(V) x_i - V X2     (W_ij = w, V_ij = v_ij)
-// Per label bucket: G = X1 X2^T and P = X1 Ad^T as FP64 GEMMs (cuBLAS; the
-// FP64 tensor cores), one fused kernel for e, w, v, the energy sums and W, V
-// (written over G, P), two more FP64 GEMMs for g, and a contraction of g with
-// each query atom's Jacobian.  Query rows are processed in chunks that keep
-// the two (rows x training atoms) matrices within the workspace budget.
-#include <cublas_v2.h>
+// Per label bucket: G = X1 X2^T and P = X1 Ad^T as FP64-class products on the
+// int8 tensor cores (ozaki.h: 7 digit planes per operand, exact int32 level
+// sums combined in FP64), one fused kernel for e, w, v, the energy sums and
+// W, V (written over G, P), two more such products for g (contracting over the
+// label's training atoms, in chunks of 65,536), and a contraction of g with
+// each query atom's Jacobian.  Every product is oriented so that the rows of
+// its first operand run along the output's contiguous dimension (coalesced
+// epilogue stores).  Query rows are processed in chunks that keep the two
+// (rows x training atoms) matrices within the workspace budget.
 
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <memory>
 #include <vector>
 
 #include "kfb_internal.h"
+#include "ozaki.h"
 
 namespace kfb {
-
-kfb_status blas_for_stream(cudaStream_t s, cublasHandle_t *out);
 
 namespace {
 
 unsigned nblk(long long n, int t) { return (unsigned)std::max<long long>(1, (n + t - 1) / t); }
-
-#define KFB_BLAS_TRY(expr)                                                                  \
-    do {                                                                                    \
-        cublasStatus_t _b = (expr);                                                         \
-        if (_b != CUBLAS_STATUS_SUCCESS)                                                    \
-            return set_error(KFB_ERR_CUDA, "%s failed: cublas status %d", #expr, (int)_b);  \
-    } while (0)
 
 // Ad[b, j, :] = dX2[b, j] (rep x 3 n_b) . alpha[off_b : off_b + 3 n_b]; zero
 // for padded atoms.  Block per (b, j), threads over k.
@@ -187,31 +183,98 @@ size_t workspace_budget() {
     return (size_t)(gb * (1ull << 30));
 }
 
+// FP64-class products on the int8 tensor cores (ozaki.h): 7 digit planes per
+// operand (about 48 significant bits), exact int32 level sums combined in FP64.
+constexpr int MV_S = 7;
+constexpr int MV_KMAX = 65536;   // K of one product (int32 level sums stay exact)
+
+// Digit planes of one operand, the buffers grown on demand.
+struct MvOperand {
+    DevBuf d, e;
+    OzSlices sl;
+    kfb_status reserve(long long rows, int K, cudaStream_t s) {
+        const int kp = oz_kp(std::max(K, 1));
+        const size_t nd = (size_t)MV_S * (size_t)std::max<long long>(rows, 1) * kp;
+        const size_t ne = (size_t)std::max<long long>(rows, 1) * sizeof(int);
+        if (d.bytes < nd) {
+            d.release();
+            KFB_TRY(d.alloc(nd, s));
+        }
+        if (e.bytes < ne) {
+            e.release();
+            KFB_TRY(e.alloc(ne, s));
+        }
+        sl.d = d.as<int8_t>();
+        sl.e = e.as<int>();
+        sl.S = MV_S;
+        sl.rows = rows;
+        sl.kp = kp;
+        return KFB_OK;
+    }
+    // rows of a row-major source (ld between rows)
+    kfb_status rows_of(const double *src, long long rows, int K, long long ld, cudaStream_t s) {
+        KFB_TRY(reserve(rows, K, s));
+        return oz_slice_rows<double>(src, rows, K, ld, sl, s);
+    }
+    // rows of the transpose of a row-major source: row i = column i
+    kfb_status cols_of(const double *src, long long rows, int K, long long ld, DevBuf &mx,
+                       cudaStream_t s) {
+        KFB_TRY(reserve(rows, K, s));
+        if (mx.bytes < (size_t)rows * 8) {
+            mx.release();
+            KFB_TRY(mx.alloc((size_t)rows * 8, s));
+        }
+        return oz_slice_colmajor(src, rows, K, ld, sl, mx.as<unsigned long long>(), s);
+    }
+};
+
+// C[j * ldc + i] (or +=) alpha sum_k A[i][k] B[j][k] for i < M (rows of A),
+// j < N (rows of B): A's rows run along C's contiguous dimension, so the
+// epilogue's stores are coalesced.
+kfb_status mv_gemm(const OzSlices &A, const OzSlices &B, int M, int N, double *C, long long ldc,
+                   double alpha, bool add, int *err, cudaStream_t s) {
+    OzGen g;
+    g.mode = OZ_GEN_RECT;
+    g.M = M;
+    g.N = N;
+    OzEpi epi;
+    epi.c = C;
+    epi.ldr = 1;
+    epi.ldc = ldc;
+    epi.mode = add ? OZ_ADD : OZ_STORE;
+    epi.alpha = alpha;
+    return oz_gemm_gen(A, B, g, epi, err, s);
+}
+
 template <class Tin>
 kfb_status matvec_t(const Tin *x1, const Tin *dx1, const Tin *x2, const double *ad,
                     const double *alpha_e, const SetView &s1, const SetView &s2, int rep,
                     double sigma, double *E, double *F, cudaStream_t s) {
-    cublasHandle_t h = nullptr;
-    KFB_TRY(blas_for_stream(s, &h));
     if (E) KFB_TRY(zero(E, (size_t)s1.nm * sizeof(double), s));
     std::vector<int> off1;
     const long long naq1 = deriv_offsets(s1, off1);
     if (F) KFB_TRY(zero(F, (size_t)std::max<long long>(naq1, 1) * sizeof(double), s));
     const std::vector<int> labels = collect_labels(s1, &s2);
     if (labels.empty()) return KFB_OK;
+    if (!device_is_sm100())
+        return set_error(KFB_ERR_UNSUPPORTED, "the contracted prediction needs an sm_100 (B200) device");
     const Buckets b1 = make_buckets(s1, labels), b2 = make_buckets(s2, labels);
     std::vector<int> n1v(s1.nm);
     for (int m = 0; m < s1.nm; ++m) n1v[m] = s1.natoms(m);
-    DevBuf dn1, doff1, didx1, dmol1, didx2, dmol2;
+    DevBuf dn1, doff1, didx1, dmol1, didx2, dmol2, derr, mx;
     KFB_TRY(upload(dn1, n1v, s));
     KFB_TRY(upload(doff1, off1, s));
     KFB_TRY(upload(didx1, b1.src, s));
     KFB_TRY(upload(dmol1, b1.mol, s));
     KFB_TRY(upload(didx2, b2.src, s));
     KFB_TRY(upload(dmol2, b2.mol, s));
+    // one pipeline-timeout flag for every tensor-core product of the call
+    KFB_TRY(derr.alloc(sizeof(int), s));
+    KFB_TRY(zero(derr.ptr, sizeof(int), s));
+    int *err = derr.as<int>();
     const double c = -1.0 / (2.0 * sigma * sigma), is2 = 1.0 / (sigma * sigma), is4 = is2 * is2;
-    const double one = 1.0, zerod = 0.0, mone = -1.0;
     const bool with_ad = ad != nullptr, with_f = F != nullptr;
+    MvOperand X2s, Ads, X1s, Ms;
     for (int l = 0; l < (int)labels.size(); ++l) {
         const int sa = b1.lab_start[l], r1 = b1.lab_start[l + 1] - sa;
         const int sb = b2.lab_start[l], r2 = b2.lab_start[l + 1] - sb;
@@ -233,8 +296,28 @@ kfb_status matvec_t(const Tin *x1, const Tin *dx1, const Tin *x2, const double *
             X2l.as<double>(), with_ad ? Adl.as<double>() : nullptr, dmol2.as<int>() + sb,
             alpha_e, r2, rep, scl.as<double>(), ael.as<double>());
         KFB_CUDA_TRY(cudaGetLastError());
+        // digit planes of the training rows (K = rep) and, for the force
+        // products g = W Ad - V X2 (K = r2, in chunks of MV_KMAX), of their
+        // transposes
+        KFB_TRY(X2s.rows_of(X2l.as<double>(), r2, rep, rep, s));
+        if (with_ad) KFB_TRY(Ads.rows_of(Adl.as<double>(), r2, rep, rep, s));
+        const int nkc = (r2 + MV_KMAX - 1) / MV_KMAX;
+        std::vector<std::unique_ptr<MvOperand>> X2t, Adt;
+        if (with_f)
+            for (int kc = 0; kc < nkc; ++kc) {
+                const int k0 = kc * MV_KMAX, kn = std::min(MV_KMAX, r2 - k0);
+                X2t.emplace_back(new MvOperand);
+                KFB_TRY(X2t.back()->cols_of(X2l.as<double>() + (size_t)k0 * rep, rep, kn, rep,
+                                            mx, s));
+                if (with_ad) {
+                    Adt.emplace_back(new MvOperand);
+                    KFB_TRY(Adt.back()->cols_of(Adl.as<double>() + (size_t)k0 * rep, rep, kn,
+                                                rep, mx, s));
+                }
+            }
         // query rows in chunks: G and P (r1c x r2 each), X1 and g (r1c x rep)
-        const size_t per_row = ((size_t)2 * r2 + 2 * rep + 2) * sizeof(double);
+        const size_t per_row = ((size_t)2 * r2 + 2 * rep + 2) * sizeof(double) +
+                               (size_t)MV_S * (std::min(r2, MV_KMAX) + rep + 64);
         const int chunk = (int)std::max<size_t>(1, std::min<size_t>(r1, workspace_budget() / per_row));
         DevBuf X1c, n1c, Gm, Pm, gm, rowv;
         KFB_TRY(X1c.alloc((size_t)chunk * rep * sizeof(double), s));
@@ -250,41 +333,48 @@ kfb_status matvec_t(const Tin *x1, const Tin *dx1, const Tin *x2, const double *
             gather_f64_kernel<Tin><<<rc, 128, 0, s>>>(x1, didx1.as<int>() + sa + q0, rc, rep,
                                                       X1c.as<double>(), n1c.as<double>());
             KFB_CUDA_TRY(cudaGetLastError());
-            // row-major C (rc x r2) = A (rc x rep) B^T (B r2 x rep): column-major
-            // C^T = B A^T
-            KFB_BLAS_TRY(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, r2, rc, rep, &one,
-                                     X2l.as<double>(), rep, X1c.as<double>(), rep, &zerod,
-                                     Gm.as<double>(), r2));
+            KFB_TRY(X1s.rows_of(X1c.as<double>(), rc, rep, rep, s));
+            // G (rc x r2 row-major) = X1 X2^T, P = X1 Ad^T
+            KFB_TRY(mv_gemm(X2s.sl, X1s.sl, r2, rc, Gm.as<double>(), r2, 1.0, false, err, s));
             if (with_ad)
-                KFB_BLAS_TRY(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, r2, rc, rep, &one,
-                                         Adl.as<double>(), rep, X1c.as<double>(), rep, &zerod,
-                                         Pm.as<double>(), r2));
+                KFB_TRY(mv_gemm(Ads.sl, X1s.sl, r2, rc, Pm.as<double>(), r2, 1.0, false, err, s));
             pair_weights_kernel<<<rc, 256, 0, s>>>(
                 Gm.as<double>(), Pm.as<double>(), r2, n1c.as<double>(), n2l.as<double>(),
                 scl.as<double>(), ael.as<double>(), dmol1.as<int>() + sa + q0, with_ad ? 1 : 0,
                 with_f ? 1 : 0, c, is2, is4, E, with_f ? rowv.as<double>() : nullptr);
             KFB_CUDA_TRY(cudaGetLastError());
             if (!with_f) continue;
-            // g = W Ad + rowsum(V) x1 - V X2: row-major C (rc x rep) = M (rc x r2) B
-            // (B r2 x rep): column-major C^T = B^T M^T
-            if (with_ad)
-                KFB_BLAS_TRY(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, rep, rc, r2, &one,
-                                         Adl.as<double>(), rep, Gm.as<double>(), r2, &zerod,
-                                         gm.as<double>(), rep));
-            else
+            // g = W Ad + rowsum(V) x1 - V X2 (rc x rep row-major), W over G and V over P
+            if (with_ad) {
+                for (int kc = 0; kc < nkc; ++kc) {
+                    const int k0 = kc * MV_KMAX, kn = std::min(MV_KMAX, r2 - k0);
+                    KFB_TRY(Ms.rows_of(Gm.as<double>() + k0, rc, kn, r2, s));
+                    KFB_TRY(mv_gemm(Adt[kc]->sl, Ms.sl, rep, rc, gm.as<double>(), rep, 1.0,
+                                    kc > 0, err, s));
+                }
+            } else {
                 KFB_TRY(zero(gm.ptr, (size_t)rc * rep * sizeof(double), s));
+            }
             add_row_scaled_kernel<<<nblk((long long)rc * rep, 256), 256, 0, s>>>(
                 X1c.as<double>(), rowv.as<double>(), rc, rep, gm.as<double>());
             KFB_CUDA_TRY(cudaGetLastError());
-            KFB_BLAS_TRY(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, rep, rc, r2, &mone,
-                                     X2l.as<double>(), rep, Pm.as<double>(), r2, &one,
-                                     gm.as<double>(), rep));
+            for (int kc = 0; kc < nkc; ++kc) {
+                const int k0 = kc * MV_KMAX, kn = std::min(MV_KMAX, r2 - k0);
+                KFB_TRY(Ms.rows_of(Pm.as<double>() + k0, rc, kn, r2, s));
+                KFB_TRY(mv_gemm(X2t[kc]->sl, Ms.sl, rep, rc, gm.as<double>(), rep, -1.0, true,
+                                err, s));
+            }
             force_contract_kernel<Tin><<<rc, 128, 0, s>>>(
                 dx1, didx1.as<int>() + sa + q0, dmol1.as<int>() + sa + q0, dn1.as<int>(),
                 doff1.as<int>(), s1.ma, rep, gm.as<double>(), F);
             KFB_CUDA_TRY(cudaGetLastError());
         }
     }
+    int herr = 0;
+    KFB_CUDA_TRY(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    KFB_CUDA_TRY(cudaStreamSynchronize(s));
+    if (herr)
+        return set_error(KFB_ERR_TIMEOUT, "contracted prediction: a tensor-core pipeline wait timed out");
     return KFB_OK;
 }
 

@@ -542,6 +542,92 @@ kfb_status oz_slice_cols(const double *src, long long rows, int K, long long ld,
     return KFB_OK;
 }
 
+namespace {
+
+// mx[r] = max over k in this block's chunk of |src[k * ld + r]| (a column-major
+// source read along r), combined across chunks by an atomic max on the bit
+// pattern (non-negative doubles order like their 64-bit integers).
+__global__ void colmajor_absmax_kernel(const double *__restrict__ src, long long rows, int K,
+                                       long long ld, int kchunk,
+                                       unsigned long long *__restrict__ mx) {
+    const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= rows) return;
+    const int k0 = blockIdx.y * kchunk, k1 = min(K, k0 + kchunk);
+    double m = 0.0;
+    for (int k = k0; k < k1; ++k) m = fmax(m, fabs(src[(long long)k * ld + r]));
+    atomicMax(mx + r, (unsigned long long)__double_as_longlong(m));
+}
+
+// Digits of a 32 (rows) x 32 (k) tile of a column-major source: staged in
+// shared memory (read along the rows), written as 4 consecutive k per thread
+// and plane (32-byte row segments).  Columns K .. kp-1 get zero digits.
+template <int S>
+__global__ void __launch_bounds__(256)
+    colmajor_digits_kernel(const double *__restrict__ src, long long rows, int K, long long ld,
+                           int kp, const unsigned long long *__restrict__ mx,
+                           int8_t *__restrict__ d, int *__restrict__ e) {
+    __shared__ double t[32][33];
+    const long long r0 = (long long)blockIdx.x * 32;
+    const int k0 = blockIdx.y * 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int i = warp; i < 32; i += 8) {
+        const int k = k0 + i;
+        const long long r = r0 + lane;
+        t[i][lane] = (k < K && r < rows) ? src[(long long)k * ld + r] : 0.0;
+    }
+    __syncthreads();
+    const int rr = warp * 4 + (lane >> 3), kk = (lane & 7) * 4;
+    const long long r = r0 + rr;
+    if (r >= rows) return;
+    const int ex = oz_row_exponent(__longlong_as_double((long long)mx[r]));
+    if (blockIdx.y == 0 && kk == 0) e[r] = ex;
+    int8_t dg[4][S];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) oz_digits<S>(ldexp(t[kk + c][rr], -ex), dg[c]);
+    const long long plane = rows * (long long)kp;
+#pragma unroll
+    for (int sl = 0; sl < S; ++sl) {
+        const uint32_t wv = (uint32_t)(uint8_t)dg[0][sl] | ((uint32_t)(uint8_t)dg[1][sl] << 8) |
+                            ((uint32_t)(uint8_t)dg[2][sl] << 16) |
+                            ((uint32_t)(uint8_t)dg[3][sl] << 24);
+        *reinterpret_cast<uint32_t *>(d + sl * plane + r * kp + k0 + kk) = wv;
+    }
+}
+
+}  // namespace
+
+kfb_status oz_slice_colmajor(const double *src, long long rows, int K, long long ld,
+                             const OzSlices &o, unsigned long long *scratch_max, cudaStream_t s) {
+    KFB_TRY(oz_check(o, K));
+    if (rows <= 0) return KFB_OK;
+    KFB_TRY(zero(scratch_max, (size_t)rows * sizeof(unsigned long long), s));
+    if (K > 0) {
+        const int kchunk = 256;
+        const dim3 gm((unsigned)((rows + 255) / 256), (unsigned)((K + kchunk - 1) / kchunk));
+        colmajor_absmax_kernel<<<gm, 256, 0, s>>>(src, rows, K, ld, kchunk, scratch_max);
+        KFB_CUDA_TRY(cudaGetLastError());
+    }
+    const dim3 gd((unsigned)((rows + 31) / 32), (unsigned)(o.kp / 32));
+    switch (o.S) {
+#define KFB_OZ_CM(SS)                                                                          \
+    case SS:                                                                                   \
+        colmajor_digits_kernel<SS><<<gd, 256, 0, s>>>(src, rows, K, ld, o.kp, scratch_max,    \
+                                                      o.d, o.e);                               \
+        break;
+        KFB_OZ_CM(2)
+        KFB_OZ_CM(3)
+        KFB_OZ_CM(4)
+        KFB_OZ_CM(5)
+        KFB_OZ_CM(6)
+        KFB_OZ_CM(7)
+#undef KFB_OZ_CM
+        default:
+            return set_error(KFB_ERR_INVALID_ARG, "digit planes S=%d outside 2..%d", o.S, OZ_MAXS);
+    }
+    KFB_CUDA_TRY(cudaGetLastError());
+    return KFB_OK;
+}
+
 int oz_gen_tiles(const OzGen &g, int S) {
     if (g.M <= 0 || g.N <= 0) return 0;
     const int BN = oz_bn(S);

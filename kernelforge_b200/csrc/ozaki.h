@@ -51,6 +51,11 @@ kfb_status oz_slice_rows(const T *src, long long rows, int K, long long ld, cons
 // Slice rows of a column-major source: a[r][k] = src[k * ld + r] (K <= 512).
 kfb_status oz_slice_cols(const double *src, long long rows, int K, long long ld,
                          const OzSlices &out, cudaStream_t s);
+// The same for any K (<= 65536): row maxima in a first pass (scratch_max, one
+// 64-bit word per row), then the digits through shared-memory tiles.
+kfb_status oz_slice_colmajor(const double *src, long long rows, int K, long long ld,
+                             const OzSlices &out, unsigned long long *scratch_max,
+                             cudaStream_t s);
 
 // One output tile: rows a0 .. a0 + m - 1 of A against rows b0 .. b0 + n - 1 of
 // B (m <= OZ_BM, n <= oz_bn(S)).  Output element (i, j) goes to
