@@ -314,14 +314,88 @@ class _FP64Solver:
         if st == _lib.KFB_ERR_NOT_PD:
             raise RuntimeError(f"DPFTRF failed, info={info.value}")
         _lib.check(st)
-        return alpha, self.l2, {}
+        # (K + l2 I) alpha = y, so the fitted values K alpha are y - l2 alpha
+        return alpha, np.asarray(y, np.float64) - self.l2 * alpha.cpu().numpy(), self.l2, {}
+
+
+def _truncated_eigensolve(A, b, rtol, atol, max_rank):
+    """x = sum over kept eigenpairs of v (v . b) / lambda, keeping eigenvalues
+    above max(atol, rtol lambda_max) (the largest max_rank of them, if set)."""
+    import torch
+    lam, V = torch.linalg.eigh(A)
+    lam_max = float(lam[-1])
+    tau = max(float(atol), float(rtol) * lam_max)
+    idx = torch.nonzero(lam > tau).flatten()
+    if max_rank is not None:
+        idx = idx[max(0, idx.numel() - int(max_rank)):]
+    if idx.numel() == 0:
+        raise RuntimeError(f"Truncated eigensolve kept no eigenpairs. lambda_max={lam_max:.3e}, "
+                           f"tau={tau:.3e}.")
+    Vk = V[:, idx]
+    x = Vk @ ((Vk.T @ b) / lam[idx])
+    return x, {"rank": int(idx.numel()), "n": int(A.shape[0]), "lam_min": float(lam[0]),
+               "lam_max": lam_max, "tau": tau, "dropped": int(A.shape[0] - idx.numel())}
+
+
+def _jacobi_cg(A, b, rtol, atol, max_iter, restart=50):
+    """Conjugate gradients with the inverse diagonal as preconditioner; every
+    `restart` steps the residual is recomputed from x and the direction reset."""
+    import torch
+    d = A.diagonal()
+    minv = torch.where(d > torch.finfo(A.dtype).eps, 1.0 / d, torch.ones_like(d))
+    x = torch.zeros_like(b)
+    r = b.clone()
+    tol = max(float(atol), float(rtol) * float(torch.linalg.vector_norm(b)))
+    limit = 10 * A.shape[0] if max_iter is None else int(max_iter)
+    res = float(torch.linalg.vector_norm(r))
+    it = 0
+    z = minv * r
+    p = z.clone()
+    rz = torch.dot(r, z)
+    while res > tol:
+        if it >= limit:
+            raise RuntimeError(f"CG did not converge within the iteration budget. "
+                               f"residual={res:.3e}, tol={tol:.3e}, max_iter={limit}.")
+        it += 1
+        Ap = A @ p
+        curv = float(torch.dot(p, Ap))
+        if not (curv > 0.0) or not np.isfinite(curv):
+            raise RuntimeError(f"CG breakdown: non-positive search-direction curvature at "
+                               f"iteration {it} (p^T K p={curv:.3e}).")
+        step = rz / curv
+        x = x + step * p
+        r = b - A @ x if it % restart == 0 else r - step * Ap
+        res = float(torch.linalg.vector_norm(r))
+        z = minv * r
+        rz_new = torch.dot(r, z)
+        p = z.clone() if it % restart == 0 else z + (rz_new / rz) * p
+        rz = rz_new
+    return x, {"iterations": it, "max_iter": limit, "residual_norm": res, "tol": tol,
+               "n": int(A.shape[0]), "restart_period": restart}
 
 
 class _MixedSolver(_FP64Solver):
     """Energy and energy+force kernel matrices on the tensor cores (split fp16,
-    FP32 RFP) and the mixed solve (FP32-class factor, FP64 refinement; lambda
-    raised, and reported, when the FP32-stored matrix is indefinite at l2).
-    Force-only matrices stay on the FP64 path."""
+    FP32 RFP).  ``method``:
+      "cholesky"  the mixed solve (FP32-class factor, FP64 refinement; lambda
+                  raised, and reported, when the FP32-stored matrix is
+                  indefinite at l2);
+      "eigh"      a truncated eigensolve of K + l2 I (models/cuda_local_krr.py:176-211);
+      "cg"        Jacobi-preconditioned conjugate gradients (:214-290);
+    the last two in FP64 on the dense matrix, with ``scaling`` "diagonal_scale"
+    solving D (K + l2 I) D z = D y, alpha = D z, D = diag(K + l2 I)^(-1/2)
+    (:293-315), or "none".  Force-only matrices stay on the FP64 path."""
+
+    def __init__(self, sigma, l2, method="cholesky", scaling="diagonal_scale",
+                 spectral=(3e-6, 0.0, None), cg=(2e-2, 0.0, None)):
+        super().__init__(sigma, l2)
+        if method not in ("cholesky", "eigh", "cg"):
+            raise ValueError(f"Unsupported solver '{method}'. Expected 'cholesky', 'eigh', "
+                             f"or 'cg'.")
+        if scaling not in ("none", "diagonal_scale"):
+            raise ValueError(f"Unsupported preprocessing '{scaling}'. Expected 'none' or "
+                             f"'diagonal_scale'.")
+        self.method, self.scaling, self.spectral, self.cg = method, scaling, spectral, cg
 
     def solve(self, ds: _DeviceSet, mode, y):
         import torch
@@ -335,9 +409,34 @@ class _MixedSolver(_FP64Solver):
             K = clk.kernel_gaussian_symm_rfp(ds.X, ds.Q, ds.N, self.sigma)
         else:
             K = clk.kernel_gaussian_full_symm_rfp(ds.X, ds.dX, ds.Q, ds.N, self.sigma)
-        alpha, info = cgk.krr_solve_mixed(K, torch.as_tensor(y, dtype=torch.float64).to("cuda"),
-                                          l2=self.l2, uplo="L", lambda_floor=True)
-        return alpha, float(info.get("lambda_eff", self.l2)), info
+        yd = torch.as_tensor(y, dtype=torch.float64).to("cuda")
+        if self.method == "cholesky":
+            alpha, info = cgk.krr_solve_mixed(K, yd, l2=self.l2, uplo="L", lambda_floor=True)
+            lam = float(info.get("lambda_eff", self.l2))
+            return alpha, np.asarray(y, np.float64) - lam * alpha.cpu().numpy(), lam, info
+        n = yd.numel()
+        dense = torch.empty((n, n), dtype=torch.float32, device="cuda")
+        _lib.check(_lib.lib().kfb_rfp_to_full(K.data_ptr(), n, _lib.KFB_RFP_L, _lib.KFB_F32,
+                                              dense.data_ptr(), stream_handle()))
+        del K
+        Kd = dense.double()
+        del dense
+        A = Kd.clone()
+        A.diagonal().add_(float(self.l2))
+        dsc = None
+        b = yd
+        if self.scaling == "diagonal_scale":
+            dsc = torch.rsqrt(torch.clamp(A.diagonal(), min=torch.finfo(A.dtype).eps))
+            A.mul_(dsc[:, None]).mul_(dsc[None, :])
+            b = dsc * yd
+        if self.method == "eigh":
+            z, info = _truncated_eigensolve(A, b, *self.spectral)
+        else:
+            z, info = _jacobi_cg(A, b, *self.cg)
+        del A
+        alpha = z if dsc is None else dsc * z
+        info = dict(info, solver=self.method, preprocessing=self.scaling)
+        return alpha, (Kd @ alpha).cpu().numpy(), float(self.l2), info
 
 
 # --------------------------------------------------------------------------
@@ -365,11 +464,10 @@ class BaseModel:
         self._train = _DeviceSet.compute(mols, self.elements, self.repr_params, self._dtype)
         self._n_train = len(mols)
         y = labels.target()
-        alpha, l2_eff, info = self._solver().solve(self._train, labels.mode, y)
-        self._set_coefficients(alpha, y, l2_eff, info)
+        alpha, y_fit, l2_eff, info = self._solver().solve(self._train, labels.mode, y)
+        self._set_coefficients(alpha, y, y_fit, l2_eff, info)
         self.train_score_ = {k: ModelScore.of(ref, pred) for k, (ref, pred) in
-                             _Labels.pairs(self.training_mode_, y,
-                                           y - l2_eff * self._alpha_host(),
+                             _Labels.pairs(self.training_mode_, y, y_fit,
                                            self._n_train).items()}
         self.is_fitted_ = True
         return self
@@ -415,10 +513,11 @@ class BaseModel:
         return model
 
     # ---- shared internals ---------------------------------------------------
-    def _set_coefficients(self, alpha, y, l2_eff, info):
+    def _set_coefficients(self, alpha, y, y_fit, l2_eff, info):
         """Keep the coefficients (device FP64) and J^T alpha_F of the force rows."""
         self._alpha = alpha
         self._y_train = np.asarray(y, np.float64)
+        self._y_fit = np.asarray(y_fit, np.float64)
         self._l2_eff = l2_eff
         self.solve_info_ = info
         nm = self._n_train
@@ -492,6 +591,7 @@ class LocalKRRModel(BaseModel):
         self._n_train = len(self._train.N)
         self._alpha = torch.as_tensor(d["alpha"], dtype=torch.float64).to("cuda")
         self._y_train = d.get("y_train", np.zeros(0))
+        self._y_fit = self._y_train - self.l2 * d["alpha"] if self._y_train.size else self._y_train
         self._l2_eff = self.l2
         ad = d.get("alpha_desc")
         self._adesc = None if ad is None else torch.as_tensor(ad, dtype=torch.float64).to("cuda")
@@ -503,19 +603,19 @@ class LocalKRRModel(BaseModel):
 
 class CudaLocalKRRModel(BaseModel):
     """FCHL19 local KRR with the kernel matrix on the tensor cores (split fp16,
-    FP32 RFP) and the FP32-factor / FP64-refinement solve; descriptors float32
-    on the device.  ``solver``, ``preprocessing`` and the spectral / CG settings
-    are validated and saved; every solver name runs the mixed Cholesky solve.
-    force_only training runs the FP64 path.  Energy-only models predict zero
-    forces, as the reference's CUDA model does."""
+    FP32 RFP); descriptors float32 on the device.  ``solver``: "eigh" (the
+    reference's default: truncated eigensolve), "cg" (Jacobi-preconditioned
+    CG) or "cholesky" (the FP32-factor / FP64-refinement solve, the fast one),
+    with ``preprocessing`` "diagonal_scale" or "none"; unknown names raise
+    ValueError when fit runs, as in the reference.  force_only training runs
+    the FP64 path.  Energy-only models predict zero forces, as the reference's
+    CUDA model does."""
 
     _dtype = "float32"
 
     def __init__(self, sigma=2.0, l2=1e-4, elements=None, repr_params=None, solver="eigh",
                  preprocessing="diagonal_scale", spectral_rtol=3e-6, spectral_atol=0.0,
                  spectral_max_rank=None, cg_rtol=2e-2, cg_atol=0.0, cg_max_iter=None):
-        if solver not in ("cholesky", "eigh", "cg"):
-            raise ValueError("solver must be 'cholesky', 'eigh' or 'cg'")
         self.sigma, self.l2 = sigma, l2
         self.elements = sorted(elements) if elements is not None else list(_DEFAULT_ELEMENTS)
         self.repr_params = repr_params if repr_params is not None else {}
@@ -526,7 +626,9 @@ class CudaLocalKRRModel(BaseModel):
         self.is_fitted_ = False
 
     def _solver(self):
-        return _MixedSolver(self.sigma, self.l2)
+        return _MixedSolver(self.sigma, self.l2, self.solver, self.preprocessing,
+                            (self.spectral_rtol, self.spectral_atol, self.spectral_max_rank),
+                            (self.cg_rtol, self.cg_atol, self.cg_max_iter))
 
     def _forward(self, query):
         E, F = super()._forward(query)
@@ -552,7 +654,7 @@ class CudaLocalKRRModel(BaseModel):
                "max_atoms": int(self._train.X.shape[1]), "rep_size": int(self._train.X.shape[2]),
                "naq_train": self._train.naq, "baseline_elements": self.baseline_elements_,
                "element_energies": self.element_energies_, "alpha": alpha,
-               "y_train": self._y_train, "y_pred_train": self._y_train - self._l2_eff * alpha,
+               "y_train": self._y_train, "y_pred_train": self._y_fit,
                "X_train": self._train.host("X").astype(np.float32),
                "dX_train": self._train.host("dX").astype(np.float32),
                "Q_train": self._train.Q, "N_train": self._train.N,
@@ -583,6 +685,7 @@ class CudaLocalKRRModel(BaseModel):
         self._n_train = int(d["n_train"])
         self._alpha = torch.as_tensor(d["alpha"], dtype=torch.float64).to("cuda")
         self._y_train = d.get("y_train", np.zeros(0)).astype(np.float64)
+        self._y_fit = d.get("y_pred_train", self._y_train - self.l2 * d["alpha"])
         self._l2_eff = self.l2
         # J^T alpha_F in FP64 from the stored Jacobians and the FP64 coefficients
         # (the file's alpha_desc_F is a float32 copy)
