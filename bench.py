@@ -59,11 +59,13 @@ def parse():
                     help="skip the FP64-GPU fit and the accuracy check (profiling runs)")
     ap.add_argument("--workload", default="fit10k",
                     choices=["fit10k", "config1", "config3", "config4", "config5",
-                             "cosmlp_step", "repr", "rff_force"],
+                             "cosmlp_step", "repr", "rff_force", "cholesky"],
                     help="fit10k (default): the 10,000-molecule kernel + solve; config1: FP64 "
                          "1,000-molecule fit+predict; config3: Jacobian kernel 1,000 x 1,000 "
                          "molecules; config4: energy+force kernel of 300 x 21-atom molecules "
                          "+ solve; config5: learned feature map vs RFF vs exact KRR")
+    ap.add_argument("--chol-n", type=int, default=10000,
+                    help="cholesky: order of the SPD test matrix")
     ap.add_argument("--c4-nmol", type=int, default=300,
                     help="config4 training molecules (smaller values: profiling cases)")
     ap.add_argument("--c3-nmol", type=int, default=1000,
@@ -1271,12 +1273,71 @@ def run_rff_force(args):
                         "traffic": None, "kernel": "force features (3 fp16 products)"}})
 
 
+def run_cholesky(args):
+    """The RFP Cholesky factorisation alone (rfp_potrf) of an SPD matrix of
+    order --chol-n (G G^T / n + 0.1 I, G Gaussian): FP32-class (FP32 RFP input,
+    4 digit planes) and FP64-class (FP64 input, 7 planes).  The rate is the
+    logical n^3 / 3 FLOP per factorisation over the event-timed duration; the
+    tensor-core bound of an S-plane product is S (S + 1) / 2 int8 MMAs per
+    logical one at twice the measured bf16 rate."""
+    import torch
+
+    from kernelforge_b200 import _lib
+    from kernelforge_b200 import cuda_global_kernels as cgk
+    n = args.chol_n
+    g = torch.Generator(device="cuda").manual_seed(SEED)
+    G = torch.randn(n, n, device="cuda", dtype=torch.float64, generator=g) / n ** 0.5
+    A = G @ G.T + 0.1 * torch.eye(n, device="cuda", dtype=torch.float64)
+    del G
+    peaks, peak_kind = load_peaks()
+    bf16 = peaks.get("bf16_tflops")
+    flops = n ** 3 / 3.0
+    out = {}
+    s = torch.cuda.current_stream().cuda_stream
+    for name, dt, tdt, planes in (("fp32_class", _lib.KFB_F32, torch.float32, 4),
+                                  ("fp64_class", _lib.KFB_F64, torch.float64, 7)):
+        Ad = A.to(tdt).contiguous()
+        arf0 = torch.empty(n * (n + 1) // 2, device="cuda", dtype=tdt)
+        _lib.check(_lib.lib().kfb_full_to_rfp(Ad.data_ptr(), n, _lib.KFB_RFP_L, dt,
+                                              arf0.data_ptr(), s))
+        del Ad
+        arf = arf0.clone()
+
+        def step():
+            arf.copy_(arf0)
+            return cgk.rfp_potrf(arf, n, 0.0, "L")
+
+        copy_ms = _events_ms(lambda: arf.copy_(arf0), args.steps, max(args.warmup, 3))
+        ms = _events_ms(step, args.steps, max(args.warmup, 3)) - copy_ms
+        # |L L^T - A| on a sample of rows, relative to max |A|
+        Lf = torch.empty(n, n, device="cuda", dtype=tdt)
+        _lib.check(_lib.lib().kfb_rfp_to_full(arf.data_ptr(), n, _lib.KFB_RFP_L, dt,
+                                              Lf.data_ptr(), s))
+        L = torch.tril(Lf.double())
+        idx = torch.arange(0, n, max(1, n // 256), device="cuda")
+        err = ((L[idx] @ L.T - A[idx]).abs().max() / A.abs().max()).item()
+        achieved = flops / (ms * 1e-3) / 1e12
+        bound = 2.0 * bf16 / (planes * (planes + 1) / 2) if bf16 else None
+        out[name] = {"ms": ms, "digit_planes": planes, "logical_tflops": achieved,
+                     "tensor_bound_tflops": bound,
+                     "frac": achieved / bound if bound else None,
+                     "max_rel_residual_rows": err}
+        del arf, arf0, Lf, L
+        torch.cuda.empty_cache()
+    _line("RFP Cholesky factorisation: logical TFLOP/s (n^3/3)", out["fp32_class"]["logical_tflops"],
+          "TFLOP/s", out["fp32_class"]["ms"], args,
+          f"rfp_potrf of an SPD matrix of order {n}: FP64 diagonal blocks and panels, "
+          "int8 tensor-core trailing updates (digit planes)", "int8 digit planes / f32 / f64",
+          {"factor": out, "peak_kind": f"{peak_kind} bf16 x2 (int8) / MMAs per product"})
+
+
 def main():
     args = parse()
     if args.workload != "fit10k":
         {"config1": run_config1, "config3": run_config3, "config4": run_config4,
          "config5": run_config5, "cosmlp_step": run_cosmlp_step,
-         "repr": run_repr, "rff_force": run_rff_force}[args.workload](args)
+         "repr": run_repr, "rff_force": run_rff_force,
+         "cholesky": run_cholesky}[args.workload](args)
         return
     rank, world, local = dist_setup(args.gpus)
     try:
