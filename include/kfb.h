@@ -46,7 +46,7 @@ typedef enum kfb_status {
     KFB_ERR_INVALID_ARG = 1,    /* reference: std::invalid_argument -> ValueError */
     KFB_ERR_NOT_PD = 2,         /* Cholesky info > 0 (leading minor not positive) */
     KFB_ERR_ALLOC = 3,          /* device allocation failed */
-    KFB_ERR_CUDA = 4,           /* CUDA / cuBLAS / cuSOLVER error */
+    KFB_ERR_CUDA = 4,           /* CUDA / cuBLAS error */
     KFB_ERR_TIMEOUT = 5,        /* a bounded device-side wait gave up */
     KFB_ERR_NO_CONVERGENCE = 6, /* iterative refinement missed its tolerance */
     KFB_ERR_UNSUPPORTED = 7     /* device or configuration not supported */

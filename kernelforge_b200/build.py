@@ -2,7 +2,7 @@
 
 Every translation unit is compiled by nvcc for sm_100a only
 (-gencode arch=compute_100a,code=sm_100a) and linked against the CUDA runtime,
-cuBLAS and cuSOLVER of the CUDA toolkit.  The result is
+cuBLAS of the CUDA toolkit.  The result is
 kernelforge_b200/libkfb.so; it is loaded with ctypes by kernelforge_b200._lib.
 
 Usage: python -m kernelforge_b200.build [--force] [-v]

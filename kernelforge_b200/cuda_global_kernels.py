@@ -62,19 +62,22 @@ def rfp_potrs(L_rfp, B, uplo="L"):
 
 def krr_solve_mixed(K_rfp, y, l2=0.0, uplo="L", tol=1e-10, maxit=500, *, lambda_floor=False,
                     factor="fp64"):
-    """(K + l2 I) alpha = y with an FP32 RFP kernel matrix (not modified): FP32
-    Cholesky factor (dominant eigenpair deflated), FP64 conjugate-gradient
+    """(K + l2 I) alpha = y with an FP32 RFP kernel matrix (not modified): a
+    Cholesky factor as preconditioner (an FP32-class one with the dominant
+    eigenpair deflated, or an FP64-class one), FP64 conjugate-gradient
     refinement of residuals against K.  Returns (alpha float64, info dict).
 
     Raises RuntimeError if K + l2 I is indefinite at FP32 storage precision;
     with ``lambda_floor=True`` l2 is raised in x10 steps until it is not, and
     info["lambda_eff"] reports the value used.
 
-    ``factor``: precision of the Cholesky factor behind the refinement.  On
-    B200 cuSOLVER's FP64 Cholesky runs as fast as the FP32 one (FP64 tensor
-    cores), and an FP64 factor leaves one or two refinement steps instead of
-    about ten latency-bound FP32 triangular-solve pairs, so "fp64" (default) is
-    the faster choice here; "fp32" keeps the factor in FP32 as well."""
+    ``factor``: precision of the Cholesky factor behind the refinement, both
+    this library's tensor-core factorisation (FP64 diagonal blocks and panels,
+    int8 digit-plane trailing updates): "fp64" (default) an FP64-class factor
+    (7 digit planes), one or two refinement steps; "fp32" an FP32-class factor
+    (4 planes, FP32 diagonal blocks), about six steps.  At n = 10,000 the
+    whole solve takes 22.9 ms and 25.5 ms respectively on one B200.
+    """
     require_cuda()
     import torch
     if K_rfp.dtype != torch.float32 or not K_rfp.is_cuda or not K_rfp.is_contiguous():
