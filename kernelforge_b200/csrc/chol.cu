@@ -18,8 +18,12 @@
 //   3. inner update       the outer panel's remaining columns (all rows below
 //                         them) -= L_21 L_21^T, K = 128 (tensor cores);
 // then, once per outer panel, the panel is sliced again (one row scale over
-// its 512 columns) and everything right of it is updated in one tensor-core
-// product with K = 512 on the lower triangle only.  The FP64 read-modify-write
+// its 512 columns) and everything right of it is updated by tensor-core
+// products with K = 512 on the lower triangle only: the next outer panel's
+// columns on a high-priority stream, the rest on a low-priority stream with one
+// CTA per tile, so that the next panel's diagonal blocks, panels and inner
+// updates run while that bulk update proceeds (look-ahead; the digit planes of
+// consecutive outer panels alternate between two buffers).  The FP64 read-modify-write
 // of the trailing matrix, the memory cost of a right-looking factorisation,
 // thereby happens once per 512 columns instead of once per 128.
 // The block order is that of LAPACK's right-looking dpotrf with the panel's
@@ -120,11 +124,21 @@ __global__ void __launch_bounds__(BLK_THREADS, 1)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const double *blk = A + (long long)c0 * ld + c0;
     if constexpr (sizeof(F) == 8) {
+        if (w == NB && (ld & 1) == 0 && (c0 & 1) == 0) {
+            // a full block, 16-byte aligned rows: pairs of rows per copy (the
+            // strict upper triangle comes along and is never read)
 #pragma unroll 4
-        for (int idx = tid; idx < NB * NB; idx += BLK_THREADS) {
-            const int k = idx / NB, r = idx - k * NB;
-            const bool v = r < w && k < w && r >= k;
-            cp_async(T + k * LDT + r, v ? blk + (long long)k * ld + r : blk, 8, v);
+            for (int idx = tid; idx < NB * NB / 2; idx += BLK_THREADS) {
+                const int k = idx / (NB / 2), r = 2 * (idx - k * (NB / 2));
+                cp_async(T + k * LDT + r, blk + (long long)k * ld + r, 16, true);
+            }
+        } else {
+#pragma unroll 4
+            for (int idx = tid; idx < NB * NB; idx += BLK_THREADS) {
+                const int k = idx / NB, r = idx - k * NB;
+                const bool v = r < w && k < w && r >= k;
+                cp_async(T + k * LDT + r, v ? blk + (long long)k * ld + r : blk, 8, v);
+            }
         }
         cp_async_wait_all();
     } else {
@@ -200,19 +214,23 @@ __global__ void __launch_bounds__(BLK_THREADS, 1)
         __syncthreads();
         if (*flag) return;   // block-uniform after the barrier
         if (warp == 0) {
-            // (b) W_pp = L_pp^{-1}, lane = column l, rows by forward substitution:
-            // W[r][l] = (delta_rl - sum_{k < r} L[r][k] W[k][l]) / L[r][r]
-            F x[SB];
+            // (b) W_pp = L_pp^{-1}, lane = column l, forward substitution in
+            // right-looking order: W[r][l] = s[r] / L[r][r], then
+            // s[r'] -= L[r'][r] W[r][l] for r' > r (column r of L read as a
+            // broadcast), so each row adds one FMA and one multiply to the
+            // dependent chain instead of a dot product
+            F sacc[SB];
 #pragma unroll
-            for (int r = 0; r < SB; ++r) {
-                F s = (r == lane) ? F(1) : F(0);
-#pragma unroll
-                for (int k = 0; k < r; ++k) s = fma(-T[(o + k) * LDT + o + r], x[k], s);
-                x[r] = (r < wp && lane < wp) ? s * rd[r] : F(0);
-            }
+            for (int r = 0; r < SB; ++r) sacc[r] = (r == lane) ? F(1) : F(0);
             F *Wp = WB + wblk(p, p) * SB * LDW + lane * LDW;
 #pragma unroll
-            for (int r = 0; r < SB; ++r) Wp[r] = x[r];
+            for (int r = 0; r < SB; ++r) {
+                const F xr = (r < wp && lane < wp) ? sacc[r] * rd[r] : F(0);
+                Wp[r] = xr;
+#pragma unroll
+                for (int r2 = r + 1; r2 < SB; ++r2)
+                    sacc[r2] = fma(-T[(o + r) * LDT + o + r2], xr, sacc[r2]);
+            }
         }
         __syncthreads();
         const int rb = o + wp, mr = w - rb;
@@ -325,12 +343,18 @@ __global__ void __launch_bounds__(BLK_THREADS, 1)
         const int k = idx / NB, r = idx - k * NB;
         if (r < w && r >= k) ablk[(long long)k * ld + r] = (double)T[k * LDT + r];
     }
-    for (int idx = tid; idx < NB * NB; idx += BLK_THREADS) {
-        const int c = idx / NB, r = idx - c * NB;
-        double v = 0.0;
-        if (r < w && c < w && r >= c)
-            v = (double)WB[wblk(r / SB, c / SB) * SB * LDW + (c % SB) * LDW + (r % SB)];
-        Wout[idx] = v;
+    // W column-major, two rows per 16-byte store
+    for (int idx = tid; idx < NB * NB / 2; idx += BLK_THREADS) {
+        const int c = idx / (NB / 2), r = 2 * (idx - c * (NB / 2));
+        double v[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int rr = r + u;
+            v[u] = (rr < w && c < w && rr >= c)
+                       ? (double)WB[wblk(rr / SB, c / SB) * SB * LDW + (c % SB) * LDW + (rr % SB)]
+                       : 0.0;
+        }
+        reinterpret_cast<double2 *>(Wout)[idx] = make_double2(v[0], v[1]);
     }
 }
 
@@ -455,6 +479,46 @@ kfb_status panel(int S, double *A, long long ld, int c0, int r0, int m, const do
 
 }  // namespace
 
+namespace {
+
+// The two streams of the look-ahead, per device: the critical path (diagonal
+// blocks, panels, the updates the next panel waits for) at the highest
+// priority, the bulk trailing updates at the lowest.
+struct CholStreams {
+    cudaStream_t crit = nullptr, bulk = nullptr;
+};
+
+kfb_status chol_streams(CholStreams *&out) {
+    static CholStreams per_dev[16];
+    int dev = 0;
+    KFB_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 16) return set_error(KFB_ERR_UNSUPPORTED, "device index %d", dev);
+    CholStreams &cs = per_dev[dev];
+    if (!cs.crit) {
+        int least = 0, greatest = 0;
+        KFB_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        KFB_CUDA_TRY(cudaStreamCreateWithPriority(&cs.crit, cudaStreamNonBlocking, greatest));
+        KFB_CUDA_TRY(cudaStreamCreateWithPriority(&cs.bulk, cudaStreamNonBlocking, least));
+    }
+    out = &cs;
+    return KFB_OK;
+}
+
+// Events of one factorisation, destroyed with it.
+struct CholEvents {
+    cudaEvent_t ev[6] = {};
+    kfb_status init() {
+        for (auto &e : ev) KFB_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        return KFB_OK;
+    }
+    ~CholEvents() {
+        for (auto &e : ev)
+            if (e) cudaEventDestroy(e);
+    }
+};
+
+}  // namespace
+
 kfb_status chol_dense(double *A, int n, long long ld, int slices, int *info, cudaStream_t s) {
     *info = 0;
     if (n <= 0) return KFB_OK;
@@ -473,19 +537,46 @@ kfb_status chol_dense(double *A, int n, long long ld, int slices, int *info, cud
     }
     // the diagonal blocks in FP32 for an FP32-class factor (4 or fewer planes)
     const bool f32blk = slices <= 4;
+    CholStreams *cs = nullptr;
+    KFB_TRY(chol_streams(cs));
+    const cudaStream_t sc = cs->crit, sb = cs->bulk;
+    CholEvents E;
+    KFB_TRY(E.init());
+    cudaEvent_t ev_start = E.ev[0], ev_slice = E.ev[1], ev_bulk = E.ev[2], ev_crit_end = E.ev[3],
+                ev_bulk_end = E.ev[4];
+    // everything below is ordered after the caller's work on s
+    KFB_CUDA_TRY(cudaEventRecord(ev_start, s));
+    KFB_CUDA_TRY(cudaStreamWaitEvent(sc, ev_start, 0));
+    KFB_CUDA_TRY(cudaStreamWaitEvent(sb, ev_start, 0));
     // flags: [0] info, [1] skip, [2] GEMM pipeline error
-    DevBuf flags, Wd, psl, pex, osl, oex;
-    KFB_TRY(flags.alloc(4 * sizeof(int), s));
-    KFB_TRY(zero(flags.ptr, 4 * sizeof(int), s));
+    DevBuf flags, Wd, psl, pex, osl[2], oex[2];
+    KFB_TRY(flags.alloc(4 * sizeof(int), sc));
+    KFB_TRY(zero(flags.ptr, 4 * sizeof(int), sc));
     int *d_info = flags.as<int>(), *d_skip = d_info + 1, *d_err = d_info + 2;
     const long long mmax = std::max(n - NB, 1);
-    KFB_TRY(Wd.alloc((size_t)NB * NB * sizeof(double), s));
-    KFB_TRY(psl.alloc((size_t)slices * mmax * NB, s));
-    KFB_TRY(pex.alloc((size_t)mmax * sizeof(int), s));
-    if (n > NB2) {
-        KFB_TRY(osl.alloc((size_t)slices * (n - NB2) * NB2, s));
-        KFB_TRY(oex.alloc((size_t)(n - NB2) * sizeof(int), s));
-    }
+    KFB_TRY(Wd.alloc((size_t)NB * NB * sizeof(double), sc));
+    KFB_TRY(psl.alloc((size_t)slices * mmax * NB, sc));
+    KFB_TRY(pex.alloc((size_t)mmax * sizeof(int), sc));
+    if (n > NB2)
+        for (int b = 0; b < 2; ++b) {
+            KFB_TRY(osl[b].alloc((size_t)slices * (n - NB2) * NB2, sc));
+            KFB_TRY(oex[b].alloc((size_t)(n - NB2) * sizeof(int), sc));
+        }
+    // on an early (error) return, let both streams finish before the buffers
+    // above are released (destroyed after this guard)
+    struct Drain {
+        cudaStream_t a, b;
+        bool armed = true;
+        ~Drain() {
+            if (armed) {
+                cudaStreamSynchronize(a);
+                cudaStreamSynchronize(b);
+            }
+        }
+    } drain{sc, sb};
+    // the bulk stream's first work reads buffers allocated on the critical one
+    KFB_CUDA_TRY(cudaEventRecord(ev_slice, sc));
+    KFB_CUDA_TRY(cudaStreamWaitEvent(sb, ev_slice, 0));
     OzEpi epi;
     epi.c = A;
     epi.ldr = 1;
@@ -493,62 +584,92 @@ kfb_status chol_dense(double *A, int n, long long ld, int slices, int *info, cud
     epi.skip = d_skip;
     epi.mode = OZ_ADD;
     epi.alpha = -1.0;
-    for (int o0 = 0; o0 < n; o0 += NB2) {
+    OzEpi epi_bulk = epi;
+    epi_bulk.one_tile_per_cta = 1;
+    bool bulk_pending = false;   // a bulk update was enqueued and not waited for
+    for (int o0 = 0, P = 0; o0 < n; o0 += NB2, ++P) {
         const int ow = std::min(NB2, n - o0);   // outer panel: columns o0 .. o0 + ow - 1
         for (int c0 = o0; c0 < o0 + ow; c0 += NB) {
             const int w = std::min(NB, n - c0);
             const int r0 = c0 + w, m = n - r0;
             if (f32blk)
-                chol_block_kernel<float><<<1, BLK_THREADS, blk_smem<float>(), s>>>(
+                chol_block_kernel<float><<<1, BLK_THREADS, blk_smem<float>(), sc>>>(
                     A, ld, c0, w, Wd.as<double>(), d_info, d_skip);
             else
-                chol_block_kernel<double><<<1, BLK_THREADS, blk_smem<double>(), s>>>(
+                chol_block_kernel<double><<<1, BLK_THREADS, blk_smem<double>(), sc>>>(
                     A, ld, c0, w, Wd.as<double>(), d_info, d_skip);
             KFB_CUDA_TRY(cudaGetLastError());
             if (m == 0) break;
             // L21 = A21 W^T and its digit planes
             KFB_TRY(panel(slices, A, ld, c0, r0, m, Wd.as<double>(), psl.as<int8_t>(),
-                          pex.as<int>(), d_skip, s));
+                          pex.as<int>(), d_skip, sc));
             // the rest of the outer panel: columns r0 .. o0 + ow - 1, every row
             // below them, -= L21 L21^T (a lower trapezoid)
             const int nin = o0 + ow - r0;
             if (nin > 0) {
-                OzSlices P;
-                P.d = psl.as<int8_t>();
-                P.e = pex.as<int>();
-                P.S = slices;
-                P.rows = m;
-                P.kp = NB;
+                OzSlices Pl;
+                Pl.d = psl.as<int8_t>();
+                Pl.e = pex.as<int>();
+                Pl.S = slices;
+                Pl.rows = m;
+                Pl.kp = NB;
                 OzGen g;
                 g.mode = OZ_GEN_LOWER;
                 g.M = m;
                 g.N = nin;
                 g.c_off = (long long)r0 * ld + r0;
-                KFB_TRY(oz_gemm_gen(P, P, g, epi, d_err, s));
+                KFB_TRY(oz_gemm_gen(Pl, Pl, g, epi, d_err, sc));
             }
         }
-        // everything right of the outer panel: A22 -= L_panel L_panel^T with
-        // K = ow (the panel sliced once more, a row scale over all its columns)
+        // everything right of the outer panel -= L_panel L_panel^T (K = ow, the
+        // panel sliced once more with one row scale over its columns), in two
+        // parts: the next outer panel's columns on the critical stream (the
+        // next panel's blocks wait for them), the rest on the bulk stream,
+        // where it overlaps the next panel's blocks, panels and inner updates
         const int R = o0 + ow, M = n - R;
-        if (M > 0) {
-            OzSlices O;
-            O.d = osl.as<int8_t>();
-            O.e = oex.as<int>();
-            O.S = slices;
-            O.rows = M;
-            O.kp = oz_kp(ow);
-            KFB_TRY(oz_slice_cols(A + (long long)o0 * ld + R, M, ow, ld, O, s));
-            OzGen g;
-            g.mode = OZ_GEN_LOWER;
-            g.M = M;
-            g.N = M;
-            g.c_off = (long long)R * ld + R;
-            KFB_TRY(oz_gemm_gen(O, O, g, epi, d_err, s));
+        if (M <= 0) continue;
+        OzSlices O;
+        O.d = osl[P & 1].as<int8_t>();
+        O.e = oex[P & 1].as<int>();
+        O.S = slices;
+        O.rows = M;
+        O.kp = oz_kp(ow);
+        KFB_TRY(oz_slice_cols(A + (long long)o0 * ld + R, M, ow, ld, O, sc));
+        KFB_CUDA_TRY(cudaEventRecord(ev_slice, sc));
+        // the previous bulk update wrote these columns too: wait for it
+        if (bulk_pending) KFB_CUDA_TRY(cudaStreamWaitEvent(sc, ev_bulk, 0));
+        const int na = std::min(NB2, M);
+        OzGen ga;
+        ga.mode = OZ_GEN_LOWER;
+        ga.M = M;
+        ga.N = na;
+        ga.c_off = (long long)R * ld + R;
+        KFB_TRY(oz_gemm_gen(O, O, ga, epi, d_err, sc));
+        if (M > na) {
+            KFB_CUDA_TRY(cudaStreamWaitEvent(sb, ev_slice, 0));
+            OzGen gb;
+            gb.mode = OZ_GEN_LOWER;
+            gb.M = M - na;
+            gb.N = M - na;
+            gb.a_base = na;
+            gb.b_base = na;
+            gb.c_off = (long long)(R + na) * ld + (R + na);
+            KFB_TRY(oz_gemm_gen(O, O, gb, epi_bulk, d_err, sb));
+            KFB_CUDA_TRY(cudaEventRecord(ev_bulk, sb));
+            bulk_pending = true;
+        } else {
+            bulk_pending = false;
         }
     }
+    // join both streams back into the caller's
+    KFB_CUDA_TRY(cudaEventRecord(ev_crit_end, sc));
+    KFB_CUDA_TRY(cudaEventRecord(ev_bulk_end, sb));
+    KFB_CUDA_TRY(cudaStreamWaitEvent(s, ev_crit_end, 0));
+    KFB_CUDA_TRY(cudaStreamWaitEvent(s, ev_bulk_end, 0));
     int h[3] = {0, 0, 0};
     KFB_CUDA_TRY(cudaMemcpyAsync(h, d_info, 3 * sizeof(int), cudaMemcpyDeviceToHost, s));
     KFB_CUDA_TRY(cudaStreamSynchronize(s));
+    drain.armed = false;   // both streams joined into s, which is idle now
     if (h[2]) return set_error(KFB_ERR_TIMEOUT, "Cholesky: a tensor-core pipeline wait timed out");
     *info = h[0];
     return KFB_OK;

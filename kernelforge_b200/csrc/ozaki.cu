@@ -460,7 +460,7 @@ kfb_status launch(const OzSlices &A, const OzSlices &B, const OzTile *tiles, con
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
         attr[S] = true;
     }
-    const int grid = std::min(ntiles, device_sm_count());
+    const int grid = epi.one_tile_per_cta ? ntiles : std::min(ntiles, device_sm_count());
     oz_gemm_kernel<S><<<grid, NUM_THREADS, C::SMEM, s>>>(ta, tb, A.rows, B.rows, A.kp, A.e, B.e,
                                                          tiles, gen, ntiles, epi, err);
     KFB_CUDA_TRY(cudaGetLastError());

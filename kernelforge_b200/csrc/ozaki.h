@@ -76,6 +76,10 @@ struct OzEpi {
     int mode = OZ_STORE;
     double alpha = 1.0;
     const int *skip = nullptr;   // device flag: when non-zero the launch does nothing
+    // one CTA per tile instead of one persistent CTA per SM: the SMs free up
+    // tile by tile, so kernels of a higher-priority stream can start between
+    // tiles (the Cholesky's look-ahead runs its bulk updates this way)
+    int one_tile_per_cta = 0;
 };
 
 // C tiles = alpha * A . B^T (both operands sliced with the same S and kp).
