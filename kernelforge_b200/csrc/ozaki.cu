@@ -366,22 +366,18 @@ __global__ void slice_cols_kernel(const double *__restrict__ src, long long rows
     const long long r0 = (long long)blockIdx.x * 32;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     {
-        // eight independent column loads in flight per warp, then the stores
+        // every load of the tile in flight at once (cp.async, 8 bytes each;
+        // rows beyond the source are zero-filled)
         const long long r = r0 + lane;
         const bool ok = r < rows;
-        for (int k0 = warp; k0 < K; k0 += 8 * nw) {
-            double v[8];
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const int k = k0 + u * nw;
-                v[u] = (ok && k < K) ? src[(long long)k * ld + r] : 0.0;
-            }
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const int k = k0 + u * nw;
-                if (k < K) tile[k * 33 + lane] = v[u];
-            }
+        const double *col0 = src + (ok ? r : 0);
+        for (int k = warp; k < K; k += nw) {
+            const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(tile + k * 33 + lane));
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d),
+                         "l"(col0 + (long long)k * ld), "r"(ok ? 8 : 0)
+                         : "memory");
         }
+        asm volatile("cp.async.wait_all;" ::: "memory");
     }
     __syncthreads();
     const long long plane = rows * (long long)kp;
