@@ -28,8 +28,12 @@
 #include <cublas_v2.h>
 
 #include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdlib>
 #include <memory>
 #include <numeric>
+#include <string>
 #include <tuple>
 #include <type_traits>
 
@@ -1219,6 +1223,78 @@ __global__ void __launch_bounds__(256) hess_rank_kernel(
     }
 }
 
+// ------------------------------------------------- Y on the tensor cores
+// Without the rank term, Y_p[(c, k)][i] = sum_j W_p[i][j] J_b[j][k][c] is one
+// GEMM per molecule b over the batch's pairs that share it: A = the Jacobian
+// of b with rows (c, k) and the atoms j as K (jk_split_kernel, once per call),
+// B = the pairs' weight rows (p, i) in b order (w_split_kernel, per batch),
+// and the grouped GEMM's EPI_YSPLIT epilogue writes the fp16 pair of Y where
+// the contraction reads it.  K = kj = ma2 rounded up to 16; entries of atoms
+// j >= n_b are zero in A, entries of other-label pairs are zero in W.
+
+// Jk[((b ld + c) rep + k) kj + j] = scale * dX[b][j][k][c] as an fp16 pair,
+// rows c < 3 n_b; block per (k, b), eight atoms j per pass.
+template <class T>
+__global__ void __launch_bounds__(128) jk_split_kernel(const T *__restrict__ dx, int ma, int rep,
+                                                       int kj, const int *__restrict__ nat,
+                                                       float scale, __half *__restrict__ hi,
+                                                       __half *__restrict__ lo) {
+    extern __shared__ float jk_s[];  // [8][ld + 1]
+    const int k = blockIdx.x, b = blockIdx.y;
+    const int nb = min(max(nat[b], 0), ma), ld = 3 * ma, nc = 3 * nb;
+    for (int j0 = 0; j0 < kj; j0 += 8) {
+        __syncthreads();
+        for (int e = threadIdx.x; e < 8 * nc; e += blockDim.x) {
+            const int r = e / nc, c = e - r * nc, j = j0 + r;
+            jk_s[r * (ld + 1) + c] =
+                j < nb ? (float)dx[(((size_t)b * ma + j) * rep + k) * ld + c] * scale : 0.f;
+        }
+        __syncthreads();
+        for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+            unsigned hw[4], lw[4];
+#pragma unroll
+            for (int r = 0; r < 8; r += 2) {
+                const float2 v = make_float2(jk_s[r * (ld + 1) + c], jk_s[(r + 1) * (ld + 1) + c]);
+                const __half2 h = __float22half2_rn(v);
+                const float2 hf = __half22float2(h);
+                const __half2 l = __float22half2_rn(make_float2(v.x - hf.x, v.y - hf.y));
+                hw[r / 2] = *reinterpret_cast<const unsigned *>(&h);
+                lw[r / 2] = *reinterpret_cast<const unsigned *>(&l);
+            }
+            const size_t o = (((size_t)b * ld + c) * rep + k) * (size_t)kj + j0;
+            *reinterpret_cast<uint4 *>(hi + o) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+            *reinterpret_cast<uint4 *>(lo + o) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+        }
+    }
+}
+
+// Ws[r kj + j] = scale * W[border[q]][i][j] (r = q ma1 + i) as an fp16 pair,
+// zero for j >= ma2; a thread per (row, eight columns).
+__global__ void w_split_kernel(const float *__restrict__ W, const int *__restrict__ border,
+                               int nrows, int ma1, int ma2, int kj, float scale,
+                               __half *__restrict__ hi, __half *__restrict__ lo) {
+    const int ng = kj / 8;
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (long long)nrows * ng) return;
+    const int r = (int)(e / ng), j0 = (int)(e - (long long)r * ng) * 8;
+    const int q = r / ma1, i = r - q * ma1;
+    const float *w = W + ((size_t)border[q] * ma1 + i) * ma2;
+    unsigned hw[4], lw[4];
+#pragma unroll
+    for (int u = 0; u < 8; u += 2) {
+        const float2 v = make_float2(j0 + u < ma2 ? w[j0 + u] * scale : 0.f,
+                                     j0 + u + 1 < ma2 ? w[j0 + u + 1] * scale : 0.f);
+        const __half2 h = __float22half2_rn(v);
+        const float2 hf = __half22float2(h);
+        const __half2 l = __float22half2_rn(make_float2(v.x - hf.x, v.y - hf.y));
+        hw[u / 2] = *reinterpret_cast<const unsigned *>(&h);
+        lw[u / 2] = *reinterpret_cast<const unsigned *>(&l);
+    }
+    const size_t o = (size_t)r * kj + j0;
+    *reinterpret_cast<uint4 *>(hi + o) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+    *reinterpret_cast<uint4 *>(lo + o) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+}
+
 template <class T, int MODE>
 kfb_status launch_hess_y(const HessPair *pairs, int np, const T *x1, const T *x2, const T *dx2,
                          const int *perm1, const int *lab1, const int *perm2, const int *lab2,
@@ -1693,6 +1769,67 @@ kfb_status jacobian_core(const DerivSet &outer, const DerivSet &inner, int rep, 
 // Hessian core: H_ab blocks for the listed molecule pairs, through `sink`
 // (rows offset by off1[a], columns by off2[b]).
 // ---------------------------------------------------------------------------
+// Y of a batch by the tensor cores: a GEMM problem per molecule b of the
+// batch (pairs with that b, in b order, as columns (q, i)), see jk_split_kernel.
+kfb_status hess_y_gemm(const HessPair *pairs, int np, int ma1, int ma2, int rep, int kj,
+                       const float *W, const DevBuf &jkh, const DevBuf &jkl, float jk_scale,
+                       float w_scale, float y_scale, DevBuf &wsh, DevBuf &wsl, DevBuf &d_ymap,
+                       DevBuf &d_border, long long jk_rows, __half *yhi, __half *ylo,
+                       cudaStream_t s) {
+    const int ld2 = 3 * ma2;
+    std::vector<int> border(np);
+    for (int p = 0; p < np; ++p) border[p] = p;
+    std::stable_sort(border.begin(), border.end(),
+                     [&](int x, int y) { return pairs[x].b < pairs[y].b; });
+    std::vector<int2> ymap((size_t)np * ma1);
+    std::vector<TcProb> probs;
+    for (int q = 0; q < np;) {
+        const HessPair &pr = pairs[border[q]];
+        int q1 = q;
+        for (; q1 < np && pairs[border[q1]].b == pr.b; ++q1) {
+            const int p = border[q1];
+            for (int i = 0; i < ma1; ++i)
+                ymap[(size_t)q1 * ma1 + i] = make_int2(i < pairs[p].na ? p : -1, i);
+        }
+        TcProb pb{};
+        pb.a_row0 = (int)((long long)pr.b * ld2 * rep);
+        pb.b_row0 = q * ma1;
+        pb.M = 3 * pr.nb * rep;
+        pb.N = (q1 - q) * ma1;
+        pb.K = kj;
+        pb.alpha = (double)y_scale / ((double)jk_scale * (double)w_scale);
+        probs.push_back(pb);
+        q = q1;
+    }
+    KFB_CUDA_TRY(cudaMemcpyAsync(d_border.ptr, border.data(), (size_t)np * sizeof(int),
+                                 cudaMemcpyHostToDevice, s));
+    KFB_CUDA_TRY(cudaMemcpyAsync(d_ymap.ptr, ymap.data(), ymap.size() * sizeof(int2),
+                                 cudaMemcpyHostToDevice, s));
+    const int nrows = np * ma1;
+    const long long nthr = (long long)nrows * (kj / 8);
+    w_split_kernel<<<(unsigned)((nthr + 255) / 256), 256, 0, s>>>(
+        W, d_border.as<int>(), nrows, ma1, ma2, kj, w_scale, wsh.as<__half>(), wsl.as<__half>());
+    KFB_CUDA_TRY(cudaGetLastError());
+    TcOperand A, B;
+    A.hi = jkh.ptr;
+    A.lo = jkl.ptr;
+    A.rows = jk_rows;
+    A.cols = kj;
+    B.hi = wsh.ptr;
+    B.lo = wsl.ptr;
+    B.rows = nrows;
+    B.cols = kj;
+    TcEpi epi;
+    epi.mode = EPI_YSPLIT;
+    epi.ymap = d_ymap.as<int2>();
+    epi.yhi = yhi;
+    epi.ylo = ylo;
+    epi.y_rep = rep;
+    epi.y_ma1 = ma1;
+    epi.y_ld2 = ld2;
+    return tc_gemm_grouped(A, B, 3, false, probs, ElemSink(), s, epi);
+}
+
 template <class T>
 kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double sigma,
                         bool symmetric, bool tc, ElemSink sink, cudaStream_t s) {
@@ -1766,6 +1903,12 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
     DevBuf d_l1, d_l2, d_sums, d_invc, d_amx, xh1, xl1, jrh, jrl, d_pb, d_jbm, d_P, d_nat2,
         d_n1, xh2, xl2, d_n2, d_G, jr1h, jr1l, d_pb1, d_Q, d_off1, d_off2, d_nat1;
     float xs2_scale = 1.f;
+    // Y on the tensor cores (rank term outside Y): set 2's Jacobian as rows
+    // (b, c, k) with kj atom columns, resident for the call
+    bool ygemm = false;
+    int kj = 0;
+    float w_scale = 1.f;
+    DevBuf jkh, jkl, wsh, wsl, d_ymap, d_border;
     if constexpr (std::is_same<T, float>::value) {
         const std::vector<int> labs1 = collect_labels(s1.v, nullptr);
         const long long pbytes = Mrows * bcols * (long long)sizeof(float);
@@ -1907,6 +2050,40 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
             KFB_TRY(d_P.alloc((size_t)bcap * Mrows * bcols * sizeof(float), s));
             KFB_TRY(d_G.alloc((size_t)bcap * Mrows * ma2 * sizeof(float), s));
             if (hrank) KFB_TRY(d_Q.alloc((size_t)bcap * ma2 * Mq * sizeof(float), s));
+            if (hrank) {
+                kj = (ma2 + 15) / 16 * 16;
+                const long long jk_rows = (long long)s2.v.nm * ld2 * rep;
+                const long long jk_bytes = jk_rows * kj * 2 * (long long)sizeof(__half);
+                size_t free_b = 0, total_b = 0;
+                KFB_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+                const char *ye = std::getenv("KFB_HESSIAN_Y");
+                ygemm = !(ye && std::string(ye) == "cuda-core") && rep % 8 == 0 &&
+                        jk_rows < INT_MAX &&
+                        (long long)batch * ma1 < INT_MAX &&
+                        jk_bytes + (long long)budget_bytes() <= (long long)free_b;
+            }
+            if (ygemm) {
+                TraceScope tr_j("hessian:jk-split", s);
+                const size_t jk_elems = (size_t)s2.v.nm * ld2 * rep * kj;
+                KFB_TRY(jkh.alloc(jk_elems * sizeof(__half), s));
+                KFB_TRY(jkl.alloc(jk_elems * sizeof(__half), s));
+                const size_t jsm = (size_t)8 * (ld2 + 1) * sizeof(float);
+                if (jsm > 48 * 1024)
+                    KFB_CUDA_TRY(cudaFuncSetAttribute(jk_split_kernel<float>,
+                                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                      (int)jsm));
+                jk_split_kernel<float><<<dim3((unsigned)rep, (unsigned)s2.v.nm), 128, jsm, s>>>(
+                    static_cast<const float *>(s2.dx), ma2, rep, kj, d_nat2.as<int>(), jr_scale,
+                    jkh.as<__half>(), jkl.as<__half>());
+                KFB_CUDA_TRY(cudaGetLastError());
+                KFB_TRY(wsh.alloc((size_t)batch * ma1 * kj * sizeof(__half), s));
+                KFB_TRY(wsl.alloc((size_t)batch * ma1 * kj * sizeof(__half), s));
+                KFB_TRY(d_ymap.alloc((size_t)batch * ma1 * sizeof(int2), s));
+                KFB_TRY(d_border.alloc((size_t)batch * sizeof(int), s));
+                // 0 < w <= 1 / sigma^2: a fixed power of two brings it under 2^14
+                w_scale = std::exp2(std::floor(std::log2(16384.0 * sigma * sigma)));
+            }
+            note_path(ygemm ? "hessian:y-gemm" : "hessian:y-cuda-core");
         }
     } else {
         note_path("hessian:cuda-core-t");
@@ -1973,6 +2150,8 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
                 eg.zf32 = d_G.as<float>();
                 eg.ld = pg.N;
                 KFB_TRY(tc_gemm_grouped(A, B2, 3, false, {pg}, ElemSink(), s, eg));
+                // the Y GEMM reads every weight: those of other-label pairs are 0
+                if (ygemm) KFB_TRY(zero(W.ptr, (size_t)np * ma1 * ma2 * sizeof(float), s));
                 hess_t_p_kernel<<<np, 256, smem_p, s>>>(
                     dpairs.as<HessPair>(), d_G.as<float>(), pg.N, d_n1.as<float>(),
                     symmetric ? d_n1.as<float>() : d_n2.as<float>(), d_perm1.as<int>(),
@@ -1992,7 +2171,12 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
         float y_scale = 1.f;
         if (tc) {
             KFB_TRY(pow2_from_device(yamax.as<float>(), s, &y_scale));
-            if (hrank)
+            if (ygemm)
+                KFB_TRY(hess_y_gemm(pairs.data() + p0, np, ma1, ma2, rep, kj, W.as<float>(),
+                                    jkh, jkl, jr_scale, w_scale, y_scale, wsh, wsl, d_ymap,
+                                    d_border, (long long)s2.v.nm * ld2 * rep, yth.as<__half>(),
+                                    ytl.as<__half>(), s));
+            else if (hrank)
                 KFB_TRY((launch_hess_y<T, 3>(dpairs.as<HessPair>(), np, x1p, x2p, dx2p,
                                              d_perm1.as<int>(), d_lab1.as<int>(),
                                              d_perm2.as<int>(), d_lab2.as<int>(), ma1, ma2, rep,

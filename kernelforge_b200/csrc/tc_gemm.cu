@@ -15,6 +15,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <climits>
 #include <mutex>
 
 #include "derivs.h"
@@ -66,11 +67,31 @@ __device__ __forceinline__ bool wait_bar(uint32_t bar, uint32_t parity, int *err
     }
 }
 
+// Tile t of the launch: problems own consecutive tile ranges starting at
+// tstart[p] (tstart[nprobs] = all tiles), row blocks outer, column blocks
+// inner.  The largest p with tstart[p] <= t owns t (empty problems share their
+// start with the next one and are skipped).
+__device__ __forceinline__ TcTile tile_at(const TcProb *__restrict__ probs,
+                                          const int *__restrict__ tstart, int nprobs, int t) {
+    int lo = 0, hi = nprobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (tstart[mid] <= t)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const int loc = t - tstart[lo];
+    const int ntn = (probs[lo].N + BN - 1) / BN;
+    const int mt = loc / ntn;
+    return TcTile{lo, mt * BM, (loc - mt * ntn) * BN, 0};
+}
+
 template <int NPROD>
 __global__ void __launch_bounds__(NUM_THREADS, 1)
     tc_gemm_kernel(const __grid_constant__ CUtensorMap ta_hi, const __grid_constant__ CUtensorMap ta_lo,
                    const __grid_constant__ CUtensorMap tb_hi, const __grid_constant__ CUtensorMap tb_lo,
-                   const TcProb *__restrict__ probs, const TcTile *__restrict__ tiles, int ntiles,
+                   const TcProb *__restrict__ probs, const int *__restrict__ tstart, int nprobs, int ntiles,
                    uint32_t idesc, ElemSink sink, TcEpi epi, int *err) {
     using C = Cfg<NPROD>;
     extern __shared__ uint8_t smem_raw[];
@@ -116,7 +137,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             uint32_t ph = 0;
             bool ok = true;
             for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-                const TcTile tl = tiles[t];
+                const TcTile tl = tile_at(probs, tstart, nprobs, t);
                 const TcProb pb = probs[tl.prob];
                 const int nkb = (pb.K + BK - 1) / BK;
                 for (int kb = 0; kb < nkb; ++kb) {
@@ -148,7 +169,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             uint32_t ph = 0, aph = 0;
             bool ok = true;
             for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-                const TcProb pb = probs[tiles[t].prob];
+                const TcProb pb = probs[tile_at(probs, tstart, nprobs, t).prob];
                 const int nkb = (pb.K + BK - 1) / BK;
                 if (!wait_bar(tempty_bar(acc), aph ^ 1u, err)) break;
                 tc_fence_after();
@@ -195,7 +216,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
         int acc = 0;
         uint32_t aph = 0;
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-            const TcTile tl = tiles[t];
+            const TcTile tl = tile_at(probs, tstart, nprobs, t);
             const TcProb pb = probs[tl.prob];
             const bool got = wait_bar(tfull_bar(acc), aph, err);
             if (!__all_sync(0xffffffffu, got)) break;
@@ -220,6 +241,52 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                                            (double)v[j] * pb.alpha, pb.diag);
                         }
                     }
+                    continue;
+                }
+                if (epi.mode == EPI_YSPLIT) {
+                    // lane l: the (p, i) part of column n0 + l's offset; the
+                    // 32 x 32 block is turned in shared memory so that each lane
+                    // writes 8 consecutive k of one column (octets never cross
+                    // a c boundary: rep % 8 == 0) as 16 bytes of yhi and of ylo
+                    const int nl = n0 + lane;
+                    long long cb = -1;
+                    if (nl < pb.N) {
+                        const int2 pi = epi.ymap[pb.b_row0 + nl];
+                        if (pi.x >= 0)
+                            cb = ((long long)pi.x * epi.y_ld2 * epi.y_ma1 + pi.y) * epi.y_rep;
+                    }
+                    float(*scr)[33] = molsum_scr[warp - EPI_WARP0];
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) scr[lane][j] = v[j];
+                    __syncwarp();
+                    const int o = lane & 3;
+                    const int mo = tl.m0 + q * 32 + o * 8;
+                    const bool ovalid = mo < pb.M;
+                    const int yc = mo / epi.y_rep;
+                    const long long roff =
+                        (long long)yc * epi.y_ma1 * epi.y_rep + (mo - yc * epi.y_rep);
+                    const float alpha = (float)pb.alpha;
+#pragma unroll
+                    for (int g = 0; g < 4; ++g) {
+                        const int j = g * 8 + (lane >> 2);
+                        const long long base = __shfl_sync(0xffffffffu, cb, j);
+                        if (!ovalid || base < 0) continue;
+                        unsigned hw[4], lw[4];
+#pragma unroll
+                        for (int r = 0; r < 8; r += 2) {
+                            const float2 x = make_float2(scr[o * 8 + r][j] * alpha,
+                                                         scr[o * 8 + r + 1][j] * alpha);
+                            const __half2 hv = __float22half2_rn(x);
+                            const float2 hf = __half22float2(hv);
+                            const __half2 lv = __float22half2_rn(make_float2(x.x - hf.x, x.y - hf.y));
+                            hw[r / 2] = *reinterpret_cast<const unsigned *>(&hv);
+                            lw[r / 2] = *reinterpret_cast<const unsigned *>(&lv);
+                        }
+                        const size_t off = (size_t)(base + roff);
+                        *reinterpret_cast<uint4 *>(epi.yhi + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+                        *reinterpret_cast<uint4 *>(epi.ylo + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+                    }
+                    __syncwarp();  // scr is rewritten by the next chunk
                     continue;
                 }
                 const int nvalid = min(32, pb.N - n0);
@@ -443,15 +510,19 @@ kfb_status launch(const TcOperand &A, const TcOperand &B, bool bf16,
                   const std::vector<TcProb> &probs, const ElemSink &sink, const TcEpi &epi,
                   int *err_flag, cudaStream_t s) {
     using C = Cfg<NPROD>;
-    std::vector<TcTile> tiles;
+    std::vector<int> tstart(probs.size() + 1);
+    long long ntiles = 0;
     for (int p = 0; p < (int)probs.size(); ++p) {
         const TcProb &pb = probs[p];
         if (pb.K % 16 != 0 || pb.a_k0 % 8 != 0 || pb.b_k0 % 8 != 0)
             return set_error(KFB_ERR_INVALID_ARG, "tc_gemm: K and column offsets must be multiples of 16 / 8");
-        for (int m0 = 0; m0 < pb.M; m0 += BM)
-            for (int n0 = 0; n0 < pb.N; n0 += BN) tiles.push_back(TcTile{p, m0, n0, 0});
+        tstart[p] = (int)ntiles;
+        if (pb.M > 0 && pb.N > 0)
+            ntiles += (long long)((pb.M + BM - 1) / BM) * ((pb.N + BN - 1) / BN);
+        if (ntiles >= INT_MAX) return set_error(KFB_ERR_INVALID_ARG, "tc_gemm: too many tiles");
     }
-    if (tiles.empty()) return KFB_OK;
+    tstart[probs.size()] = (int)ntiles;
+    if (ntiles == 0) return KFB_OK;
     TcEpi e = epi;
     if (e.mode != EPI_SINK) {
         auto al = [](const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
@@ -472,7 +543,7 @@ kfb_status launch(const TcOperand &A, const TcOperand &B, bool bf16,
     }
     DevBuf dp, dt, derr;
     KFB_TRY(upload(dp, probs, s));
-    KFB_TRY(upload(dt, tiles, s));
+    KFB_TRY(upload(dt, tstart, s));
     int *errp = err_flag;
     if (!errp) {
         KFB_TRY(derr.alloc(sizeof(int), s));
@@ -485,10 +556,10 @@ kfb_status launch(const TcOperand &A, const TcOperand &B, bool bf16,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
         attr = true;
     }
-    const int grid = std::min((int)tiles.size(), device_sm_count());
+    const int grid = std::min((int)ntiles, device_sm_count());
     const uint32_t idesc = make_idesc(BM, BN, bf16 ? 1 : 0);
     tc_gemm_kernel<NPROD><<<grid, NUM_THREADS, C::SMEM, s>>>(
-        ma_hi, ma_lo, mb_hi, mb_lo, dp.as<TcProb>(), dt.as<TcTile>(), (int)tiles.size(), idesc,
+        ma_hi, ma_lo, mb_hi, mb_lo, dp.as<TcProb>(), dt.as<int>(), (int)probs.size(), (int)ntiles, idesc,
         sink, e, errp);
     KFB_CUDA_TRY(cudaGetLastError());
     if (err_flag) return KFB_OK;

@@ -46,12 +46,18 @@ struct TcTile {
 //   EPI_SIN_RUNSUM molsum[mol[row] * ld + col] +=
 //                      scale * sin(aux[atom[row] * ld_aux + col]) * alpha * acc,
 //                  runs of rows with one destination summed as above
+//   EPI_YSPLIT     the Hessian's Y in the layout its contraction reads: problem
+//                  row m = (c, k) = (m / y_rep, m % y_rep), column n ->
+//                  (p, i) = ymap[b_row0 + n] (p < 0: skipped), and the fp16 pair
+//                  of alpha * acc goes to yhi / ylo[((p y_ld2 + c) y_ma1 + i) y_rep + k]
+//                  (y_rep % 8 == 0, yhi / ylo 16-byte aligned)
 enum TcEpiMode : int {
     EPI_SINK = 0,
     EPI_DENSE = 1,
     EPI_DSIN_T = 2,
     EPI_COS_MOLSUM = 3,
-    EPI_SIN_RUNSUM = 4
+    EPI_SIN_RUNSUM = 4,
+    EPI_YSPLIT = 5
 };
 
 struct TcEpi {
@@ -68,6 +74,9 @@ struct TcEpi {
     float *molsum = nullptr;
     long long ld = 0, ld_t = 0, ld_aux = 0;
     float scale = 1.f;
+    const int2 *ymap = nullptr;   // EPI_YSPLIT
+    __half *yhi = nullptr, *ylo = nullptr;
+    int y_rep = 0, y_ma1 = 0, y_ld2 = 0;
 };
 
 // nprod = 3: split operands, hi*hi + hi*lo + lo*hi; nprod = 1: hi only.

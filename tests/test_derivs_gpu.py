@@ -144,20 +144,26 @@ def test_jacobian_chunked_outer_molecules(precision, rep, monkeypatch):
               o.kernel_gaussian_jacobian(X1, X2, dX2, Q1, Q2, N1, N2, s), precision)
 
 
-@pytest.mark.parametrize("gb,path", [("0.00005", "hessian:rank-in-y"),
-                                      ("0.0001", "hessian:rank-kernel"),
-                                      ("4", "hessian:rank-kernel")])
-def test_hessian_tensor_core_batches(gb, path, monkeypatch):
+@pytest.mark.parametrize("gb,ycore,path", [
+    ("0.00005", None, ["hessian:rank-in-y", "hessian:y-cuda-core"]),
+    ("0.0001", None, ["hessian:rank-kernel", "hessian:y-gemm"]),
+    ("4", None, ["hessian:rank-kernel", "hessian:y-gemm"]),
+    ("4", "cuda-core", ["hessian:rank-kernel", "hessian:y-cuda-core"])])
+def test_hessian_tensor_core_batches(gb, ycore, path, monkeypatch):
     """Tensor-core Hessians with kernel 1 in GEMM form: a workspace of ~100 kB
     gives batches of a few molecule pairs spanning at most two molecules b (the
     projection buffer's capacity), the default one batch; symmetric RFP,
     asymmetric and full energy+force kernels against the oracle.  At ~54 kB the
     projection and rank buffers (18 kB each here) no longer fit half the
-    workspace together, so the rank term stays inside Y; the path log shows
-    which of the two forms each call took."""
+    workspace together, so the rank term stays inside Y (CUDA-core Y kernel);
+    with the rank term outside, Y is a tensor-core GEMM per molecule b unless
+    KFB_HESSIAN_Y=cuda-core keeps the CUDA-core kernel.  The path log shows
+    which forms each call took."""
     from kernelforge_b200 import _lib
     from kernelforge_b200 import local_kernels as lk
     monkeypatch.setenv("KFB_WORKSPACE_GB", gb)
+    if ycore:
+        monkeypatch.setenv("KFB_HESSIAN_Y", ycore)
     rep = 48
     X1, dX1, Q1, N1 = make_set(7, 6, rep, 3, 41)
     X2, dX2, Q2, N2 = make_set(5, 6, rep, 3, 42)
@@ -172,10 +178,10 @@ def test_hessian_tensor_core_batches(gb, path, monkeypatch):
     _lib.path_log_clear()
     close(lk.kernel_gaussian_hessian_symm_rfp(X1, dX1, Q1, N1, s, precision=p),
           o.kernel_gaussian_hessian_symm_rfp(X1, dX1, Q1, N1, s), p)
-    assert _lib.path_log() == [path]
+    assert _lib.path_log() == path
     _lib.path_log_clear()
     close(lk.kernel_gaussian_hessian(X1, dX1, X2, dX2, Q1, Q2, N1, N2, s, precision=p),
           o.kernel_gaussian_hessian(X1, dX1, X2, dX2, Q1, Q2, N1, N2, s), p)
-    assert _lib.path_log() == [path]
+    assert _lib.path_log() == path
     close(lk.kernel_gaussian_full(X1, dX1, X2, dX2, Q1, Q2, N1, N2, s, precision=p),
           o.kernel_gaussian_full(X1, dX1, X2, dX2, Q1, Q2, N1, N2, s), p)
