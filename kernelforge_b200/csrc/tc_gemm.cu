@@ -28,25 +28,53 @@ namespace {
 
 using namespace tc;
 
-constexpr int BM = 128, BN = 128, BK = 64;
-constexpr int TILE_A = BM * BK * 2, TILE_B = BN * BK * 2;
-constexpr int EPI_WARP0 = 4, NUM_EPI_WARPS = 8;
-constexpr int NUM_THREADS = 32 * (EPI_WARP0 + NUM_EPI_WARPS);
+constexpr int BM = 128, BN = 128;
+// Warps 0-3: TMA producer, MMA issuer, TMEM allocator, idle; then NEPI epilogue
+// warps (NEPI / 4 column groups of four row quarters).  NEPI = 8 serves every
+// epilogue mode with 64-element K blocks (128-byte swizzled rows); NEPI = 16
+// only EPI_YSPLIT (short K, many stores): more warps in flight (register cap 96
+// at 640 threads) and 32-element K blocks (64-byte swizzle), so that four
+// stages fit next to its scratch.
+constexpr int EPI_WARP0 = 4;
 constexpr int TMEM_COLS = 2 * BN;
-constexpr int STAGE_BUDGET = 196608;
 
-template <int NPROD>
+template <int NPROD, int NEPI>
 struct Cfg {
+    static constexpr int THREADS = 32 * (EPI_WARP0 + NEPI);
+    static constexpr int BK = NEPI == 8 ? 64 : 32;
+    static constexpr int TILE_A = BM * BK * 2, TILE_B = BN * BK * 2;
+    static constexpr int STAGE_BUDGET = NEPI == 8 ? 196608 : 131072;
     static constexpr int NOP = NPROD == 3 ? 2 : 1;  // arrays per operand
     static constexpr int STAGE = NOP * (TILE_A + TILE_B);
     static constexpr int NSTAGE = STAGE_BUDGET / STAGE > 6 ? 6 : STAGE_BUDGET / STAGE;
     static constexpr int OFF_BARS = NSTAGE * STAGE;
     static constexpr int NBARS = 2 * NSTAGE + 5;
     static constexpr int OFF_TMEM = OFF_BARS + NBARS * 8;
-    static constexpr int SMEM = OFF_TMEM + 16 + 1024;
+    // NEPI = 16: the epilogue scratch is dynamic (static shared memory stops at
+    // 48 KB), and launches of at most MAXP_SMEM problems read their problem
+    // table (and tile starts) from a shared-memory copy
+    static constexpr int OFF_SCR = OFF_TMEM + 16;
+    static constexpr int MAXP_SMEM = NEPI == 8 ? 0 : 64;
+    static constexpr int OFF_PROBS = OFF_SCR + (NEPI == 8 ? 0 : NEPI * 32 * 33 * 4);
+    static constexpr int OFF_TSTART = OFF_PROBS + MAXP_SMEM * (int)sizeof(TcProb);
+    static constexpr int SMEM = OFF_TSTART + (MAXP_SMEM > 0 ? (MAXP_SMEM + 1) * 4 : 0) + 1024;
 };
 
 constexpr unsigned long long WAIT_LIMIT_NS = 2000000000ull;
+
+// K-major shared-memory descriptor of a BK-element (16-bit) row: 128-byte
+// swizzle (8-row groups 1024 bytes apart) for BK = 64, 64-byte swizzle (512
+// bytes apart) for BK = 32; sm_100 version bit.
+template <int BK>
+__device__ __forceinline__ uint64_t sdesc_k(uint32_t saddr) {
+    if constexpr (BK == 64) {
+        return sdesc(saddr);
+    } else {
+        static_assert(BK == 32, "K block");
+        return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)1 << 16) |
+               ((uint64_t)(512 >> 4) << 32) | ((uint64_t)1 << 46) | ((uint64_t)4 << 61);
+    }
+}
 
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
     const __nv_bfloat162 t = __floats2bfloat162_rn(a, b);
@@ -87,13 +115,13 @@ __device__ __forceinline__ TcTile tile_at(const TcProb *__restrict__ probs,
     return TcTile{lo, mt * BM, (loc - mt * ntn) * BN, 0};
 }
 
-template <int NPROD>
-__global__ void __launch_bounds__(NUM_THREADS, 1)
+template <int NPROD, int NEPI>
+__global__ void __launch_bounds__(Cfg<NPROD, NEPI>::THREADS, 1)
     tc_gemm_kernel(const __grid_constant__ CUtensorMap ta_hi, const __grid_constant__ CUtensorMap ta_lo,
                    const __grid_constant__ CUtensorMap tb_hi, const __grid_constant__ CUtensorMap tb_lo,
                    const TcProb *__restrict__ probs, const int *__restrict__ tstart, int nprobs, int ntiles,
                    uint32_t idesc, ElemSink sink, TcEpi epi, int *err) {
-    using C = Cfg<NPROD>;
+    using C = Cfg<NPROD, NEPI>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
@@ -114,7 +142,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
         }
         for (int a = 0; a < 2; ++a) {
             mbar_init(tfull_bar(a), 1);
-            mbar_init(tempty_bar(a), NUM_EPI_WARPS);
+            mbar_init(tempty_bar(a), NEPI);
         }
         mbar_init(done_bar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -125,6 +153,18 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                      "r"(TMEM_COLS)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    const TcProb *P = probs;
+    const int *TS = tstart;
+    if constexpr (C::MAXP_SMEM > 0) {
+        if (nprobs <= C::MAXP_SMEM) {
+            TcProb *ps = reinterpret_cast<TcProb *>(smem + C::OFF_PROBS);
+            int *ts = reinterpret_cast<int *>(smem + C::OFF_TSTART);
+            for (int i = threadIdx.x; i < nprobs; i += blockDim.x) ps[i] = probs[i];
+            for (int i = threadIdx.x; i <= nprobs; i += blockDim.x) ts[i] = tstart[i];
+            P = ps;
+            TS = ts;
+        }
     }
     tc_fence_before();
     __syncthreads();
@@ -137,9 +177,9 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             uint32_t ph = 0;
             bool ok = true;
             for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-                const TcTile tl = tile_at(probs, tstart, nprobs, t);
-                const TcProb pb = probs[tl.prob];
-                const int nkb = (pb.K + BK - 1) / BK;
+                const TcTile tl = tile_at(P, TS, nprobs, t);
+                const TcProb pb = P[tl.prob];
+                const int nkb = (pb.K + C::BK - 1) / C::BK;
                 for (int kb = 0; kb < nkb; ++kb) {
                     if (!wait_bar(empty_bar(stage), ph ^ 1u, err)) {
                         ok = false;
@@ -147,13 +187,14 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                     }
                     const uint32_t sa = s_base + stage * C::STAGE;
                     mbar_expect_tx(full_bar(stage), C::STAGE);
-                    const int xa = pb.a_k0 + kb * BK, xb = pb.b_k0 + kb * BK;
+                    const int xa = pb.a_k0 + kb * C::BK, xb = pb.b_k0 + kb * C::BK;
                     tma_load_2d(sa, &ta_hi, xa, pb.a_row0 + tl.m0, full_bar(stage));
-                    tma_load_2d(sa + C::NOP * TILE_A, &tb_hi, xb, pb.b_row0 + tl.n0,
+                    tma_load_2d(sa + C::NOP * C::TILE_A, &tb_hi, xb, pb.b_row0 + tl.n0,
                                 full_bar(stage));
                     if (NPROD == 3) {
-                        tma_load_2d(sa + TILE_A, &ta_lo, xa, pb.a_row0 + tl.m0, full_bar(stage));
-                        tma_load_2d(sa + 2 * TILE_A + TILE_B, &tb_lo, xb, pb.b_row0 + tl.n0,
+                        tma_load_2d(sa + C::TILE_A, &ta_lo, xa, pb.a_row0 + tl.m0,
+                                    full_bar(stage));
+                        tma_load_2d(sa + 2 * C::TILE_A + C::TILE_B, &tb_lo, xb, pb.b_row0 + tl.n0,
                                     full_bar(stage));
                     }
                     if (++stage == C::NSTAGE) {
@@ -169,8 +210,8 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             uint32_t ph = 0, aph = 0;
             bool ok = true;
             for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-                const TcProb pb = probs[tile_at(probs, tstart, nprobs, t).prob];
-                const int nkb = (pb.K + BK - 1) / BK;
+                const TcProb pb = P[tile_at(P, TS, nprobs, t).prob];
+                const int nkb = (pb.K + C::BK - 1) / C::BK;
                 if (!wait_bar(tempty_bar(acc), aph ^ 1u, err)) break;
                 tc_fence_after();
                 const uint32_t dtm = tmem_base + (uint32_t)(acc * BN);
@@ -181,14 +222,15 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                     }
                     tc_fence_after();
                     const uint32_t sa = s_base + stage * C::STAGE;
-                    const int nks = min(BK / 16, (pb.K - kb * BK) / 16);
+                    const int nks = min(C::BK / 16, (pb.K - kb * C::BK) / 16);
                     for (int ks = 0; ks < nks; ++ks) {
-                        const uint64_t ahi = sdesc(sa + ks * 32);
-                        const uint64_t bhi = sdesc(sa + C::NOP * TILE_A + ks * 32);
+                        const uint64_t ahi = sdesc_k<C::BK>(sa + ks * 32);
+                        const uint64_t bhi = sdesc_k<C::BK>(sa + C::NOP * C::TILE_A + ks * 32);
                         umma_f16_idesc(dtm, ahi, bhi, idesc, (kb | ks) != 0 ? 1u : 0u);
                         if (NPROD == 3) {
-                            const uint64_t alo = sdesc(sa + TILE_A + ks * 32);
-                            const uint64_t blo = sdesc(sa + 2 * TILE_A + TILE_B + ks * 32);
+                            const uint64_t alo = sdesc_k<C::BK>(sa + C::TILE_A + ks * 32);
+                            const uint64_t blo =
+                                sdesc_k<C::BK>(sa + 2 * C::TILE_A + C::TILE_B + ks * 32);
                             umma_f16_idesc(dtm, ahi, blo, idesc, 1u);
                             umma_f16_idesc(dtm, alo, bhi, idesc, 1u);
                         }
@@ -211,13 +253,43 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
         }
     } else if (warp >= EPI_WARP0) {
         const int q = warp & 3;
-        const int h = (warp - EPI_WARP0) >> 2;  // column half
-        __shared__ float molsum_scr[NUM_EPI_WARPS][32][33];
+        const int h = (warp - EPI_WARP0) >> 2;  // column group
+        constexpr int CPW = (BN / 32) / (NEPI / 4);  // 32-column chunks per warp
+        __shared__ float molsum_static[NEPI == 8 ? NEPI : 1][32][33];
+        float(*molsum_scr)[32][33] =
+            NEPI == 8 ? molsum_static : reinterpret_cast<float(*)[32][33]>(smem + C::OFF_SCR);
         int acc = 0;
         uint32_t aph = 0;
+        // the tile's problem (and for EPI_YSPLIT the (p, i) offset of this
+        // lane's column); NEPI = 16 fetches them one tile ahead, so that the
+        // dependent loads overlap the stores of the tile before
+        TcTile tl_n{};
+        TcProb pb_n{};
+        long long cb_n = -1;
+        auto fetch = [&](int t) {
+            tl_n = tile_at(P, TS, nprobs, t);
+            pb_n = P[tl_n.prob];
+            if constexpr (NEPI == 16) {
+                const int nl = tl_n.n0 + h * 32 + lane;
+                cb_n = -1;
+                if (nl < pb_n.N) {
+                    const int2 pi = epi.ymap[pb_n.b_row0 + nl];
+                    if (pi.x >= 0)
+                        cb_n = ((long long)pi.x * epi.y_ld2 * epi.y_ma1 + pi.y) * epi.y_rep;
+                }
+            }
+        };
+        if constexpr (NEPI == 16) {
+            if ((int)blockIdx.x < ntiles) fetch(blockIdx.x);
+        }
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-            const TcTile tl = tile_at(probs, tstart, nprobs, t);
-            const TcProb pb = probs[tl.prob];
+            if constexpr (NEPI == 8) fetch(t);
+            const TcTile tl = tl_n;
+            const TcProb pb = pb_n;
+            const long long cb_t = cb_n;
+            if constexpr (NEPI == 16) {
+                if (t + (int)gridDim.x < ntiles) fetch(t + gridDim.x);
+            }
             const bool got = wait_bar(tfull_bar(acc), aph, err);
             if (!__all_sync(0xffffffffu, got)) break;
             tc_fence_after();
@@ -226,34 +298,30 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             const long long grow = (long long)pb.row_off + m;
             const uint32_t tbase = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN);
 #pragma unroll 1
-            for (int cc = 0; cc < BN / 64; ++cc) {
-                const int c = h * (BN / 64) + cc;
+            for (int cc = 0; cc < CPW; ++cc) {
+                const int c = h * CPW + cc;
                 float v[32];
                 tmem_ld32(tbase + (uint32_t)(c * 32), v);
-                const int n0 = tl.n0 + c * 32;
-                if (epi.mode == EPI_SINK) {
-                    if (mvalid) {
-#pragma unroll
-                        for (int j = 0; j < 32; ++j) {
-                            const int n = n0 + j;
-                            if (n < pb.N)
-                                sink_store(sink, pb.row_off + m, pb.col_off + n,
-                                           (double)v[j] * pb.alpha, pb.diag);
-                        }
-                    }
-                    continue;
+                if constexpr (NEPI == 16) {  // one chunk per warp: release the accumulator now
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(tempty_bar(acc));
                 }
-                if (epi.mode == EPI_YSPLIT) {
+                const int n0 = tl.n0 + c * 32;
+                if (NEPI == 16 || epi.mode == EPI_YSPLIT) {
                     // lane l: the (p, i) part of column n0 + l's offset; the
                     // 32 x 32 block is turned in shared memory so that each lane
                     // writes 8 consecutive k of one column (octets never cross
                     // a c boundary: rep % 8 == 0) as 16 bytes of yhi and of ylo
-                    const int nl = n0 + lane;
-                    long long cb = -1;
-                    if (nl < pb.N) {
-                        const int2 pi = epi.ymap[pb.b_row0 + nl];
-                        if (pi.x >= 0)
-                            cb = ((long long)pi.x * epi.y_ld2 * epi.y_ma1 + pi.y) * epi.y_rep;
+                    long long cb = cb_t;
+                    if constexpr (NEPI == 8) {
+                        const int nl = n0 + lane;
+                        cb = -1;
+                        if (nl < pb.N) {
+                            const int2 pi = epi.ymap[pb.b_row0 + nl];
+                            if (pi.x >= 0)
+                                cb = ((long long)pi.x * epi.y_ld2 * epi.y_ma1 + pi.y) * epi.y_rep;
+                        }
                     }
                     float(*scr)[33] = molsum_scr[warp - EPI_WARP0];
 #pragma unroll
@@ -287,6 +355,18 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                         *reinterpret_cast<uint4 *>(epi.ylo + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
                     }
                     __syncwarp();  // scr is rewritten by the next chunk
+                    continue;
+                }
+                if (epi.mode == EPI_SINK) {
+                    if (mvalid) {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) {
+                            const int n = n0 + j;
+                            if (n < pb.N)
+                                sink_store(sink, pb.row_off + m, pb.col_off + n,
+                                           (double)v[j] * pb.alpha, pb.diag);
+                        }
+                    }
                     continue;
                 }
                 const int nvalid = min(32, pb.N - n0);
@@ -455,9 +535,11 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                     __syncwarp();
                 }
             }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(tempty_bar(acc));
+            if constexpr (NEPI == 8) {
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(tempty_bar(acc));
+            }
             if (++acc == 2) {
                 acc = 0;
                 aph ^= 1u;
@@ -489,19 +571,32 @@ PFN_cuTensorMapEncodeTiled_v12000 encoder() {
 }
 
 kfb_status map2d(CUtensorMap *m, const void *ptr, long long rows, long long cols, int box_rows,
-                 bool bf16) {
+                 bool bf16, int box_cols = 64) {
     auto enc = encoder();
     if (!enc) return set_error(KFB_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
     if (cols % 8 != 0) return set_error(KFB_ERR_INVALID_ARG, "TMA operand rows must be 16-byte multiples");
     cuuint64_t gdim[2] = {(cuuint64_t)cols, (cuuint64_t)std::max<long long>(rows, 1)};
     cuuint64_t gstride[1] = {(cuuint64_t)cols * 2};
-    cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
+    cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
     CUresult r = enc(m, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16,
                      2, const_cast<void *>(ptr), gdim, gstride, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     box_cols == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return set_error(KFB_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return KFB_OK;
+}
+
+template <int NPROD, int NEPI>
+kfb_status set_smem_attr() {
+    static bool done = false;
+    if (!done) {
+        KFB_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_kernel<NPROD, NEPI>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          Cfg<NPROD, NEPI>::SMEM));
+        done = true;
+    }
     return KFB_OK;
 }
 
@@ -509,7 +604,6 @@ template <int NPROD>
 kfb_status launch(const TcOperand &A, const TcOperand &B, bool bf16,
                   const std::vector<TcProb> &probs, const ElemSink &sink, const TcEpi &epi,
                   int *err_flag, cudaStream_t s) {
-    using C = Cfg<NPROD>;
     std::vector<int> tstart(probs.size() + 1);
     long long ntiles = 0;
     for (int p = 0; p < (int)probs.size(); ++p) {
@@ -531,12 +625,14 @@ kfb_status launch(const TcOperand &A, const TcOperand &B, bool bf16,
         for (const TcProb &pb : probs) v = v && pb.col_off % 8 == 0;
         e.vec = v ? 1 : 0;
     }
+    const bool ysplit = e.mode == EPI_YSPLIT;
+    const int bk = ysplit ? Cfg<NPROD, 16>::BK : Cfg<NPROD, 8>::BK;
     CUtensorMap ma_hi, ma_lo, mb_hi, mb_lo;
-    KFB_TRY(map2d(&ma_hi, A.hi, A.rows, A.cols, BM, bf16));
-    KFB_TRY(map2d(&mb_hi, B.hi, B.rows, B.cols, BN, bf16));
+    KFB_TRY(map2d(&ma_hi, A.hi, A.rows, A.cols, BM, bf16, bk));
+    KFB_TRY(map2d(&mb_hi, B.hi, B.rows, B.cols, BN, bf16, bk));
     if (NPROD == 3) {
-        KFB_TRY(map2d(&ma_lo, A.lo, A.rows, A.cols, BM, bf16));
-        KFB_TRY(map2d(&mb_lo, B.lo, B.rows, B.cols, BN, bf16));
+        KFB_TRY(map2d(&ma_lo, A.lo, A.rows, A.cols, BM, bf16, bk));
+        KFB_TRY(map2d(&mb_lo, B.lo, B.rows, B.cols, BN, bf16, bk));
     } else {
         ma_lo = ma_hi;
         mb_lo = mb_hi;
@@ -550,17 +646,20 @@ kfb_status launch(const TcOperand &A, const TcOperand &B, bool bf16,
         KFB_TRY(zero(derr.ptr, sizeof(int), s));
         errp = derr.as<int>();
     }
-    static bool attr = false;
-    if (!attr) {
-        KFB_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_kernel<NPROD>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
-        attr = true;
-    }
+    if (ysplit)
+        KFB_TRY((set_smem_attr<NPROD, 16>()));
+    else
+        KFB_TRY((set_smem_attr<NPROD, 8>()));
     const int grid = std::min((int)ntiles, device_sm_count());
     const uint32_t idesc = make_idesc(BM, BN, bf16 ? 1 : 0);
-    tc_gemm_kernel<NPROD><<<grid, NUM_THREADS, C::SMEM, s>>>(
-        ma_hi, ma_lo, mb_hi, mb_lo, dp.as<TcProb>(), dt.as<int>(), (int)probs.size(), (int)ntiles, idesc,
-        sink, e, errp);
+    if (ysplit)
+        tc_gemm_kernel<NPROD, 16><<<grid, Cfg<NPROD, 16>::THREADS, Cfg<NPROD, 16>::SMEM, s>>>(
+            ma_hi, ma_lo, mb_hi, mb_lo, dp.as<TcProb>(), dt.as<int>(), (int)probs.size(),
+            (int)ntiles, idesc, sink, e, errp);
+    else
+        tc_gemm_kernel<NPROD, 8><<<grid, Cfg<NPROD, 8>::THREADS, Cfg<NPROD, 8>::SMEM, s>>>(
+            ma_hi, ma_lo, mb_hi, mb_lo, dp.as<TcProb>(), dt.as<int>(), (int)probs.size(),
+            (int)ntiles, idesc, sink, e, errp);
     KFB_CUDA_TRY(cudaGetLastError());
     if (err_flag) return KFB_OK;
     int herr = 0;
