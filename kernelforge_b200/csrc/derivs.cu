@@ -2113,9 +2113,15 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
         if (tc) KFB_TRY(zero(yamax.ptr, sizeof(float), s));
         if constexpr (std::is_same<T, float>::value) {
             if (pform) {
+                // rows of the batch's molecules a only (pairs sorted by a):
+                // P and G keep their global row index
+                const int arow0 = pairs[p0].a * ma1;
+                const int arows = (pairs[p0 + np - 1].a + 1) * ma1 - arow0;
                 TcProb pp{};
+                pp.a_row0 = arow0;
+                pp.row_off = arow0;
                 pp.b_row0 = (int)((long long)bmin * bcols);
-                pp.M = (int)Mrows;
+                pp.M = arows;
                 pp.N = (int)((long long)(bmax - bmin + 1) * bcols);
                 pp.K = rep;
                 pp.alpha = 1.0 / ((double)xs_scale * (double)jr_scale);
@@ -2135,8 +2141,10 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
                 KFB_TRY(tc_gemm_grouped(A, B, 3, false, {pp}, ElemSink(), s, epi));
                 // centred dot products of the batch's atom pairs
                 TcProb pg{};
+                pg.a_row0 = arow0;
+                pg.row_off = arow0;
                 pg.b_row0 = bmin * ma2;
-                pg.M = (int)Mrows;
+                pg.M = arows;
                 pg.N = (bmax - bmin + 1) * ma2;
                 pg.K = rep;
                 pg.alpha = 1.0 / ((double)xs_scale * (double)xs2_scale);
