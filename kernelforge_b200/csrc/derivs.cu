@@ -760,14 +760,17 @@ __global__ void jmax_per_mol_kernel(const T *__restrict__ dx, int ma, int rep,
 // Kernel 1 with t from P: the same outputs as hess_t_kernel (W, Tt, bound;
 // without the rank term in Y (rank_in_y = 0) the bound is max|J_b| sum_j w_ij);
 // weights from the centred dot products G[(a, i)][(b - b0) * ma2 + j] (row
-// length ldg) and the norms; t by a warp per (same-label pair, 32 columns).  P rows are set-1 padded atoms,
-// P columns ((b - b0) * ma2 + j) * ld2 + c with row length ldp.
+// length ldg) and the norms; t by a warp per (same-label pair, 32 columns).  P
+// (row length ldp) holds the projections of same-label atoms only: atom (a, i)
+// of molecules a0.. has row prow[(a - a0) ma1 + i], atom (b, j) of molecules
+// b0.. the columns from pcol[(b - b0) ma2 + j] (its 3 ma2 coordinates).
 __global__ void __launch_bounds__(256) hess_t_p_kernel(
     const HessPair *__restrict__ pairs, const float *__restrict__ G, long long ldg,
     const float *__restrict__ n1, const float *__restrict__ n2, const int *__restrict__ perm1,
     const int *__restrict__ lab1, const int *__restrict__ perm2, const int *__restrict__ lab2,
     int ma1, int ma2, float c2, float is2, float is4, const float *__restrict__ P,
-    long long ldp, int b0, const float *__restrict__ PB, const float *__restrict__ jbmax,
+    long long ldp, const int *__restrict__ prow, const int *__restrict__ pcol, int a0, int b0,
+    const float *__restrict__ PB, const float *__restrict__ jbmax,
     int rank_in_y, float *__restrict__ W, float *__restrict__ Tt, float *__restrict__ bound) {
     extern __shared__ __align__(16) unsigned char ht_raw[];
     int4 *groups = reinterpret_cast<int4 *>(ht_raw);  // ma1
@@ -833,7 +836,8 @@ __global__ void __launch_bounds__(256) hess_t_p_kernel(
     __syncthreads();
     // t'_ij = w'_ij (P - PB), a warp per (pair, 32 columns)
     const int nchunk = (ncol + 31) / 32;
-    const float *Prow0 = P + (size_t)pr.a * ma1 * ldp + (size_t)(pr.b - b0) * ma2 * ld2;
+    const int *prow_a = prow + (size_t)(pr.a - a0) * ma1;
+    const int *pcol_b = pcol + (size_t)(pr.b - b0) * ma2;
     const float *PBb = PB + (size_t)pr.b * ma2 * ld2;
     for (int it = warp; it < npairs * nchunk; it += nwarp) {
         const int q = it / nchunk, cc = it - q * nchunk;
@@ -843,7 +847,7 @@ __global__ void __launch_bounds__(256) hess_t_p_kernel(
         float t = 0.f;
         if (c < ncol)
             t = w2s[i * ma2 + j] *
-                (Prow0[(size_t)i * ldp + (size_t)j * ld2 + c] - PBb[(size_t)j * ld2 + c]);
+                (P[(size_t)prow_a[i] * ldp + pcol_b[j] + c] - PBb[(size_t)j * ld2 + c]);
         if (c < ncol) Tt[(wbase + (size_t)i * ma2 + j) * ld2 + c] = t;
         if (bound && rank_in_y) {
             float m = fabsf(t);
@@ -1112,11 +1116,12 @@ __global__ void __launch_bounds__(256, 2) hess_y_kernel(
 // ------------------------------------------------------- Hessian rank term
 // With Y_i = sum_j w_ij J_j (MODE 3) the contraction leaves out
 //   -sum_i J_i^T sum_j d_ij t'_ij^T = -sum_{i, j same label} s_ij t'_ij^T,
-//   s_ij[c'] = J_i[:, c'] . (x_i - x_j) = PB1[(a, i)][c'] - Q[(b - b0, j)][(a, i, c') - qc0],
+//   s_ij[c'] = J_i[:, c'] . (x_i - x_j) = PB1[(a, i)][c'] - Q[qrow(b, j)][qcol(a, i) + c'],
 // PB1 = (x_i - mu_l) . J_i[:, c'] and Q = (x_j - mu_l) . J_i[:, c'] (one
-// projection GEMM per batch over its molecules b and the range of set-1 rows
-// from column qc0 that its molecules a cover; mu_l the label centre that also
-// centres P).  This kernel adds that term to the pair's Hessian block after
+// projection GEMM problem per label and batch over the label's atoms of the
+// batch's molecules b and the Jacobian rows of its atoms in the batch's
+// molecules a; mu_l the label centre that also centres P).  qrow / qcol map
+// atoms of molecules b0.. / a0.. to their row / first column of Q.  This kernel adds that term to the pair's Hessian block after
 // the contraction wrote it: block per (pair, 64 x 64 tile of (c', c)),
 // 256 threads of 4 x 4 register tiles, the same-label pairs in chunks of HR_Q
 // with their s and t' rows staged in shared memory.  Every output element
@@ -1126,8 +1131,8 @@ constexpr int HR_Q = 32, HR_T = 64, HR_MAXA = 64;
 __global__ void __launch_bounds__(256) hess_rank_kernel(
     const HessPair *__restrict__ pairs, const int *__restrict__ perm1,
     const int *__restrict__ lab1, const int *__restrict__ perm2, const int *__restrict__ lab2,
-    int ma1, int ma2, const float *__restrict__ Q, long long ldq, int b0, long long qc0,
-    const float *__restrict__ PB1, const float *__restrict__ Tt, const int *__restrict__ off1,
+    int ma1, int ma2, const float *__restrict__ Q, long long ldq, const int *__restrict__ qrow,
+    const int *__restrict__ qcol, int a0, int b0, const float *__restrict__ PB1, const float *__restrict__ Tt, const int *__restrict__ off1,
     const int *__restrict__ off2, int symmetric, ElemSink sink) {
     __shared__ int4 groups[HR_MAXA];
     __shared__ int pa[HR_MAXA], pb[HR_MAXA], la[HR_MAXA], lb[HR_MAXA], gstart[HR_MAXA + 1];
@@ -1162,7 +1167,8 @@ __global__ void __launch_bounds__(256) hess_rank_kernel(
     const int npairs = gstart[ngroups];
     const int ty = tid >> 4, tx = tid & 15;
     const size_t arow = (size_t)pr.a * ma1;
-    const float *Qb = Q + (size_t)(pr.b - b0) * ma2 * ldq;
+    const int *qrow_b = qrow + (size_t)(pr.b - b0) * ma2;
+    const int *qcol_a = qcol + (size_t)(pr.a - a0) * ma1;
     const float *Tp = Tt + (size_t)p * ma1 * ma2 * ld2;
     float acc[4][4] = {};
     for (int q0 = 0; q0 < npairs; q0 += HR_Q) {
@@ -1188,7 +1194,7 @@ __global__ void __launch_bounds__(256) hess_rank_kernel(
             if (i >= 0) {
                 const size_t col = (arow + i) * ld1;
                 if (r0 + r < m1)
-                    sv = PB1[col + r0 + r] - Qb[(size_t)j * ldq + (col - qc0) + r0 + r];
+                    sv = PB1[col + r0 + r] - Q[(size_t)qrow_b[j] * ldq + qcol_a[i] + r0 + r];
                 if (c0 + r < n2) tv = Tp[((size_t)i * ma2 + j) * ld2 + c0 + r];
             }
             Ss[qq][r] = sv;
@@ -1769,6 +1775,124 @@ kfb_status jacobian_core(const DerivSet &outer, const DerivSet &inner, int rep, 
 // Hessian core: H_ab blocks for the listed molecule pairs, through `sink`
 // (rows offset by off1[a], columns by off2[b]).
 // ---------------------------------------------------------------------------
+// Atoms of a set in label-major order (label index, then molecule, then atom):
+// cum[l (nm + 1) + m] = label-l atoms in molecules < m, start[l] = label-major
+// index of label l's first atom, rank[m ma + i] = label-major index of atom
+// (m, i) (-1: no label index), src[r] = m ma + i of label-major atom r.  The
+// label-l atoms of molecules m0..m1 are the contiguous range from first(l, m0).
+struct LabelMajor {
+    int L = 0, nm = 0, n = 0;
+    std::vector<int> cum, start, rank, src, lab;
+    void build(const std::vector<int> &lidx, int nm_, int ma, int L_) {
+        L = L_;
+        nm = nm_;
+        lab = lidx;
+        cum.assign((size_t)L * (nm + 1), 0);
+        for (int m = 0; m < nm; ++m) {
+            for (int l = 0; l < L; ++l) cum[(size_t)l * (nm + 1) + m + 1] = cum[(size_t)l * (nm + 1) + m];
+            for (int i = 0; i < ma; ++i) {
+                const int l = lidx[(size_t)m * ma + i];
+                if (l >= 0) ++cum[(size_t)l * (nm + 1) + m + 1];
+            }
+        }
+        start.assign(L + 1, 0);
+        for (int l = 0; l < L; ++l) start[l + 1] = start[l] + cum[(size_t)l * (nm + 1) + nm];
+        n = start[L];
+        rank.assign((size_t)nm * ma, -1);
+        src.assign(n, 0);
+        std::vector<int> within(L);
+        for (int m = 0; m < nm; ++m) {
+            std::fill(within.begin(), within.end(), 0);
+            for (int i = 0; i < ma; ++i) {
+                const int l = lidx[(size_t)m * ma + i];
+                if (l < 0) continue;
+                const int r = first(l, m) + within[l]++;
+                rank[(size_t)m * ma + i] = r;
+                src[r] = m * ma + i;
+            }
+        }
+    }
+    int first(int l, int m) const { return start[l] + cum[(size_t)l * (nm + 1) + m]; }
+    int count(int l, int m0, int m1) const {
+        return cum[(size_t)l * (nm + 1) + m1 + 1] - cum[(size_t)l * (nm + 1) + m0];
+    }
+};
+
+// dst rows r = src rows srcrow[r] of an fp16 pair (rep entries per row)
+__global__ void gather_rows_kernel(const __half *__restrict__ shi, const __half *__restrict__ slo,
+                                   const int *__restrict__ srcrow, int rep,
+                                   __half *__restrict__ dhi, __half *__restrict__ dlo) {
+    const size_t r = blockIdx.x, sr = (size_t)srcrow[r];
+    for (int k = threadIdx.x; k < rep; k += blockDim.x) {
+        dhi[r * rep + k] = shi[sr * rep + k];
+        dlo[r * rep + k] = slo[sr * rep + k];
+    }
+}
+
+// Label-major copy (lm.n rows) of a split row array in atom order.
+kfb_status label_major_rows(const LabelMajor &lm, const DevBuf &hi, const DevBuf &lo, int rep,
+                            DevBuf &dhi, DevBuf &dlo, cudaStream_t s) {
+    if (lm.n == 0) return KFB_OK;
+    DevBuf d_src;
+    KFB_TRY(upload(d_src, lm.src, s));
+    KFB_TRY(dhi.alloc((size_t)lm.n * rep * sizeof(__half), s));
+    KFB_TRY(dlo.alloc((size_t)lm.n * rep * sizeof(__half), s));
+    gather_rows_kernel<<<(unsigned)lm.n, 128, 0, s>>>(hi.as<__half>(), lo.as<__half>(),
+                                                     d_src.as<int>(), rep, dhi.as<__half>(),
+                                                     dlo.as<__half>());
+    KFB_CUDA_TRY(cudaGetLastError());
+    return KFB_OK;
+}
+
+// Projection problems of a batch, one per label: rows = the label-l atoms of
+// molecules r0..r1 of set R (its label-major rows), columns = cw rows per
+// label-l atom of molecules c0..c1 of set C (label-major blocks of cw rows);
+// problem rows stacked from 0.  rowmap[(m - r0) mar + i] = output row of atom
+// (m, i), colmap[(m - c0) mac + j] = first output column of atom (m, j) (-1:
+// no problem).  Returns the output row length (widest problem, rounded up to 8).
+long long label_problems(const LabelMajor &R, int r0, int r1, int mar, const LabelMajor &C,
+                         int c0, int c1, int mac, int cw, int K, double alpha,
+                         std::vector<TcProb> &probs, std::vector<int> &rowmap,
+                         std::vector<int> &colmap) {
+    probs.clear();
+    std::vector<int> rowbase(R.L, -1);
+    long long ld = 0;
+    int rb = 0;
+    for (int l = 0; l < R.L; ++l) {
+        const int M = R.count(l, r0, r1), Nn = C.count(l, c0, c1);
+        if (M == 0 || Nn == 0) continue;
+        TcProb p{};
+        p.a_row0 = R.first(l, r0);
+        p.b_row0 = C.first(l, c0) * cw;
+        p.M = M;
+        p.N = Nn * cw;
+        p.K = K;
+        p.row_off = rb;
+        p.alpha = alpha;
+        probs.push_back(p);
+        rowbase[l] = rb;
+        rb += M;
+        ld = std::max(ld, (long long)p.N);
+    }
+    rowmap.assign((size_t)(r1 - r0 + 1) * mar, -1);
+    for (int m = r0; m <= r1; ++m)
+        for (int i = 0; i < mar; ++i) {
+            const size_t a = (size_t)m * mar + i;
+            const int l = R.lab[a];
+            if (l >= 0 && rowbase[l] >= 0)
+                rowmap[(size_t)(m - r0) * mar + i] = rowbase[l] + R.rank[a] - R.first(l, r0);
+        }
+    colmap.assign((size_t)(c1 - c0 + 1) * mac, -1);
+    for (int m = c0; m <= c1; ++m)
+        for (int j = 0; j < mac; ++j) {
+            const size_t a = (size_t)m * mac + j;
+            const int l = C.lab[a];
+            if (l >= 0 && rowbase[l] >= 0)
+                colmap[(size_t)(m - c0) * mac + j] = (C.rank[a] - C.first(l, c0)) * cw;
+        }
+    return (ld + 7) / 8 * 8;
+}
+
 // Y of a batch by the tensor cores: a GEMM problem per molecule b of the
 // batch (pairs with that b, in b order, as columns (q, i)), see jk_split_kernel.
 kfb_status hess_y_gemm(const HessPair *pairs, int np, int ma1, int ma2, int rep, int kj,
@@ -1902,6 +2026,12 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
     float xs_scale = 1.f, jr_scale = 1.f, jr1_scale = 1.f;
     DevBuf d_l1, d_l2, d_sums, d_invc, d_amx, xh1, xl1, jrh, jrl, d_pb, d_jbm, d_P, d_nat2,
         d_n1, xh2, xl2, d_n2, d_G, jr1h, jr1l, d_pb1, d_Q, d_off1, d_off2, d_nat1;
+    // the P and Q projections pair same-label atoms only: their operands in
+    // label-major order (x1L/x2L: centred descriptor rows, jrh/jr1h: Jacobian
+    // rows), one GEMM problem per label, and per-batch maps from atoms to rows
+    // and columns of P and Q
+    LabelMajor lm1, lm2;
+    DevBuf x1Lh, x1Ll, x2Lh, x2Ll, d_rank1, d_rank2, d_prow, d_pcol, d_qrow, d_qcol;
     float xs2_scale = 1.f;
     // Y on the tensor cores (rank term outside Y): set 2's Jacobian as rows
     // (b, c, k) with kj atom columns, resident for the call
@@ -1952,6 +2082,8 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
                     l2[(size_t)m * ma2 + j] = lab_index(s2.v.q[(size_t)m * ma2 + j]);
             }
             for (int l = 0; l < L; ++l) invc[l] = cnt[l] > 0.0 ? 1.0 / cnt[l] : 0.0;
+            lm1.build(l1, s1.v.nm, ma1, L);
+            lm2.build(l2, s2.v.nm, ma2, L);
             KFB_TRY(upload(d_l1, l1, s));
             KFB_TRY(upload(d_l2, l2, s));
             KFB_TRY(upload(d_invc, invc, s));
@@ -2001,12 +2133,16 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
                     xs2_scale, xh2.as<__half>(), xl2.as<__half>(), d_n2.as<float>());
                 KFB_CUDA_TRY(cudaGetLastError());
             }
-            const size_t jr_elems = (size_t)s2.v.nm * bcols * rep;
+            KFB_TRY(label_major_rows(lm1, xh1, xl1, rep, x1Lh, x1Ll, s));
+            if (!symmetric) KFB_TRY(label_major_rows(lm2, xh2, xl2, rep, x2Lh, x2Ll, s));
+            // set-2 Jacobian rows, label-major blocks of ld2 rows per atom
+            KFB_TRY(upload(d_rank2, lm2.rank, s));
+            const size_t jr_elems = std::max<size_t>(1, (size_t)lm2.n * ld2 * rep);
             KFB_TRY(jrh.alloc(jr_elems * sizeof(__half), s));
             KFB_TRY(jrl.alloc(jr_elems * sizeof(__half), s));
             KFB_TRY(transpose_split_dx_rows<float>(dx2f, s2.v.nm, ma2, rep, d_nat2.as<int>(),
                                                    jrh.as<__half>(), jrl.as<__half>(),
-                                                   &jr_scale, s));
+                                                   &jr_scale, s, d_rank2.as<int>()));
             KFB_TRY(d_pb.alloc((size_t)s2.v.nm * bcols * sizeof(float), s));
             pb_kernel<float><<<(unsigned)(s2.v.nm * ma2), 128, 0, s>>>(
                 x2f, dx2f, d_l2.as<int>(), ma2, rep, d_sums.as<double>(), d_invc.as<double>(),
@@ -2025,11 +2161,13 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
                     std::vector<int> nat1(s1.v.nm);
                     for (int m = 0; m < s1.v.nm; ++m) nat1[m] = s1.v.natoms(m);
                     KFB_TRY(upload(d_nat1, nat1, s));
-                    KFB_TRY(jr1h.alloc((size_t)Mq * rep * sizeof(__half), s));
-                    KFB_TRY(jr1l.alloc((size_t)Mq * rep * sizeof(__half), s));
-                    KFB_TRY(transpose_split_dx_rows<float>(dx1f, s1.v.nm, ma1, rep,
-                                                           d_nat1.as<int>(), jr1h.as<__half>(),
-                                                           jr1l.as<__half>(), &jr1_scale, s));
+                    KFB_TRY(upload(d_rank1, lm1.rank, s));
+                    const size_t jr1_elems = std::max<size_t>(1, (size_t)lm1.n * ld1 * rep);
+                    KFB_TRY(jr1h.alloc(jr1_elems * sizeof(__half), s));
+                    KFB_TRY(jr1l.alloc(jr1_elems * sizeof(__half), s));
+                    KFB_TRY(transpose_split_dx_rows<float>(
+                        dx1f, s1.v.nm, ma1, rep, d_nat1.as<int>(), jr1h.as<__half>(),
+                        jr1l.as<__half>(), &jr1_scale, s, d_rank1.as<int>()));
                     KFB_TRY(d_pb1.alloc((size_t)Mq * sizeof(float), s));
                     pb_kernel<float><<<(unsigned)Mrows, 128, 0, s>>>(
                         x1f, dx1f, d_l1.as<int>(), ma1, rep, d_sums.as<double>(),
@@ -2047,9 +2185,17 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
                 span_max = std::max(span_max, pairs[q1].b - pairs[q0].b + 1);
             }
             bcap = std::min(bcap, span_max);
-            KFB_TRY(d_P.alloc((size_t)bcap * Mrows * bcols * sizeof(float), s));
+            // label blocks of P and Q: at most the batch's rows, row length
+            // rounded up to 8
+            KFB_TRY(d_P.alloc((size_t)Mrows * ((size_t)bcap * bcols + 8) * sizeof(float), s));
             KFB_TRY(d_G.alloc((size_t)bcap * Mrows * ma2 * sizeof(float), s));
-            if (hrank) KFB_TRY(d_Q.alloc((size_t)bcap * ma2 * Mq * sizeof(float), s));
+            if (hrank) KFB_TRY(d_Q.alloc((size_t)bcap * ma2 * (Mq + 8) * sizeof(float), s));
+            KFB_TRY(d_prow.alloc((size_t)Mrows * sizeof(int), s));
+            KFB_TRY(d_pcol.alloc((size_t)s2.v.nm * ma2 * sizeof(int), s));
+            if (hrank) {
+                KFB_TRY(d_qrow.alloc((size_t)s2.v.nm * ma2 * sizeof(int), s));
+                KFB_TRY(d_qcol.alloc((size_t)Mrows * sizeof(int), s));
+            }
             if (hrank) {
                 kj = (ma2 + 15) / 16 * 16;
                 const long long jk_rows = (long long)s2.v.nm * ld2 * rep;
@@ -2115,30 +2261,37 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
             if (pform) {
                 // rows of the batch's molecules a only (pairs sorted by a):
                 // P and G keep their global row index
-                const int arow0 = pairs[p0].a * ma1;
-                const int arows = (pairs[p0 + np - 1].a + 1) * ma1 - arow0;
-                TcProb pp{};
-                pp.a_row0 = arow0;
-                pp.row_off = arow0;
-                pp.b_row0 = (int)((long long)bmin * bcols);
-                pp.M = arows;
-                pp.N = (int)((long long)(bmax - bmin + 1) * bcols);
-                pp.K = rep;
-                pp.alpha = 1.0 / ((double)xs_scale * (double)jr_scale);
+                const int amin = pairs[p0].a, amax = pairs[p0 + np - 1].a;
+                const int arow0 = amin * ma1;
+                const int arows = (amax + 1) * ma1 - arow0;
+                std::vector<TcProb> pps;
+                std::vector<int> prow, pcol;
+                const long long ldp = label_problems(
+                    lm1, amin, amax, ma1, lm2, bmin, bmax, ma2, ld2, rep,
+                    1.0 / ((double)xs_scale * (double)jr_scale), pps, prow, pcol);
+                KFB_CUDA_TRY(cudaMemcpyAsync(d_prow.ptr, prow.data(), prow.size() * sizeof(int),
+                                             cudaMemcpyHostToDevice, s));
+                KFB_CUDA_TRY(cudaMemcpyAsync(d_pcol.ptr, pcol.data(), pcol.size() * sizeof(int),
+                                             cudaMemcpyHostToDevice, s));
                 TcOperand A, B;
-                A.hi = xh1.ptr;
-                A.lo = xl1.ptr;
-                A.rows = Mrows;
+                A.hi = x1Lh.ptr;
+                A.lo = x1Ll.ptr;
+                A.rows = lm1.n;
                 A.cols = rep;
                 B.hi = jrh.ptr;
                 B.lo = jrl.ptr;
-                B.rows = (long long)s2.v.nm * bcols;
+                B.rows = (long long)lm2.n * ld2;
                 B.cols = rep;
                 TcEpi epi;
                 epi.mode = EPI_DENSE;
                 epi.zf32 = d_P.as<float>();
-                epi.ld = pp.N;
-                KFB_TRY(tc_gemm_grouped(A, B, 3, false, {pp}, ElemSink(), s, epi));
+                epi.ld = ldp;
+                KFB_TRY(tc_gemm_grouped(A, B, 3, false, pps, ElemSink(), s, epi));
+                TcOperand A1;  // centred set-1 rows in atom order
+                A1.hi = xh1.ptr;
+                A1.lo = xl1.ptr;
+                A1.rows = Mrows;
+                A1.cols = rep;
                 // centred dot products of the batch's atom pairs
                 TcProb pg{};
                 pg.a_row0 = arow0;
@@ -2157,14 +2310,15 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
                 eg.mode = EPI_DENSE;
                 eg.zf32 = d_G.as<float>();
                 eg.ld = pg.N;
-                KFB_TRY(tc_gemm_grouped(A, B2, 3, false, {pg}, ElemSink(), s, eg));
+                KFB_TRY(tc_gemm_grouped(A1, B2, 3, false, {pg}, ElemSink(), s, eg));
                 // the Y GEMM reads every weight: those of other-label pairs are 0
                 if (ygemm) KFB_TRY(zero(W.ptr, (size_t)np * ma1 * ma2 * sizeof(float), s));
                 hess_t_p_kernel<<<np, 256, smem_p, s>>>(
                     dpairs.as<HessPair>(), d_G.as<float>(), pg.N, d_n1.as<float>(),
                     symmetric ? d_n1.as<float>() : d_n2.as<float>(), d_perm1.as<int>(),
                     d_lab1.as<int>(), d_perm2.as<int>(), d_lab2.as<int>(), ma1, ma2, c2, is2, is4,
-                    d_P.as<float>(), pp.N, bmin, d_pb.as<float>(), d_jbm.as<float>(),
+                    d_P.as<float>(), ldp, d_prow.as<int>(), d_pcol.as<int>(), amin, bmin,
+                    d_pb.as<float>(), d_jbm.as<float>(),
                     hrank ? 0 : 1, W.as<T>(), Tt.as<T>(), yamax.as<float>());
                 KFB_CUDA_TRY(cudaGetLastError());
             }
@@ -2251,36 +2405,41 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
             if constexpr (std::is_same<T, float>::value) {
                 if (hrank) {
                     TraceScope tr_r("hessian:rank", s);
-                    // set-1 rows of the batch's molecules a (pairs sorted by a)
-                    const long long rows_a = (long long)ma1 * ld1;
+                    // set-2 atoms of the batch's molecules b against the set-1
+                    // Jacobian rows of its molecules a (pairs sorted by a),
+                    // same label only
                     const int amin = pairs[p0].a, amax = pairs[p0 + np - 1].a;
-                    TcProb pq{};
-                    pq.a_row0 = bmin * ma2;
-                    pq.b_row0 = (int)(amin * rows_a);
-                    pq.M = (bmax - bmin + 1) * ma2;
-                    pq.N = (int)((amax - amin + 1) * rows_a);
-                    pq.K = rep;
-                    pq.alpha = 1.0 / ((double)xs2_scale * (double)jr1_scale);
+                    std::vector<TcProb> pqs;
+                    std::vector<int> qrow, qcol;
+                    const long long ldq = label_problems(
+                        lm2, bmin, bmax, ma2, lm1, amin, amax, ma1, ld1, rep,
+                        1.0 / ((double)xs2_scale * (double)jr1_scale), pqs, qrow, qcol);
+                    KFB_CUDA_TRY(cudaMemcpyAsync(d_qrow.ptr, qrow.data(),
+                                                 qrow.size() * sizeof(int),
+                                                 cudaMemcpyHostToDevice, s));
+                    KFB_CUDA_TRY(cudaMemcpyAsync(d_qcol.ptr, qcol.data(),
+                                                 qcol.size() * sizeof(int),
+                                                 cudaMemcpyHostToDevice, s));
                     TcOperand Aq, Bq;
-                    Aq.hi = symmetric ? xh1.ptr : xh2.ptr;
-                    Aq.lo = symmetric ? xl1.ptr : xl2.ptr;
-                    Aq.rows = (long long)s2.v.nm * ma2;
+                    Aq.hi = symmetric ? x1Lh.ptr : x2Lh.ptr;
+                    Aq.lo = symmetric ? x1Ll.ptr : x2Ll.ptr;
+                    Aq.rows = lm2.n;
                     Aq.cols = rep;
                     Bq.hi = symmetric ? jrh.ptr : jr1h.ptr;
                     Bq.lo = symmetric ? jrl.ptr : jr1l.ptr;
-                    Bq.rows = Mq;
+                    Bq.rows = (long long)lm1.n * ld1;
                     Bq.cols = rep;
                     TcEpi eq;
                     eq.mode = EPI_DENSE;
                     eq.zf32 = d_Q.as<float>();
-                    eq.ld = pq.N;
-                    KFB_TRY(tc_gemm_grouped(Aq, Bq, 3, false, {pq}, ElemSink(), s, eq));
+                    eq.ld = ldq;
+                    KFB_TRY(tc_gemm_grouped(Aq, Bq, 3, false, pqs, ElemSink(), s, eq));
                     const unsigned tiles =
                         (unsigned)(((ld1 + HR_T - 1) / HR_T) * ((ld2 + HR_T - 1) / HR_T));
                     hess_rank_kernel<<<dim3(tiles, (unsigned)np), 256, 0, s>>>(
                         dpairs.as<HessPair>(), d_perm1.as<int>(), d_lab1.as<int>(),
-                        d_perm2.as<int>(), d_lab2.as<int>(), ma1, ma2, d_Q.as<float>(), pq.N, bmin,
-                        (long long)pq.b_row0,
+                        d_perm2.as<int>(), d_lab2.as<int>(), ma1, ma2, d_Q.as<float>(), ldq,
+                        d_qrow.as<int>(), d_qcol.as<int>(), amin, bmin,
                         symmetric ? d_pb.as<float>() : d_pb1.as<float>(), Tt.as<float>(),
                         d_off1.as<int>(), d_off2.as<int>(), symmetric ? 1 : 0, sink);
                     KFB_CUDA_TRY(cudaGetLastError());

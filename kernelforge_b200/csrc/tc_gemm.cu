@@ -777,14 +777,16 @@ __global__ void __launch_bounds__(256) transpose_split_dx_kernel(
 // memory; atoms j >= nat[m] and columns c >= 3 nat[m] are not written.
 template <class T>
 __global__ void __launch_bounds__(256) transpose_split_dx_rows_kernel(
-    const T *__restrict__ dx, int ma, int rep, const int *__restrict__ nat, float scale,
-    __half *__restrict__ hi, __half *__restrict__ lo) {
+    const T *__restrict__ dx, int ma, int rep, const int *__restrict__ nat,
+    const int *__restrict__ blockmap, float scale, __half *__restrict__ hi,
+    __half *__restrict__ lo) {
     __shared__ float tile[32][33];
     const int mj = blockIdx.x, m = mj / ma, j = mj - m * ma;
     const int na = min(max(nat[m], 0), ma);
     const int k0 = blockIdx.y * 32, c0 = blockIdx.z * 32;
     const int ld = 3 * ma;
-    if (j >= na || c0 >= 3 * na) return;
+    const int dst = blockmap ? blockmap[mj] : mj;  // block-uniform
+    if (j >= na || c0 >= 3 * na || dst < 0) return;
     const T *base = dx + (size_t)mj * rep * ld;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int r = warp; r < 32; r += 8) {
@@ -797,7 +799,7 @@ __global__ void __launch_bounds__(256) transpose_split_dx_rows_kernel(
         if (c >= ld || k >= rep) continue;
         const float v = tile[lane][r];
         const __half h = __float2half_rn(v);
-        const size_t o = ((size_t)mj * ld + c) * rep + k;
+        const size_t o = ((size_t)dst * ld + c) * rep + k;
         hi[o] = h;
         lo[o] = __float2half_rn(v - __half2float(h));
     }
@@ -906,7 +908,8 @@ kfb_status transpose_split_dx(const T *dx, int nm, int ma, int rep, const int *n
 
 template <class T>
 kfb_status transpose_split_dx_rows(const T *dx, int nm, int ma, int rep, const int *nat,
-                                   __half *hi, __half *lo, float *scale, cudaStream_t s) {
+                                   __half *hi, __half *lo, float *scale, cudaStream_t s,
+                                   const int *blockmap) {
     *scale = 1.f;
     if (nm <= 0) return KFB_OK;
     {
@@ -920,7 +923,8 @@ kfb_status transpose_split_dx_rows(const T *dx, int nm, int ma, int rep, const i
         KFB_TRY(pow2_from_device(d.as<float>(), s, scale));
     }
     dim3 grid((unsigned)(nm * ma), (unsigned)((rep + 31) / 32), (unsigned)((3 * ma + 31) / 32));
-    transpose_split_dx_rows_kernel<T><<<grid, 256, 0, s>>>(dx, ma, rep, nat, *scale, hi, lo);
+    transpose_split_dx_rows_kernel<T><<<grid, 256, 0, s>>>(dx, ma, rep, nat, blockmap, *scale,
+                                                           hi, lo);
     KFB_CUDA_TRY(cudaGetLastError());
     return KFB_OK;
 }
@@ -942,7 +946,8 @@ template kfb_status split_rows<float>(const float *, long long, __half *, __half
 template kfb_status split_rows<double>(const double *, long long, __half *, __half *, float *,
                                        cudaStream_t);
 template kfb_status transpose_split_dx_rows<float>(const float *, int, int, int, const int *,
-                                                   __half *, __half *, float *, cudaStream_t);
+                                                   __half *, __half *, float *, cudaStream_t,
+                                                   const int *);
 template kfb_status transpose_split_dx<float>(const float *, int, int, int, const int *, __half *,
                                               __half *, float *, cudaStream_t);
 template kfb_status transpose_split_dx<double>(const double *, int, int, int, const int *,

@@ -102,10 +102,12 @@ kfb_status split_rows(const T *src, long long n, __half *hi, __half *lo, float *
                       cudaStream_t s);
 // Jr[(m, j, c)][k] = dX[m][j][k][c] as scaled fp16 pairs: a K-major row of rep
 // per (atom, coordinate column); rows of padding atoms and columns are not
-// written.
+// written.  blockmap (device, per atom m * ma + j, optional) moves atom (m, j)'s
+// 3 ma rows to block blockmap[m * ma + j] (< 0: not written).
 template <class T>
 kfb_status transpose_split_dx_rows(const T *dx, int nm, int ma, int rep, const int *nat,
-                                   __half *hi, __half *lo, float *scale, cudaStream_t s);
+                                   __half *hi, __half *lo, float *scale, cudaStream_t s,
+                                   const int *blockmap = nullptr);
 template <class T>
 kfb_status transpose_split_dx(const T *dx, int nm, int ma, int rep, const int *nat, __half *hi,
                               __half *lo, float *scale, cudaStream_t s);
