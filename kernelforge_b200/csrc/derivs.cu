@@ -2361,6 +2361,7 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
         if (tc) {
             std::vector<TcProb> tprobs;
             tprobs.reserve(np);
+            const bool narrow = ld1 <= 64;
             for (int k = 0; k < np;) {
                 const HessPair &pr = pairs[p0 + k];
                 const bool dg = symmetric && pr.a == pr.b;
@@ -2376,31 +2377,38 @@ kfb_status hessian_core(const DerivSet &s1, const DerivSet &s2, int rep, double 
                     ncols += 3 * q.nb;
                     ++k1;
                 }
+                // molecules a of at most 21 atoms: Y rows as M (up to 128 of the
+                // merged pairs) and a's 3 n_a Jacobian rows as N in 64-column
+                // tiles, stored transposed; else a's rows as M, Y rows as N
                 TcProb p{};
-                p.a_row0 = pr.a * ld1;
+                p.a_row0 = narrow ? k * ld2 : pr.a * ld1;
                 p.a_k0 = 0;
-                p.b_row0 = k * ld2;
+                p.b_row0 = narrow ? pr.a * ld1 : k * ld2;
                 p.b_k0 = 0;
-                p.M = 3 * pr.na;
-                p.N = ncols;
+                p.M = narrow ? ncols : 3 * pr.na;
+                p.N = narrow ? 3 * pr.na : ncols;
                 p.K = pr.na * rep;
-                p.row_off = off1[pr.a];
-                p.col_off = off2[pr.b];
+                p.row_off = narrow ? off2[pr.b] : off1[pr.a];
+                p.col_off = narrow ? off1[pr.a] : off2[pr.b];
                 p.diag = dg ? 1 : 0;
                 p.alpha = 1.0 / ((double)jt_scale * (double)y_scale);
                 tprobs.push_back(p);
                 k = k1;
             }
-            TcOperand A, B;
-            A.hi = jth.ptr;
-            A.lo = jtl.ptr;
-            A.rows = (long long)s1.v.nm * ld1;
-            A.cols = (long long)ma1 * rep;
-            B.hi = yth.ptr;
-            B.lo = ytl.ptr;
-            B.rows = (long long)np * ld2;
-            B.cols = (long long)ma1 * rep;
-            KFB_TRY(tc_gemm_grouped(A, B, 3, false, tprobs, sink, s));
+            TcOperand J, Yo;
+            J.hi = jth.ptr;
+            J.lo = jtl.ptr;
+            J.rows = (long long)s1.v.nm * ld1;
+            J.cols = (long long)ma1 * rep;
+            Yo.hi = yth.ptr;
+            Yo.lo = ytl.ptr;
+            Yo.rows = (long long)np * ld2;
+            Yo.cols = (long long)ma1 * rep;
+            TcEpi ec;
+            ec.tile_n64 = narrow ? 1 : 0;
+            ec.sink_t = narrow ? 1 : 0;
+            KFB_TRY(tc_gemm_grouped(narrow ? Yo : J, narrow ? J : Yo, 3, false, tprobs, sink, s,
+                                    ec));
             tr_g.reset();
             if constexpr (std::is_same<T, float>::value) {
                 if (hrank) {

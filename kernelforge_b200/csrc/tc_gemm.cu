@@ -28,7 +28,7 @@ namespace {
 
 using namespace tc;
 
-constexpr int BM = 128, BN = 128;
+constexpr int BM = 128;
 // Warps 0-3: TMA producer, MMA issuer, TMEM allocator, idle; then NEPI epilogue
 // warps (NEPI / 4 column groups of four row quarters).  NEPI = 8 serves every
 // epilogue mode with 64-element K blocks (128-byte swizzled rows); NEPI = 16
@@ -36,10 +36,11 @@ constexpr int BM = 128, BN = 128;
 // at 640 threads) and 32-element K blocks (64-byte swizzle), so that four
 // stages fit next to its scratch.
 constexpr int EPI_WARP0 = 4;
-constexpr int TMEM_COLS = 2 * BN;
 
-template <int NPROD, int NEPI>
+template <int NPROD, int NEPI, int BNT = 128>
 struct Cfg {
+    static constexpr int BN = BNT;  // tile columns (64: narrow-N problems, NEPI = 8 only)
+    static constexpr int TMEM_COLS = 2 * BN;
     static constexpr int THREADS = 32 * (EPI_WARP0 + NEPI);
     static constexpr int BK = NEPI == 8 ? 64 : 32;
     static constexpr int TILE_A = BM * BK * 2, TILE_B = BN * BK * 2;
@@ -100,7 +101,8 @@ __device__ __forceinline__ bool wait_bar(uint32_t bar, uint32_t parity, int *err
 // inner.  The largest p with tstart[p] <= t owns t (empty problems share their
 // start with the next one and are skipped).
 __device__ __forceinline__ TcTile tile_at(const TcProb *__restrict__ probs,
-                                          const int *__restrict__ tstart, int nprobs, int t) {
+                                          const int *__restrict__ tstart, int nprobs, int t,
+                                          int bn) {
     int lo = 0, hi = nprobs - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
@@ -110,18 +112,18 @@ __device__ __forceinline__ TcTile tile_at(const TcProb *__restrict__ probs,
             hi = mid - 1;
     }
     const int loc = t - tstart[lo];
-    const int ntn = (probs[lo].N + BN - 1) / BN;
+    const int ntn = (probs[lo].N + bn - 1) / bn;
     const int mt = loc / ntn;
-    return TcTile{lo, mt * BM, (loc - mt * ntn) * BN, 0};
+    return TcTile{lo, mt * BM, (loc - mt * ntn) * bn, 0};
 }
 
-template <int NPROD, int NEPI>
-__global__ void __launch_bounds__(Cfg<NPROD, NEPI>::THREADS, 1)
+template <int NPROD, int NEPI, int BNT>
+__global__ void __launch_bounds__(Cfg<NPROD, NEPI, BNT>::THREADS, 1)
     tc_gemm_kernel(const __grid_constant__ CUtensorMap ta_hi, const __grid_constant__ CUtensorMap ta_lo,
                    const __grid_constant__ CUtensorMap tb_hi, const __grid_constant__ CUtensorMap tb_lo,
                    const TcProb *__restrict__ probs, const int *__restrict__ tstart, int nprobs, int ntiles,
                    uint32_t idesc, ElemSink sink, TcEpi epi, int *err) {
-    using C = Cfg<NPROD, NEPI>;
+    using C = Cfg<NPROD, NEPI, BNT>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
@@ -150,7 +152,7 @@ __global__ void __launch_bounds__(Cfg<NPROD, NEPI>::THREADS, 1)
     if (warp == 2) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          smem_u32(tmem_holder)),
-                     "r"(TMEM_COLS)
+                     "r"(C::TMEM_COLS)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -177,7 +179,7 @@ __global__ void __launch_bounds__(Cfg<NPROD, NEPI>::THREADS, 1)
             uint32_t ph = 0;
             bool ok = true;
             for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-                const TcTile tl = tile_at(P, TS, nprobs, t);
+                const TcTile tl = tile_at(P, TS, nprobs, t, C::BN);
                 const TcProb pb = P[tl.prob];
                 const int nkb = (pb.K + C::BK - 1) / C::BK;
                 for (int kb = 0; kb < nkb; ++kb) {
@@ -210,11 +212,11 @@ __global__ void __launch_bounds__(Cfg<NPROD, NEPI>::THREADS, 1)
             uint32_t ph = 0, aph = 0;
             bool ok = true;
             for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-                const TcProb pb = P[tile_at(P, TS, nprobs, t).prob];
+                const TcProb pb = P[tile_at(P, TS, nprobs, t, C::BN).prob];
                 const int nkb = (pb.K + C::BK - 1) / C::BK;
                 if (!wait_bar(tempty_bar(acc), aph ^ 1u, err)) break;
                 tc_fence_after();
-                const uint32_t dtm = tmem_base + (uint32_t)(acc * BN);
+                const uint32_t dtm = tmem_base + (uint32_t)(acc * C::BN);
                 for (int kb = 0; kb < nkb; ++kb) {
                     if (!wait_bar(full_bar(stage), ph, err)) {
                         ok = false;
@@ -254,7 +256,7 @@ __global__ void __launch_bounds__(Cfg<NPROD, NEPI>::THREADS, 1)
     } else if (warp >= EPI_WARP0) {
         const int q = warp & 3;
         const int h = (warp - EPI_WARP0) >> 2;  // column group
-        constexpr int CPW = (BN / 32) / (NEPI / 4);  // 32-column chunks per warp
+        constexpr int CPW = (C::BN / 32) / (NEPI / 4);  // 32-column chunks per warp
         __shared__ float molsum_static[NEPI == 8 ? NEPI : 1][32][33];
         float(*molsum_scr)[32][33] =
             NEPI == 8 ? molsum_static : reinterpret_cast<float(*)[32][33]>(smem + C::OFF_SCR);
@@ -267,7 +269,7 @@ __global__ void __launch_bounds__(Cfg<NPROD, NEPI>::THREADS, 1)
         TcProb pb_n{};
         long long cb_n = -1;
         auto fetch = [&](int t) {
-            tl_n = tile_at(P, TS, nprobs, t);
+            tl_n = tile_at(P, TS, nprobs, t, C::BN);
             pb_n = P[tl_n.prob];
             if constexpr (NEPI == 16) {
                 const int nl = tl_n.n0 + h * 32 + lane;
@@ -296,7 +298,7 @@ __global__ void __launch_bounds__(Cfg<NPROD, NEPI>::THREADS, 1)
             const int m = tl.m0 + q * 32 + lane;
             const bool mvalid = m < pb.M;
             const long long grow = (long long)pb.row_off + m;
-            const uint32_t tbase = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN);
+            const uint32_t tbase = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * C::BN);
 #pragma unroll 1
             for (int cc = 0; cc < CPW; ++cc) {
                 const int c = h * CPW + cc;
@@ -362,9 +364,14 @@ __global__ void __launch_bounds__(Cfg<NPROD, NEPI>::THREADS, 1)
 #pragma unroll
                         for (int j = 0; j < 32; ++j) {
                             const int n = n0 + j;
-                            if (n < pb.N)
-                                sink_store(sink, pb.row_off + m, pb.col_off + n,
-                                           (double)v[j] * pb.alpha, pb.diag);
+                            if (n < pb.N) {
+                                if (epi.sink_t)
+                                    sink_store(sink, pb.col_off + n, pb.row_off + m,
+                                               (double)v[j] * pb.alpha, pb.diag);
+                                else
+                                    sink_store(sink, pb.row_off + m, pb.col_off + n,
+                                               (double)v[j] * pb.alpha, pb.diag);
+                            }
                         }
                     }
                     continue;
@@ -551,7 +558,7 @@ __global__ void __launch_bounds__(Cfg<NPROD, NEPI>::THREADS, 1)
     if (warp == 2) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
-                     "r"(TMEM_COLS)
+                     "r"(C::TMEM_COLS)
                      : "memory");
     }
 }
@@ -588,15 +595,23 @@ kfb_status map2d(CUtensorMap *m, const void *ptr, long long rows, long long cols
     return KFB_OK;
 }
 
-template <int NPROD, int NEPI>
-kfb_status set_smem_attr() {
+template <int NPROD, int NEPI, int BNT>
+kfb_status launch_cfg(const CUtensorMap &ma_hi, const CUtensorMap &ma_lo, const CUtensorMap &mb_hi,
+                      const CUtensorMap &mb_lo, const TcProb *probs, const int *tstart,
+                      int nprobs, int ntiles, bool bf16, const ElemSink &sink, const TcEpi &e,
+                      int *errp, cudaStream_t s) {
+    using C = Cfg<NPROD, NEPI, BNT>;
     static bool done = false;
     if (!done) {
-        KFB_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_kernel<NPROD, NEPI>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          Cfg<NPROD, NEPI>::SMEM));
+        KFB_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_kernel<NPROD, NEPI, BNT>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
         done = true;
     }
+    const int grid = std::min(ntiles, device_sm_count());
+    const uint32_t idesc = make_idesc(BM, C::BN, bf16 ? 1 : 0);
+    tc_gemm_kernel<NPROD, NEPI, BNT><<<grid, C::THREADS, C::SMEM, s>>>(
+        ma_hi, ma_lo, mb_hi, mb_lo, probs, tstart, nprobs, ntiles, idesc, sink, e, errp);
+    KFB_CUDA_TRY(cudaGetLastError());
     return KFB_OK;
 }
 
@@ -604,6 +619,9 @@ template <int NPROD>
 kfb_status launch(const TcOperand &A, const TcOperand &B, bool bf16,
                   const std::vector<TcProb> &probs, const ElemSink &sink, const TcEpi &epi,
                   int *err_flag, cudaStream_t s) {
+    const bool ysplit = epi.mode == EPI_YSPLIT;
+    const bool narrow = !ysplit && epi.tile_n64;
+    const int bn = narrow ? 64 : 128;
     std::vector<int> tstart(probs.size() + 1);
     long long ntiles = 0;
     for (int p = 0; p < (int)probs.size(); ++p) {
@@ -612,7 +630,7 @@ kfb_status launch(const TcOperand &A, const TcOperand &B, bool bf16,
             return set_error(KFB_ERR_INVALID_ARG, "tc_gemm: K and column offsets must be multiples of 16 / 8");
         tstart[p] = (int)ntiles;
         if (pb.M > 0 && pb.N > 0)
-            ntiles += (long long)((pb.M + BM - 1) / BM) * ((pb.N + BN - 1) / BN);
+            ntiles += (long long)((pb.M + BM - 1) / BM) * ((pb.N + bn - 1) / bn);
         if (ntiles >= INT_MAX) return set_error(KFB_ERR_INVALID_ARG, "tc_gemm: too many tiles");
     }
     tstart[probs.size()] = (int)ntiles;
@@ -625,14 +643,13 @@ kfb_status launch(const TcOperand &A, const TcOperand &B, bool bf16,
         for (const TcProb &pb : probs) v = v && pb.col_off % 8 == 0;
         e.vec = v ? 1 : 0;
     }
-    const bool ysplit = e.mode == EPI_YSPLIT;
     const int bk = ysplit ? Cfg<NPROD, 16>::BK : Cfg<NPROD, 8>::BK;
     CUtensorMap ma_hi, ma_lo, mb_hi, mb_lo;
     KFB_TRY(map2d(&ma_hi, A.hi, A.rows, A.cols, BM, bf16, bk));
-    KFB_TRY(map2d(&mb_hi, B.hi, B.rows, B.cols, BN, bf16, bk));
+    KFB_TRY(map2d(&mb_hi, B.hi, B.rows, B.cols, bn, bf16, bk));
     if (NPROD == 3) {
         KFB_TRY(map2d(&ma_lo, A.lo, A.rows, A.cols, BM, bf16, bk));
-        KFB_TRY(map2d(&mb_lo, B.lo, B.rows, B.cols, BN, bf16, bk));
+        KFB_TRY(map2d(&mb_lo, B.lo, B.rows, B.cols, bn, bf16, bk));
     } else {
         ma_lo = ma_hi;
         mb_lo = mb_hi;
@@ -647,20 +664,17 @@ kfb_status launch(const TcOperand &A, const TcOperand &B, bool bf16,
         errp = derr.as<int>();
     }
     if (ysplit)
-        KFB_TRY((set_smem_attr<NPROD, 16>()));
+        KFB_TRY((launch_cfg<NPROD, 16, 128>(ma_hi, ma_lo, mb_hi, mb_lo, dp.as<TcProb>(),
+                                            dt.as<int>(), (int)probs.size(), (int)ntiles, bf16,
+                                            sink, e, errp, s)));
+    else if (narrow)
+        KFB_TRY((launch_cfg<NPROD, 8, 64>(ma_hi, ma_lo, mb_hi, mb_lo, dp.as<TcProb>(),
+                                          dt.as<int>(), (int)probs.size(), (int)ntiles, bf16,
+                                          sink, e, errp, s)));
     else
-        KFB_TRY((set_smem_attr<NPROD, 8>()));
-    const int grid = std::min((int)ntiles, device_sm_count());
-    const uint32_t idesc = make_idesc(BM, BN, bf16 ? 1 : 0);
-    if (ysplit)
-        tc_gemm_kernel<NPROD, 16><<<grid, Cfg<NPROD, 16>::THREADS, Cfg<NPROD, 16>::SMEM, s>>>(
-            ma_hi, ma_lo, mb_hi, mb_lo, dp.as<TcProb>(), dt.as<int>(), (int)probs.size(),
-            (int)ntiles, idesc, sink, e, errp);
-    else
-        tc_gemm_kernel<NPROD, 8><<<grid, Cfg<NPROD, 8>::THREADS, Cfg<NPROD, 8>::SMEM, s>>>(
-            ma_hi, ma_lo, mb_hi, mb_lo, dp.as<TcProb>(), dt.as<int>(), (int)probs.size(),
-            (int)ntiles, idesc, sink, e, errp);
-    KFB_CUDA_TRY(cudaGetLastError());
+        KFB_TRY((launch_cfg<NPROD, 8, 128>(ma_hi, ma_lo, mb_hi, mb_lo, dp.as<TcProb>(),
+                                           dt.as<int>(), (int)probs.size(), (int)ntiles, bf16,
+                                           sink, e, errp, s)));
     if (err_flag) return KFB_OK;
     int herr = 0;
     KFB_CUDA_TRY(cudaMemcpyAsync(&herr, derr.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));

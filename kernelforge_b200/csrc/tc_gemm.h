@@ -62,6 +62,8 @@ enum TcEpiMode : int {
 
 struct TcEpi {
     int mode = EPI_SINK;
+    int tile_n64 = 0;  // 128 x 64 tiles (problems with N <= 64 waste no MMA columns)
+    int sink_t = 0;    // EPI_SINK: alpha * acc stored at (col, row) instead of (row, col)
     int vec = 0;         // set by tc_gemm_grouped: 16-byte row stores allowed
     int accumulate = 0;  // EPI_DENSE: zf32 += z (atomic; split-K problems)
     float *zf32 = nullptr;
