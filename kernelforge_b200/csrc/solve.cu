@@ -565,9 +565,11 @@ kfb_status mixed_core(const ApplyFn &A, const float *B, int n, kfb_layout uplo, 
     // The factor: the dense lower triangle of F factored by chol_dense (panel
     // solves and trailing updates on the int8 tensor cores) with 4 digit planes
     // (FP32-class: the north-star precision of the preconditioner) or, with
-    // KFB_SOLVE_FP64_FACTOR, 7 (FP64-class); held in FP64 either way, so the
-    // preconditioner out = F^{-1} x is the pair of blocked FP64 sweeps of
-    // trsv.cu.
+    // KFB_SOLVE_FP64_FACTOR, 6 (42-bit digits: as a preconditioner of the FP64
+    // conjugate gradients it needs as few steps as 7 planes, two at n = 10,000,
+    // for 21 instead of 28 int8 products per update); held in FP64 either way,
+    // so the preconditioner out = F^{-1} x is the pair of blocked FP64 sweeps
+    // of trsv.cu.
     const bool f64 = (flags & KFB_SOLVE_FP64_FACTOR) != 0;
     DevBuf Fd, ttmp;
     TrsvPlan trsv;
@@ -578,7 +580,7 @@ kfb_status mixed_core(const ApplyFn &A, const float *B, int n, kfb_layout uplo, 
         dense_deflate_kernel<double><<<gt, b2, 0, s>>>(B, n, uplo, v, fcoef, diag,
                                                        Fd.as<double>());
         KFB_CUDA_TRY(cudaGetLastError());
-        KFB_TRY(chol_dense(Fd.as<double>(), n, n, f64 ? 7 : 4, &finfo, s));
+        KFB_TRY(chol_dense(Fd.as<double>(), n, n, f64 ? 6 : 4, &finfo, s));
         if (finfo == 0) KFB_TRY(trsv.prepare(Fd.as<double>(), n, s));
         return KFB_OK;
     };
