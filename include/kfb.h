@@ -240,9 +240,12 @@ kfb_status kfb_cho_solve_rfp(void *arf, const double *y, int n, double l2, kfb_l
                              double *alpha, int *info, void *stream);
 
 /* Mixed-precision KRR solve: (K + l2 I) alpha = y with K given as an FP32 RFP
- * array (not modified).  The factor is FP32 (RFP Cholesky of K with its
- * dominant eigenpair deflated, plus (l2 + shift) I); residuals, corrections and
- * norms are FP64 (conjugate-gradient refinement preconditioned by the FP32
+ * array (not modified).  The factor is this library's tensor-core Cholesky of
+ * the dense lower triangle of K + (l2 + shift) I: FP32-class by default (K's
+ * dominant eigenpair deflated, 4 digit planes of 7 bits in the int8 trailing
+ * updates, FP32 diagonal blocks) or FP64-class with KFB_SOLVE_FP64_FACTOR (6
+ * planes, FP64 diagonal blocks, no deflation); residuals, corrections and
+ * norms are FP64 (conjugate-gradient refinement preconditioned by the
  * factor).  Stops at ||r|| <= tol * ||y||; KFB_ERR_NOT_PD if K + l2 I is
  * indefinite at FP32 storage precision (unless KFB_SOLVE_LAMBDA_FLOOR).
  * No reference counterpart: it replaces the reference's FP32 rfp_potrf +
@@ -260,9 +263,9 @@ typedef struct kfb_solve_info {
 #define KFB_SOLVE_LAMBDA_FLOOR 1  /* if K + l2 I is indefinite at FP32 storage
                                      precision, raise l2 (x10 steps) until it is
                                      not, and report it in lambda_eff */
-#define KFB_SOLVE_FP64_FACTOR 2   /* factor in FP64 (dense) instead of FP32; the
-                                     refinement then converges in one or two
-                                     steps */
+#define KFB_SOLVE_FP64_FACTOR 2   /* FP64-class factor instead of FP32-class;
+                                     the refinement then converges in one or
+                                     two steps */
 
 kfb_status kfb_krr_solve_mixed(const float *k_rfp, const double *y, int n, double l2,
                                kfb_layout uplo, double tol, int maxit, int flags,

@@ -74,9 +74,10 @@ def krr_solve_mixed(K_rfp, y, l2=0.0, uplo="L", tol=1e-10, maxit=500, *, lambda_
     ``factor``: precision of the Cholesky factor behind the refinement, both
     this library's tensor-core factorisation (FP64 diagonal blocks and panels,
     int8 digit-plane trailing updates): "fp64" (default) an FP64-class factor
-    (7 digit planes), one or two refinement steps; "fp32" an FP32-class factor
-    (4 planes, FP32 diagonal blocks), about six steps.  At n = 10,000 the
-    whole solve takes 22.9 ms and 25.5 ms respectively on one B200.
+    (6 digit planes of 7 bits), one or two refinement steps; "fp32" an
+    FP32-class factor (4 planes, FP32 diagonal blocks), about six steps.  At
+    n = 10,000 the whole solve takes 15.9 ms and 22.8 ms respectively on one
+    B200.
     """
     require_cuda()
     import torch
