@@ -144,6 +144,43 @@ def test_jacobian_chunked_outer_molecules(precision, rep, monkeypatch):
               o.kernel_gaussian_jacobian(X1, X2, dX2, Q1, Q2, N1, N2, s), precision)
 
 
+@pytest.mark.parametrize("ma1,ma2", [(23, 5), (4, 23)])
+def test_tensor_core_hessian_large_molecules(ma1, ma2):
+    """Set-1 molecules of more than 21 atoms (more than 64 Jacobian rows) take
+    the contraction with their Jacobian rows as M; smaller ones take the pairs'
+    Y rows as M and 64-column tiles; 23-atom molecules b (69 columns of Y) are
+    never merged into one problem.  Both sides, asymmetric and symmetric,
+    against the oracle at the split-fp16 tolerance."""
+    from kernelforge_b200 import local_kernels as lk
+    rep = 48
+    X1, dX1, Q1, N1 = make_set(4, ma1, rep, 3, 51, n_min=ma1 - 2)
+    X2, dX2, Q2, N2 = make_set(3, ma2, rep, 3, 52, n_min=ma2 - 2)
+    sc = 1.0 / np.sqrt(rep)
+    X1 *= 2 * sc
+    X2 *= 2 * sc
+    dX1 *= sc
+    dX2 *= sc
+    s = 2.0
+    p = "split_f16"
+    close(lk.kernel_gaussian_hessian(X1, dX1, X2, dX2, Q1, Q2, N1, N2, s, precision=p),
+          o.kernel_gaussian_hessian(X1, dX1, X2, dX2, Q1, Q2, N1, N2, s), p)
+    Xs, dXs, Qs, Ns = (X1, dX1, Q1, N1) if ma1 > ma2 else (X2, dX2, Q2, N2)
+    close(lk.kernel_gaussian_hessian_symm_rfp(Xs, dXs, Qs, Ns, s, precision=p),
+          o.kernel_gaussian_hessian_symm_rfp(Xs, dXs, Qs, Ns, s), p)
+
+
+def test_tensor_core_hessian_disjoint_labels():
+    """No atom of set 2 shares a label with set 1: every projection problem
+    list is empty and the tensor-core Hessian is exactly zero."""
+    from kernelforge_b200 import local_kernels as lk
+    rep = 48
+    X1, dX1, Q1, N1 = make_set(3, 6, rep, 1, 53, species=[1])
+    X2, dX2, Q2, N2 = make_set(4, 6, rep, 1, 54, species=[2])
+    H = lk.kernel_gaussian_hessian(X1, dX1, X2, dX2, Q1, Q2, N1, N2, 2.0, precision="split_f16")
+    assert H.shape == (int(3 * N1.sum()), int(3 * N2.sum()))
+    assert not np.any(H)
+
+
 @pytest.mark.parametrize("gb,ycore,path", [
     ("0.00005", None, ["hessian:rank-in-y", "hessian:y-cuda-core"]),
     ("0.0001", None, ["hessian:rank-kernel", "hessian:y-gemm"]),
