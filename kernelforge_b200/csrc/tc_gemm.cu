@@ -102,7 +102,7 @@ __device__ __forceinline__ bool wait_bar(uint32_t bar, uint32_t parity, int *err
 // start with the next one and are skipped).
 __device__ __forceinline__ TcTile tile_at(const TcProb *__restrict__ probs,
                                           const int *__restrict__ tstart, int nprobs, int t,
-                                          int bn) {
+                                          int bn, bool n_outer = false) {
     int lo = 0, hi = nprobs - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
@@ -112,6 +112,11 @@ __device__ __forceinline__ TcTile tile_at(const TcProb *__restrict__ probs,
             hi = mid - 1;
     }
     const int loc = t - tstart[lo];
+    if (n_outer) {
+        const int ntm = (probs[lo].M + BM - 1) / BM;
+        const int nt = loc / ntm;
+        return TcTile{lo, (loc - nt * ntm) * BM, nt * bn, 0};
+    }
     const int ntn = (probs[lo].N + bn - 1) / bn;
     const int mt = loc / ntn;
     return TcTile{lo, mt * BM, (loc - mt * ntn) * bn, 0};
@@ -179,7 +184,7 @@ __global__ void __launch_bounds__(Cfg<NPROD, NEPI, BNT>::THREADS, 1)
             uint32_t ph = 0;
             bool ok = true;
             for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-                const TcTile tl = tile_at(P, TS, nprobs, t, C::BN);
+                const TcTile tl = tile_at(P, TS, nprobs, t, C::BN, NEPI == 16);
                 const TcProb pb = P[tl.prob];
                 const int nkb = (pb.K + C::BK - 1) / C::BK;
                 for (int kb = 0; kb < nkb; ++kb) {
@@ -212,7 +217,7 @@ __global__ void __launch_bounds__(Cfg<NPROD, NEPI, BNT>::THREADS, 1)
             uint32_t ph = 0, aph = 0;
             bool ok = true;
             for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-                const TcProb pb = P[tile_at(P, TS, nprobs, t, C::BN).prob];
+                const TcProb pb = P[tile_at(P, TS, nprobs, t, C::BN, NEPI == 16).prob];
                 const int nkb = (pb.K + C::BK - 1) / C::BK;
                 if (!wait_bar(tempty_bar(acc), aph ^ 1u, err)) break;
                 tc_fence_after();
@@ -269,7 +274,7 @@ __global__ void __launch_bounds__(Cfg<NPROD, NEPI, BNT>::THREADS, 1)
         TcProb pb_n{};
         long long cb_n = -1;
         auto fetch = [&](int t) {
-            tl_n = tile_at(P, TS, nprobs, t, C::BN);
+            tl_n = tile_at(P, TS, nprobs, t, C::BN, NEPI == 16);
             pb_n = P[tl_n.prob];
             if constexpr (NEPI == 16) {
                 const int nl = tl_n.n0 + h * 32 + lane;
