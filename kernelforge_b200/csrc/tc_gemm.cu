@@ -54,11 +54,15 @@ struct Cfg {
     // NEPI = 16: the epilogue scratch is dynamic (static shared memory stops at
     // 48 KB), and launches of at most MAXP_SMEM problems read their problem
     // table (and tile starts) from a shared-memory copy
-    static constexpr int OFF_SCR = OFF_TMEM + 16;
+    // (rows of 36 floats: 16-byte aligned for the epilogue's vector reads)
+    static constexpr int OFF_SCR = (OFF_TMEM + 16 + 15) / 16 * 16;
+    static constexpr int SCR_LD = 36;
     static constexpr int MAXP_SMEM = NEPI == 8 ? 0 : 64;
-    static constexpr int OFF_PROBS = OFF_SCR + (NEPI == 8 ? 0 : NEPI * 32 * 33 * 4);
+    static constexpr int OFF_PROBS = OFF_SCR + (NEPI == 8 ? 0 : NEPI * 32 * SCR_LD * 4);
     static constexpr int OFF_TSTART = OFF_PROBS + MAXP_SMEM * (int)sizeof(TcProb);
     static constexpr int SMEM = OFF_TSTART + (MAXP_SMEM > 0 ? (MAXP_SMEM + 1) * 4 : 0) + 1024;
+    static_assert(OFF_SCR % 16 == 0 && OFF_PROBS % 16 == 0, "shared-memory alignment");
+    static_assert(SMEM <= 227 * 1024, "shared memory budget");
 };
 
 constexpr unsigned long long WAIT_LIMIT_NS = 2000000000ull;
@@ -330,9 +334,21 @@ __global__ void __launch_bounds__(Cfg<NPROD, NEPI, BNT>::THREADS, 1)
                                 cb = ((long long)pi.x * epi.y_ld2 * epi.y_ma1 + pi.y) * epi.y_rep;
                         }
                     }
+                    // NEPI = 16: the block column-major in rows of 36 floats (the
+                    // column j of 32 rows is row j of the scratch), so a lane's 8
+                    // rows of one column are two 16-byte loads; the writes (bank
+                    // 4 j + lane) and the loads (8 lanes of a phase: two columns,
+                    // four octets) are free of bank conflicts
+                    float *scrv = reinterpret_cast<float *>(smem + C::OFF_SCR) +
+                                  (size_t)(warp - EPI_WARP0) * 32 * C::SCR_LD;
                     float(*scr)[33] = molsum_scr[warp - EPI_WARP0];
+                    if constexpr (NEPI == 16) {
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) scr[lane][j] = v[j];
+                        for (int j = 0; j < 32; ++j) scrv[j * C::SCR_LD + lane] = v[j];
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) scr[lane][j] = v[j];
+                    }
                     __syncwarp();
                     const int o = lane & 3;
                     const int mo = tl.m0 + q * 32 + o * 8;
@@ -346,11 +362,22 @@ __global__ void __launch_bounds__(Cfg<NPROD, NEPI, BNT>::THREADS, 1)
                         const int j = g * 8 + (lane >> 2);
                         const long long base = __shfl_sync(0xffffffffu, cb, j);
                         if (!ovalid || base < 0) continue;
+                        float xs[8];
+                        if constexpr (NEPI == 16) {
+                            const float4 x0 = *reinterpret_cast<const float4 *>(
+                                scrv + j * C::SCR_LD + o * 8);
+                            const float4 x1 = *reinterpret_cast<const float4 *>(
+                                scrv + j * C::SCR_LD + o * 8 + 4);
+                            xs[0] = x0.x; xs[1] = x0.y; xs[2] = x0.z; xs[3] = x0.w;
+                            xs[4] = x1.x; xs[5] = x1.y; xs[6] = x1.z; xs[7] = x1.w;
+                        } else {
+#pragma unroll
+                            for (int r = 0; r < 8; ++r) xs[r] = scr[o * 8 + r][j];
+                        }
                         unsigned hw[4], lw[4];
 #pragma unroll
                         for (int r = 0; r < 8; r += 2) {
-                            const float2 x = make_float2(scr[o * 8 + r][j] * alpha,
-                                                         scr[o * 8 + r + 1][j] * alpha);
+                            const float2 x = make_float2(xs[r] * alpha, xs[r + 1] * alpha);
                             const __half2 hv = __float22half2_rn(x);
                             const float2 hf = __half22float2(hv);
                             const __half2 lv = __float22half2_rn(make_float2(x.x - hf.x, x.y - hf.y));
