@@ -564,7 +564,7 @@ kfb_status mixed_core(const ApplyFn &A, const float *B, int n, kfb_layout uplo, 
 
     // The factor: the dense lower triangle of F factored by chol_dense (panel
     // solves and trailing updates on the int8 tensor cores) with 4 digit planes
-    // (FP32-class: the north-star precision of the preconditioner) or, with
+    // (FP32-class: the precision asked of the preconditioner) or, with
     // KFB_SOLVE_FP64_FACTOR, 6 (42-bit digits: as a preconditioner of the FP64
     // conjugate gradients it needs as few steps as 7 planes, two at n = 10,000,
     // for 21 instead of 28 int8 products per update); held in FP64 either way,
